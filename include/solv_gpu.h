@@ -1,0 +1,168 @@
+/*
+ * solv_gpu.h -- C-ABI of the B200 face-addressed Krylov solvers
+ * (libsolv_gpu.so).
+ *
+ * Drop-in for the linear-solver hot path of spray-simulation:
+ *
+ *   subroutine solv_cg  (imat,reduc,n_iter,phi,res0,res0_n,not_r0)
+ *                                     spray-simulation/solv_cg.f90:7-13
+ *   subroutine solv_bicg(imat,reduc,n_iter,phi,res0,res0_n,not_r0)
+ *                                     spray-simulation/solv_bicg.f90:7-13
+ *   subroutine solv_res (phi,res0,res0_n,not_r0)       solv_res.f90:5-9
+ *   subroutine solv_precond(imat,c,c_r)                solv_precond.f90:5-7
+ *   subroutine solv_direct(imat,c,c_r,x,b)             solv_direct.f90:5-8
+ *
+ * The reference takes its matrix from module globals pl, ng(:)%{ip,in,p,n}
+ * and v_lst (solv_data.f90:10-22, wired by grd_solv.f90:7-24); here the
+ * matrix is handed over once per structure with solv_gpu_matrix_set (the
+ * grd_solv step) and its coefficients refreshed with solv_gpu_matrix_values
+ * (what cfd_setup.f90 does before every solve).  v_lst is derived from the
+ * face list in ascending face order, the order grd_conn.f90:129-152 gives.
+ *
+ * Conventions (as the Fortran):
+ *   - indices are 1-based; in[f] == 0 marks a boundary face (skipped);
+ *   - phi is cell-major,   phi[(ip-1)*n_vc + ivc]    (phi(ip)%vc(ivc));
+ *   - res0 is column-major, res0[ivc*n_cell + ip-1]  (res0(ip,ivc));
+ *     on entry the right-hand side b, on exit the initial residual;
+ *   - res0_n[ivc] returns the initial L1 norms (not the final ones);
+ *   - the stopping rule is |r|_1 / (|r0|_1 + 1e-20) < reduc, per component.
+ *   - imat: 0 Jacobi, 1 DIC, 2 DILU (solv_precond.f90:13-24).
+ * Every pointer argument is a HOST pointer unless the name ends in _dev.
+ * The reference has no error return; these return a status code.
+ *
+ * Thread-safety: one context per host thread / stream; a context is not
+ * re-entrant (the reference keeps its matrix in module globals, too).
+ */
+#ifndef SOLV_GPU_H
+#define SOLV_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SOLV_GPU_OK 0           /* every component reached reduc           */
+#define SOLV_GPU_MAXITER 1      /* a component stopped at n_iter (the
+                                   reference's normal exit with a cap)     */
+#define SOLV_GPU_NAN 3          /* NaN / Inf seen in a reduction           */
+#define SOLV_GPU_BAD_INPUT 4    /* index out of range, sizes, null, ...    */
+#define SOLV_GPU_DEVICE_ERROR 5 /* CUDA error (message: solv_gpu_last_error) */
+#define SOLV_GPU_NO_MATRIX 7    /* no solv_gpu_matrix_set yet              */
+#define SOLV_GPU_ZERO_RHS 8     /* maxval(res0_n) < small: returned early
+                                   exactly as solv_cg.f90:21 does          */
+
+#define SOLV_GPU_MAX_VC 4
+
+/* option keys for solv_gpu_set_option */
+#define SOLV_OPT_PRECISION 1    /* 0 = FP64 (default); 1 = FP32 inner
+                                   Krylov + FP64 iterative refinement      */
+#define SOLV_OPT_INNER_REDUC 2  /* inner relative drop per refinement
+                                   sweep (FP32 mode), default 1e-4         */
+#define SOLV_OPT_GRAPH_ITERS 3  /* Krylov iterations per CUDA-graph launch
+                                   (0 = no graphs, plain launches)         */
+#define SOLV_OPT_BLOCK 4        /* threads per block for the cell kernels  */
+#define SOLV_OPT_GRID_PER_SM 5  /* resident blocks per SM for reductions   */
+#define SOLV_OPT_MAX_REFINE 6   /* cap on refinement sweeps (FP32 mode)    */
+
+typedef struct solv_gpu_ctx solv_gpu_ctx;
+
+typedef struct {
+  int n_vc;                      /* components solved                      */
+  int iters[SOLV_GPU_MAX_VC];    /* Krylov iterations (inner, summed over
+                                    refinement sweeps in FP32 mode)        */
+  double ratio[SOLV_GPU_MAX_VC]; /* last |r|_1 / |r0|_1 per component      */
+  int status;                    /* as the return value                    */
+  int n_levels;                  /* wavefront levels of the factorisation  */
+  int refinements;               /* FP64 refinement sweeps (FP32 mode)     */
+  int graph_launches;            /* CUDA-graph launches in the solve       */
+  int kernel_launches;           /* kernels launched in the solve          */
+  double solve_ms;               /* device time of the solve (events)      */
+} solv_gpu_stats;
+
+/* -- context ------------------------------------------------------------ */
+int solv_gpu_create(solv_gpu_ctx **ctx, int device);
+int solv_gpu_destroy(solv_gpu_ctx *ctx);
+/* Run on a caller stream (a cudaStream_t); NULL restores the own stream. */
+int solv_gpu_set_stream(solv_gpu_ctx *ctx, void *stream);
+int solv_gpu_set_option(solv_gpu_ctx *ctx, int key, double value);
+const char *solv_gpu_status_string(int status);
+const char *solv_gpu_last_error(const solv_gpu_ctx *ctx);
+
+/* -- matrix (grd_solv.f90:7-24 + the coefficient fill of cfd_setup) ----- */
+/* Structure + coefficients.  ip/in/p/n have n_face entries (interior and
+ * boundary faces, as size(ng)), pl has n_cell.  Replaces the module
+ * globals ng, pl, v_lst of solv_data.f90:10-22. */
+int solv_gpu_matrix_set(solv_gpu_ctx *ctx, int n_cell, int n_face,
+                        const int *ip, const int *in, const double *p,
+                        const double *n, const double *pl);
+/* New coefficients for the same structure (host pointers). */
+int solv_gpu_matrix_values(solv_gpu_ctx *ctx, const double *p,
+                           const double *n, const double *pl);
+/* Same, device pointers (coefficients assembled on the GPU). */
+int solv_gpu_matrix_values_dev(solv_gpu_ctx *ctx, const double *p_dev,
+                               const double *n_dev, const double *pl_dev);
+/* Wavefront levels of the lower-triangular DAG (the sweep depth). */
+int solv_gpu_matrix_levels(const solv_gpu_ctx *ctx);
+
+/* -- the hot path ------------------------------------------------------- */
+/* solv_res.f90:5-30 */
+int solv_gpu_res(solv_gpu_ctx *ctx, int n_vc, const double *phi,
+                 double *res0, double *res0_n, int not_r0);
+/* solv_precond.f90:5-30: c = 1/(d+small), c_r = d (n_cell each) */
+int solv_gpu_precond(solv_gpu_ctx *ctx, int imat, double *c, double *c_r);
+/* solv_direct.f90:5-43: x = M^-1 b with the given c, c_r */
+int solv_gpu_direct(solv_gpu_ctx *ctx, int imat, const double *c,
+                    const double *c_r, double *x, const double *b);
+/* y = A x with the face-loop arithmetic of solv_cg.f90:56-64 */
+int solv_gpu_spmv(solv_gpu_ctx *ctx, const double *x, double *y);
+/* solv_cg.f90:7-87 */
+int solv_gpu_cg(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
+                int n_vc, double *phi, double *res0, double *res0_n,
+                int not_r0, solv_gpu_stats *stats);
+/* solv_bicg.f90:7-121 */
+int solv_gpu_bicg(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
+                  int n_vc, double *phi, double *res0, double *res0_n,
+                  int not_r0, solv_gpu_stats *stats);
+
+/* Device-resident forms: phi_dev / res0_dev in the caller layouts above,
+ * already in HBM; res0_n stays a host array.  Same semantics. */
+int solv_gpu_cg_dev(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
+                    int n_vc, double *phi_dev, double *res0_dev,
+                    double *res0_n, int not_r0, solv_gpu_stats *stats);
+int solv_gpu_bicg_dev(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
+                      int n_vc, double *phi_dev, double *res0_dev,
+                      double *res0_n, int not_r0, solv_gpu_stats *stats);
+int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
+                      int repeat, float *ms_per_call);
+
+/* -- Fortran bindings (gfortran mangling, everything by reference) ------ */
+/* ctx is passed as an integer(c_intptr_t) holding the context address.
+ * status receives the return code.  Mirrors parms_solv_ in
+ * pcns/src/parms_intf.h:9-11, the reference's own C-from-Fortran shim. */
+void solv_gpu_create_(int64_t *ctx, int *device, int *status);
+void solv_gpu_destroy_(int64_t *ctx, int *status);
+void solv_gpu_matrix_set_(int64_t *ctx, int *n_cell, int *n_face,
+                          const int *ip, const int *in, const double *p,
+                          const double *n, const double *pl, int *status);
+void solv_gpu_matrix_values_(int64_t *ctx, const double *p, const double *n,
+                             const double *pl, int *status);
+void solv_gpu_res_(int64_t *ctx, int *n_vc, const double *phi, double *res0,
+                   double *res0_n, int *not_r0, int *status);
+void solv_gpu_precond_(int64_t *ctx, int *imat, double *c, double *c_r,
+                       int *status);
+void solv_gpu_direct_(int64_t *ctx, int *imat, const double *c,
+                      const double *c_r, double *x, const double *b,
+                      int *status);
+void solv_gpu_cg_(int64_t *ctx, int *imat, double *reduc, int *n_iter,
+                  int *n_vc, double *phi, double *res0, double *res0_n,
+                  int *not_r0, int *status);
+void solv_gpu_bicg_(int64_t *ctx, int *imat, double *reduc, int *n_iter,
+                    int *n_vc, double *phi, double *res0, double *res0_n,
+                    int *not_r0, int *status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

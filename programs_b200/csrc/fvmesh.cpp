@@ -1,0 +1,498 @@
+// fvmesh.cpp -- host-side hex mesh generation, Gambit reading, renumbering,
+// face-list emission and matrix assembly for the face-addressed solvers.
+//
+// Connectivity: spray-simulation/grd_conn.f90:45-152.  Geometry:
+// spray-simulation/grd_geom.f90:31-43, 119-208.  Coefficients:
+// spray-simulation/cfd_setup.f90:324-330 (momentum, upwind) and
+// cfd_setup.f90:604-646 (pressure correction; here with unit density,
+// unit d-coefficient so the face coefficient is area / l_pn).
+#include "fvmesh.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <random>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+namespace {
+
+// Brick element, Gambit vertex order (x fastest): local faces as vertex
+// lists, outward normals by the right-hand rule.  This is the Gambit
+// "brick" face table the reference reads from gambit.vrt (type 4); it is a
+// file-format fact, so it is the same here.
+constexpr int kHexFaces[6][4] = {{0, 1, 5, 4}, {1, 3, 7, 5}, {3, 2, 6, 7},
+                                 {2, 0, 4, 6}, {1, 0, 2, 3}, {4, 5, 7, 6}};
+
+struct V3 {
+  double x, y, z;
+};
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator*(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline double mag(V3 a) { return std::sqrt(dot(a, a)); }
+
+}  // namespace
+
+struct fvm_mesh {
+  std::vector<V3> vert;
+  std::vector<int32_t> cell_vert;  // 8 per cell, 0-based vertex ids
+  std::vector<int32_t> cell_nbr;   // 6 per cell, 0-based cell id or -1
+  // derived face list (0-based owner/neighbour, local face of the owner)
+  std::vector<int32_t> f_ip, f_in;
+  std::vector<int8_t> f_loc;
+  std::vector<V3> xc;              // cell centres
+  int n_cell = 0;
+  int n_bface = 0;
+
+  void emit_faces() {
+    f_ip.clear();
+    f_in.clear();
+    f_loc.clear();
+    n_bface = 0;
+    size_t est = (size_t)n_cell * 3 + 64;
+    f_ip.reserve(est);
+    f_in.reserve(est);
+    f_loc.reserve(est);
+    for (int c = 0; c < n_cell; ++c) {
+      for (int k = 0; k < 6; ++k) {
+        int nb = cell_nbr[(size_t)c * 6 + k];
+        if (nb >= 0 && nb < c) continue;  // already emitted by the lower cell
+        f_ip.push_back(c);
+        f_in.push_back(nb);  // -1 = boundary
+        f_loc.push_back((int8_t)k);
+        if (nb < 0) ++n_bface;
+      }
+    }
+  }
+
+  void centres() {
+    xc.resize(n_cell);
+    for (int c = 0; c < n_cell; ++c) {
+      V3 s{0, 0, 0};
+      for (int v = 0; v < 8; ++v) s = s + vert[cell_vert[(size_t)c * 8 + v]];
+      xc[c] = s * (1.0 / 8.0);
+    }
+  }
+
+  // grd_geom.f90:119-147 (3-d branch) and :161-198.
+  void face_geom(size_t f, double &s, V3 &nrm, V3 &xf, double &l_pn,
+                 double &w_fp) const {
+    int c = f_ip[f];
+    int k = f_loc[f];
+    V3 v[4];
+    for (int i = 0; i < 4; ++i) v[i] = vert[cell_vert[(size_t)c * 8 + kHexFaces[k][i]]];
+    V3 acc{0, 0, 0};
+    double area = 0.0;
+    V3 e_prev = v[1] - v[0];
+    for (int i = 2; i < 4; ++i) {
+      V3 e = v[i] - v[0];
+      V3 t = cross(e_prev, e) * 0.5;
+      double a = mag(t);
+      acc = acc + t * (1.0 / a);
+      area += a;
+      e_prev = e;
+    }
+    nrm = acc * (1.0 / 2.0);
+    s = area;
+    xf = (v[0] + v[1] + v[2] + v[3]) * 0.25;
+    V3 xp_aux = xf - nrm * dot(xf - xc[c], nrm);
+    int nb = f_in[f];
+    if (nb >= 0) {
+      V3 xn_aux = xf - nrm * dot(xf - xc[nb], nrm);
+      l_pn = mag(xn_aux - xp_aux);
+      w_fp = mag(xf - xp_aux) / l_pn;
+    } else {
+      l_pn = mag(xf - xp_aux);
+      w_fp = 1.0;
+    }
+  }
+};
+
+extern "C" {
+
+fvm_mesh *fvm_mesh_hex(int nx, int ny, int nz, double jitter, uint64_t seed,
+                       int permute) {
+  if (nx < 1 || ny < 1 || nz < 1) return nullptr;
+  auto *m = new fvm_mesh();
+  std::mt19937_64 rng(seed);
+  auto uni = [&rng]() {  // [-1, 1)
+    return (double)(rng() >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+  };
+  const int vx = nx + 1, vy = ny + 1, vz = nz + 1;
+  const double hx = 1.0 / nx, hy = 1.0 / ny, hz = 1.0 / nz;
+  m->vert.resize((size_t)vx * vy * vz);
+  for (int k = 0; k < vz; ++k)
+    for (int j = 0; j < vy; ++j)
+      for (int i = 0; i < vx; ++i) {
+        V3 x{i * hx, j * hy, k * hz};
+        bool interior = i > 0 && i < nx && j > 0 && j < ny && k > 0 && k < nz;
+        double dx = uni(), dy = uni(), dz = uni();
+        if (interior) {
+          x.x += jitter * hx * dx;
+          x.y += jitter * hy * dy;
+          x.z += jitter * hz * dz;
+        }
+        m->vert[((size_t)k * vy + j) * vx + i] = x;
+      }
+  const int N = nx * ny * nz;
+  m->n_cell = N;
+  // lexicographic cell id -> stored cell id
+  std::vector<int32_t> id(N);
+  std::iota(id.begin(), id.end(), 0);
+  if (permute) {
+    for (int i = N - 1; i > 0; --i) {
+      uint64_t r = rng() % (uint64_t)(i + 1);
+      std::swap(id[i], id[(int)r]);
+    }
+  }
+  m->cell_vert.resize((size_t)N * 8);
+  m->cell_nbr.assign((size_t)N * 6, -1);
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        int lex = (k * ny + j) * nx + i;
+        int c = id[lex];
+        int32_t *cv = &m->cell_vert[(size_t)c * 8];
+        for (int b = 0; b < 8; ++b) {
+          int di = b & 1, dj = (b >> 1) & 1, dk = (b >> 2) & 1;
+          cv[b] = ((k + dk) * vy + (j + dj)) * vx + (i + di);
+        }
+        int32_t *cn = &m->cell_nbr[(size_t)c * 6];
+        // local face order: -y, +x, +y, -x, -z, +z
+        cn[0] = j > 0 ? id[lex - nx] : -1;
+        cn[1] = i < nx - 1 ? id[lex + 1] : -1;
+        cn[2] = j < ny - 1 ? id[lex + nx] : -1;
+        cn[3] = i > 0 ? id[lex - 1] : -1;
+        cn[4] = k > 0 ? id[lex - nx * ny] : -1;
+        cn[5] = k < nz - 1 ? id[lex + nx * ny] : -1;
+      }
+  m->centres();
+  m->emit_faces();
+  return m;
+}
+
+fvm_mesh *fvm_mesh_read_neu(const char *path) {
+  std::ifstream in(path);
+  if (!in) return nullptr;
+  auto *m = new fvm_mesh();
+  std::string line;
+  int n_vrt = 0, n_vol = 0;
+  bool ok_sizes = false;
+  while (std::getline(in, line)) {
+    if (line.find("NUMNP") != std::string::npos) {
+      std::getline(in, line);
+      std::istringstream ss(line);
+      ss >> n_vrt >> n_vol;
+      ok_sizes = n_vrt > 0 && n_vol > 0;
+    } else if (line.find("NODAL COORDINATES") != std::string::npos && ok_sizes) {
+      m->vert.resize(n_vrt);
+      for (int i = 0; i < n_vrt; ++i) {
+        int idx;
+        double x, y, z;
+        in >> idx >> x >> y >> z;
+        if (!in || idx < 1 || idx > n_vrt) { delete m; return nullptr; }
+        m->vert[idx - 1] = {x, y, z};
+      }
+    } else if (line.find("ELEMENTS/CELLS") != std::string::npos && ok_sizes) {
+      m->n_cell = n_vol;
+      m->cell_vert.resize((size_t)n_vol * 8);
+      for (int e = 0; e < n_vol; ++e) {
+        int idx, ty, nv;
+        in >> idx >> ty >> nv;
+        if (!in || ty != 4 || nv != 8 || idx < 1 || idx > n_vol) {
+          delete m;  // only brick elements are supported
+          return nullptr;
+        }
+        for (int v = 0; v < 8; ++v) {
+          int g;
+          in >> g;
+          m->cell_vert[(size_t)(idx - 1) * 8 + v] = g - 1;
+        }
+      }
+    }
+  }
+  if (m->n_cell == 0 || m->vert.empty()) { delete m; return nullptr; }
+  // hashed face matching: key = sorted vertex quadruple
+  m->cell_nbr.assign((size_t)m->n_cell * 6, -1);
+  struct Key {
+    std::array<int32_t, 4> v;
+    bool operator==(const Key &o) const { return v == o.v; }
+  };
+  struct H {
+    size_t operator()(const Key &k) const {
+      uint64_t h = 1469598103934665603ull;
+      for (int x : k.v) { h ^= (uint64_t)(uint32_t)x; h *= 1099511628211ull; }
+      return (size_t)h;
+    }
+  };
+  std::unordered_map<Key, int64_t, H> open;
+  open.reserve((size_t)m->n_cell * 4);
+  for (int c = 0; c < m->n_cell; ++c)
+    for (int k = 0; k < 6; ++k) {
+      Key key;
+      for (int i = 0; i < 4; ++i) key.v[i] = m->cell_vert[(size_t)c * 8 + kHexFaces[k][i]];
+      std::sort(key.v.begin(), key.v.end());
+      auto it = open.find(key);
+      if (it == open.end()) {
+        open.emplace(key, (int64_t)c * 6 + k);
+      } else {
+        int64_t o = it->second;
+        m->cell_nbr[(size_t)o] = c;
+        m->cell_nbr[(size_t)c * 6 + k] = (int)(o / 6);
+        open.erase(it);
+      }
+    }
+  m->centres();
+  m->emit_faces();
+  return m;
+}
+
+void fvm_mesh_free(fvm_mesh *m) { delete m; }
+
+void fvm_mesh_sizes(const fvm_mesh *m, int *n_cell, int *n_face, int *n_bface,
+                    int *n_vert) {
+  if (n_cell) *n_cell = m->n_cell;
+  if (n_face) *n_face = (int)m->f_ip.size();
+  if (n_bface) *n_bface = m->n_bface;
+  if (n_vert) *n_vert = (int)m->vert.size();
+}
+
+void fvm_mesh_faces(const fvm_mesh *m, int *ip, int *in) {
+  size_t F = m->f_ip.size();
+  for (size_t f = 0; f < F; ++f) {
+    ip[f] = m->f_ip[f] + 1;
+    in[f] = m->f_in[f] + 1;  // -1 -> 0
+  }
+}
+
+void fvm_mesh_face_geom(const fvm_mesh *m, double *s, double *nrm, double *xf,
+                        double *l_pn, double *w_fp) {
+  size_t F = m->f_ip.size();
+  for (size_t f = 0; f < F; ++f) {
+    double a, l, w;
+    V3 nn, x;
+    m->face_geom(f, a, nn, x, l, w);
+    if (s) s[f] = a;
+    if (nrm) { nrm[3 * f] = nn.x; nrm[3 * f + 1] = nn.y; nrm[3 * f + 2] = nn.z; }
+    if (xf) { xf[3 * f] = x.x; xf[3 * f + 1] = x.y; xf[3 * f + 2] = x.z; }
+    if (l_pn) l_pn[f] = l;
+    if (w_fp) w_fp[f] = w;
+  }
+}
+
+void fvm_mesh_cell_geom(const fvm_mesh *m, double *xc, double *vol) {
+  for (int c = 0; c < m->n_cell; ++c)
+    if (xc) { xc[3 * c] = m->xc[c].x; xc[3 * c + 1] = m->xc[c].y; xc[3 * c + 2] = m->xc[c].z; }
+  if (vol) {
+    // grd_geom.f90:150-152,172-174: divergence theorem with x * n_x.
+    for (int c = 0; c < m->n_cell; ++c) vol[c] = 0.0;
+    size_t F = m->f_ip.size();
+    for (size_t f = 0; f < F; ++f) {
+      double a, l, w;
+      V3 nn, x;
+      m->face_geom(f, a, nn, x, l, w);
+      double vp = x.x * a * nn.x;
+      vol[m->f_ip[f]] += vp;
+      if (m->f_in[f] >= 0) vol[m->f_in[f]] -= vp;
+    }
+  }
+}
+
+int fvm_mesh_renumber(fvm_mesh *m, int method, int *perm) {
+  const int N = m->n_cell;
+  std::vector<int32_t> order;  // order[new] = old
+  order.reserve(N);
+  if (method == 1) {
+    // Reverse Cuthill-McKee: BFS from a pseudo-peripheral cell (repeated
+    // BFS to the farthest, least-connected cell), neighbours by degree.
+    auto degree = [&](int c) {
+      int d = 0;
+      for (int k = 0; k < 6; ++k) d += m->cell_nbr[(size_t)c * 6 + k] >= 0;
+      return d;
+    };
+    std::vector<int32_t> level(N, -1);
+    auto bfs_far = [&](int start) {
+      std::fill(level.begin(), level.end(), -1);
+      std::vector<int32_t> q;
+      q.reserve(N);
+      q.push_back(start);
+      level[start] = 0;
+      for (size_t h = 0; h < q.size(); ++h) {
+        int c = q[h];
+        for (int k = 0; k < 6; ++k) {
+          int nb = m->cell_nbr[(size_t)c * 6 + k];
+          if (nb >= 0 && level[nb] < 0) { level[nb] = level[c] + 1; q.push_back(nb); }
+        }
+      }
+      int best = q.back(), bl = level[best], bd = degree(best);
+      for (int c : q)
+        if (level[c] == bl && degree(c) < bd) { best = c; bd = degree(c); }
+      return std::make_pair(best, bl);
+    };
+    std::vector<char> seen(N, 0);
+    for (int s0 = 0; s0 < N; ++s0) {
+      if (seen[s0]) continue;
+      int root = s0;
+      auto r = bfs_far(root);
+      for (int it = 0; it < 4; ++it) {
+        auto r2 = bfs_far(r.first);
+        if (r2.second <= r.second) break;
+        r = r2;
+      }
+      root = r.first;
+      size_t h = order.size();
+      order.push_back(root);
+      seen[root] = 1;
+      for (; h < order.size(); ++h) {
+        int c = order[h];
+        int nb[6], nn = 0;
+        for (int k = 0; k < 6; ++k) {
+          int x = m->cell_nbr[(size_t)c * 6 + k];
+          if (x >= 0 && !seen[x]) nb[nn++] = x;
+        }
+        std::stable_sort(nb, nb + nn, [&](int a, int b) { return degree(a) < degree(b); });
+        for (int i = 0; i < nn; ++i) { seen[nb[i]] = 1; order.push_back(nb[i]); }
+      }
+    }
+    std::reverse(order.begin(), order.end());
+  } else if (method == 2) {
+    // Morton (Z-order) key of the cell centre, 21 bits per axis.
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (const V3 &x : m->xc) {
+      lo[0] = std::min(lo[0], x.x); hi[0] = std::max(hi[0], x.x);
+      lo[1] = std::min(lo[1], x.y); hi[1] = std::max(hi[1], x.y);
+      lo[2] = std::min(lo[2], x.z); hi[2] = std::max(hi[2], x.z);
+    }
+    auto spread = [](uint64_t v) {
+      v &= 0x1fffff;
+      v = (v | v << 32) & 0x1f00000000ffffull;
+      v = (v | v << 16) & 0x1f0000ff0000ffull;
+      v = (v | v << 8) & 0x100f00f00f00f00full;
+      v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+      v = (v | v << 2) & 0x1249249249249249ull;
+      return v;
+    };
+    std::vector<uint64_t> key(N);
+    for (int c = 0; c < N; ++c) {
+      uint64_t q[3];
+      const double xs[3] = {m->xc[c].x, m->xc[c].y, m->xc[c].z};
+      for (int d = 0; d < 3; ++d) {
+        double t = (xs[d] - lo[d]) / std::max(hi[d] - lo[d], 1e-300);
+        q[d] = (uint64_t)std::min(2097151.0, std::max(0.0, t * 2097151.0));
+      }
+      key[c] = spread(q[0]) | spread(q[1]) << 1 | spread(q[2]) << 2;
+    }
+    order.resize(N);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return key[a] < key[b]; });
+  } else if (method == 3) {
+    if (!perm) return -1;
+    order.assign(N, -1);
+    for (int c = 0; c < N; ++c) {
+      int nw = perm[c] - 1;
+      if (nw < 0 || nw >= N || order[nw] >= 0) return -1;
+      order[nw] = c;
+    }
+  } else {
+    return -1;
+  }
+  std::vector<int32_t> newid(N);
+  for (int i = 0; i < N; ++i) newid[order[i]] = i;
+  std::vector<int32_t> cv((size_t)N * 8), cn((size_t)N * 6);
+  std::vector<V3> xc(N);
+  for (int i = 0; i < N; ++i) {
+    int o = order[i];
+    std::memcpy(&cv[(size_t)i * 8], &m->cell_vert[(size_t)o * 8], 8 * sizeof(int32_t));
+    for (int k = 0; k < 6; ++k) {
+      int nb = m->cell_nbr[(size_t)o * 6 + k];
+      cn[(size_t)i * 6 + k] = nb >= 0 ? newid[nb] : -1;
+    }
+    xc[i] = m->xc[o];
+  }
+  m->cell_vert.swap(cv);
+  m->cell_nbr.swap(cn);
+  m->xc.swap(xc);
+  m->emit_faces();
+  if (perm && method != 3)
+    for (int c = 0; c < N; ++c) perm[c] = newid[c] + 1;
+  return 0;
+}
+
+void fvm_assemble_pressure(const fvm_mesh *m, int pin, double *p, double *n,
+                           double *pl) {
+  const int N = m->n_cell;
+  const size_t F = m->f_ip.size();
+  for (int c = 0; c < N; ++c) pl[c] = 0.0;
+  const int pc = pin - 1;
+  for (size_t f = 0; f < F; ++f) {
+    p[f] = 0.0;
+    n[f] = 0.0;
+    int a = m->f_ip[f], b = m->f_in[f];
+    if (b < 0) continue;  // all-Neumann boundary
+    double s, l, w;
+    V3 nn, x;
+    m->face_geom(f, s, nn, x, l, w);
+    double d = s / l;
+    pl[a] += d;
+    pl[b] += d;
+    if (a == pc || b == pc) continue;  // pinned cell: drop both couplings
+    p[f] = -d;
+    n[f] = -d;
+  }
+}
+
+double fvm_assemble_momentum(const fvm_mesh *m, double gamma, double pe_max,
+                             double cfl, double *p, double *n, double *pl) {
+  const int N = m->n_cell;
+  const size_t F = m->f_ip.size();
+  // cell size from the mean volume
+  double h = std::cbrt(1.0 / (double)N);
+  const double U0 = pe_max * gamma / h;
+  const double dt = cfl * h / U0;
+  const double tp = 2.0 * M_PI;
+  std::vector<double> vol(N);
+  fvm_mesh_cell_geom(m, nullptr, vol.data());
+  for (int c = 0; c < N; ++c) pl[c] = 0.0;
+  for (size_t f = 0; f < F; ++f) {
+    double s, l, w;
+    V3 nn, x;
+    m->face_geom(f, s, nn, x, l, w);
+    int a = m->f_ip[f], b = m->f_in[f];
+    double d = gamma * s / l;
+    double u = U0 * std::sin(tp * x.x) * std::cos(tp * x.y) * std::cos(tp * x.z);
+    double v = -U0 * std::cos(tp * x.x) * std::sin(tp * x.y) * std::cos(tp * x.z);
+    double c = s * (u * nn.x + v * nn.y);
+    if (b >= 0) {
+      p[f] = -d + std::min(c, 0.0);
+      n[f] = -d - std::max(c, 0.0);
+      pl[a] -= p[f];
+      pl[b] -= n[f];
+    } else {
+      p[f] = -d;  // wall: zero flux, Dirichlet diffusion
+      n[f] = 0.0;
+      pl[a] -= p[f];
+    }
+  }
+  for (int c = 0; c < N; ++c) pl[c] += vol[c] / dt;
+  return dt;
+}
+
+void fvm_uniform(uint64_t seed, int64_t count, double *out) {
+  std::mt19937_64 rng(seed);
+  for (int64_t i = 0; i < count; ++i)
+    out[i] = (double)(rng() >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}
+
+}  // extern "C"

@@ -1,0 +1,83 @@
+/*
+ * fvmesh.h -- host-side unstructured hex mesh, face list and matrix
+ * assembly for the face-addressed solvers.
+ *
+ * The face list follows the spray-simulation connectivity rules: faces are
+ * emitted cell by cell in ascending cell order, each cell's local faces in
+ * its element-table order; a face shared with an already visited
+ * (lower-numbered) cell is not emitted again, so every interior face has
+ * owner ip < neighbour in and boundary faces have in = 0
+ * (grd_conn.f90:45-113).  Geometry follows grd_geom.f90:31-43 (cell centre
+ * = vertex average) and :119-208 (triangle-fan area and normal, face centre,
+ * auxiliary poles, l_pn, w_fp).  All indices exposed here are 1-based.
+ */
+#ifndef FVMESH_H
+#define FVMESH_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fvm_mesh fvm_mesh;
+
+/* nx*ny*nz hex cells on the unit box, interior vertices jittered uniformly
+ * by +-jitter*h per axis, cells randomly permuted when permute != 0.  The
+ * generator draws from std::mt19937_64(seed). */
+fvm_mesh *fvm_mesh_hex(int nx, int ny, int nz, double jitter, uint64_t seed,
+                       int permute);
+
+/* Gambit neutral file reader (grd_read.f90) with hashed face matching in
+ * place of the quadratic search of grd_conn.f90:77-93.  NULL on error. */
+fvm_mesh *fvm_mesh_read_neu(const char *path);
+
+void fvm_mesh_free(fvm_mesh *m);
+
+/* n_cell, n_face (interior + boundary), n_bface, n_vert */
+void fvm_mesh_sizes(const fvm_mesh *m, int *n_cell, int *n_face, int *n_bface,
+                    int *n_vert);
+
+/* ng(:)%ip / ng(:)%in, 1-based, in = 0 on boundary faces. */
+void fvm_mesh_faces(const fvm_mesh *m, int *ip, int *in);
+
+/* Per-face geometry (any output may be NULL): area s, normal (3 per face,
+ * outward from the owner), centre (3 per face), l_pn, w_fp. */
+void fvm_mesh_face_geom(const fvm_mesh *m, double *s, double *nrm, double *xf,
+                        double *l_pn, double *w_fp);
+
+/* Cell centres (3 per cell) and volumes (either may be NULL). */
+void fvm_mesh_cell_geom(const fvm_mesh *m, double *xc, double *vol);
+
+/* Renumber cells.  method 1 = reverse Cuthill-McKee, 2 = Morton
+ * space-filling curve of the cell centres, 3 = a given permutation in
+ * perm (new 1-based index of old cell i).  The face list is re-emitted
+ * under the new numbering.  On return perm (if not NULL and method != 3)
+ * holds the permutation applied.  Returns 0, or -1 on bad input. */
+int fvm_mesh_renumber(fvm_mesh *m, int method, int *perm);
+
+/* Pressure-correction Poisson matrix: p = n = -area/l_pn on interior
+ * faces, pl = sum of area/l_pn, boundaries all-Neumann; cell `pin`
+ * (1-based, 0 for none) is pinned by zeroing both off-diagonals of every
+ * face that touches it, which keeps the matrix symmetric positive definite.
+ * Boundary faces get p = n = 0. */
+void fvm_assemble_pressure(const fvm_mesh *m, int pin, double *p, double *n,
+                           double *pl);
+
+/* Momentum convection-diffusion matrix, first-order upwind
+ * (cfd_setup.f90:324-330): p = -d + min(c,0), n = -d - max(c,0),
+ * pl = -sum(off-diagonals) + V/dt, with d = gamma*area/l_pn and c the
+ * face flux of a Taylor-Green field u = U0 (sin X cos Y cos Z,
+ * -cos X sin Y cos Z, 0), X = 2 pi x, scaled so the largest cell Peclet
+ * number U0*h/gamma is pe_max.  Walls are Dirichlet (d on the boundary
+ * face, zero flux).  dt = cfl*h/U0.  Returns dt. */
+double fvm_assemble_momentum(const fvm_mesh *m, double gamma, double pe_max,
+                             double cfl, double *p, double *n, double *pl);
+
+/* Uniform [-1,1) values from std::mt19937_64(seed) (53-bit mantissa). */
+void fvm_uniform(uint64_t seed, int64_t count, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

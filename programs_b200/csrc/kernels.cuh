@@ -1,0 +1,768 @@
+// kernels.cuh -- sm_100a kernels of the face-addressed Krylov solvers.
+//
+// Storage (built on the host by solv_gpu.cu):
+//   * cells live in an internal order: wavefront level of the lower-
+//     triangular DAG first, then the caller's index, so every level of the
+//     DIC/DILU sweeps is one contiguous range and "neighbour j is below
+//     cell i in the caller's order" is exactly "j < i" internally;
+//   * each cell's interior faces form one row of a sliced ELL (32 cells per
+//     slice, slot-major inside a slice, so a warp reads 32 consecutive
+//     words per slot); slots keep the cell's faces in ascending face order,
+//     which is the order the reference's face loop adds them in;
+//   * vectors with V components are cell-interleaved: x[i*V + v].
+// FP64 arithmetic uses explicit _rn intrinsics (no FMA contraction), so
+// matrix products, residuals and sweeps are bit-identical to the in-order
+// CPU restatement; reductions use a fixed tree and are run-to-run
+// deterministic.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sg {
+
+constexpr double kSmall = 1e-20;  // spray-simulation/precision.f90:8
+constexpr double kLarge = 1e20;   // spray-simulation/precision.f90:9
+constexpr int kWarp = 32;
+
+// ---- precision helpers ---------------------------------------------------
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul(float a, float b) { return a * b; }
+__device__ __forceinline__ float add(float a, float b) { return a + b; }
+__device__ __forceinline__ float sub(float a, float b) { return a - b; }
+// Reduction term: always formed and accumulated in FP64.
+__device__ __forceinline__ double prod(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double prod(float a, float b) { return __dmul_rn((double)a, (double)b); }
+
+// ---- per (system, component) Krylov state ---------------------------------
+struct Lane {
+  double s, beta, alpha, pq;           // CG: s = r.z, beta, alpha
+  double rho, beta0, gam, omeg;        // BiCGSTAB (alpha shared)
+  double res0_n, ratio, reduc, l1;
+  int iter, n_iter, active, status;
+};
+enum : int { kLaneRunning = 0, kLaneConverged = 1, kLaneMaxIter = 2, kLaneNaN = 3 };
+
+template <typename T>
+struct Rows {
+  const int* __restrict__ slice_ptr;    // element offset of each slice
+  const uint8_t* __restrict__ slice_w;  // slots in each slice
+  const int* __restrict__ col;          // internal column, -1 = padding
+  const T* __restrict__ val;            // A(i, col) for the matrix product
+  const T* __restrict__ sval;           // sweep coefficient (ng%n below, ng%p above)
+  const T* __restrict__ diag;           // pl
+};
+
+// Reduction geometry: each block works on one segment (system) and strides
+// through that segment's cells; partial sums go to part[], and the last
+// block of a segment to finish (ticket) combines them in block order.
+struct SegMap {
+  const int* __restrict__ blk_seg;
+  const int* __restrict__ blk_rank;
+  const int* __restrict__ seg_nblk;
+  const int* __restrict__ seg_blk0;
+  const int* __restrict__ seg_c0;
+  const int* __restrict__ seg_c1;
+  unsigned int* ticket;
+  int* n_active;  // lanes still iterating (host polls this)
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum of NR values; result valid in thread 0.  Fixed order.
+template <int NR>
+__device__ __forceinline__ void block_sum(double (&v)[NR]) {
+  __shared__ double sh[NR][32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) v[k] = warp_sum(v[k]);
+  if (l == 0) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) sh[k][w] = v[k];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+      double t = l < nw ? sh[k][l] : 0.0;
+      v[k] = warp_sum(t);
+    }
+  }
+  __syncthreads();
+}
+
+// Commit this block's partials; returns true in the segment's last block,
+// with the segment totals in tot[] (valid in every thread of that block).
+template <int NR>
+__device__ __forceinline__ bool seg_commit(const SegMap& sm, int b, int s,
+                                           double* __restrict__ part,
+                                           double (&v)[NR], double (&tot)[NR]) {
+  __shared__ bool last;
+  __shared__ double tsh[NR];
+  block_sum<NR>(v);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) part[(size_t)b * NR + k] = v[k];
+    __threadfence();
+    unsigned t = atomicAdd(&sm.ticket[s], 1u);
+    last = (t == (unsigned)sm.seg_nblk[s] - 1u);
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  const int nb = sm.seg_nblk[s], b0 = sm.seg_blk0[s];
+  double acc[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) acc[k] = 0.0;
+  for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) acc[k] += __ldcg(&part[(size_t)(b0 + j) * NR + k]);
+  }
+  block_sum<NR>(acc);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NR; ++k) tsh[k] = acc[k];
+    sm.ticket[s] = 0u;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < NR; ++k) tot[k] = tsh[k];
+  return true;
+}
+
+__device__ __forceinline__ void lane_stop(Lane& L, int status, int* n_active) {
+  if (L.active) {
+    L.active = 0;
+    L.status = status;
+    atomicSub(n_active, 1);
+  }
+}
+
+// Row walk helpers ---------------------------------------------------------
+template <typename T>
+struct RowIt {
+  int base, w;
+  __device__ __forceinline__ RowIt(const Rows<T>& R, int i) {
+    const int sl = i >> 5;
+    base = __ldg(&R.slice_ptr[sl]) + (i & 31);
+    w = __ldg(&R.slice_w[sl]);
+  }
+};
+
+// y = A x for V interleaved components; y_i = pl_i x_i + sum in face order.
+template <typename T, int V>
+__device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
+                                          const T* __restrict__ x, T (&y)[V]) {
+  RowIt<T> it(R, i);
+  const T d = R.diag[i];
+#pragma unroll
+  for (int v = 0; v < V; ++v) y[v] = mul(d, x[(size_t)i * V + v]);
+  for (int k = 0; k < it.w; ++k) {
+    const int e = it.base + k * kWarp;
+    const int j = __ldg(&R.col[e]);
+    if (j >= 0) {
+      const T a = R.val[e];
+#pragma unroll
+      for (int v = 0; v < V; ++v) y[v] = add(y[v], mul(a, x[(size_t)j * V + v]));
+    }
+  }
+}
+
+// ---- layout conversion ---------------------------------------------------
+// caller phi (cell-major [N][V], caller order) -> internal interleaved
+template <typename T>
+__global__ void k_phi_in(int n, int V, const int* __restrict__ old_of_new,
+                         const double* __restrict__ src, T* __restrict__ dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int o = old_of_new[i];
+    for (int v = 0; v < V; ++v) dst[(size_t)i * V + v] = (T)src[(size_t)o * V + v];
+  }
+}
+template <typename T>
+__global__ void k_phi_out(int n, int V, const int* __restrict__ old_of_new,
+                          const T* __restrict__ src, double* __restrict__ dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int o = old_of_new[i];
+    for (int v = 0; v < V; ++v) dst[(size_t)o * V + v] = (double)src[(size_t)i * V + v];
+  }
+}
+// caller res0 (column-major [V][N]) <-> internal interleaved
+__global__ void k_col_in(int n, int V, const int* __restrict__ old_of_new,
+                         const double* __restrict__ src, double* __restrict__ dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int o = old_of_new[i];
+    for (int v = 0; v < V; ++v) dst[(size_t)i * V + v] = src[(size_t)v * n + o];
+  }
+}
+__global__ void k_col_out(int n, int V, const int* __restrict__ old_of_new,
+                          const double* __restrict__ src, double* __restrict__ dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int o = old_of_new[i];
+    for (int v = 0; v < V; ++v) dst[(size_t)v * n + o] = src[(size_t)i * V + v];
+  }
+}
+
+// ---- matrix values ---------------------------------------------------------
+// slot_src = 2*face + (1 if the row's cell is the face neighbour), -1 pad.
+// val: the coefficient the face loop multiplies x(other cell) by for this
+// row (ng%p for the owner's row, ng%n for the neighbour's row);
+// sval: the sweep coefficient, ng%n for a lower neighbour, ng%p for an
+// upper one (solv_direct.f90:19,33).
+template <typename T>
+__global__ void k_fill_values(int n, const int* __restrict__ slice_ptr,
+                              const uint8_t* __restrict__ slice_w,
+                              const int* __restrict__ slot_src, const int* __restrict__ col,
+                              const double* __restrict__ p, const double* __restrict__ nn,
+                              T* __restrict__ val, T* __restrict__ sval) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int sl = i >> 5, base = slice_ptr[sl] + (i & 31), w = slice_w[sl];
+    for (int k = 0; k < w; ++k) {
+      const int e = base + k * kWarp;
+      const int s = slot_src[e];
+      if (s < 0) {
+        val[e] = (T)0;
+        if (sval) sval[e] = (T)0;
+        continue;
+      }
+      const int f = s >> 1;
+      val[e] = (T)((s & 1) ? nn[f] : p[f]);
+      if (sval) sval[e] = (T)(col[e] < i ? nn[f] : p[f]);
+    }
+  }
+}
+template <typename T>
+__global__ void k_fill_diag(int n, const int* __restrict__ old_of_new,
+                            const double* __restrict__ pl, T* __restrict__ diag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    diag[i] = (T)pl[old_of_new[i]];
+}
+template <typename Tsrc, typename Tdst>
+__global__ void k_convert(long long n, const Tsrc* __restrict__ a, Tdst* __restrict__ b) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    b[e] = (Tdst)a[e];
+}
+
+// ---- residual: solv_res.f90:12-29 ----------------------------------------
+// r_i = ((b_i - pl_i phi_i) - a_1 phi_j1) - ...; L1 norm per component.
+template <int V>
+__global__ void k_res(Rows<double> R, SegMap sm, const double* __restrict__ phi,
+                      double* __restrict__ r, int not_r0, double* __restrict__ part,
+                      Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double l1[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) l1[v] = 0.0;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+    double y[V];
+    if (!not_r0) {
+      RowIt<double> it(R, i);
+      const double d = R.diag[i];
+#pragma unroll
+      for (int v = 0; v < V; ++v) y[v] = sub(r[(size_t)i * V + v], mul(d, phi[(size_t)i * V + v]));
+      for (int k = 0; k < it.w; ++k) {
+        const int e = it.base + k * kWarp;
+        const int j = __ldg(&R.col[e]);
+        if (j >= 0) {
+          const double a = R.val[e];
+#pragma unroll
+          for (int v = 0; v < V; ++v) y[v] = sub(y[v], mul(a, phi[(size_t)j * V + v]));
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < V; ++v) r[(size_t)i * V + v] = y[v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < V; ++v) y[v] = r[(size_t)i * V + v];
+    }
+#pragma unroll
+    for (int v = 0; v < V; ++v) l1[v] += fabs(y[v]);
+  }
+  double tot[V];
+  if (seg_commit<V>(sm, b, s, part, l1, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) lanes[s * V + v].res0_n = tot[v];
+  }
+}
+
+// ---- preconditioner: solv_precond.f90:10-29, one wavefront level -----------
+// c_i = pl_i - sum_{j<i} (n*n) c_j   (DIC)   or  - (p*c_j)*n  (DILU);
+// c_r = c; c = 1/(c + small).  face p/n looked up through slot_src.
+__global__ void k_precond_level(int i0, int i1, int imat, Rows<double> R,
+                                const int* __restrict__ slot_src,
+                                const double* __restrict__ fp, const double* __restrict__ fn,
+                                double* __restrict__ c, double* __restrict__ c_r) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1) return;
+  RowIt<double> it(R, i);
+  double d = R.diag[i];
+  if (imat > 0) {
+    for (int k = 0; k < it.w; ++k) {
+      const int e = it.base + k * kWarp;
+      const int j = R.col[e];
+      if (j >= 0 && j < i) {
+        const int f = slot_src[e] >> 1;
+        const double cj = __ldcg(&c[j]);
+        if (imat == 1) {
+          const double nf = fn[f];
+          d = sub(d, mul(mul(nf, nf), cj));
+        } else if (imat == 2) {
+          d = sub(d, mul(mul(fp[f], cj), fn[f]));
+        }
+      }
+    }
+  }
+  c_r[i] = d;
+  c[i] = 1.0 / add(d, kSmall);
+}
+
+// ---- sweeps: solv_direct.f90:11-38, one wavefront level --------------------
+// forward: x_i = (b_i - sum_{j<i} n x_j) * c_i
+template <typename T, int V>
+__global__ void k_fwd_level(int i0, int i1, Rows<T> R, const T* __restrict__ c,
+                            const T* __restrict__ bvec, T* __restrict__ x,
+                            const int* __restrict__ n_active) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1 || (n_active && *n_active == 0)) return;
+  RowIt<T> it(R, i);
+  T acc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = bvec[(size_t)i * V + v];
+  for (int k = 0; k < it.w; ++k) {
+    const int e = it.base + k * kWarp;
+    const int j = __ldg(&R.col[e]);
+    if (j >= 0 && j < i) {
+      const T a = R.sval[e];
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, __ldcg(&x[(size_t)j * V + v])));
+    }
+  }
+  const T ci = c[i];
+#pragma unroll
+  for (int v = 0; v < V; ++v) x[(size_t)i * V + v] = mul(acc[v], ci);
+}
+// backward, with the x = x*c_r scaling of :26 fused in:
+// x_i = (x_i c_r_i - sum_{j>i} p x_j) * c_i
+template <typename T, int V>
+__global__ void k_bwd_level(int i0, int i1, Rows<T> R, const T* __restrict__ c,
+                            const T* __restrict__ c_r, T* __restrict__ x,
+                            const int* __restrict__ n_active) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1 || (n_active && *n_active == 0)) return;
+  RowIt<T> it(R, i);
+  const T cr = c_r[i];
+  T acc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = mul(x[(size_t)i * V + v], cr);
+  for (int k = 0; k < it.w; ++k) {
+    const int e = it.base + k * kWarp;
+    const int j = __ldg(&R.col[e]);
+    if (j > i) {
+      const T a = R.sval[e];
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, __ldcg(&x[(size_t)j * V + v])));
+    }
+  }
+  const T ci = c[i];
+#pragma unroll
+  for (int v = 0; v < V; ++v) x[(size_t)i * V + v] = mul(acc[v], ci);
+}
+// Jacobi: x = b*c (solv_direct.f90:41)
+template <typename T, int V>
+__global__ void k_jacobi(int n, const T* __restrict__ c, const T* __restrict__ bvec,
+                         T* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const T ci = c[i];
+#pragma unroll
+    for (int v = 0; v < V; ++v) x[(size_t)i * V + v] = mul(bvec[(size_t)i * V + v], ci);
+  }
+}
+
+// ---- plain matrix product (benchmarks / solv_gpu_spmv) ---------------------
+template <typename T, int V>
+__global__ void k_spmv(int n, Rows<T> R, const T* __restrict__ x, T* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    T t[V];
+    row_apply<T, V>(R, i, x, t);
+#pragma unroll
+    for (int v = 0; v < V; ++v) y[(size_t)i * V + v] = t[v];
+  }
+}
+
+// ======================= CG: solv_cg.f90:26-84 =============================
+// Lane init for CG: s = large, iter = 0, active = 1.
+__global__ void k_lane_init(Lane* lanes, int nl, int n_iter, double reduc, int* n_active) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l == 0) *n_active = nl;
+  if (l >= nl) return;
+  Lane L;
+  L.s = kLarge; L.beta = 0.0; L.alpha = 1.0; L.pq = 0.0;   // solv_cg.f90:29
+  L.rho = 0.0; L.beta0 = 1.0; L.gam = 1.0; L.omeg = 0.0;   // solv_bicg.f90:31-33
+  L.res0_n = lanes[l].res0_n;
+  L.ratio = 0.0; L.reduc = reduc; L.l1 = 0.0;
+  L.iter = 0; L.n_iter = n_iter; L.active = 1; L.status = kLaneRunning;
+  if (n_iter <= 0) { L.active = 0; L.status = kLaneMaxIter; atomicSub(n_active, 1); }
+  lanes[l] = L;
+}
+
+// s = r.z with z = M^-1 r (Jacobi: z = c r, computed here); then
+// beta = (1/s_old) s, s_old = s  (solv_cg.f90:44-50)
+template <typename T, int V, bool JAC>
+__global__ void k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
+                        const T* __restrict__ z, double* __restrict__ part,
+                        Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) any |= lanes[s * V + v].active != 0;
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = 0.0;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const T ri = r[(size_t)i * V + v];
+      const T zi = JAC ? mul(ri, c[i]) : z[(size_t)i * V + v];
+      acc[v] += prod(ri, zi);
+    }
+  }
+  double tot[V];
+  if (seg_commit<V>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      Lane& L = lanes[s * V + v];
+      if (!L.active) continue;
+      double beta = 1.0 / L.s;   // :44
+      L.s = tot[v];              // :47
+      L.beta = beta * L.s;       // :50
+    }
+  }
+}
+
+// p = z + beta p  (solv_cg.f90:53)
+template <typename T, int V, bool JAC>
+__global__ void k_cg_p(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
+                       const T* __restrict__ z, T* __restrict__ p,
+                       const Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool act[V];
+  T beta[V];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    act[v] = lanes[s * V + v].active != 0;
+    beta[v] = (T)lanes[s * V + v].beta;
+    any |= act[v];
+  }
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if (!act[v]) continue;
+      const size_t k = (size_t)i * V + v;
+      const T zi = JAC ? mul(r[k], c[i]) : z[k];
+      p[k] = add(zi, mul(beta[v], p[k]));
+    }
+  }
+}
+
+// q = A p and p.q; alpha = s / (p.q + small)   (solv_cg.f90:56-68)
+template <typename T, int V>
+__global__ void k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
+                          double* __restrict__ part, Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) any |= lanes[s * V + v].active != 0;
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = 0.0;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+    T y[V];
+    row_apply<T, V>(R, i, p, y);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      q[(size_t)i * V + v] = y[v];
+      acc[v] += prod(p[(size_t)i * V + v], y[v]);
+    }
+  }
+  double tot[V];
+  if (seg_commit<V>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      Lane& L = lanes[s * V + v];
+      if (!L.active) continue;
+      L.pq = tot[v];
+      L.alpha = L.s / (tot[v] + kSmall);  // :67-68
+    }
+  }
+}
+
+// phi += alpha p; r -= alpha q; L1 = sum|r|; stop test (solv_cg.f90:73-82).
+// With JAC, also s_next = r.(c r) and beta for the next iteration.
+template <typename T, int V, bool JAC>
+__global__ void k_cg_update(SegMap sm, const T* __restrict__ c, T* __restrict__ phi,
+                            T* __restrict__ r, const T* __restrict__ p,
+                            const T* __restrict__ q, double* __restrict__ part,
+                            Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool act[V];
+  T alpha[V];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    act[v] = lanes[s * V + v].active != 0;
+    alpha[v] = (T)lanes[s * V + v].alpha;
+    any |= act[v];
+  }
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  constexpr int NR = JAC ? 2 * V : V;
+  double acc[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) acc[k] = 0.0;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if (!act[v]) continue;
+      const size_t k = (size_t)i * V + v;
+      phi[k] = add(phi[k], mul(alpha[v], p[k]));
+      const T rn = sub(r[k], mul(alpha[v], q[k]));
+      r[k] = rn;
+      acc[v] += (double)fabs(rn);
+      if (JAC) acc[V + v] += prod(rn, mul(rn, c[i]));
+    }
+  }
+  double tot[NR];
+  if (seg_commit<NR>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      Lane& L = lanes[s * V + v];
+      if (!L.active) continue;
+      L.iter += 1;
+      L.l1 = tot[v];
+      const double ratio = tot[v] / (L.res0_n + kSmall);  // :81
+      L.ratio = ratio;
+      if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);
+      else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);  // :82
+      else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
+      if (JAC && L.active) {
+        double beta = 1.0 / L.s;
+        L.s = tot[V + v];
+        L.beta = beta * L.s;
+      }
+    }
+  }
+}
+
+// ===================== BiCGSTAB: solv_bicg.f90:27-118 ======================
+// rho = r.r0; omeg = rho*gam/(alpha*beta0+small); beta0 = rho  (:48-50)
+template <typename T, int V>
+__global__ void k_bi_rho(SegMap sm, const T* __restrict__ r, const T* __restrict__ r0,
+                         double* __restrict__ part, Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) any |= lanes[s * V + v].active != 0;
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = 0.0;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] += prod(r[(size_t)i * V + v], r0[(size_t)i * V + v]);
+  }
+  double tot[V];
+  if (seg_commit<V>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      Lane& L = lanes[s * V + v];
+      if (!L.active) continue;
+      L.rho = tot[v];
+      L.omeg = L.rho * L.gam / (L.alpha * L.beta0 + kSmall);
+      L.beta0 = L.rho;
+    }
+  }
+}
+
+// p = r + omeg (p - alpha u); with JAC also z = c p  (:54-58)
+template <typename T, int V, bool JAC>
+__global__ void k_bi_p(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
+                       T* __restrict__ p, const T* __restrict__ u, T* __restrict__ z,
+                       const Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool act[V];
+  T om[V], al[V];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    act[v] = lanes[s * V + v].active != 0;
+    om[v] = (T)lanes[s * V + v].omeg;
+    al[v] = (T)lanes[s * V + v].alpha;
+    any |= act[v];
+  }
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if (!act[v]) continue;
+      const size_t k = (size_t)i * V + v;
+      const T pn = add(r[k], mul(om[v], sub(p[k], mul(al[v], u[k]))));
+      p[k] = pn;
+      if (JAC) z[k] = mul(pn, c[i]);
+    }
+  }
+}
+
+// y = A z, and dots: MODE 0 -> y.r0 (gam = rho/(y.r0+small), :72-73)
+//                    MODE 1 -> y.r, y.y (alpha = (y.r)/(y.y+small), :98-100)
+template <typename T, int V, int MODE>
+__global__ void k_bi_spmv(Rows<T> R, SegMap sm, const T* __restrict__ z, T* __restrict__ y,
+                          const T* __restrict__ w, double* __restrict__ part,
+                          Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) any |= lanes[s * V + v].active != 0;
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  constexpr int NR = MODE == 0 ? V : 2 * V;
+  double acc[NR];
+#pragma unroll
+  for (int k = 0; k < NR; ++k) acc[k] = 0.0;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+    T t[V];
+    row_apply<T, V>(R, i, z, t);
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      y[(size_t)i * V + v] = t[v];
+      acc[v] += prod(t[v], w[(size_t)i * V + v]);
+      if (MODE == 1) acc[V + v] += prod(t[v], t[v]);
+    }
+  }
+  double tot[NR];
+  if (seg_commit<NR>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      Lane& L = lanes[s * V + v];
+      if (!L.active) continue;
+      if (MODE == 0) {
+        L.gam = L.rho / (tot[v] + kSmall);
+      } else {
+        L.alpha = tot[v] / (tot[V + v] + kSmall);
+      }
+    }
+  }
+}
+
+// phi += gam z; r -= gam u; with JAC also z = c r   (:77-84)
+template <typename T, int V, bool JAC>
+__global__ void k_bi_half(SegMap sm, const T* __restrict__ c, T* __restrict__ phi,
+                          T* __restrict__ r, T* __restrict__ z, const T* __restrict__ u,
+                          const Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool act[V];
+  T g[V];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    act[v] = lanes[s * V + v].active != 0;
+    g[v] = (T)lanes[s * V + v].gam;
+    any |= act[v];
+  }
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if (!act[v]) continue;
+      const size_t k = (size_t)i * V + v;
+      phi[k] = add(phi[k], mul(g[v], z[k]));
+      const T rn = sub(r[k], mul(g[v], u[k]));
+      r[k] = rn;
+      if (JAC) z[k] = mul(rn, c[i]);
+    }
+  }
+}
+
+// phi += alpha z; r -= alpha v; L1; stop test; rho_next = r.r0 with the
+// omeg / beta0 update of the next iteration's head (:105-116, :48-50).
+template <typename T, int V>
+__global__ void k_bi_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
+                            const T* __restrict__ z, const T* __restrict__ vv,
+                            const T* __restrict__ r0, double* __restrict__ part,
+                            Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool act[V];
+  T al[V];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) {
+    act[v] = lanes[s * V + v].active != 0;
+    al[v] = (T)lanes[s * V + v].alpha;
+    any |= act[v];
+  }
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[2 * V];
+#pragma unroll
+  for (int k = 0; k < 2 * V; ++k) acc[k] = 0.0;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      if (!act[v]) continue;
+      const size_t k = (size_t)i * V + v;
+      phi[k] = add(phi[k], mul(al[v], z[k]));
+      const T rn = sub(r[k], mul(al[v], vv[k]));
+      r[k] = rn;
+      acc[v] += (double)fabs(rn);
+      acc[V + v] += prod(rn, r0[k]);
+    }
+  }
+  double tot[2 * V];
+  if (seg_commit<2 * V>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      Lane& L = lanes[s * V + v];
+      if (!L.active) continue;
+      L.iter += 1;
+      L.l1 = tot[v];
+      const double ratio = tot[v] / (L.res0_n + kSmall);
+      L.ratio = ratio;
+      if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);
+      else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);
+      else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
+      if (L.active) {
+        L.rho = tot[V + v];
+        L.omeg = L.rho * L.gam / (L.alpha * L.beta0 + kSmall);
+        L.beta0 = L.rho;
+      }
+    }
+  }
+}
+
+}  // namespace sg

@@ -1,0 +1,1049 @@
+// solv_gpu.cu -- host runtime and C-ABI of the B200 face-addressed Krylov
+// solvers (include/solv_gpu.h).
+//
+// Hot path replaced: spray-simulation/solv_cg.f90, solv_bicg.f90,
+// solv_precond.f90, solv_direct.f90, solv_res.f90 over the matrix of
+// solv_data.f90 (ng, pl, v_lst).  The matrix is copied to HBM once per
+// structure, re-laid out (wavefront-level-major cell order, sliced ELL
+// rows in face order) and kept resident; solves run as a chain of fused
+// kernels with the Krylov scalars kept on the device, so the host only
+// polls a convergence counter every `graph_iters` iterations.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/solv_gpu.h"
+#include "kernels.cuh"
+
+using sg::Lane;
+using sg::Rows;
+using sg::SegMap;
+
+namespace {
+
+constexpr int kMaxV = 4;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+  void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, b ? b : 16);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Host-side description of the segment (system) -> block map.
+struct SegHost {
+  std::vector<int> blk_seg, blk_rank, seg_nblk, seg_blk0, seg_c0, seg_c1;
+  int total_blk = 0;
+};
+
+}  // namespace
+
+struct solv_gpu_ctx {
+  int dev = 0;
+  cudaStream_t own = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int n_sm = 148;
+  // options
+  int precision = 0;
+  double inner_reduc = 1e-4;
+  int graph_iters = 16;
+  int block = 256;
+  int grid_per_sm = 4;
+  int max_refine = 30;
+
+  // matrix (caller sizes)
+  bool has_matrix = false;
+  int N = 0, F = 0;
+  bool orient_std = true;
+  std::vector<int> lvl_ptr;  // wavefront level ranges in internal order
+  long long n_slots = 0;
+  int n_slice = 0;
+  DevBuf old_of_new, slice_ptr, slice_w, col, slot_src, val, sval, diag, fp, fn;
+  DevBuf valf, svalf, diagf;  // FP32 copies for the mixed-precision inner solve
+  bool f32_valid = false;
+
+  // segment map (single system: one segment)
+  SegHost seg;
+  DevBuf d_seg;  // packed ints
+  DevBuf ticket, n_active, lanes, part;
+  int* h_n_active = nullptr;  // pinned
+
+  // workspace
+  DevBuf w_phi, w_r0, w_r, w_p, w_q, w_v, w_z, w_c, w_cr, w_in, w_out;
+  DevBuf wf_r, wf_p, wf_q, wf_v, wf_z, wf_phi, wf_c, wf_cr, wf_r0;  // FP32
+  DevBuf w_x, w_b;  // solv_gpu_direct / spmv staging
+
+  // captured iteration graphs, keyed by (solver, imat, V, fp32)
+  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;
+  int launches = 0;
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+int set_err(solv_gpu_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                   \
+  do {                                                                        \
+    cudaError_t e_ = (expr);                                                  \
+    if (e_ != cudaSuccess)                                                    \
+      return set_err(ctx, SOLV_GPU_DEVICE_ERROR,                              \
+                     std::string(#expr) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+void drop_graphs(solv_gpu_ctx* c) {
+  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  c->graphs.clear();
+}
+
+SegMap segmap(solv_gpu_ctx* c) {
+  const int nb = c->seg.total_blk, ns = (int)c->seg.seg_nblk.size();
+  int* base = c->d_seg.as<int>();
+  SegMap m;
+  m.blk_seg = base;
+  m.blk_rank = base + nb;
+  m.seg_nblk = base + 2 * nb;
+  m.seg_blk0 = base + 2 * nb + ns;
+  m.seg_c0 = base + 2 * nb + 2 * ns;
+  m.seg_c1 = base + 2 * nb + 3 * ns;
+  m.ticket = c->ticket.as<unsigned int>();
+  m.n_active = c->n_active.as<int>();
+  return m;
+}
+
+// Blocks per segment proportional to its size, at least one each.
+int build_segments(solv_gpu_ctx* c, const std::vector<int>& seg_c0,
+                   const std::vector<int>& seg_c1) {
+  SegHost& s = c->seg;
+  s = SegHost();
+  const int ns = (int)seg_c0.size();
+  long long total = 0;
+  for (int k = 0; k < ns; ++k) total += seg_c1[k] - seg_c0[k];
+  const long long cap = (long long)c->n_sm * c->grid_per_sm;
+  for (int k = 0; k < ns; ++k) {
+    long long n = seg_c1[k] - seg_c0[k];
+    long long want = (n + c->block - 1) / c->block;
+    long long share = total > 0 ? (cap * n + total - 1) / total : 1;
+    int nb = (int)std::max(1LL, std::min(want, share));
+    s.seg_blk0.push_back(s.total_blk);
+    s.seg_nblk.push_back(nb);
+    s.seg_c0.push_back(seg_c0[k]);
+    s.seg_c1.push_back(seg_c1[k]);
+    for (int r = 0; r < nb; ++r) {
+      s.blk_seg.push_back(k);
+      s.blk_rank.push_back(r);
+    }
+    s.total_blk += nb;
+  }
+  std::vector<int> packed;
+  packed.insert(packed.end(), s.blk_seg.begin(), s.blk_seg.end());
+  packed.insert(packed.end(), s.blk_rank.begin(), s.blk_rank.end());
+  packed.insert(packed.end(), s.seg_nblk.begin(), s.seg_nblk.end());
+  packed.insert(packed.end(), s.seg_blk0.begin(), s.seg_blk0.end());
+  packed.insert(packed.end(), s.seg_c0.begin(), s.seg_c0.end());
+  packed.insert(packed.end(), s.seg_c1.begin(), s.seg_c1.end());
+  CUDA_TRY(c, c->d_seg.ensure(packed.size() * sizeof(int)));
+  CUDA_TRY(c, cudaMemcpyAsync(c->d_seg.p, packed.data(), packed.size() * sizeof(int),
+                              cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, c->ticket.ensure(ns * sizeof(unsigned)));
+  CUDA_TRY(c, cudaMemsetAsync(c->ticket.p, 0, ns * sizeof(unsigned), c->stream));
+  CUDA_TRY(c, c->lanes.ensure((size_t)ns * kMaxV * sizeof(Lane)));
+  CUDA_TRY(c, c->part.ensure((size_t)s.total_blk * 2 * kMaxV * sizeof(double)));
+  CUDA_TRY(c, c->n_active.ensure(sizeof(int)));
+  drop_graphs(c);
+  return SOLV_GPU_OK;
+}
+
+template <typename T>
+Rows<T> rows(solv_gpu_ctx* c) {
+  Rows<T> R;
+  R.slice_ptr = c->slice_ptr.as<int>();
+  R.slice_w = c->slice_w.as<uint8_t>();
+  R.col = c->col.as<int>();
+  if constexpr (std::is_same<T, double>::value) {
+    R.val = c->val.as<double>();
+    R.sval = c->orient_std ? c->val.as<double>() : c->sval.as<double>();
+    R.diag = c->diag.as<double>();
+  } else {
+    R.val = c->valf.as<float>();
+    R.sval = c->orient_std ? c->valf.as<float>() : c->svalf.as<float>();
+    R.diag = c->diagf.as<float>();
+  }
+  return R;
+}
+
+int grid_for(solv_gpu_ctx* c, long long n) {
+  long long g = (n + c->block - 1) / c->block;
+  long long cap = (long long)c->n_sm * 16;
+  return (int)std::max(1LL, std::min(g, cap));
+}
+
+// ---- matrix structure --------------------------------------------------------
+int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in) {
+  if (N <= 0 || F < 0 || !ip || !in)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set: bad sizes or null pointers");
+  // validate + per-cell interior degree
+  std::vector<int> deg(N, 0);
+  bool orient = true;
+  for (int f = 0; f < F; ++f) {
+    int a = ip[f], b = in[f];
+    if (a < 1 || a > N || b < 0 || b > N || a == b)
+      return set_err(c, SOLV_GPU_BAD_INPUT,
+                     "matrix_set: face " + std::to_string(f + 1) + " has ip=" +
+                         std::to_string(a) + " in=" + std::to_string(b));
+    if (b > 0) {
+      deg[a - 1]++;
+      deg[b - 1]++;
+      if (b < a) orient = false;
+    }
+  }
+  std::vector<long long> rp(N + 1, 0);
+  for (int i = 0; i < N; ++i) rp[i + 1] = rp[i] + deg[i];
+  // rows in caller numbering, faces ascending (grd_conn.f90:129-152)
+  std::vector<int> rnb(rp[N]), rsrc(rp[N]);
+  std::vector<long long> fill(rp.begin(), rp.end() - 1);
+  for (int f = 0; f < F; ++f) {
+    int a = ip[f] - 1, b = in[f] - 1;
+    if (b < 0) continue;
+    rnb[fill[a]] = b;
+    rsrc[fill[a]++] = 2 * f;
+    rnb[fill[b]] = a;
+    rsrc[fill[b]++] = 2 * f + 1;
+  }
+  // wavefront levels of the lower DAG (neighbour index below the cell)
+  std::vector<int> lev(N, 0);
+  int nl = 0;
+  for (int i = 0; i < N; ++i) {
+    int l = 0;
+    for (long long k = rp[i]; k < rp[i + 1]; ++k)
+      if (rnb[k] < i) l = std::max(l, lev[rnb[k]] + 1);
+    lev[i] = l;
+    nl = std::max(nl, l + 1);
+  }
+  // internal order: level-major, caller order inside a level
+  std::vector<int> cnt(nl + 1, 0);
+  for (int i = 0; i < N; ++i) cnt[lev[i] + 1]++;
+  for (int l = 0; l < nl; ++l) cnt[l + 1] += cnt[l];
+  c->lvl_ptr.assign(cnt.begin(), cnt.end());
+  std::vector<int> old_of_new(N), new_of_old(N);
+  {
+    std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+    for (int i = 0; i < N; ++i) {
+      int k = pos[lev[i]]++;
+      old_of_new[k] = i;
+      new_of_old[i] = k;
+    }
+  }
+  // sliced ELL, 32 cells per slice
+  const int ns = (N + 31) / 32;
+  std::vector<int> sp(ns + 1, 0);
+  std::vector<uint8_t> sw(ns, 0);
+  long long total = 0;
+  for (int s = 0; s < ns; ++s) {
+    int w = 0;
+    for (int l = 0; l < 32; ++l) {
+      int i = s * 32 + l;
+      if (i < N) w = std::max(w, deg[old_of_new[i]]);
+    }
+    if (w > 255) return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set: a cell has more than 255 faces");
+    sw[s] = (uint8_t)w;
+    if (total > (1LL << 31) - 1 - 32LL * w)
+      return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set: too many matrix entries for int32 offsets");
+    sp[s] = (int)total;
+    total += 32LL * w;
+  }
+  sp[ns] = (int)total;
+  std::vector<int> hcol(total, -1), hsrc(total, -1);
+  for (int s = 0; s < ns; ++s)
+    for (int l = 0; l < 32; ++l) {
+      int i = s * 32 + l;
+      if (i >= N) continue;
+      int o = old_of_new[i];
+      int k = 0;
+      for (long long q = rp[o]; q < rp[o + 1]; ++q, ++k) {
+        long long e = sp[s] + (long long)k * 32 + l;
+        hcol[e] = new_of_old[rnb[q]];
+        hsrc[e] = rsrc[q];
+      }
+    }
+  drop_graphs(c);
+  c->N = N;
+  c->F = F;
+  c->orient_std = orient;
+  c->n_slots = total;
+  c->n_slice = ns;
+  c->f32_valid = false;
+  cudaStream_t st = c->stream;
+  CUDA_TRY(c, c->old_of_new.ensure(N * sizeof(int)));
+  CUDA_TRY(c, c->slice_ptr.ensure((ns + 1) * sizeof(int)));
+  CUDA_TRY(c, c->slice_w.ensure(ns));
+  CUDA_TRY(c, c->col.ensure(total * sizeof(int)));
+  CUDA_TRY(c, c->slot_src.ensure(total * sizeof(int)));
+  CUDA_TRY(c, c->val.ensure(total * sizeof(double)));
+  if (!orient) CUDA_TRY(c, c->sval.ensure(total * sizeof(double)));
+  CUDA_TRY(c, c->diag.ensure(N * sizeof(double)));
+  CUDA_TRY(c, c->fp.ensure(std::max(F, 1) * sizeof(double)));
+  CUDA_TRY(c, c->fn.ensure(std::max(F, 1) * sizeof(double)));
+  CUDA_TRY(c, cudaMemcpyAsync(c->old_of_new.p, old_of_new.data(), N * sizeof(int), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->slice_ptr.p, sp.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->slice_w.p, sw.data(), ns, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->col.p, hcol.data(), total * sizeof(int), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, cudaMemcpyAsync(c->slot_src.p, hsrc.data(), total * sizeof(int), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(c, cudaStreamSynchronize(st));  // host vectors die here
+  int rc = build_segments(c, {0}, {N});
+  if (rc) return rc;
+  c->has_matrix = true;
+  return SOLV_GPU_OK;
+}
+
+int matrix_values_dev(solv_gpu_ctx* c, const double* p, const double* n, const double* pl) {
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  const int N = c->N;
+  if (p != c->fp.as<double>() && c->F > 0)
+    CUDA_TRY(c, cudaMemcpyAsync(c->fp.p, p, c->F * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  if (n != c->fn.as<double>() && c->F > 0)
+    CUDA_TRY(c, cudaMemcpyAsync(c->fn.p, n, c->F * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  sg::k_fill_values<double><<<grid_for(c, N), c->block, 0, c->stream>>>(
+      N, c->slice_ptr.as<int>(), c->slice_w.as<uint8_t>(), c->slot_src.as<int>(),
+      c->col.as<int>(), c->fp.as<double>(), c->fn.as<double>(), c->val.as<double>(),
+      c->orient_std ? nullptr : c->sval.as<double>());
+  sg::k_fill_diag<double><<<grid_for(c, N), c->block, 0, c->stream>>>(
+      N, c->old_of_new.as<int>(), pl, c->diag.as<double>());
+  CUDA_TRY(c, cudaGetLastError());
+  c->f32_valid = false;
+  return SOLV_GPU_OK;
+}
+
+int ensure_f32_matrix(solv_gpu_ctx* c) {
+  if (c->f32_valid) return SOLV_GPU_OK;
+  CUDA_TRY(c, c->valf.ensure(c->n_slots * sizeof(float)));
+  CUDA_TRY(c, c->diagf.ensure(c->N * sizeof(float)));
+  sg::k_convert<double, float><<<grid_for(c, c->n_slots), c->block, 0, c->stream>>>(
+      c->n_slots, c->val.as<double>(), c->valf.as<float>());
+  if (!c->orient_std) {
+    CUDA_TRY(c, c->svalf.ensure(c->n_slots * sizeof(float)));
+    sg::k_convert<double, float><<<grid_for(c, c->n_slots), c->block, 0, c->stream>>>(
+        c->n_slots, c->sval.as<double>(), c->svalf.as<float>());
+  }
+  sg::k_convert<double, float><<<grid_for(c, c->N), c->block, 0, c->stream>>>(
+      c->N, c->diag.as<double>(), c->diagf.as<float>());
+  CUDA_TRY(c, cudaGetLastError());
+  c->f32_valid = true;
+  return SOLV_GPU_OK;
+}
+
+// ---- building blocks -----------------------------------------------------------
+template <int V>
+void launch_res(solv_gpu_ctx* c, const double* phi, double* r, int not_r0) {
+  sg::k_res<V><<<c->seg.total_blk, c->block, 0, c->stream>>>(
+      rows<double>(c), segmap(c), phi, r, not_r0, c->part.as<double>(), c->lanes.as<Lane>());
+  c->launches++;
+}
+
+int run_res(solv_gpu_ctx* c, int V, const double* phi, double* r, int not_r0) {
+  switch (V) {
+    case 1: launch_res<1>(c, phi, r, not_r0); break;
+    case 2: launch_res<2>(c, phi, r, not_r0); break;
+    case 3: launch_res<3>(c, phi, r, not_r0); break;
+    case 4: launch_res<4>(c, phi, r, not_r0); break;
+    default: return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
+  }
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
+}
+
+// solv_precond: c, c_r in internal order (FP64)
+void launch_precond(solv_gpu_ctx* c, int imat, double* cc, double* cr) {
+  if (imat <= 0) {
+    sg::k_precond_level<<<(c->N + c->block - 1) / c->block, c->block, 0, c->stream>>>(
+        0, c->N, 0, rows<double>(c), c->slot_src.as<int>(), c->fp.as<double>(),
+        c->fn.as<double>(), cc, cr);
+    c->launches++;
+    return;
+  }
+  const int nl = (int)c->lvl_ptr.size() - 1;
+  for (int l = 0; l < nl; ++l) {
+    int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
+    sg::k_precond_level<<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
+        i0, i1, imat, rows<double>(c), c->slot_src.as<int>(), c->fp.as<double>(),
+        c->fn.as<double>(), cc, cr);
+    c->launches++;
+  }
+}
+
+// x = M^-1 b  (solv_direct), internal order, V components
+template <typename T, int V>
+void launch_direct(solv_gpu_ctx* c, int imat, const T* cc, const T* cr, T* x, const T* b,
+                   const int* n_active) {
+  if (imat <= 0) {
+    sg::k_jacobi<T, V><<<grid_for(c, c->N), c->block, 0, c->stream>>>(c->N, cc, b, x);
+    c->launches++;
+    return;
+  }
+  const int nl = (int)c->lvl_ptr.size() - 1;
+  Rows<T> R = rows<T>(c);
+  for (int l = 0; l < nl; ++l) {
+    int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
+    sg::k_fwd_level<T, V><<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
+        i0, i1, R, cc, b, x, n_active);
+  }
+  for (int l = nl - 1; l >= 0; --l) {
+    int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
+    sg::k_bwd_level<T, V><<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
+        i0, i1, R, cc, cr, x, n_active);
+  }
+  c->launches += 2 * nl;
+}
+
+// Workspace for V components in precision T.
+template <typename T>
+struct WS {
+  T *phi, *r, *r0, *p, *q, *v, *z, *c, *cr;
+};
+
+template <typename T>
+int ensure_ws(solv_gpu_ctx* c, int V, WS<T>& w) {
+  const size_t nv = (size_t)c->N * V * sizeof(T), n1 = (size_t)c->N * sizeof(T);
+  bool f = std::is_same<T, float>::value;
+  DevBuf* b[9];
+  if (!f) {
+    DevBuf* bd[9] = {&c->w_phi, &c->w_r, &c->w_r0, &c->w_p, &c->w_q, &c->w_v, &c->w_z, &c->w_c, &c->w_cr};
+    std::copy(bd, bd + 9, b);
+  } else {
+    DevBuf* bf[9] = {&c->wf_phi, &c->wf_r, &c->wf_r0, &c->wf_p, &c->wf_q, &c->wf_v, &c->wf_z, &c->wf_c, &c->wf_cr};
+    std::copy(bf, bf + 9, b);
+  }
+  for (int k = 0; k < 9; ++k) {
+    void* old = b[k]->p;
+    CUDA_TRY(c, b[k]->ensure(k < 7 ? nv : n1));
+    if (old != b[k]->p) drop_graphs(c);
+  }
+  w.phi = b[0]->as<T>(); w.r = b[1]->as<T>(); w.r0 = b[2]->as<T>(); w.p = b[3]->as<T>();
+  w.q = b[4]->as<T>(); w.v = b[5]->as<T>(); w.z = b[6]->as<T>(); w.c = b[7]->as<T>();
+  w.cr = b[8]->as<T>();
+  return SOLV_GPU_OK;
+}
+
+// One CG iteration (solv_cg.f90:37-84) on workspace w.
+template <typename T, int V>
+void cg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
+  SegMap sm = segmap(c);
+  double* part = c->part.as<double>();
+  Lane* lanes = c->lanes.as<Lane>();
+  const int G = c->seg.total_blk, B = c->block;
+  cudaStream_t st = c->stream;
+  if (imat > 0) {
+    launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active);
+    sg::k_cg_rz<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, part, lanes);
+    sg::k_cg_p<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes);
+    sg::k_cg_spmv<T, V><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, part, lanes);
+    sg::k_cg_update<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.p, w.q, part, lanes);
+    c->launches += 4;
+  } else {
+    sg::k_cg_p<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes);
+    sg::k_cg_spmv<T, V><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, part, lanes);
+    sg::k_cg_update<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.p, w.q, part, lanes);
+    c->launches += 3;
+  }
+}
+
+// One BiCGSTAB iteration (solv_bicg.f90:42-118); rho/omeg of its head were
+// produced by the previous k_bi_update (or k_bi_rho before the first).
+template <typename T, int V>
+void bicg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
+  SegMap sm = segmap(c);
+  double* part = c->part.as<double>();
+  Lane* lanes = c->lanes.as<Lane>();
+  const int G = c->seg.total_blk, B = c->block;
+  cudaStream_t st = c->stream;
+  // w.q holds u, w.v holds v
+  if (imat > 0) {
+    sg::k_bi_p<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.p, w.q, w.z, lanes);
+    launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.p, sm.n_active);
+  } else {
+    sg::k_bi_p<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.r, w.p, w.q, w.z, lanes);
+  }
+  sg::k_bi_spmv<T, V, 0><<<G, B, 0, st>>>(rows<T>(c), sm, w.z, w.q, w.r0, part, lanes);
+  if (imat > 0) {
+    sg::k_bi_half<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.z, w.q, lanes);
+    launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active);
+  } else {
+    sg::k_bi_half<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.z, w.q, lanes);
+  }
+  sg::k_bi_spmv<T, V, 1><<<G, B, 0, st>>>(rows<T>(c), sm, w.z, w.v, w.r, part, lanes);
+  sg::k_bi_update<T, V><<<G, B, 0, st>>>(sm, w.phi, w.r, w.z, w.v, w.r0, part, lanes);
+  c->launches += 5;
+}
+
+// Run Krylov iterations until every lane stops (device counter), launching
+// `graph_iters` iterations per CUDA-graph launch.
+template <typename T, int V>
+int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& graph_launches) {
+  const int K = c->graph_iters;
+  auto body = [&]() {
+    if (solver == 0) cg_iteration<T, V>(c, imat, w);
+    else bicg_iteration<T, V>(c, imat, w);
+  };
+  cudaGraphExec_t exec = nullptr;
+  if (K > 0) {
+    auto key = std::make_tuple(solver, imat > 0 ? imat : 0, V, (int)std::is_same<T, float>::value);
+    auto it = c->graphs.find(key);
+    if (it != c->graphs.end()) {
+      exec = it->second;
+    } else {
+      cudaGraph_t g;
+      CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int l0 = c->launches;
+      for (int k = 0; k < K; ++k) body();
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      c->launches = l0;
+      CUDA_TRY(c, e);
+      e = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      CUDA_TRY(c, e);
+      c->graphs[key] = exec;
+    }
+  }
+  int done = 0;
+  int per_launch_kernels = 0;
+  {
+    // kernels per iteration (for the launch count statistics)
+    int l0 = c->launches;
+    // count by dry accounting: replicate the arithmetic of body()
+    int nl = (int)c->lvl_ptr.size() - 1;
+    int sweep = imat > 0 ? 2 * nl : 1;
+    if (solver == 0) per_launch_kernels = imat > 0 ? sweep + 4 : 3;
+    else per_launch_kernels = imat > 0 ? 2 * sweep + 5 : 5;
+    c->launches = l0;
+  }
+  while (done < n_iter) {
+    if (exec) {
+      CUDA_TRY(c, cudaGraphLaunch(exec, c->stream));
+      graph_launches++;
+      c->launches += K * per_launch_kernels;
+      done += K;
+    } else {
+      body();
+      done += 1;
+    }
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_n_active, c->n_active.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (*c->h_n_active <= 0) break;
+  }
+  return SOLV_GPU_OK;
+}
+
+__global__ void k_set_res0n(Lane* lanes, int nl, const double* r0n) {
+  int l = threadIdx.x;
+  if (l < nl) lanes[l].res0_n = r0n[l];
+}
+
+// Full FP64 solve (solver 0 = CG, 1 = BiCGSTAB) on device buffers in the
+// caller layouts.
+template <int V>
+int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
+               double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
+               solv_gpu_stats* st) {
+  WS<double> w;
+  int rc = ensure_ws<double>(c, V, w);
+  if (rc) return rc;
+  const int N = c->N;
+  cudaStream_t s = c->stream;
+  const int* o2n = c->old_of_new.as<int>();
+  sg::k_phi_in<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, phi_dev, w.phi);
+  sg::k_col_in<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, res0_dev, w.r0);
+  c->launches += 2;
+  rc = run_res(c, V, w.phi, w.r0, not_r0);  // solv_res: r0 = b - A phi, res0_n
+  if (rc) return rc;
+  // res0 out = initial residual (solv_cg.f90:20)
+  sg::k_col_out<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.r0, res0_dev);
+  c->launches++;
+  Lane hl[kMaxV];
+  CUDA_TRY(c, cudaMemcpyAsync(hl, c->lanes.p, V * sizeof(Lane), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  double mx = -HUGE_VAL;
+  for (int v = 0; v < V; ++v) {
+    res0_n[v] = hl[v].res0_n;
+    mx = std::max(mx, res0_n[v]);
+  }
+  if (st) st->n_vc = V;
+  if (mx < sg::kSmall) {  // solv_cg.f90:21 early return
+    if (st) st->status = SOLV_GPU_ZERO_RHS;
+    return SOLV_GPU_OK;
+  }
+  launch_precond(c, imat, w.c, w.cr);  // solv_precond
+  CUDA_TRY(c, cudaMemcpyAsync(w.r, w.r0, (size_t)N * V * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(c, cudaMemsetAsync(w.p, 0, (size_t)N * V * sizeof(double), s));
+  CUDA_TRY(c, cudaMemsetAsync(w.q, 0, (size_t)N * V * sizeof(double), s));
+  CUDA_TRY(c, cudaMemsetAsync(w.v, 0, (size_t)N * V * sizeof(double), s));
+  CUDA_TRY(c, cudaMemsetAsync(w.z, 0, (size_t)N * V * sizeof(double), s));
+  sg::k_lane_init<<<1, 32, 0, s>>>(c->lanes.as<Lane>(), V, n_iter, reduc, c->n_active.as<int>());
+  SegMap sm = segmap(c);
+  if (solver == 0) {
+    if (imat <= 0) {
+      sg::k_cg_rz<double, V, true><<<c->seg.total_blk, c->block, 0, s>>>(
+          sm, w.c, w.r, w.z, c->part.as<double>(), c->lanes.as<Lane>());
+      c->launches++;
+    }
+  } else {
+    sg::k_bi_rho<double, V><<<c->seg.total_blk, c->block, 0, s>>>(
+        sm, w.r, w.r0, c->part.as<double>(), c->lanes.as<Lane>());
+    c->launches++;
+  }
+  c->launches += 2;
+  CUDA_TRY(c, cudaGetLastError());
+  int gl = 0;
+  rc = iterate<double, V>(c, solver, imat, n_iter, w, gl);
+  if (rc) return rc;
+  sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.phi, phi_dev);
+  c->launches++;
+  CUDA_TRY(c, cudaMemcpyAsync(hl, c->lanes.p, V * sizeof(Lane), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  int status = SOLV_GPU_OK;
+  for (int v = 0; v < V; ++v) {
+    if (hl[v].status == sg::kLaneNaN) status = SOLV_GPU_NAN;
+    else if (hl[v].status != sg::kLaneConverged && status == SOLV_GPU_OK) status = SOLV_GPU_MAXITER;
+  }
+  if (st) {
+    for (int v = 0; v < V; ++v) {
+      st->iters[v] = hl[v].iter;
+      st->ratio[v] = hl[v].ratio;
+    }
+    st->status = status;
+    st->graph_launches += gl;
+  }
+  return status;
+}
+
+int solve_dispatch(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int V,
+                   double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
+                   solv_gpu_stats* st);
+
+}  // namespace
+
+// =============================== C-ABI ========================================
+extern "C" {
+
+const char* solv_gpu_status_string(int s) {
+  switch (s) {
+    case SOLV_GPU_OK: return "ok";
+    case SOLV_GPU_MAXITER: return "iteration cap reached";
+    case SOLV_GPU_NAN: return "NaN/Inf in a reduction";
+    case SOLV_GPU_BAD_INPUT: return "bad input";
+    case SOLV_GPU_DEVICE_ERROR: return "CUDA error";
+    case SOLV_GPU_NO_MATRIX: return "no matrix set";
+    case SOLV_GPU_ZERO_RHS: return "zero initial residual (early return)";
+    default: return "unknown status";
+  }
+}
+
+const char* solv_gpu_last_error(const solv_gpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int solv_gpu_create(solv_gpu_ctx** out, int device) {
+  if (!out) return SOLV_GPU_BAD_INPUT;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return SOLV_GPU_DEVICE_ERROR;
+  if (device < 0 || device >= ndev) return SOLV_GPU_BAD_INPUT;
+  auto* c = new solv_gpu_ctx();
+  c->dev = device;
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMallocHost(&c->h_n_active, sizeof(int)) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    delete c;
+    return SOLV_GPU_DEVICE_ERROR;
+  }
+  c->stream = c->own;
+  cudaDeviceGetAttribute(&c->n_sm, cudaDevAttrMultiProcessorCount, device);
+  *out = c;
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_destroy(solv_gpu_ctx* c) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  cudaSetDevice(c->dev);
+  cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  if (c->h_n_active) cudaFreeHost(c->h_n_active);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  cudaStream_t own = c->own;
+  delete c;  // DevBufs free their memory
+  if (own) cudaStreamDestroy(own);
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_set_stream(solv_gpu_ctx* c, void* stream) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->own;
+  if (s != c->stream) {
+    drop_graphs(c);
+    c->stream = s;
+  }
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  switch (key) {
+    case SOLV_OPT_PRECISION:
+      if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "precision must be 0 or 1");
+      c->precision = (int)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_INNER_REDUC:
+      if (!(value > 0 && value < 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "inner reduc must be in (0,1)");
+      c->inner_reduc = value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_GRAPH_ITERS:
+      if (value < 0 || value > 1024) return set_err(c, SOLV_GPU_BAD_INPUT, "graph iters in 0..1024");
+      c->graph_iters = (int)value;
+      drop_graphs(c);
+      return SOLV_GPU_OK;
+    case SOLV_OPT_BLOCK: {
+      int b = (int)value;
+      if (b < 64 || b > 1024 || (b & 31)) return set_err(c, SOLV_GPU_BAD_INPUT, "block must be a multiple of 32 in 64..1024");
+      c->block = b;
+      if (c->has_matrix) return build_segments(c, {0}, {c->N});
+      return SOLV_GPU_OK;
+    }
+    case SOLV_OPT_GRID_PER_SM: {
+      int g = (int)value;
+      if (g < 1 || g > 64) return set_err(c, SOLV_GPU_BAD_INPUT, "grid per SM in 1..64");
+      c->grid_per_sm = g;
+      if (c->has_matrix) return build_segments(c, {0}, {c->N});
+      return SOLV_GPU_OK;
+    }
+    case SOLV_OPT_MAX_REFINE:
+      if (value < 1 || value > 1000) return set_err(c, SOLV_GPU_BAD_INPUT, "max refine in 1..1000");
+      c->max_refine = (int)value;
+      return SOLV_GPU_OK;
+    default:
+      return set_err(c, SOLV_GPU_BAD_INPUT, "unknown option key");
+  }
+}
+
+int solv_gpu_matrix_set(solv_gpu_ctx* c, int n_cell, int n_face, const int* ip, const int* in,
+                        const double* p, const double* n, const double* pl) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!p || !n || !pl) return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set: null coefficient pointer");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  c->has_matrix = false;
+  int rc = matrix_structure(c, n_cell, n_face, ip, in);
+  if (rc) return rc;
+  return solv_gpu_matrix_values(c, p, n, pl);
+}
+
+int solv_gpu_matrix_values(solv_gpu_ctx* c, const double* p, const double* n, const double* pl) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (!p || !n || !pl) return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_values: null pointer");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  CUDA_TRY(c, c->w_in.ensure((size_t)c->N * sizeof(double)));
+  if (c->F > 0) {
+    CUDA_TRY(c, cudaMemcpyAsync(c->fp.p, p, c->F * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(c->fn.p, n, c->F * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(c->w_in.p, pl, c->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = matrix_values_dev(c, c->fp.as<double>(), c->fn.as<double>(), c->w_in.as<double>());
+  if (rc) return rc;
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_matrix_values_dev(solv_gpu_ctx* c, const double* p, const double* n, const double* pl) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!p || !n || !pl) return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_values_dev: null pointer");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  return matrix_values_dev(c, p, n, pl);
+}
+
+int solv_gpu_matrix_levels(const solv_gpu_ctx* c) {
+  if (!c || !c->has_matrix) return -1;
+  return (int)c->lvl_ptr.size() - 1;
+}
+
+int solv_gpu_res(solv_gpu_ctx* c, int n_vc, const double* phi, double* res0, double* res0_n,
+                 int not_r0) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (n_vc < 1 || n_vc > kMaxV || !phi || !res0 || !res0_n)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "res: n_vc must be 1..4 and pointers non-null");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const int N = c->N, V = n_vc;
+  const size_t bytes = (size_t)N * V * sizeof(double);
+  CUDA_TRY(c, c->w_in.ensure(bytes));
+  CUDA_TRY(c, c->w_out.ensure(bytes));
+  CUDA_TRY(c, c->w_x.ensure(bytes));
+  CUDA_TRY(c, c->w_b.ensure(bytes));
+  cudaStream_t s = c->stream;
+  const int* o2n = c->old_of_new.as<int>();
+  CUDA_TRY(c, cudaMemcpyAsync(c->w_in.p, phi, bytes, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(c->w_out.p, res0, bytes, cudaMemcpyHostToDevice, s));
+  sg::k_phi_in<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, c->w_in.as<double>(), c->w_x.as<double>());
+  sg::k_col_in<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, c->w_out.as<double>(), c->w_b.as<double>());
+  int rc = run_res(c, V, c->w_x.as<double>(), c->w_b.as<double>(), not_r0);
+  if (rc) return rc;
+  sg::k_col_out<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, c->w_b.as<double>(), c->w_out.as<double>());
+  CUDA_TRY(c, cudaMemcpyAsync(res0, c->w_out.p, bytes, cudaMemcpyDeviceToHost, s));
+  Lane hl[kMaxV];
+  CUDA_TRY(c, cudaMemcpyAsync(hl, c->lanes.p, V * sizeof(Lane), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  for (int v = 0; v < V; ++v) res0_n[v] = hl[v].res0_n;
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_precond(solv_gpu_ctx* c, int imat, double* cc, double* cr) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (!cc || !cr) return set_err(c, SOLV_GPU_BAD_INPUT, "precond: null pointer");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const int N = c->N;
+  const size_t bytes = (size_t)N * sizeof(double);
+  CUDA_TRY(c, c->w_x.ensure(bytes));
+  CUDA_TRY(c, c->w_b.ensure(bytes));
+  CUDA_TRY(c, c->w_out.ensure(bytes));
+  cudaStream_t s = c->stream;
+  const int* o2n = c->old_of_new.as<int>();
+  launch_precond(c, imat, c->w_x.as<double>(), c->w_b.as<double>());
+  sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, c->w_x.as<double>(), c->w_out.as<double>());
+  CUDA_TRY(c, cudaMemcpyAsync(cc, c->w_out.p, bytes, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, c->w_b.as<double>(), c->w_out.as<double>());
+  CUDA_TRY(c, cudaMemcpyAsync(cr, c->w_out.p, bytes, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_direct(solv_gpu_ctx* c, int imat, const double* cc, const double* cr, double* x,
+                    const double* b) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (!cc || !cr || !x || !b) return set_err(c, SOLV_GPU_BAD_INPUT, "direct: null pointer");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const int N = c->N;
+  const size_t bytes = (size_t)N * sizeof(double);
+  WS<double> w;
+  int rc = ensure_ws<double>(c, 1, w);
+  if (rc) return rc;
+  CUDA_TRY(c, c->w_in.ensure(bytes));
+  cudaStream_t s = c->stream;
+  const int* o2n = c->old_of_new.as<int>();
+  auto up = [&](const double* h, double* d) -> int {
+    CUDA_TRY(c, cudaMemcpyAsync(c->w_in.p, h, bytes, cudaMemcpyHostToDevice, s));
+    sg::k_phi_in<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, c->w_in.as<double>(), d);
+    return SOLV_GPU_OK;
+  };
+  if ((rc = up(cc, w.c)) || (rc = up(cr, w.cr)) || (rc = up(b, w.r))) return rc;
+  launch_direct<double, 1>(c, imat, w.c, w.cr, w.z, w.r, nullptr);
+  sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, w.z, c->w_in.as<double>());
+  CUDA_TRY(c, cudaMemcpyAsync(x, c->w_in.p, bytes, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_spmv_dev(solv_gpu_ctx* c, const double* x_dev, double* y_dev, int repeat,
+                      float* ms_per_call) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const int N = c->N;
+  const size_t bytes = (size_t)N * sizeof(double);
+  CUDA_TRY(c, c->w_x.ensure(bytes));
+  CUDA_TRY(c, c->w_b.ensure(bytes));
+  cudaStream_t s = c->stream;
+  const int* o2n = c->old_of_new.as<int>();
+  sg::k_phi_in<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, x_dev, c->w_x.as<double>());
+  if (repeat < 1) repeat = 1;
+  CUDA_TRY(c, cudaEventRecord(c->ev0, s));
+  for (int k = 0; k < repeat; ++k)
+    sg::k_spmv<double, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<double>(c), c->w_x.as<double>(),
+                                                           c->w_b.as<double>());
+  CUDA_TRY(c, cudaEventRecord(c->ev1, s));
+  sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, c->w_b.as<double>(), y_dev);
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  CUDA_TRY(c, cudaGetLastError());
+  if (ms_per_call) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    *ms_per_call = ms / repeat;
+  }
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_spmv(solv_gpu_ctx* c, const double* x, double* y) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (!x || !y) return set_err(c, SOLV_GPU_BAD_INPUT, "spmv: null pointer");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const size_t bytes = (size_t)c->N * sizeof(double);
+  CUDA_TRY(c, c->w_in.ensure(bytes));
+  CUDA_TRY(c, c->w_out.ensure(bytes));
+  CUDA_TRY(c, cudaMemcpyAsync(c->w_in.p, x, bytes, cudaMemcpyHostToDevice, c->stream));
+  int rc = solv_gpu_spmv_dev(c, c->w_in.as<double>(), c->w_out.as<double>(), 1, nullptr);
+  if (rc) return rc;
+  CUDA_TRY(c, cudaMemcpyAsync(y, c->w_out.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return SOLV_GPU_OK;
+}
+
+static int solve_common(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int n_vc,
+                        double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
+                        solv_gpu_stats* st) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (n_vc < 1 || n_vc > kMaxV) return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
+  if (imat < 0 || imat > 2) return set_err(c, SOLV_GPU_BAD_INPUT, "imat must be 0, 1 or 2");
+  if (!phi_dev || !res0_dev || !res0_n) return set_err(c, SOLV_GPU_BAD_INPUT, "null pointer");
+  if (st) {
+    std::memset(st, 0, sizeof(*st));
+    st->n_levels = (int)c->lvl_ptr.size() - 1;
+  }
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  c->launches = 0;
+  CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+  int rc = solve_dispatch(c, solver, imat, reduc, n_iter, n_vc, phi_dev, res0_dev, res0_n, not_r0, st);
+  CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+  CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+  if (st) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    st->solve_ms = ms;
+    st->kernel_launches = c->launches;
+    if (rc != SOLV_GPU_OK && rc != SOLV_GPU_MAXITER && rc != SOLV_GPU_NAN) st->status = rc;
+  }
+  return rc;
+}
+
+static int solve_host(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int n_vc,
+                      double* phi, double* res0, double* res0_n, int not_r0, solv_gpu_stats* st) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (n_vc < 1 || n_vc > kMaxV) return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
+  if (!phi || !res0 || !res0_n) return set_err(c, SOLV_GPU_BAD_INPUT, "null pointer");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const size_t bytes = (size_t)c->N * n_vc * sizeof(double);
+  CUDA_TRY(c, c->w_in.ensure(bytes));
+  CUDA_TRY(c, c->w_out.ensure(bytes));
+  CUDA_TRY(c, cudaMemcpyAsync(c->w_in.p, phi, bytes, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->w_out.p, res0, bytes, cudaMemcpyHostToDevice, c->stream));
+  int rc = solve_common(c, solver, imat, reduc, n_iter, n_vc, c->w_in.as<double>(),
+                        c->w_out.as<double>(), res0_n, not_r0, st);
+  if (rc != SOLV_GPU_OK && rc != SOLV_GPU_MAXITER && rc != SOLV_GPU_NAN) return rc;
+  CUDA_TRY(c, cudaMemcpyAsync(phi, c->w_in.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(res0, c->w_out.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  return rc;
+}
+
+int solv_gpu_cg(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc, double* phi,
+                double* res0, double* res0_n, int not_r0, solv_gpu_stats* st) {
+  return solve_host(c, 0, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st);
+}
+int solv_gpu_bicg(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc, double* phi,
+                  double* res0, double* res0_n, int not_r0, solv_gpu_stats* st) {
+  return solve_host(c, 1, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st);
+}
+int solv_gpu_cg_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc, double* phi,
+                    double* res0, double* res0_n, int not_r0, solv_gpu_stats* st) {
+  return solve_common(c, 0, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st);
+}
+int solv_gpu_bicg_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc, double* phi,
+                      double* res0, double* res0_n, int not_r0, solv_gpu_stats* st) {
+  return solve_common(c, 1, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st);
+}
+
+// ---- Fortran bindings ----------------------------------------------------------
+static solv_gpu_ctx* fctx(int64_t* h) { return h ? reinterpret_cast<solv_gpu_ctx*>(*h) : nullptr; }
+
+void solv_gpu_create_(int64_t* h, int* device, int* status) {
+  solv_gpu_ctx* c = nullptr;
+  int rc = solv_gpu_create(&c, device ? *device : 0);
+  if (h) *h = reinterpret_cast<int64_t>(c);
+  if (status) *status = rc;
+}
+void solv_gpu_destroy_(int64_t* h, int* status) {
+  int rc = solv_gpu_destroy(fctx(h));
+  if (h) *h = 0;
+  if (status) *status = rc;
+}
+void solv_gpu_matrix_set_(int64_t* h, int* n_cell, int* n_face, const int* ip, const int* in,
+                          const double* p, const double* n, const double* pl, int* status) {
+  int rc = (n_cell && n_face) ? solv_gpu_matrix_set(fctx(h), *n_cell, *n_face, ip, in, p, n, pl)
+                              : SOLV_GPU_BAD_INPUT;
+  if (status) *status = rc;
+}
+void solv_gpu_matrix_values_(int64_t* h, const double* p, const double* n, const double* pl,
+                             int* status) {
+  int rc = solv_gpu_matrix_values(fctx(h), p, n, pl);
+  if (status) *status = rc;
+}
+void solv_gpu_res_(int64_t* h, int* n_vc, const double* phi, double* res0, double* res0_n,
+                   int* not_r0, int* status) {
+  int rc = (n_vc && not_r0) ? solv_gpu_res(fctx(h), *n_vc, phi, res0, res0_n, *not_r0)
+                            : SOLV_GPU_BAD_INPUT;
+  if (status) *status = rc;
+}
+void solv_gpu_precond_(int64_t* h, int* imat, double* cc, double* cr, int* status) {
+  int rc = imat ? solv_gpu_precond(fctx(h), *imat, cc, cr) : SOLV_GPU_BAD_INPUT;
+  if (status) *status = rc;
+}
+void solv_gpu_direct_(int64_t* h, int* imat, const double* cc, const double* cr, double* x,
+                      const double* b, int* status) {
+  int rc = imat ? solv_gpu_direct(fctx(h), *imat, cc, cr, x, b) : SOLV_GPU_BAD_INPUT;
+  if (status) *status = rc;
+}
+void solv_gpu_cg_(int64_t* h, int* imat, double* reduc, int* n_iter, int* n_vc, double* phi,
+                  double* res0, double* res0_n, int* not_r0, int* status) {
+  int rc = (imat && reduc && n_iter && n_vc && not_r0)
+               ? solv_gpu_cg(fctx(h), *imat, *reduc, *n_iter, *n_vc, phi, res0, res0_n, *not_r0, nullptr)
+               : SOLV_GPU_BAD_INPUT;
+  if (status) *status = rc;
+}
+void solv_gpu_bicg_(int64_t* h, int* imat, double* reduc, int* n_iter, int* n_vc, double* phi,
+                    double* res0, double* res0_n, int* not_r0, int* status) {
+  int rc = (imat && reduc && n_iter && n_vc && not_r0)
+               ? solv_gpu_bicg(fctx(h), *imat, *reduc, *n_iter, *n_vc, phi, res0, res0_n, *not_r0, nullptr)
+               : SOLV_GPU_BAD_INPUT;
+  if (status) *status = rc;
+}
+
+}  // extern "C"
+
+namespace {
+int solve_dispatch(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int V,
+                   double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
+                   solv_gpu_stats* st) {
+  switch (V) {
+    case 1: return solve_fp64<1>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st);
+    case 2: return solve_fp64<2>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st);
+    case 3: return solve_fp64<3>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st);
+    case 4: return solve_fp64<4>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st);
+  }
+  return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
+}
+}  // namespace

@@ -1,0 +1,194 @@
+"""Face-addressed meshes and matrices (host side, ``libfvmesh.so``).
+
+A :class:`Mesh` owns a hex mesh and exposes the spray-simulation face list
+(``ng(:)%ip``, ``ng(:)%in``, 1-based, ``in = 0`` on boundary faces; see
+spray-simulation/grd_conn.f90:99-113) plus the matrices the solvers take:
+
+* :meth:`Mesh.pressure` -- the pressure-correction Poisson system
+  (p = n = -area/l_pn, pl = sum area/l_pn, one pinned cell);
+* :meth:`Mesh.momentum` -- first-order upwind convection-diffusion with a
+  Taylor-Green flux and a 1/dt diagonal (cfd_setup.f90:324-330, 473-518).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import load
+
+_i32p = ctypes.POINTER(ctypes.c_int)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def _lib():
+    lib = load("libfvmesh.so")
+    if not getattr(lib, "_typed", False):
+        lib.fvm_mesh_hex.restype = ctypes.c_void_p
+        lib.fvm_mesh_hex.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                     ctypes.c_uint64, ctypes.c_int]
+        lib.fvm_mesh_read_neu.restype = ctypes.c_void_p
+        lib.fvm_mesh_read_neu.argtypes = [ctypes.c_char_p]
+        lib.fvm_mesh_free.argtypes = [ctypes.c_void_p]
+        lib.fvm_mesh_sizes.argtypes = [ctypes.c_void_p, _i32p, _i32p, _i32p, _i32p]
+        lib.fvm_mesh_faces.argtypes = [ctypes.c_void_p, _i32p, _i32p]
+        lib.fvm_mesh_face_geom.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, _f64p]
+        lib.fvm_mesh_cell_geom.argtypes = [ctypes.c_void_p, _f64p, _f64p]
+        lib.fvm_mesh_renumber.restype = ctypes.c_int
+        lib.fvm_mesh_renumber.argtypes = [ctypes.c_void_p, ctypes.c_int, _i32p]
+        lib.fvm_assemble_pressure.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p, _f64p]
+        lib.fvm_assemble_momentum.restype = ctypes.c_double
+        lib.fvm_assemble_momentum.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_double, _f64p, _f64p, _f64p]
+        lib.fvm_uniform.argtypes = [ctypes.c_uint64, ctypes.c_int64, _f64p]
+        lib._typed = True
+    return lib
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+@dataclass
+class FaceMatrix:
+    """The solver's matrix: ng(:)%{ip,in,p,n} and pl (solv_data.f90:14-22)."""
+    n_cell: int
+    ip: np.ndarray  # int32, 1-based
+    inb: np.ndarray  # int32, 1-based, 0 = boundary
+    p: np.ndarray
+    n: np.ndarray
+    pl: np.ndarray
+
+    @property
+    def n_face(self) -> int:
+        return int(self.ip.shape[0])
+
+    def to_scipy(self):
+        """Assemble A as scipy CSR (test / reference use)."""
+        import scipy.sparse as sp
+        m = self.inb > 0
+        a = self.ip[m] - 1
+        b = self.inb[m] - 1
+        rows = np.concatenate([np.arange(self.n_cell), a, b])
+        cols = np.concatenate([np.arange(self.n_cell), b, a])
+        vals = np.concatenate([self.pl, self.p[m], self.n[m]])
+        return sp.csr_matrix((vals, (rows, cols)), shape=(self.n_cell, self.n_cell))
+
+
+class Mesh:
+    RCM = 1
+    SFC = 2
+
+    def __init__(self, handle: int):
+        if not handle:
+            raise RuntimeError("mesh construction failed")
+        self._h = ctypes.c_void_p(handle)
+        self._lib = _lib()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.fvm_mesh_free(h)
+            self._h = ctypes.c_void_p(0)
+
+    @classmethod
+    def hex(cls, nx: int, ny: int | None = None, nz: int | None = None, jitter: float = 0.15,
+            seed: int = 0, permute: bool = True) -> "Mesh":
+        ny = nx if ny is None else ny
+        nz = nx if nz is None else nz
+        return cls(_lib().fvm_mesh_hex(nx, ny, nz, jitter, seed, 1 if permute else 0))
+
+    @classmethod
+    def read_neu(cls, path: str) -> "Mesh":
+        h = _lib().fvm_mesh_read_neu(path.encode())
+        if not h:
+            raise RuntimeError(f"cannot read Gambit neutral file {path}")
+        return cls(h)
+
+    def sizes(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        self._lib.fvm_mesh_sizes(self._h, *[ctypes.byref(x) for x in v])
+        return tuple(x.value for x in v)  # n_cell, n_face, n_bface, n_vert
+
+    @property
+    def n_cell(self) -> int:
+        return self.sizes()[0]
+
+    @property
+    def n_face(self) -> int:
+        return self.sizes()[1]
+
+    def faces(self):
+        F = self.n_face
+        ip = np.empty(F, np.int32)
+        inb = np.empty(F, np.int32)
+        self._lib.fvm_mesh_faces(self._h, _p(ip, _i32p), _p(inb, _i32p))
+        return ip, inb
+
+    def face_geom(self):
+        F = self.n_face
+        s = np.empty(F)
+        nrm = np.empty((F, 3))
+        xf = np.empty((F, 3))
+        l_pn = np.empty(F)
+        w_fp = np.empty(F)
+        self._lib.fvm_mesh_face_geom(self._h, _p(s, _f64p), _p(nrm, _f64p), _p(xf, _f64p),
+                                     _p(l_pn, _f64p), _p(w_fp, _f64p))
+        return s, nrm, xf, l_pn, w_fp
+
+    def cell_geom(self):
+        N = self.n_cell
+        xc = np.empty((N, 3))
+        vol = np.empty(N)
+        self._lib.fvm_mesh_cell_geom(self._h, _p(xc, _f64p), _p(vol, _f64p))
+        return xc, vol
+
+    def renumber(self, method: int) -> np.ndarray:
+        """Renumber cells in place (RCM or SFC); returns new index of old cell (1-based)."""
+        perm = np.empty(self.n_cell, np.int32)
+        rc = self._lib.fvm_mesh_renumber(self._h, method, _p(perm, _i32p))
+        if rc != 0:
+            raise ValueError("renumber failed")
+        return perm
+
+    def permute(self, perm: np.ndarray) -> None:
+        """Apply a given permutation (new 1-based index of old cell i)."""
+        perm = np.ascontiguousarray(perm, np.int32)
+        if self._lib.fvm_mesh_renumber(self._h, 3, _p(perm, _i32p)) != 0:
+            raise ValueError("bad permutation")
+
+    def pressure(self, pin: int = 1) -> FaceMatrix:
+        ip, inb = self.faces()
+        F, N = ip.shape[0], self.n_cell
+        p = np.empty(F)
+        n = np.empty(F)
+        pl = np.empty(N)
+        self._lib.fvm_assemble_pressure(self._h, pin, _p(p, _f64p), _p(n, _f64p), _p(pl, _f64p))
+        return FaceMatrix(N, ip, inb, p, n, pl)
+
+    def momentum(self, gamma: float = 1e-3, pe_max: float = 50.0, cfl: float = 5.0):
+        ip, inb = self.faces()
+        F, N = ip.shape[0], self.n_cell
+        p = np.empty(F)
+        n = np.empty(F)
+        pl = np.empty(N)
+        dt = self._lib.fvm_assemble_momentum(self._h, gamma, pe_max, cfl, _p(p, _f64p),
+                                             _p(n, _f64p), _p(pl, _f64p))
+        return FaceMatrix(N, ip, inb, p, n, pl), dt
+
+
+def uniform(seed: int, count: int) -> np.ndarray:
+    """Uniform [-1, 1) from std::mt19937_64(seed), as the C++ generator draws."""
+    out = np.empty(count)
+    _lib().fvm_uniform(seed, count, _p(out, _f64p))
+    return out
+
+
+def poisson_rhs(n_cell: int, seed: int, pin: int = 1) -> np.ndarray:
+    """uniform[-1,1] with its mean removed; zero at the pinned cell."""
+    b = uniform(seed, n_cell)
+    b -= b.mean()
+    if pin > 0:
+        b[pin - 1] = 0.0
+    return b

@@ -1,0 +1,250 @@
+"""Python mirror of the spray-simulation solver subroutines on the C-ABI of
+``libsolv_gpu.so`` (include/solv_gpu.h).
+
+The reference keeps the matrix in module globals (solv_data.f90:10-22) and
+exposes
+
+    solv_cg(imat, reduc, n_iter, phi, res0, res0_n, not_r0)     solv_cg.f90:7
+    solv_bicg(imat, reduc, n_iter, phi, res0, res0_n, not_r0)   solv_bicg.f90:7
+    solv_res(phi, res0, res0_n, not_r0)                         solv_res.f90:5
+    solv_precond(imat, c, c_r)                                  solv_precond.f90:5
+    solv_direct(imat, c, c_r, x, b)                             solv_direct.f90:5
+
+:class:`GpuSolver` holds one device context with the matrix resident in
+HBM and offers the same calls.  ``phi`` is (n_cell, n_vc) cell-major like
+``phi(ip)%vc``; ``res0`` is (n_cell, n_vc) like Fortran ``res0(ip,ivc)``
+(passed column-major to the library).  Arrays are updated in place, as the
+Fortran ``intent(inout)`` arguments are.  There is no CPU fallback: without
+a GPU or the built library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import load
+
+OK, MAXITER, NAN, BAD_INPUT, DEVICE_ERROR, NO_MATRIX, ZERO_RHS = 0, 1, 3, 4, 5, 7, 8
+MAX_VC = 4
+OPT_PRECISION, OPT_INNER_REDUC, OPT_GRAPH_ITERS, OPT_BLOCK, OPT_GRID_PER_SM, OPT_MAX_REFINE = (
+    1, 2, 3, 4, 5, 6)
+
+_i32p = ctypes.POINTER(ctypes.c_int)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("n_vc", ctypes.c_int), ("iters", ctypes.c_int * MAX_VC),
+                ("ratio", ctypes.c_double * MAX_VC), ("status", ctypes.c_int),
+                ("n_levels", ctypes.c_int), ("refinements", ctypes.c_int),
+                ("graph_launches", ctypes.c_int), ("kernel_launches", ctypes.c_int),
+                ("solve_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        V = self.n_vc
+        return {"iters": list(self.iters[:V]), "ratio": list(self.ratio[:V]),
+                "status": self.status, "n_levels": self.n_levels,
+                "refinements": self.refinements, "graph_launches": self.graph_launches,
+                "kernel_launches": self.kernel_launches, "solve_ms": self.solve_ms}
+
+
+# Exported symbols of include/solv_gpu.h (the tests check them all).
+EXPORTS = [
+    "solv_gpu_create", "solv_gpu_destroy", "solv_gpu_set_stream", "solv_gpu_set_option",
+    "solv_gpu_status_string", "solv_gpu_last_error", "solv_gpu_matrix_set",
+    "solv_gpu_matrix_values", "solv_gpu_matrix_values_dev", "solv_gpu_matrix_levels",
+    "solv_gpu_res", "solv_gpu_precond", "solv_gpu_direct", "solv_gpu_spmv", "solv_gpu_cg",
+    "solv_gpu_bicg", "solv_gpu_cg_dev", "solv_gpu_bicg_dev", "solv_gpu_spmv_dev",
+    "solv_gpu_create_", "solv_gpu_destroy_", "solv_gpu_matrix_set_", "solv_gpu_matrix_values_",
+    "solv_gpu_res_", "solv_gpu_precond_", "solv_gpu_direct_", "solv_gpu_cg_", "solv_gpu_bicg_",
+]
+
+
+def lib():
+    L = load("libsolv_gpu.so")
+    if getattr(L, "_typed", False):
+        return L
+    vp = ctypes.c_void_p
+    L.solv_gpu_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int]
+    L.solv_gpu_destroy.argtypes = [vp]
+    L.solv_gpu_set_stream.argtypes = [vp, vp]
+    L.solv_gpu_set_option.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.solv_gpu_status_string.restype = ctypes.c_char_p
+    L.solv_gpu_status_string.argtypes = [ctypes.c_int]
+    L.solv_gpu_last_error.restype = ctypes.c_char_p
+    L.solv_gpu_last_error.argtypes = [vp]
+    L.solv_gpu_matrix_set.argtypes = [vp, ctypes.c_int, ctypes.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
+    L.solv_gpu_matrix_values.argtypes = [vp, _f64p, _f64p, _f64p]
+    L.solv_gpu_matrix_values_dev.argtypes = [vp, vp, vp, vp]
+    L.solv_gpu_matrix_levels.argtypes = [vp]
+    L.solv_gpu_res.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, ctypes.c_int]
+    L.solv_gpu_precond.argtypes = [vp, ctypes.c_int, _f64p, _f64p]
+    L.solv_gpu_direct.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p]
+    L.solv_gpu_spmv.argtypes = [vp, _f64p, _f64p]
+    for fn in (L.solv_gpu_cg, L.solv_gpu_bicg):
+        fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _f64p,
+                       _f64p, _f64p, ctypes.c_int, ctypes.POINTER(Stats)]
+    for fn in (L.solv_gpu_cg_dev, L.solv_gpu_bicg_dev):
+        fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, vp, vp,
+                       _f64p, ctypes.c_int, ctypes.POINTER(Stats)]
+    L.solv_gpu_spmv_dev.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L._typed = True
+    return L
+
+
+class SolverError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"status {code}: {msg}")
+        self.code = code
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+class GpuSolver:
+    """One device context: the matrix of solv_data.f90 resident in HBM."""
+
+    def __init__(self, device: int = 0):
+        self._lib = lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.solv_gpu_create(ctypes.byref(h), device)
+        if rc != OK:
+            raise SolverError(rc, "solv_gpu_create failed (no CUDA device?)")
+        self._h = h
+        self.n_cell = 0
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.solv_gpu_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, allow=(OK,)):
+        if rc not in allow:
+            msg = self._lib.solv_gpu_last_error(self._h).decode()
+            raise SolverError(rc, msg or self._lib.solv_gpu_status_string(rc).decode())
+        return rc
+
+    # -- configuration -------------------------------------------------------
+    def set_option(self, key: int, value: float):
+        self._check(self._lib.solv_gpu_set_option(self._h, key, float(value)))
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self._lib.solv_gpu_set_stream(self._h, stream_handle or None))
+
+    # -- matrix (grd_solv + coefficient fill) ----------------------------------
+    def matrix_set(self, m) -> None:
+        """m: programs_b200.mesh.FaceMatrix (or anything with n_cell, ip, inb, p, n, pl)."""
+        self._keep = [np.ascontiguousarray(m.ip, np.int32), np.ascontiguousarray(m.inb, np.int32),
+                      np.ascontiguousarray(m.p, np.float64), np.ascontiguousarray(m.n, np.float64),
+                      np.ascontiguousarray(m.pl, np.float64)]
+        ip, inb, p, n, pl = self._keep
+        self._check(self._lib.solv_gpu_matrix_set(self._h, int(m.n_cell), ip.shape[0],
+                                                  _p(ip, _i32p), _p(inb, _i32p), _p(p, _f64p),
+                                                  _p(n, _f64p), _p(pl, _f64p)))
+        self.n_cell = int(m.n_cell)
+        self._keep = None
+
+    def matrix_values(self, p, n, pl) -> None:
+        p = np.ascontiguousarray(p, np.float64)
+        n = np.ascontiguousarray(n, np.float64)
+        pl = np.ascontiguousarray(pl, np.float64)
+        self._check(self._lib.solv_gpu_matrix_values(self._h, _p(p, _f64p), _p(n, _f64p),
+                                                     _p(pl, _f64p)))
+
+    def matrix_values_dev(self, p_ptr: int, n_ptr: int, pl_ptr: int) -> None:
+        self._check(self._lib.solv_gpu_matrix_values_dev(self._h, p_ptr, n_ptr, pl_ptr))
+
+    @property
+    def levels(self) -> int:
+        return int(self._lib.solv_gpu_matrix_levels(self._h))
+
+    # -- the hot path ----------------------------------------------------------
+    @staticmethod
+    def _as_phi(phi):
+        if not (isinstance(phi, np.ndarray) and phi.dtype == np.float64 and phi.flags.c_contiguous):
+            raise TypeError("phi must be a C-contiguous float64 array (n_cell, n_vc)")
+        return phi.reshape(phi.shape[0], -1)
+
+    @staticmethod
+    def _as_res0(res0):
+        if not (isinstance(res0, np.ndarray) and res0.dtype == np.float64):
+            raise TypeError("res0 must be a float64 array (n_cell, n_vc)")
+        if res0.ndim == 2 and not res0.flags.f_contiguous:
+            raise TypeError("res0 must be Fortran-ordered like res0(ip,ivc)")
+        return res0
+
+    def solv_res(self, phi, res0, res0_n, not_r0=False):
+        phi2 = self._as_phi(phi)
+        V = phi2.shape[1]
+        self._as_res0(res0)
+        self._check(self._lib.solv_gpu_res(self._h, V, _p(phi2, _f64p), _p(res0, _f64p),
+                                           _p(res0_n, _f64p), int(bool(not_r0))))
+
+    def solv_precond(self, imat, c, c_r):
+        self._check(self._lib.solv_gpu_precond(self._h, imat, _p(c, _f64p), _p(c_r, _f64p)))
+
+    def solv_direct(self, imat, c, c_r, x, b):
+        c = np.ascontiguousarray(c, np.float64)
+        c_r = np.ascontiguousarray(c_r, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        self._check(self._lib.solv_gpu_direct(self._h, imat, _p(c, _f64p), _p(c_r, _f64p),
+                                              _p(x, _f64p), _p(b, _f64p)))
+
+    def spmv(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty_like(x)
+        self._check(self._lib.solv_gpu_spmv(self._h, _p(x, _f64p), _p(y, _f64p)))
+        return y
+
+    def _solve(self, fn, imat, reduc, n_iter, phi, res0, res0_n, not_r0):
+        phi2 = self._as_phi(phi)
+        V = phi2.shape[1]
+        self._as_res0(res0)
+        st = Stats()
+        rc = fn(self._h, imat, float(reduc), int(n_iter), V, _p(phi2, _f64p), _p(res0, _f64p),
+                _p(res0_n, _f64p), int(bool(not_r0)), ctypes.byref(st))
+        self._check(rc, allow=(OK, MAXITER))
+        return st.as_dict()
+
+    def solv_cg(self, imat, reduc, n_iter, phi, res0, res0_n, not_r0=False):
+        """solv_cg.f90:7 -- updates phi, res0 (-> initial residual), res0_n in place."""
+        return self._solve(self._lib.solv_gpu_cg, imat, reduc, n_iter, phi, res0, res0_n, not_r0)
+
+    def solv_bicg(self, imat, reduc, n_iter, phi, res0, res0_n, not_r0=False):
+        """solv_bicg.f90:7 -- same arguments as solv_cg."""
+        return self._solve(self._lib.solv_gpu_bicg, imat, reduc, n_iter, phi, res0, res0_n, not_r0)
+
+    # -- device-resident forms (torch CUDA tensors or raw device pointers) ----
+    def _solve_dev(self, fn, imat, reduc, n_iter, n_vc, phi_ptr, res0_ptr, not_r0):
+        res0_n = np.zeros(n_vc)
+        st = Stats()
+        rc = fn(self._h, imat, float(reduc), int(n_iter), n_vc, phi_ptr, res0_ptr,
+                _p(res0_n, _f64p), int(bool(not_r0)), ctypes.byref(st))
+        self._check(rc, allow=(OK, MAXITER))
+        return res0_n, st.as_dict()
+
+    def solv_cg_dev(self, imat, reduc, n_iter, n_vc, phi_ptr, res0_ptr, not_r0=False):
+        return self._solve_dev(self._lib.solv_gpu_cg_dev, imat, reduc, n_iter, n_vc, phi_ptr,
+                               res0_ptr, not_r0)
+
+    def solv_bicg_dev(self, imat, reduc, n_iter, n_vc, phi_ptr, res0_ptr, not_r0=False):
+        return self._solve_dev(self._lib.solv_gpu_bicg_dev, imat, reduc, n_iter, n_vc, phi_ptr,
+                               res0_ptr, not_r0)
+
+    def spmv_dev(self, x_ptr: int, y_ptr: int, repeat: int = 1) -> float:
+        ms = ctypes.c_float()
+        self._check(self._lib.solv_gpu_spmv_dev(self._h, x_ptr, y_ptr, repeat, ctypes.byref(ms)))
+        return ms.value
+
+
+def new_res0(n_cell: int, n_vc: int) -> np.ndarray:
+    """A Fortran-ordered res0(n_cell, n_vc) array."""
+    return np.zeros((n_cell, n_vc), order="F")
