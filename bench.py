@@ -39,7 +39,7 @@ sys.path.insert(0, ROOT)
 # reduc 1e-10), recorded from the GPU solver; the oracle matches the GPU
 # count to +-2 iterations (tests/test_gpu_parity.py).  Used only by the
 # reference arm, which cannot afford to run the ~20-minute CPU solve.
-FULL_ITERS = {(256, "pcg", 0): None}
+FULL_ITERS = {(256, "pcg", 0): 2616, (64, "pcg", 0): 715}
 
 PEAK_FALLBACK_GBS = 6650.0
 

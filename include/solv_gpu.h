@@ -137,6 +137,39 @@ int solv_gpu_bicg_dev(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
 int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
                       int repeat, float *ms_per_call);
 
+/* -- batches of independent systems ----------------------------------- */
+/* No counterpart call in the reference, which solves one system per call
+ * (solv_cg.f90:26 loops over the n_vc components of one matrix); a batch
+ * is n_sys such calls done together.  The systems are concatenated:
+ * system k owns cells cell_ptr[k]+1 .. cell_ptr[k+1] (1-based in ip/in),
+ * cell_ptr[0] = 0, and no face may couple two systems.  Each system and
+ * component iterates and stops on its own (own Krylov scalars, own
+ * res0_n, own stopping test), exactly as n_sys separate solv_cg calls. */
+int solv_gpu_matrix_set_batch(solv_gpu_ctx *ctx, int n_sys, const int *cell_ptr,
+                              int n_face, const int *ip, const int *in,
+                              const double *p, const double *n,
+                              const double *pl);
+int solv_gpu_n_systems(const solv_gpu_ctx *ctx);
+/* phi: cell-major over all cells; res0: column-major over all cells
+ * (res0[ivc*n_cell_total + i]); res0_n, iters, ratio: [k*n_vc + ivc]
+ * (iters / ratio may be NULL). */
+int solv_gpu_cg_batch(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
+                      int n_vc, double *phi, double *res0, double *res0_n,
+                      int not_r0, int *iters, double *ratio,
+                      solv_gpu_stats *stats);
+int solv_gpu_bicg_batch(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
+                        int n_vc, double *phi, double *res0, double *res0_n,
+                        int not_r0, int *iters, double *ratio,
+                        solv_gpu_stats *stats);
+int solv_gpu_cg_batch_dev(solv_gpu_ctx *ctx, int imat, double reduc,
+                          int n_iter, int n_vc, double *phi_dev,
+                          double *res0_dev, double *res0_n, int not_r0,
+                          int *iters, double *ratio, solv_gpu_stats *stats);
+int solv_gpu_bicg_batch_dev(solv_gpu_ctx *ctx, int imat, double reduc,
+                            int n_iter, int n_vc, double *phi_dev,
+                            double *res0_dev, double *res0_n, int not_r0,
+                            int *iters, double *ratio, solv_gpu_stats *stats);
+
 /* -- Fortran bindings (gfortran mangling, everything by reference) ------ */
 /* ctx is passed as an integer(c_intptr_t) holding the context address.
  * status receives the return code.  Mirrors parms_solv_ in

@@ -254,7 +254,7 @@ __global__ void k_convert(long long n, const Tsrc* __restrict__ a, Tdst* __restr
 template <int V>
 __global__ void k_res(Rows<double> R, SegMap sm, const double* __restrict__ phi,
                       double* __restrict__ r, int not_r0, double* __restrict__ part,
-                      Lane* __restrict__ lanes) {
+                      double* __restrict__ l1_out) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
   const int stride = sm.seg_nblk[s] * blockDim.x;
@@ -289,19 +289,62 @@ __global__ void k_res(Rows<double> R, SegMap sm, const double* __restrict__ phi,
   double tot[V];
   if (seg_commit<V>(sm, b, s, part, l1, tot) && threadIdx.x == 0) {
 #pragma unroll
-    for (int v = 0; v < V; ++v) lanes[s * V + v].res0_n = tot[v];
+    for (int v = 0; v < V; ++v) l1_out[s * V + v] = tot[v];
+  }
+}
+
+__global__ void k_set_res0n(Lane* lanes, int nl, const double* __restrict__ l1) {
+  for (int l = threadIdx.x; l < nl; l += blockDim.x) lanes[l].res0_n = l1[l];
+}
+
+// ---- mixed precision: FP32 inner solve inside FP64 refinement --------------
+// inner right-hand side r_f = (float) r, shadow r0_f = r_f, correction d = 0
+template <int V>
+__global__ void k_mp_start(long long nv, const double* __restrict__ r, float* __restrict__ rf,
+                           float* __restrict__ r0f, float* __restrict__ d) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nv;
+       e += (long long)gridDim.x * blockDim.x) {
+    const float t = (float)r[e];
+    rf[e] = t;
+    r0f[e] = t;
+    d[e] = 0.0f;
+  }
+}
+__global__ void k_add(long long n, double* __restrict__ x, const double* __restrict__ y) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    x[e] += y[e];
+}
+// phi += (double) d for the (system, component) lanes flagged in mask
+// (FP64 solution accumulation)
+template <int V>
+__global__ void k_mp_accum(SegMap sm, const int* __restrict__ mask, double* __restrict__ phi,
+                           const float* __restrict__ d) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool on[V];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) { on[v] = mask[s * V + v] != 0; any |= on[v]; }
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      if (on[v]) phi[(size_t)i * V + v] += (double)d[(size_t)i * V + v];
   }
 }
 
 // ---- preconditioner: solv_precond.f90:10-29, one wavefront level -----------
 // c_i = pl_i - sum_{j<i} (n*n) c_j   (DIC)   or  - (p*c_j)*n  (DILU);
 // c_r = c; c = 1/(c + small).  face p/n looked up through slot_src.
-__global__ void k_precond_level(int i0, int i1, int imat, Rows<double> R,
-                                const int* __restrict__ slot_src,
+__global__ void k_precond_level(int i0, int i1, const int* __restrict__ cells, int imat,
+                                Rows<double> R, const int* __restrict__ slot_src,
                                 const double* __restrict__ fp, const double* __restrict__ fn,
                                 double* __restrict__ c, double* __restrict__ c_r) {
-  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1) return;
+  const int t = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= i1) return;
+  const int i = cells ? cells[t] : t;
   RowIt<double> it(R, i);
   double d = R.diag[i];
   if (imat > 0) {
@@ -327,11 +370,12 @@ __global__ void k_precond_level(int i0, int i1, int imat, Rows<double> R,
 // ---- sweeps: solv_direct.f90:11-38, one wavefront level --------------------
 // forward: x_i = (b_i - sum_{j<i} n x_j) * c_i
 template <typename T, int V>
-__global__ void k_fwd_level(int i0, int i1, Rows<T> R, const T* __restrict__ c,
-                            const T* __restrict__ bvec, T* __restrict__ x,
-                            const int* __restrict__ n_active) {
-  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1 || (n_active && *n_active == 0)) return;
+__global__ void k_fwd_level(int i0, int i1, const int* __restrict__ cells, Rows<T> R,
+                            const T* __restrict__ c, const T* __restrict__ bvec,
+                            T* __restrict__ x, const int* __restrict__ n_active) {
+  const int t = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= i1 || (n_active && *n_active == 0)) return;
+  const int i = cells ? cells[t] : t;
   RowIt<T> it(R, i);
   T acc[V];
 #pragma unroll
@@ -352,11 +396,12 @@ __global__ void k_fwd_level(int i0, int i1, Rows<T> R, const T* __restrict__ c,
 // backward, with the x = x*c_r scaling of :26 fused in:
 // x_i = (x_i c_r_i - sum_{j>i} p x_j) * c_i
 template <typename T, int V>
-__global__ void k_bwd_level(int i0, int i1, Rows<T> R, const T* __restrict__ c,
-                            const T* __restrict__ c_r, T* __restrict__ x,
-                            const int* __restrict__ n_active) {
-  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1 || (n_active && *n_active == 0)) return;
+__global__ void k_bwd_level(int i0, int i1, const int* __restrict__ cells, Rows<T> R,
+                            const T* __restrict__ c, const T* __restrict__ c_r,
+                            T* __restrict__ x, const int* __restrict__ n_active) {
+  const int t = i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= i1 || (n_active && *n_active == 0)) return;
+  const int i = cells ? cells[t] : t;
   RowIt<T> it(R, i);
   const T cr = c_r[i];
   T acc[V];
@@ -401,7 +446,6 @@ __global__ void k_spmv(int n, Rows<T> R, const T* __restrict__ x, T* __restrict_
 // Lane init for CG: s = large, iter = 0, active = 1.
 __global__ void k_lane_init(Lane* lanes, int nl, int n_iter, double reduc, int* n_active) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
-  if (l == 0) *n_active = nl;
   if (l >= nl) return;
   Lane L;
   L.s = kLarge; L.beta = 0.0; L.alpha = 1.0; L.pq = 0.0;   // solv_cg.f90:29
@@ -409,7 +453,7 @@ __global__ void k_lane_init(Lane* lanes, int nl, int n_iter, double reduc, int* 
   L.res0_n = lanes[l].res0_n;
   L.ratio = 0.0; L.reduc = reduc; L.l1 = 0.0;
   L.iter = 0; L.n_iter = n_iter; L.active = 1; L.status = kLaneRunning;
-  if (n_iter <= 0) { L.active = 0; L.status = kLaneMaxIter; atomicSub(n_active, 1); }
+  if (n_iter <= 0) { L.active = 0; L.status = kLaneMaxIter; }  // n_active set by the host
   lanes[l] = L;
 }
 

@@ -72,7 +72,11 @@ struct solv_gpu_ctx {
   bool has_matrix = false;
   int N = 0, F = 0;
   bool orient_std = true;
-  std::vector<int> lvl_ptr;  // wavefront level ranges in internal order
+  int n_seg = 1;             // independent systems (block-diagonal batch)
+  std::vector<int> lvl_ptr;  // level l = lvl_cells[lvl_ptr[l] .. lvl_ptr[l+1])
+  bool lvl_contig = true;    // single system: level l is the internal range itself
+  DevBuf lvl_cells;          // internal cell ids by (level, system, caller index)
+  std::vector<int> seg_c0_caller, seg_c1_caller;  // system ranges in internal order
   long long n_slots = 0;
   int n_slice = 0;
   DevBuf old_of_new, slice_ptr, slice_w, col, slot_src, val, sval, diag, fp, fn;
@@ -82,7 +86,7 @@ struct solv_gpu_ctx {
   // segment map (single system: one segment)
   SegHost seg;
   DevBuf d_seg;  // packed ints
-  DevBuf ticket, n_active, lanes, part;
+  DevBuf ticket, n_active, lanes, part, l1, mp_mask;
   int* h_n_active = nullptr;  // pinned
 
   // workspace
@@ -169,6 +173,7 @@ int build_segments(solv_gpu_ctx* c, const std::vector<int>& seg_c0,
   CUDA_TRY(c, c->ticket.ensure(ns * sizeof(unsigned)));
   CUDA_TRY(c, cudaMemsetAsync(c->ticket.p, 0, ns * sizeof(unsigned), c->stream));
   CUDA_TRY(c, c->lanes.ensure((size_t)ns * kMaxV * sizeof(Lane)));
+  CUDA_TRY(c, c->l1.ensure((size_t)ns * kMaxV * sizeof(double)));
   CUDA_TRY(c, c->part.ensure((size_t)s.total_blk * 2 * kMaxV * sizeof(double)));
   CUDA_TRY(c, c->n_active.ensure(sizeof(int)));
   drop_graphs(c);
@@ -200,9 +205,20 @@ int grid_for(solv_gpu_ctx* c, long long n) {
 }
 
 // ---- matrix structure --------------------------------------------------------
-int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in) {
-  if (N <= 0 || F < 0 || !ip || !in)
+int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in, int nsys,
+                     const int* cell_ptr) {
+  if (N <= 0 || F < 0 || !ip || !in || nsys < 1)
     return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set: bad sizes or null pointers");
+  std::vector<int> seg_of(N, 0);
+  if (nsys > 1) {
+    if (!cell_ptr || cell_ptr[0] != 0 || cell_ptr[nsys] != N)
+      return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set_batch: cell_ptr must run 0..n_cell");
+    for (int k = 0; k < nsys; ++k) {
+      if (cell_ptr[k + 1] <= cell_ptr[k])
+        return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set_batch: empty or unordered system");
+      for (int i = cell_ptr[k]; i < cell_ptr[k + 1]; ++i) seg_of[i] = k;
+    }
+  }
   // validate + per-cell interior degree
   std::vector<int> deg(N, 0);
   bool orient = true;
@@ -213,6 +229,9 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
                      "matrix_set: face " + std::to_string(f + 1) + " has ip=" +
                          std::to_string(a) + " in=" + std::to_string(b));
     if (b > 0) {
+      if (seg_of[a - 1] != seg_of[b - 1])
+        return set_err(c, SOLV_GPU_BAD_INPUT,
+                       "matrix_set_batch: face " + std::to_string(f + 1) + " couples two systems");
       deg[a - 1]++;
       deg[b - 1]++;
       if (b < a) orient = false;
@@ -241,19 +260,38 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
     lev[i] = l;
     nl = std::max(nl, l + 1);
   }
-  // internal order: level-major, caller order inside a level
-  std::vector<int> cnt(nl + 1, 0);
-  for (int i = 0; i < N; ++i) cnt[lev[i] + 1]++;
-  for (int l = 0; l < nl; ++l) cnt[l + 1] += cnt[l];
-  c->lvl_ptr.assign(cnt.begin(), cnt.end());
+  // internal order: system-major, then level, then caller order, so each
+  // system is one contiguous range (reductions) and, for one system, each
+  // level is one contiguous range (sweeps)
   std::vector<int> old_of_new(N), new_of_old(N);
+  std::vector<int> seg_c0(nsys), seg_c1(nsys);
   {
+    std::vector<long long> key(N);
+    std::vector<int> cnt((size_t)nsys * nl + 1, 0);
+    for (int i = 0; i < N; ++i) cnt[(size_t)seg_of[i] * nl + lev[i] + 1]++;
+    for (size_t k = 0; k + 1 < cnt.size(); ++k) cnt[k + 1] += cnt[k];
     std::vector<int> pos(cnt.begin(), cnt.end() - 1);
     for (int i = 0; i < N; ++i) {
-      int k = pos[lev[i]]++;
+      int k = pos[(size_t)seg_of[i] * nl + lev[i]]++;
       old_of_new[k] = i;
       new_of_old[i] = k;
     }
+    for (int k = 0; k < nsys; ++k) {
+      seg_c0[k] = cnt[(size_t)k * nl];
+      seg_c1[k] = cnt[(size_t)(k + 1) * nl];
+    }
+  }
+  // level lists (only needed when a level spans several systems)
+  std::vector<int> lcnt(nl + 1, 0);
+  for (int i = 0; i < N; ++i) lcnt[lev[i] + 1]++;
+  for (int l = 0; l < nl; ++l) lcnt[l + 1] += lcnt[l];
+  c->lvl_ptr.assign(lcnt.begin(), lcnt.end());
+  c->lvl_contig = nsys == 1;
+  std::vector<int> lcells;
+  if (!c->lvl_contig) {
+    lcells.resize(N);
+    std::vector<int> pos(lcnt.begin(), lcnt.end() - 1);
+    for (int k = 0; k < N; ++k) lcells[pos[lev[old_of_new[k]]]++] = k;  // (level, system, index)
   }
   // sliced ELL, 32 cells per slice
   const int ns = (N + 31) / 32;
@@ -290,6 +328,7 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
   drop_graphs(c);
   c->N = N;
   c->F = F;
+  c->n_seg = nsys;
   c->orient_std = orient;
   c->n_slots = total;
   c->n_slice = ns;
@@ -310,8 +349,14 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
   CUDA_TRY(c, cudaMemcpyAsync(c->slice_w.p, sw.data(), ns, cudaMemcpyHostToDevice, st));
   CUDA_TRY(c, cudaMemcpyAsync(c->col.p, hcol.data(), total * sizeof(int), cudaMemcpyHostToDevice, st));
   CUDA_TRY(c, cudaMemcpyAsync(c->slot_src.p, hsrc.data(), total * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (!c->lvl_contig) {
+    CUDA_TRY(c, c->lvl_cells.ensure(N * sizeof(int)));
+    CUDA_TRY(c, cudaMemcpyAsync(c->lvl_cells.p, lcells.data(), N * sizeof(int), cudaMemcpyHostToDevice, st));
+  }
   CUDA_TRY(c, cudaStreamSynchronize(st));  // host vectors die here
-  int rc = build_segments(c, {0}, {N});
+  c->seg_c0_caller.assign(seg_c0.begin(), seg_c0.end());
+  c->seg_c1_caller.assign(seg_c1.begin(), seg_c1.end());
+  int rc = build_segments(c, seg_c0, seg_c1);
   if (rc) return rc;
   c->has_matrix = true;
   return SOLV_GPU_OK;
@@ -357,7 +402,7 @@ int ensure_f32_matrix(solv_gpu_ctx* c) {
 template <int V>
 void launch_res(solv_gpu_ctx* c, const double* phi, double* r, int not_r0) {
   sg::k_res<V><<<c->seg.total_blk, c->block, 0, c->stream>>>(
-      rows<double>(c), segmap(c), phi, r, not_r0, c->part.as<double>(), c->lanes.as<Lane>());
+      rows<double>(c), segmap(c), phi, r, not_r0, c->part.as<double>(), c->l1.as<double>());
   c->launches++;
 }
 
@@ -377,16 +422,17 @@ int run_res(solv_gpu_ctx* c, int V, const double* phi, double* r, int not_r0) {
 void launch_precond(solv_gpu_ctx* c, int imat, double* cc, double* cr) {
   if (imat <= 0) {
     sg::k_precond_level<<<(c->N + c->block - 1) / c->block, c->block, 0, c->stream>>>(
-        0, c->N, 0, rows<double>(c), c->slot_src.as<int>(), c->fp.as<double>(),
+        0, c->N, nullptr, 0, rows<double>(c), c->slot_src.as<int>(), c->fp.as<double>(),
         c->fn.as<double>(), cc, cr);
     c->launches++;
     return;
   }
   const int nl = (int)c->lvl_ptr.size() - 1;
+  const int* cells = c->lvl_contig ? nullptr : c->lvl_cells.as<int>();
   for (int l = 0; l < nl; ++l) {
     int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
     sg::k_precond_level<<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
-        i0, i1, imat, rows<double>(c), c->slot_src.as<int>(), c->fp.as<double>(),
+        i0, i1, cells, imat, rows<double>(c), c->slot_src.as<int>(), c->fp.as<double>(),
         c->fn.as<double>(), cc, cr);
     c->launches++;
   }
@@ -402,16 +448,17 @@ void launch_direct(solv_gpu_ctx* c, int imat, const T* cc, const T* cr, T* x, co
     return;
   }
   const int nl = (int)c->lvl_ptr.size() - 1;
+  const int* cells = c->lvl_contig ? nullptr : c->lvl_cells.as<int>();
   Rows<T> R = rows<T>(c);
   for (int l = 0; l < nl; ++l) {
     int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
     sg::k_fwd_level<T, V><<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
-        i0, i1, R, cc, b, x, n_active);
+        i0, i1, cells, R, cc, b, x, n_active);
   }
   for (int l = nl - 1; l >= 0; --l) {
     int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
     sg::k_bwd_level<T, V><<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
-        i0, i1, R, cc, cr, x, n_active);
+        i0, i1, cells, R, cc, cr, x, n_active);
   }
   c->launches += 2 * nl;
 }
@@ -555,17 +602,12 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
   return SOLV_GPU_OK;
 }
 
-__global__ void k_set_res0n(Lane* lanes, int nl, const double* r0n) {
-  int l = threadIdx.x;
-  if (l < nl) lanes[l].res0_n = r0n[l];
-}
-
 // Full FP64 solve (solver 0 = CG, 1 = BiCGSTAB) on device buffers in the
 // caller layouts.
 template <int V>
 int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
                double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
-               solv_gpu_stats* st) {
+               solv_gpu_stats* st, int* out_iters, double* out_ratio) {
   WS<double> w;
   int rc = ensure_ws<double>(c, V, w);
   if (rc) return rc;
@@ -575,22 +617,23 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   sg::k_phi_in<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, phi_dev, w.phi);
   sg::k_col_in<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, res0_dev, w.r0);
   c->launches += 2;
+  const int nl = c->n_seg * V;
   rc = run_res(c, V, w.phi, w.r0, not_r0);  // solv_res: r0 = b - A phi, res0_n
   if (rc) return rc;
+  sg::k_set_res0n<<<1, 256, 0, s>>>(c->lanes.as<Lane>(), nl, c->l1.as<double>());
   // res0 out = initial residual (solv_cg.f90:20)
   sg::k_col_out<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.r0, res0_dev);
   c->launches++;
-  Lane hl[kMaxV];
-  CUDA_TRY(c, cudaMemcpyAsync(hl, c->lanes.p, V * sizeof(Lane), cudaMemcpyDeviceToHost, s));
+  std::vector<Lane> hl(nl);
+  CUDA_TRY(c, cudaMemcpyAsync(res0_n, c->l1.p, nl * sizeof(double), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(c, cudaStreamSynchronize(s));
   double mx = -HUGE_VAL;
-  for (int v = 0; v < V; ++v) {
-    res0_n[v] = hl[v].res0_n;
-    mx = std::max(mx, res0_n[v]);
-  }
+  for (int l = 0; l < nl; ++l) mx = std::max(mx, res0_n[l]);
   if (st) st->n_vc = V;
   if (mx < sg::kSmall) {  // solv_cg.f90:21 early return
     if (st) st->status = SOLV_GPU_ZERO_RHS;
+    if (out_iters) std::fill(out_iters, out_iters + nl, 0);
+    if (out_ratio) std::fill(out_ratio, out_ratio + nl, 0.0);
     return SOLV_GPU_OK;
   }
   launch_precond(c, imat, w.c, w.cr);  // solv_precond
@@ -599,7 +642,13 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   CUDA_TRY(c, cudaMemsetAsync(w.q, 0, (size_t)N * V * sizeof(double), s));
   CUDA_TRY(c, cudaMemsetAsync(w.v, 0, (size_t)N * V * sizeof(double), s));
   CUDA_TRY(c, cudaMemsetAsync(w.z, 0, (size_t)N * V * sizeof(double), s));
-  sg::k_lane_init<<<1, 32, 0, s>>>(c->lanes.as<Lane>(), V, n_iter, reduc, c->n_active.as<int>());
+  {
+    int na = nl;
+    if (n_iter <= 0) na = 0;
+    CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  sg::k_lane_init<<<(nl + 255) / 256, 256, 0, s>>>(c->lanes.as<Lane>(), nl, n_iter, reduc,
+                                                   c->n_active.as<int>());
   SegMap sm = segmap(c);
   if (solver == 0) {
     if (imat <= 0) {
@@ -619,15 +668,17 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   if (rc) return rc;
   sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.phi, phi_dev);
   c->launches++;
-  CUDA_TRY(c, cudaMemcpyAsync(hl, c->lanes.p, V * sizeof(Lane), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->lanes.p, nl * sizeof(Lane), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(c, cudaStreamSynchronize(s));
   int status = SOLV_GPU_OK;
-  for (int v = 0; v < V; ++v) {
-    if (hl[v].status == sg::kLaneNaN) status = SOLV_GPU_NAN;
-    else if (hl[v].status != sg::kLaneConverged && status == SOLV_GPU_OK) status = SOLV_GPU_MAXITER;
+  for (int l = 0; l < nl; ++l) {
+    if (hl[l].status == sg::kLaneNaN) status = SOLV_GPU_NAN;
+    else if (hl[l].status != sg::kLaneConverged && status == SOLV_GPU_OK) status = SOLV_GPU_MAXITER;
+    if (out_iters) out_iters[l] = hl[l].iter;
+    if (out_ratio) out_ratio[l] = hl[l].ratio;
   }
   if (st) {
-    for (int v = 0; v < V; ++v) {
+    for (int v = 0; v < V && v < nl; ++v) {
       st->iters[v] = hl[v].iter;
       st->ratio[v] = hl[v].ratio;
     }
@@ -637,9 +688,187 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   return status;
 }
 
+// Mixed precision: FP32 inner Krylov solves of A d = r inside an FP64
+// iterative-refinement loop.  FP64 stays on the device for the outer
+// residual r = b - A x (k_res, bit-exact with the oracle's solv_res), the
+// inner products (every reduction accumulates in FP64) and the solution
+// accumulation x += d.  The stopping rule is the reference's, applied to
+// the true FP64 residual: |b - A x|_1 / |r0|_1 < reduc.
+template <int V>
+int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
+                double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
+                solv_gpu_stats* st, int* out_iters, double* out_ratio) {
+  WS<double> w;
+  WS<float> f;
+  int rc = ensure_ws<double>(c, V, w);
+  if (rc) return rc;
+  if ((rc = ensure_ws<float>(c, V, f))) return rc;
+  {
+    void* old = c->valf.p;
+    if ((rc = ensure_f32_matrix(c))) return rc;
+    if (old != c->valf.p) drop_graphs(c);
+  }
+  const int N = c->N;
+  const int nl = c->n_seg * V;
+  const long long NV = (long long)N * V;
+  cudaStream_t s = c->stream;
+  const int* o2n = c->old_of_new.as<int>();
+  CUDA_TRY(c, c->mp_mask.ensure(nl * sizeof(int)));
+  double* b = w.q;  // the right-hand side, kept for the outer residuals
+  sg::k_phi_in<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, phi_dev, w.phi);
+  sg::k_col_in<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, res0_dev, b);
+  CUDA_TRY(c, cudaMemcpyAsync(w.r0, b, NV * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  c->launches += 2;
+  // not_r0: b is already the residual of the incoming phi, so refine a
+  // correction from zero and add the incoming phi back at the end
+  if (not_r0) {
+    CUDA_TRY(c, cudaMemcpyAsync(w.v, w.phi, NV * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(c, cudaMemsetAsync(w.phi, 0, NV * sizeof(double), s));
+  }
+  if ((rc = run_res(c, V, w.phi, w.r0, not_r0))) return rc;
+  sg::k_col_out<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.r0, res0_dev);
+  c->launches++;
+  std::vector<double> l1(nl);
+  CUDA_TRY(c, cudaMemcpyAsync(l1.data(), c->l1.p, nl * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  double mx = -HUGE_VAL;
+  for (int l = 0; l < nl; ++l) {
+    res0_n[l] = l1[l];
+    mx = std::max(mx, l1[l]);
+  }
+  if (st) st->n_vc = V;
+  if (mx < sg::kSmall) {
+    if (st) st->status = SOLV_GPU_ZERO_RHS;
+    if (out_iters) std::fill(out_iters, out_iters + nl, 0);
+    if (out_ratio) std::fill(out_ratio, out_ratio + nl, 0.0);
+    return SOLV_GPU_OK;
+  }
+  // preconditioner in FP64 (solv_precond), rounded to FP32 for the sweeps
+  launch_precond(c, imat, w.c, w.cr);
+  sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.c, f.c);
+  sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.cr, f.cr);
+  c->launches += 2;
+
+  std::vector<int> iters(nl, 0), status_v(nl), stalls(nl, 0), mask(nl);
+  std::vector<double> ratio(nl), prev(nl);
+  std::vector<char> active(nl);
+  for (int l = 0; l < nl; ++l) {
+    ratio[l] = l1[l] / (res0_n[l] + sg::kSmall);
+    prev[l] = ratio[l];
+    active[l] = !(ratio[l] < reduc) && n_iter > 0;
+    status_v[l] = active[l] ? sg::kLaneRunning : (n_iter > 0 ? sg::kLaneConverged : sg::kLaneMaxIter);
+  }
+  const double* rcur = w.r0;  // current FP64 residual
+  int refinements = 0, gl_total = 0;
+  std::vector<Lane> hl(nl);
+  for (int k = 0; k < c->max_refine; ++k) {
+    int na = 0, cap = 0;
+    for (int l = 0; l < nl; ++l) {
+      Lane L{};
+      L.s = sg::kLarge; L.alpha = 1.0; L.beta0 = 1.0; L.gam = 1.0;
+      L.res0_n = l1[l];
+      // do not over-solve the last sweep: the inner drop needed to reach reduc
+      double need = 0.3 * reduc * (res0_n[l] + sg::kSmall) / (l1[l] + sg::kSmall);
+      L.reduc = std::min(0.5, std::max(c->inner_reduc, need));
+      L.n_iter = n_iter - iters[l];
+      L.active = active[l] && L.n_iter > 0;
+      L.status = sg::kLaneRunning;
+      mask[l] = L.active;
+      if (L.active) { ++na; cap = std::max(cap, L.n_iter); }
+      hl[l] = L;
+    }
+    if (na == 0) break;
+    ++refinements;
+    CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(c, cudaMemcpyAsync(c->mp_mask.p, mask.data(), nl * sizeof(int), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
+    sg::k_mp_start<V><<<grid_for(c, NV), c->block, 0, s>>>(NV, rcur, f.r, f.r0, f.phi);
+    CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
+    CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
+    CUDA_TRY(c, cudaMemsetAsync(f.v, 0, NV * sizeof(float), s));
+    CUDA_TRY(c, cudaMemsetAsync(f.z, 0, NV * sizeof(float), s));
+    SegMap sm = segmap(c);
+    if (solver == 0) {
+      if (imat <= 0) {
+        sg::k_cg_rz<float, V, true><<<c->seg.total_blk, c->block, 0, s>>>(
+            sm, f.c, f.r, f.z, c->part.as<double>(), c->lanes.as<Lane>());
+        c->launches++;
+      }
+    } else {
+      sg::k_bi_rho<float, V><<<c->seg.total_blk, c->block, 0, s>>>(
+          sm, f.r, f.r0, c->part.as<double>(), c->lanes.as<Lane>());
+      c->launches++;
+    }
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    int gl = 0;
+    if ((rc = iterate<float, V>(c, solver, imat, cap, f, gl))) return rc;
+    gl_total += gl;
+    CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->lanes.p, nl * sizeof(Lane), cudaMemcpyDeviceToHost, s));
+    // x += d in FP64, then the true residual r = b - A x in FP64
+    sg::k_mp_accum<V><<<c->seg.total_blk, c->block, 0, s>>>(sm, c->mp_mask.as<int>(), w.phi, f.phi);
+    CUDA_TRY(c, cudaMemcpyAsync(w.r, b, NV * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if ((rc = run_res(c, V, w.phi, w.r, 0))) return rc;
+    c->launches += 2;
+    rcur = w.r;
+    CUDA_TRY(c, cudaMemcpyAsync(l1.data(), c->l1.p, nl * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(c, cudaStreamSynchronize(s));
+    for (int l = 0; l < nl; ++l) {
+      if (!mask[l]) continue;
+      iters[l] += hl[l].iter;
+      ratio[l] = l1[l] / (res0_n[l] + sg::kSmall);
+      if (!(ratio[l] == ratio[l]) || std::isinf(ratio[l]) || hl[l].status == sg::kLaneNaN) {
+        active[l] = false;
+        status_v[l] = sg::kLaneNaN;
+      } else if (ratio[l] < reduc) {
+        active[l] = false;
+        status_v[l] = sg::kLaneConverged;
+      } else if (iters[l] >= n_iter) {
+        active[l] = false;
+        status_v[l] = sg::kLaneMaxIter;
+      } else {
+        // a sweep that does not halve the residual twice running: FP32 has
+        // reached its floor on this system
+        stalls[l] = ratio[l] > 0.5 * prev[l] ? stalls[l] + 1 : 0;
+        if (stalls[l] >= 2) {
+          active[l] = false;
+          status_v[l] = sg::kLaneMaxIter;
+        }
+      }
+      prev[l] = ratio[l];
+    }
+  }
+  for (int l = 0; l < nl; ++l)
+    if (active[l]) status_v[l] = sg::kLaneMaxIter;  // refinement cap
+  if (not_r0) {
+    sg::k_add<<<grid_for(c, NV), c->block, 0, s>>>(NV, w.phi, w.v);
+    c->launches++;
+  }
+  sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.phi, phi_dev);
+  c->launches++;
+  CUDA_TRY(c, cudaGetLastError());
+  int status = SOLV_GPU_OK;
+  for (int l = 0; l < nl; ++l) {
+    if (status_v[l] == sg::kLaneNaN) status = SOLV_GPU_NAN;
+    else if (status_v[l] != sg::kLaneConverged && status == SOLV_GPU_OK) status = SOLV_GPU_MAXITER;
+    if (out_iters) out_iters[l] = iters[l];
+    if (out_ratio) out_ratio[l] = ratio[l];
+  }
+  if (st) {
+    for (int v = 0; v < V && v < nl; ++v) {
+      st->iters[v] = iters[v];
+      st->ratio[v] = ratio[v];
+    }
+    st->status = status;
+    st->refinements = refinements;
+    st->graph_launches += gl_total;
+  }
+  return status;
+}
+
 int solve_dispatch(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int V,
                    double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
-                   solv_gpu_stats* st);
+                   solv_gpu_stats* st, int* out_iters, double* out_ratio);
 
 }  // namespace
 
@@ -726,14 +955,14 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
       int b = (int)value;
       if (b < 64 || b > 1024 || (b & 31)) return set_err(c, SOLV_GPU_BAD_INPUT, "block must be a multiple of 32 in 64..1024");
       c->block = b;
-      if (c->has_matrix) return build_segments(c, {0}, {c->N});
+      if (c->has_matrix) return build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
       return SOLV_GPU_OK;
     }
     case SOLV_OPT_GRID_PER_SM: {
       int g = (int)value;
       if (g < 1 || g > 64) return set_err(c, SOLV_GPU_BAD_INPUT, "grid per SM in 1..64");
       c->grid_per_sm = g;
-      if (c->has_matrix) return build_segments(c, {0}, {c->N});
+      if (c->has_matrix) return build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
       return SOLV_GPU_OK;
     }
     case SOLV_OPT_MAX_REFINE:
@@ -751,7 +980,7 @@ int solv_gpu_matrix_set(solv_gpu_ctx* c, int n_cell, int n_face, const int* ip, 
   if (!p || !n || !pl) return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set: null coefficient pointer");
   CUDA_TRY(c, cudaSetDevice(c->dev));
   c->has_matrix = false;
-  int rc = matrix_structure(c, n_cell, n_face, ip, in);
+  int rc = matrix_structure(c, n_cell, n_face, ip, in, 1, nullptr);
   if (rc) return rc;
   return solv_gpu_matrix_values(c, p, n, pl);
 }
@@ -808,10 +1037,8 @@ int solv_gpu_res(solv_gpu_ctx* c, int n_vc, const double* phi, double* res0, dou
   if (rc) return rc;
   sg::k_col_out<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, c->w_b.as<double>(), c->w_out.as<double>());
   CUDA_TRY(c, cudaMemcpyAsync(res0, c->w_out.p, bytes, cudaMemcpyDeviceToHost, s));
-  Lane hl[kMaxV];
-  CUDA_TRY(c, cudaMemcpyAsync(hl, c->lanes.p, V * sizeof(Lane), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaMemcpyAsync(res0_n, c->l1.p, V * sizeof(double), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(c, cudaStreamSynchronize(s));
-  for (int v = 0; v < V; ++v) res0_n[v] = hl[v].res0_n;
   return SOLV_GPU_OK;
 }
 
@@ -913,12 +1140,15 @@ int solv_gpu_spmv(solv_gpu_ctx* c, const double* x, double* y) {
 
 static int solve_common(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int n_vc,
                         double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
-                        solv_gpu_stats* st) {
+                        solv_gpu_stats* st, int* out_iters = nullptr, double* out_ratio = nullptr,
+                        bool batch = false) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
   if (n_vc < 1 || n_vc > kMaxV) return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
   if (imat < 0 || imat > 2) return set_err(c, SOLV_GPU_BAD_INPUT, "imat must be 0, 1 or 2");
   if (!phi_dev || !res0_dev || !res0_n) return set_err(c, SOLV_GPU_BAD_INPUT, "null pointer");
+  if (c->n_seg > 1 && !batch)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "a batch of systems is set: use the _batch entry points");
   if (st) {
     std::memset(st, 0, sizeof(*st));
     st->n_levels = (int)c->lvl_ptr.size() - 1;
@@ -926,7 +1156,8 @@ static int solve_common(solv_gpu_ctx* c, int solver, int imat, double reduc, int
   CUDA_TRY(c, cudaSetDevice(c->dev));
   c->launches = 0;
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-  int rc = solve_dispatch(c, solver, imat, reduc, n_iter, n_vc, phi_dev, res0_dev, res0_n, not_r0, st);
+  int rc = solve_dispatch(c, solver, imat, reduc, n_iter, n_vc, phi_dev, res0_dev, res0_n, not_r0,
+                          st, out_iters, out_ratio);
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
   CUDA_TRY(c, cudaEventSynchronize(c->ev1));
   if (st) {
@@ -940,7 +1171,8 @@ static int solve_common(solv_gpu_ctx* c, int solver, int imat, double reduc, int
 }
 
 static int solve_host(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int n_vc,
-                      double* phi, double* res0, double* res0_n, int not_r0, solv_gpu_stats* st) {
+                      double* phi, double* res0, double* res0_n, int not_r0, solv_gpu_stats* st,
+                      int* out_iters = nullptr, double* out_ratio = nullptr, bool batch = false) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
   if (n_vc < 1 || n_vc > kMaxV) return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
@@ -952,7 +1184,7 @@ static int solve_host(solv_gpu_ctx* c, int solver, int imat, double reduc, int n
   CUDA_TRY(c, cudaMemcpyAsync(c->w_in.p, phi, bytes, cudaMemcpyHostToDevice, c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(c->w_out.p, res0, bytes, cudaMemcpyHostToDevice, c->stream));
   int rc = solve_common(c, solver, imat, reduc, n_iter, n_vc, c->w_in.as<double>(),
-                        c->w_out.as<double>(), res0_n, not_r0, st);
+                        c->w_out.as<double>(), res0_n, not_r0, st, out_iters, out_ratio, batch);
   if (rc != SOLV_GPU_OK && rc != SOLV_GPU_MAXITER && rc != SOLV_GPU_NAN) return rc;
   CUDA_TRY(c, cudaMemcpyAsync(phi, c->w_in.p, bytes, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaMemcpyAsync(res0, c->w_out.p, bytes, cudaMemcpyDeviceToHost, c->stream));
@@ -975,6 +1207,43 @@ int solv_gpu_cg_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_v
 int solv_gpu_bicg_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc, double* phi,
                       double* res0, double* res0_n, int not_r0, solv_gpu_stats* st) {
   return solve_common(c, 1, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st);
+}
+
+// ---- batches of independent systems ------------------------------------------
+int solv_gpu_matrix_set_batch(solv_gpu_ctx* c, int n_sys, const int* cell_ptr, int n_face,
+                              const int* ip, const int* in, const double* p, const double* n,
+                              const double* pl) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (n_sys < 1 || !cell_ptr || !p || !n || !pl)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "matrix_set_batch: bad arguments");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  c->has_matrix = false;
+  int rc = matrix_structure(c, cell_ptr[n_sys], n_face, ip, in, n_sys, cell_ptr);
+  if (rc) return rc;
+  return solv_gpu_matrix_values(c, p, n, pl);
+}
+
+int solv_gpu_n_systems(const solv_gpu_ctx* c) { return c && c->has_matrix ? c->n_seg : 0; }
+
+int solv_gpu_cg_batch(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc, double* phi,
+                      double* res0, double* res0_n, int not_r0, int* iters, double* ratio,
+                      solv_gpu_stats* st) {
+  return solve_host(c, 0, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st, iters, ratio, true);
+}
+int solv_gpu_bicg_batch(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc, double* phi,
+                        double* res0, double* res0_n, int not_r0, int* iters, double* ratio,
+                        solv_gpu_stats* st) {
+  return solve_host(c, 1, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st, iters, ratio, true);
+}
+int solv_gpu_cg_batch_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc,
+                          double* phi, double* res0, double* res0_n, int not_r0, int* iters,
+                          double* ratio, solv_gpu_stats* st) {
+  return solve_common(c, 0, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st, iters, ratio, true);
+}
+int solv_gpu_bicg_batch_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc,
+                            double* phi, double* res0, double* res0_n, int not_r0, int* iters,
+                            double* ratio, solv_gpu_stats* st) {
+  return solve_common(c, 1, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st, iters, ratio, true);
 }
 
 // ---- Fortran bindings ----------------------------------------------------------
@@ -1037,12 +1306,21 @@ void solv_gpu_bicg_(int64_t* h, int* imat, double* reduc, int* n_iter, int* n_vc
 namespace {
 int solve_dispatch(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int V,
                    double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
-                   solv_gpu_stats* st) {
+                   solv_gpu_stats* st, int* oi, double* orat) {
+  if (c->precision == 1) {
+    switch (V) {
+      case 1: return solve_mixed<1>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+      case 2: return solve_mixed<2>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+      case 3: return solve_mixed<3>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+      case 4: return solve_mixed<4>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+    }
+    return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
+  }
   switch (V) {
-    case 1: return solve_fp64<1>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st);
-    case 2: return solve_fp64<2>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st);
-    case 3: return solve_fp64<3>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st);
-    case 4: return solve_fp64<4>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st);
+    case 1: return solve_fp64<1>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+    case 2: return solve_fp64<2>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+    case 3: return solve_fp64<3>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+    case 4: return solve_fp64<4>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
   }
   return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
 }

@@ -56,6 +56,8 @@ EXPORTS = [
     "solv_gpu_matrix_values", "solv_gpu_matrix_values_dev", "solv_gpu_matrix_levels",
     "solv_gpu_res", "solv_gpu_precond", "solv_gpu_direct", "solv_gpu_spmv", "solv_gpu_cg",
     "solv_gpu_bicg", "solv_gpu_cg_dev", "solv_gpu_bicg_dev", "solv_gpu_spmv_dev",
+    "solv_gpu_matrix_set_batch", "solv_gpu_n_systems", "solv_gpu_cg_batch", "solv_gpu_bicg_batch",
+    "solv_gpu_cg_batch_dev", "solv_gpu_bicg_batch_dev",
     "solv_gpu_create_", "solv_gpu_destroy_", "solv_gpu_matrix_set_", "solv_gpu_matrix_values_",
     "solv_gpu_res_", "solv_gpu_precond_", "solv_gpu_direct_", "solv_gpu_cg_", "solv_gpu_bicg_",
 ]
@@ -89,6 +91,15 @@ def lib():
         fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, vp, vp,
                        _f64p, ctypes.c_int, ctypes.POINTER(Stats)]
     L.solv_gpu_spmv_dev.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    L.solv_gpu_matrix_set_batch.argtypes = [vp, ctypes.c_int, _i32p, ctypes.c_int, _i32p, _i32p,
+                                            _f64p, _f64p, _f64p]
+    L.solv_gpu_n_systems.argtypes = [vp]
+    for fn in (L.solv_gpu_cg_batch, L.solv_gpu_bicg_batch):
+        fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _f64p,
+                       _f64p, _f64p, ctypes.c_int, _i32p, _f64p, ctypes.POINTER(Stats)]
+    for fn in (L.solv_gpu_cg_batch_dev, L.solv_gpu_bicg_batch_dev):
+        fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, vp, vp,
+                       _f64p, ctypes.c_int, _i32p, _f64p, ctypes.POINTER(Stats)]
     L._typed = True
     return L
 
@@ -238,6 +249,71 @@ class GpuSolver:
     def solv_bicg_dev(self, imat, reduc, n_iter, n_vc, phi_ptr, res0_ptr, not_r0=False):
         return self._solve_dev(self._lib.solv_gpu_bicg_dev, imat, reduc, n_iter, n_vc, phi_ptr,
                                res0_ptr, not_r0)
+
+    # -- batches of independent systems ----------------------------------------
+    def matrix_set_batch(self, mats) -> np.ndarray:
+        """Concatenate independent face matrices into one block-diagonal batch.
+        Returns cell_ptr (0-based offsets of each system)."""
+        ns = len(mats)
+        cell_ptr = np.zeros(ns + 1, np.int32)
+        for k, m in enumerate(mats):
+            cell_ptr[k + 1] = cell_ptr[k] + m.n_cell
+        ip = np.concatenate([m.ip + cell_ptr[k] for k, m in enumerate(mats)]).astype(np.int32)
+        inb = np.concatenate([np.where(m.inb > 0, m.inb + cell_ptr[k], 0)
+                              for k, m in enumerate(mats)]).astype(np.int32)
+        p = np.concatenate([m.p for m in mats]).astype(np.float64)
+        n = np.concatenate([m.n for m in mats]).astype(np.float64)
+        pl = np.concatenate([m.pl for m in mats]).astype(np.float64)
+        self._check(self._lib.solv_gpu_matrix_set_batch(
+            self._h, ns, _p(cell_ptr, _i32p), ip.shape[0], _p(ip, _i32p), _p(inb, _i32p),
+            _p(p, _f64p), _p(n, _f64p), _p(pl, _f64p)))
+        self.n_cell = int(cell_ptr[-1])
+        self.cell_ptr = cell_ptr
+        return cell_ptr
+
+    @property
+    def n_systems(self) -> int:
+        return int(self._lib.solv_gpu_n_systems(self._h))
+
+    def _solve_batch(self, fn, imat, reduc, n_iter, phi, res0, not_r0):
+        phi2 = self._as_phi(phi)
+        V = phi2.shape[1]
+        self._as_res0(res0)
+        nl = self.n_systems * V
+        rn = np.zeros(nl)
+        iters = np.zeros(nl, np.int32)
+        ratio = np.zeros(nl)
+        st = Stats()
+        rc = fn(self._h, imat, float(reduc), int(n_iter), V, _p(phi2, _f64p), _p(res0, _f64p),
+                _p(rn, _f64p), int(bool(not_r0)), _p(iters, _i32p), _p(ratio, _f64p),
+                ctypes.byref(st))
+        self._check(rc, allow=(OK, MAXITER))
+        d = st.as_dict()
+        d.update(res0_n=rn.reshape(-1, V), iters_all=iters.reshape(-1, V),
+                 ratio_all=ratio.reshape(-1, V))
+        return d
+
+    def solv_cg_batch(self, imat, reduc, n_iter, phi, res0, not_r0=False):
+        return self._solve_batch(self._lib.solv_gpu_cg_batch, imat, reduc, n_iter, phi, res0, not_r0)
+
+    def solv_bicg_batch(self, imat, reduc, n_iter, phi, res0, not_r0=False):
+        return self._solve_batch(self._lib.solv_gpu_bicg_batch, imat, reduc, n_iter, phi, res0,
+                                 not_r0)
+
+    def solv_batch_dev(self, solver, imat, reduc, n_iter, n_vc, phi_ptr, res0_ptr, not_r0=False):
+        fn = self._lib.solv_gpu_cg_batch_dev if solver == "cg" else self._lib.solv_gpu_bicg_batch_dev
+        nl = self.n_systems * n_vc
+        rn = np.zeros(nl)
+        iters = np.zeros(nl, np.int32)
+        ratio = np.zeros(nl)
+        st = Stats()
+        rc = fn(self._h, imat, float(reduc), int(n_iter), n_vc, phi_ptr, res0_ptr, _p(rn, _f64p),
+                int(bool(not_r0)), _p(iters, _i32p), _p(ratio, _f64p), ctypes.byref(st))
+        self._check(rc, allow=(OK, MAXITER))
+        d = st.as_dict()
+        d.update(res0_n=rn.reshape(-1, n_vc), iters_all=iters.reshape(-1, n_vc),
+                 ratio_all=ratio.reshape(-1, n_vc))
+        return d
 
     def spmv_dev(self, x_ptr: int, y_ptr: int, repeat: int = 1) -> float:
         ms = ctypes.c_float()

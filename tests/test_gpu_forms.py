@@ -1,0 +1,153 @@
+"""GPU forms beyond the plain FP64 path: mixed precision (FP32 inner Krylov
+with FP64 iterative refinement) and batches of independent systems.
+
+Mixed precision changes the arithmetic on purpose, so it is held to the
+solution, not the bits: the true FP64 residual must reach the reference's
+stopping rule (|b - A x|_1 / |r0|_1 < 1e-10) and the solution must agree
+with the FP64 oracle to 1e-8 relative.  Batches must reproduce, system by
+system, what separate solv_cg / solv_bicg calls give.
+"""
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from programs_b200.mesh import Mesh, poisson_rhs, uniform
+from programs_b200.solver import OK, OPT_PRECISION
+
+pytestmark = pytest.mark.gpu
+
+SOL_TOL = 1e-8
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
+
+
+@pytest.fixture
+def mixed(gpu):
+    gpu.set_option(OPT_PRECISION, 1)
+    yield gpu
+    gpu.set_option(OPT_PRECISION, 0)
+
+
+@pytest.mark.parametrize("imat", [0, 1, 2])
+def test_mixed_cg_pressure(mixed, imat):
+    m = Mesh.hex(16, seed=1)
+    m.renumber(Mesh.RCM)
+    A = m.pressure(pin=1)
+    o = Oracle.from_matrix(A)
+    mixed.matrix_set(A)
+    b = np.asfortranarray(poisson_rhs(A.n_cell, 2).reshape(-1, 1))
+    ref = o.solv_cg(imat, 1e-10, 5000, np.zeros((A.n_cell, 1)), b)
+    phi = np.zeros((A.n_cell, 1))
+    res0 = b.copy(order="F")
+    rn = np.zeros(1)
+    st = mixed.solv_cg(imat, 1e-10, 5000, phi, res0, rn)
+    assert st["status"] == OK and st["refinements"] >= 2
+    # the reference's stopping rule on the true FP64 residual
+    r_true = b[:, 0] - A.to_scipy() @ phi[:, 0]
+    assert np.abs(r_true).sum() / rn[0] < 1e-10
+    assert _rel(phi, ref[0]) <= SOL_TOL
+    assert np.array_equal(res0, ref[1])  # initial residual stays FP64-exact
+
+
+@pytest.mark.parametrize("imat", [0, 2])
+def test_mixed_bicg_momentum_three_components(mixed, imat):
+    m = Mesh.hex(14, seed=2)
+    m.renumber(Mesh.SFC)
+    A, _ = m.momentum()
+    o = Oracle.from_matrix(A)
+    mixed.matrix_set(A)
+    V = 3
+    b = np.asfortranarray(np.stack([uniform(30 + v, A.n_cell) for v in range(V)], axis=1))
+    ref = o.solv_bicg(imat, 1e-10, 2000, np.zeros((A.n_cell, V)), b)
+    phi = np.zeros((A.n_cell, V))
+    res0 = b.copy(order="F")
+    rn = np.zeros(V)
+    st = mixed.solv_bicg(imat, 1e-10, 2000, phi, res0, rn)
+    assert st["status"] == OK
+    S = A.to_scipy()
+    for v in range(V):
+        assert np.abs(b[:, v] - S @ phi[:, v]).sum() / rn[v] < 1e-10
+        assert _rel(phi[:, v], ref[0][:, v]) <= SOL_TOL
+
+
+def _batch_meshes(k, seed=0):
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(4), np.log(11), k)).astype(int)
+    out = []
+    for j, n in enumerate(sizes):
+        m = Mesh.hex(int(n), int(max(3, n - 1)), int(n), seed=100 + j)
+        m.renumber(Mesh.RCM if j % 2 else Mesh.SFC)
+        out.append(m)
+    return out
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("imat", [0, 1])
+def test_batch_pressure_matches_separate_solves(gpu, precision, imat):
+    meshes = _batch_meshes(7, seed=precision * 10 + imat)
+    mats = [m.pressure(pin=1) for m in meshes]
+    cell_ptr = gpu.matrix_set_batch(mats)
+    gpu.set_option(OPT_PRECISION, precision)
+    try:
+        b = np.concatenate([poisson_rhs(A.n_cell, 5 + k) for k, A in enumerate(mats)])
+        phi = np.zeros((cell_ptr[-1], 1))
+        res0 = np.asfortranarray(b.reshape(-1, 1).copy())
+        st = gpu.solv_cg_batch(imat, 1e-10, 3000, phi, res0)
+    finally:
+        gpu.set_option(OPT_PRECISION, 0)
+    assert st["status"] == OK
+    for k, A in enumerate(mats):
+        sl = slice(cell_ptr[k], cell_ptr[k + 1])
+        ref = Oracle.from_matrix(A).solv_cg(imat, 1e-10, 3000, np.zeros((A.n_cell, 1)),
+                                            b[sl].reshape(-1, 1))
+        assert _rel(phi[sl], ref[0]) <= SOL_TOL
+        assert np.array_equal(res0[sl], ref[1])
+        assert np.isclose(st["res0_n"][k, 0], ref[2][0], rtol=1e-12)
+        if precision == 0:
+            assert abs(int(st["iters_all"][k, 0]) - int(ref[3][0])) <= 2
+        assert st["ratio_all"][k, 0] < 1e-10
+
+
+def test_batch_momentum_bicg_dilu(gpu):
+    meshes = _batch_meshes(5, seed=42)
+    mats = [m.momentum()[0] for m in meshes]
+    cell_ptr = gpu.matrix_set_batch(mats)
+    V = 3
+    b = np.asfortranarray(np.stack([uniform(60 + v, cell_ptr[-1]) for v in range(V)], axis=1))
+    phi = np.zeros((cell_ptr[-1], V))
+    res0 = b.copy(order="F")
+    st = gpu.solv_bicg_batch(2, 1e-10, 1000, phi, res0)
+    assert st["status"] == OK
+    for k, A in enumerate(mats):
+        sl = slice(cell_ptr[k], cell_ptr[k + 1])
+        ref = Oracle.from_matrix(A).solv_bicg(2, 1e-10, 1000, np.zeros((A.n_cell, V)),
+                                              np.asfortranarray(b[sl]))
+        for v in range(V):
+            assert _rel(phi[sl, v], ref[0][:, v]) <= SOL_TOL
+            assert abs(int(st["iters_all"][k, v]) - int(ref[3][v])) <= 2
+
+
+def test_batch_rejects_coupled_systems(gpu):
+    from programs_b200.solver import SolverError
+    a = Mesh.hex(3, seed=1).pressure(pin=1)
+    b = Mesh.hex(3, seed=2).pressure(pin=1)
+    ip = np.concatenate([a.ip, b.ip + a.n_cell]).astype(np.int32)
+    inb = np.concatenate([a.inb, np.where(b.inb > 0, b.inb + a.n_cell, 0)]).astype(np.int32)
+    inb[np.argmax(a.inb == 0)] = a.n_cell + 1  # a face that couples the two
+    import ctypes
+    cp = np.array([0, a.n_cell, a.n_cell + b.n_cell], np.int32)
+    p = np.concatenate([a.p, b.p])
+    n = np.concatenate([a.n, b.n])
+    pl = np.concatenate([a.pl, b.pl])
+    L = gpu._lib
+    f64 = ctypes.POINTER(ctypes.c_double)
+    i32 = ctypes.POINTER(ctypes.c_int)
+    rc = L.solv_gpu_matrix_set_batch(gpu._h, 2, cp.ctypes.data_as(i32), ip.shape[0],
+                                     ip.ctypes.data_as(i32), inb.ctypes.data_as(i32),
+                                     p.ctypes.data_as(f64), n.ctypes.data_as(f64),
+                                     pl.ctypes.data_as(f64))
+    assert rc == 4
+    with pytest.raises(SolverError):
+        gpu._check(rc)
