@@ -59,12 +59,14 @@ extern "C" {
 #define SOLV_OPT_PRECISION 1    /* 0 = FP64 (default); 1 = FP32 inner
                                    Krylov + FP64 iterative refinement      */
 #define SOLV_OPT_INNER_REDUC 2  /* inner relative drop per refinement
-                                   sweep (FP32 mode), default 1e-4         */
+                                   sweep (FP32 mode), default 1e-6         */
 #define SOLV_OPT_GRAPH_ITERS 3  /* Krylov iterations per CUDA-graph launch
                                    (0 = no graphs, plain launches)         */
 #define SOLV_OPT_BLOCK 4        /* threads per block for the cell kernels  */
 #define SOLV_OPT_GRID_PER_SM 5  /* resident blocks per SM for reductions   */
 #define SOLV_OPT_MAX_REFINE 6   /* cap on refinement sweeps (FP32 mode)    */
+#define SOLV_OPT_INNER_MAX_ITER 7 /* cap on FP32 iterations per refinement
+                                   sweep (default 2000)                    */
 
 typedef struct solv_gpu_ctx solv_gpu_ctx;
 
@@ -136,6 +138,20 @@ int solv_gpu_bicg_dev(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
                       double *res0_n, int not_r0, solv_gpu_stats *stats);
 int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
                       int repeat, float *ms_per_call);
+
+/* -- autotuner ------------------------------------------------------------ */
+/* No counterpart in the reference (it has no tunables).  Times candidate
+ * launch shapes (threads per block 128/256/512, resident blocks per SM
+ * 2/4/8/16 for the reduction kernels, Krylov iterations per CUDA graph
+ * 8/32) on the current matrix with the given solver (0 CG, 1 BiCGSTAB),
+ * preconditioner, component count and the context's precision, and leaves
+ * the fastest set on the context. */
+typedef struct {
+  int block, grid_per_sm, graph_iters, candidates;
+  double ms_per_iter;
+} solv_gpu_tune;
+int solv_gpu_autotune(solv_gpu_ctx *ctx, int solver, int imat, int n_vc,
+                      solv_gpu_tune *out);
 
 /* -- batches of independent systems ----------------------------------- */
 /* No counterpart call in the reference, which solves one system per call

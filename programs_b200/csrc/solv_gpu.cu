@@ -62,11 +62,12 @@ struct solv_gpu_ctx {
   int n_sm = 148;
   // options
   int precision = 0;
-  double inner_reduc = 1e-4;
+  double inner_reduc = 1e-6;
   int graph_iters = 16;
   int block = 256;
-  int grid_per_sm = 4;
+  int grid_per_sm = 8;
   int max_refine = 30;
+  int inner_max_iter = 2000;
 
   // matrix (caller sizes)
   bool has_matrix = false;
@@ -770,7 +771,9 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
       // do not over-solve the last sweep: the inner drop needed to reach reduc
       double need = 0.3 * reduc * (res0_n[l] + sg::kSmall) / (l1[l] + sg::kSmall);
       L.reduc = std::min(0.5, std::max(c->inner_reduc, need));
-      L.n_iter = n_iter - iters[l];
+      // an FP32 sweep that cannot reach its drop (rounding floor) must not
+      // run to the outer cap: bound each sweep, the outer loop decides
+      L.n_iter = std::min(n_iter - iters[l], c->inner_max_iter);
       L.active = active[l] && L.n_iter > 0;
       L.status = sg::kLaneRunning;
       mask[l] = L.active;
@@ -968,6 +971,10 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
     case SOLV_OPT_MAX_REFINE:
       if (value < 1 || value > 1000) return set_err(c, SOLV_GPU_BAD_INPUT, "max refine in 1..1000");
       c->max_refine = (int)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_INNER_MAX_ITER:
+      if (value < 1 || value > 1e7) return set_err(c, SOLV_GPU_BAD_INPUT, "inner max iter in 1..1e7");
+      c->inner_max_iter = (int)value;
       return SOLV_GPU_OK;
     default:
       return set_err(c, SOLV_GPU_BAD_INPUT, "unknown option key");
@@ -1207,6 +1214,97 @@ int solv_gpu_cg_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_v
 int solv_gpu_bicg_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n_vc, double* phi,
                       double* res0, double* res0_n, int not_r0, solv_gpu_stats* st) {
   return solve_common(c, 1, imat, reduc, n_iter, n_vc, phi, res0, res0_n, not_r0, st);
+}
+
+// ---- autotuner -----------------------------------------------------------------
+// Chooses threads per block, resident blocks per SM of the reduction
+// kernels and Krylov iterations per CUDA graph for the current matrix,
+// solver, preconditioner, component count and precision.  Each candidate is
+// timed on the device by differencing a short and a long capped solve of a
+// seeded right-hand side (so setup and layout conversion cancel out); the
+// fastest per-iteration time wins and is left set on the context.
+int solv_gpu_autotune(solv_gpu_ctx* c, int solver, int imat, int n_vc, solv_gpu_tune* out) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (n_vc < 1 || n_vc > kMaxV || imat < 0 || imat > 2 || solver < 0 || solver > 1)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "autotune: bad solver / imat / n_vc");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const int N = c->N, V = n_vc, nl = c->n_seg * V;
+  const size_t nv = (size_t)N * V;
+  DevBuf phi, res, b;
+  CUDA_TRY(c, phi.ensure(nv * sizeof(double)));
+  CUDA_TRY(c, res.ensure(nv * sizeof(double)));
+  CUDA_TRY(c, b.ensure(nv * sizeof(double)));
+  {
+    std::vector<double> hb(nv);
+    uint64_t x = 0x9e3779b97f4a7c15ull;
+    for (size_t i = 0; i < nv; ++i) {  // splitmix64 -> uniform [-1, 1)
+      x += 0x9e3779b97f4a7c15ull;
+      uint64_t z = x;
+      z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+      z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+      z ^= z >> 31;
+      hb[i] = (double)(z >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+    }
+    CUDA_TRY(c, cudaMemcpy(b.p, hb.data(), nv * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  std::vector<double> rn(nl);
+  auto run = [&](int iters, float& ms) -> int {
+    CUDA_TRY(c, cudaMemsetAsync(phi.p, 0, nv * sizeof(double), c->stream));
+    CUDA_TRY(c, cudaMemcpyAsync(res.p, b.p, nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    solv_gpu_stats st;
+    int rc = solve_common(c, solver, imat, 1e-300, iters, V, phi.as<double>(), res.as<double>(),
+                          rn.data(), 0, &st, nullptr, nullptr, true);
+    if (rc != SOLV_GPU_OK && rc != SOLV_GPU_MAXITER) return rc;
+    ms = (float)st.solve_ms;
+    return SOLV_GPU_OK;
+  };
+  const int blocks[] = {128, 256, 512};
+  const int gps[] = {2, 4, 8, 16};
+  const int graphs[] = {8, 32};
+  const int k_short = 4, k_long = 36;
+  const int precision = c->precision;
+  // the tuner measures capped iterations: keep FP32 sweeps as long as the cap
+  const int inner_keep = c->inner_max_iter;
+  double best = 1e300;
+  int bb = c->block, bg = c->grid_per_sm, bk = c->graph_iters;
+  int tried = 0;
+  for (int gi : graphs) {
+    c->graph_iters = gi;
+    drop_graphs(c);
+    for (int bl : blocks)
+      for (int g : gps) {
+        c->block = bl;
+        c->grid_per_sm = g;
+        int rc = build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
+        if (rc) return rc;
+        float t0 = 0, t1 = 0, w = 0;
+        if ((rc = run(k_short, w))) return rc;  // warm: graph capture, workspace
+        if ((rc = run(k_short, t0)) || (rc = run(k_long, t1))) return rc;
+        double per = (t1 - t0) / (double)(k_long - k_short);
+        ++tried;
+        if (per > 0 && per < best) {
+          best = per;
+          bb = bl; bg = g; bk = gi;
+        }
+      }
+  }
+  c->precision = precision;
+  c->inner_max_iter = inner_keep;
+  c->block = bb;
+  c->grid_per_sm = bg;
+  c->graph_iters = bk;
+  drop_graphs(c);
+  int rc = build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
+  if (rc) return rc;
+  if (out) {
+    out->block = bb;
+    out->grid_per_sm = bg;
+    out->graph_iters = bk;
+    out->ms_per_iter = best;
+    out->candidates = tried;
+  }
+  return SOLV_GPU_OK;
 }
 
 // ---- batches of independent systems ------------------------------------------

@@ -49,6 +49,12 @@ class Stats(ctypes.Structure):
                 "kernel_launches": self.kernel_launches, "solve_ms": self.solve_ms}
 
 
+class Tune(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int), ("grid_per_sm", ctypes.c_int),
+                ("graph_iters", ctypes.c_int), ("candidates", ctypes.c_int),
+                ("ms_per_iter", ctypes.c_double)]
+
+
 # Exported symbols of include/solv_gpu.h (the tests check them all).
 EXPORTS = [
     "solv_gpu_create", "solv_gpu_destroy", "solv_gpu_set_stream", "solv_gpu_set_option",
@@ -57,7 +63,7 @@ EXPORTS = [
     "solv_gpu_res", "solv_gpu_precond", "solv_gpu_direct", "solv_gpu_spmv", "solv_gpu_cg",
     "solv_gpu_bicg", "solv_gpu_cg_dev", "solv_gpu_bicg_dev", "solv_gpu_spmv_dev",
     "solv_gpu_matrix_set_batch", "solv_gpu_n_systems", "solv_gpu_cg_batch", "solv_gpu_bicg_batch",
-    "solv_gpu_cg_batch_dev", "solv_gpu_bicg_batch_dev",
+    "solv_gpu_cg_batch_dev", "solv_gpu_bicg_batch_dev", "solv_gpu_autotune",
     "solv_gpu_create_", "solv_gpu_destroy_", "solv_gpu_matrix_set_", "solv_gpu_matrix_values_",
     "solv_gpu_res_", "solv_gpu_precond_", "solv_gpu_direct_", "solv_gpu_cg_", "solv_gpu_bicg_",
 ]
@@ -94,6 +100,8 @@ def lib():
     L.solv_gpu_matrix_set_batch.argtypes = [vp, ctypes.c_int, _i32p, ctypes.c_int, _i32p, _i32p,
                                             _f64p, _f64p, _f64p]
     L.solv_gpu_n_systems.argtypes = [vp]
+    L.solv_gpu_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(Tune)]
     for fn in (L.solv_gpu_cg_batch, L.solv_gpu_bicg_batch):
         fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _f64p,
                        _f64p, _f64p, ctypes.c_int, _i32p, _f64p, ctypes.POINTER(Stats)]
@@ -249,6 +257,14 @@ class GpuSolver:
     def solv_bicg_dev(self, imat, reduc, n_iter, n_vc, phi_ptr, res0_ptr, not_r0=False):
         return self._solve_dev(self._lib.solv_gpu_bicg_dev, imat, reduc, n_iter, n_vc, phi_ptr,
                                res0_ptr, not_r0)
+
+    def autotune(self, solver: str = "cg", imat: int = 0, n_vc: int = 1) -> dict:
+        """Pick launch shapes for this matrix (left set on the context)."""
+        t = Tune()
+        self._check(self._lib.solv_gpu_autotune(self._h, 0 if solver == "cg" else 1, imat, n_vc,
+                                                ctypes.byref(t)))
+        return {"block": t.block, "grid_per_sm": t.grid_per_sm, "graph_iters": t.graph_iters,
+                "candidates": t.candidates, "ms_per_iter": t.ms_per_iter}
 
     # -- batches of independent systems ----------------------------------------
     def matrix_set_batch(self, mats) -> np.ndarray:
