@@ -81,6 +81,8 @@ typedef struct {
   int graph_launches;            /* CUDA-graph launches in the solve       */
   int kernel_launches;           /* kernels launched in the solve          */
   double solve_ms;               /* device time of the solve (events)      */
+  int fallbacks;                 /* learned preconditioner handed over to
+                                    plain PCG (solv_gpu_fcg)               */
 } solv_gpu_stats;
 
 /* -- context ------------------------------------------------------------ */
@@ -138,6 +140,41 @@ int solv_gpu_bicg_dev(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
                       double *res0_n, int not_r0, solv_gpu_stats *stats);
 int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
                       int repeat, float *ms_per_call);
+
+/* -- learned preconditioner ---------------------------------------------- */
+/* No counterpart in the reference.  Flexible CG, FCG(1), whose
+ * preconditioner is a 3-layer, width-32 message-passing network over the
+ * face graph (BF16 weights, per-cell MLPs on the tensor cores, FP32
+ * accumulate), run as the FP32 inner solver of the FP64 refinement loop of
+ * SOLV_OPT_PRECISION=1.  If a sweep with the network stalls (the residual
+ * does not halve, or p.Ap <= 0), plain Jacobi-PCG takes over from the
+ * current iterate for the rest of the solve (stats.fallbacks); the FP64
+ * residual test |b - A x|_1 / |r0|_1 < reduc decides convergence either
+ * way.  Same argument meaning as solv_gpu_cg with imat ignored, n_vc = 1,
+ * one system; the matrix must be symmetric (the pressure system). */
+int solv_gpu_fcg(solv_gpu_ctx *ctx, double reduc, int n_iter, double *phi,
+                 double *res0, double *res0_n, int not_r0,
+                 solv_gpu_stats *stats);
+int solv_gpu_fcg_dev(solv_gpu_ctx *ctx, double reduc, int n_iter,
+                     double *phi_dev, double *res0_dev, double *res0_n,
+                     int not_r0, solv_gpu_stats *stats);
+/* Network parameters (FP32 master copy, solv_gpu_gnn_n_params() floats). */
+int solv_gpu_gnn_n_params(void);
+int solv_gpu_gnn_set_params(solv_gpu_ctx *ctx, const float *params, int n);
+int solv_gpu_gnn_get_params(solv_gpu_ctx *ctx, float *params, int n);
+/* z = M(r) on the current matrix; r_dev / z_dev caller order, device.
+ * path 0: inference kernels (BF16, tensor cores); 1: training kernels. */
+int solv_gpu_gnn_forward_dev(solv_gpu_ctx *ctx, const double *r_dev,
+                             double *z_dev, int path);
+/* Training: forward + backward of J = 1/2 z'Az - z'r in the Jacobi-scaled
+ * space (minimised by z = A^-1 r) for one residual; gradients add up in an
+ * FP32 accumulator (zeroed first unless accumulate); loss = J / n_cell. */
+int solv_gpu_gnn_grad_dev(solv_gpu_ctx *ctx, const double *r_dev,
+                          double *loss, int accumulate);
+int solv_gpu_gnn_get_grad(solv_gpu_ctx *ctx, float *grad, int n);
+int solv_gpu_gnn_zero_grad(solv_gpu_ctx *ctx);
+/* Adam step on the accumulated gradient (scaled by grad_scale), zeroes it. */
+int solv_gpu_gnn_adam(solv_gpu_ctx *ctx, float lr, float grad_scale);
 
 /* -- autotuner ------------------------------------------------------------ */
 /* No counterpart in the reference (it has no tunables).  Times candidate

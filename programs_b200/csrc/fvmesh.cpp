@@ -498,6 +498,93 @@ double fvm_assemble_momentum(const fvm_mesh *m, double gamma, double pe_max,
   return dt;
 }
 
+void fvm_cavity_field(const fvm_mesh *m, double u_lid, double *u) {
+  // psi = a x^2 (1-x)^2 y^2 (1-y); dpsi/dy at (0.5, 1) = a * 1/16 * (2y - 3y^2)|_1 = -a/16
+  const double a = -16.0 * u_lid;
+  for (int c = 0; c < m->n_cell; ++c) {
+    const double x = m->xc[c].x, y = m->xc[c].y, z = m->xc[c].z;
+    const double fx = x * x * (1 - x) * (1 - x), dfx = 2 * x * (1 - x) * (1 - 2 * x);
+    const double gy = y * y * (1 - y), dgy = 2 * y - 3 * y * y;
+    const double hz = std::sin(M_PI * z);
+    u[3 * c] = a * fx * dgy * hz;
+    u[3 * c + 1] = -a * dfx * gy * hz;
+    u[3 * c + 2] = 0.0;
+  }
+}
+
+void fvm_assemble_momentum_field(const fvm_mesh *m, const double *u, const double *flux,
+                                 double rho, double mu, double u_lid, double urf, double *p,
+                                 double *n, double *pl, double *rhs, double *flux_out) {
+  const int N = m->n_cell;
+  const size_t F = m->f_ip.size();
+  for (int c = 0; c < N; ++c) pl[c] = 0.0;
+  if (rhs)
+    for (size_t k = 0; k < 3 * (size_t)N; ++k) rhs[k] = 0.0;
+  for (size_t f = 0; f < F; ++f) {
+    double s, l, w;
+    V3 nn, x;
+    m->face_geom(f, s, nn, x, l, w);
+    const int a = m->f_ip[f], b = m->f_in[f];
+    const double d = mu * s / l;
+    if (b >= 0) {
+      double c;
+      if (flux) {
+        c = flux[f];
+      } else {  // linear interpolation of u to the face (cfd_setup.f90:197-203)
+        const double uf = w * u[3 * b] + (1 - w) * u[3 * a];
+        const double vf = w * u[3 * b + 1] + (1 - w) * u[3 * a + 1];
+        const double wf = w * u[3 * b + 2] + (1 - w) * u[3 * a + 2];
+        c = rho * s * (uf * nn.x + vf * nn.y + wf * nn.z);
+      }
+      if (flux_out) flux_out[f] = c;
+      p[f] = -d + std::min(c, 0.0);
+      n[f] = -d - std::max(c, 0.0);
+      pl[a] -= p[f];
+      pl[b] -= n[f];
+    } else {
+      if (flux_out) flux_out[f] = 0.0;
+      p[f] = -d;  // no-slip wall: Dirichlet diffusion, zero flux
+      n[f] = 0.0;
+      pl[a] += d;
+      // the moving lid: the y = 1 wall (outward normal +y)
+      if (rhs && nn.y > 0.9 && x.y > 1.0 - 1e-9) rhs[3 * a] += d * u_lid;
+    }
+  }
+  // under-relaxation (cfd_setup.f90:517-518)
+  for (int c = 0; c < N; ++c) {
+    pl[c] = pl[c] / urf;
+    if (rhs)
+      for (int k = 0; k < 3; ++k) rhs[3 * c + k] += (1.0 - urf) * pl[c] * u[3 * c + k];
+  }
+}
+
+void fvm_assemble_pressure_correction(const fvm_mesh *m, const double *ap, double rho, int pin,
+                                      double *p, double *n, double *pl) {
+  const int N = m->n_cell;
+  const size_t F = m->f_ip.size();
+  std::vector<double> vol(N);
+  fvm_mesh_cell_geom(m, nullptr, vol.data());
+  for (int c = 0; c < N; ++c) pl[c] = 0.0;
+  const int pc = pin - 1;
+  for (size_t f = 0; f < F; ++f) {
+    p[f] = 0.0;
+    n[f] = 0.0;
+    const int a = m->f_ip[f], b = m->f_in[f];
+    if (b < 0) continue;
+    double s, l, w;
+    V3 nn, x;
+    m->face_geom(f, s, nn, x, l, w);
+    const double p_r = w / (ap[b] + 1e-20) + (1 - w) / (ap[a] + 1e-20);
+    const double v = w * vol[b] + (1 - w) * vol[a];
+    const double d = rho * p_r * s * v / l;
+    pl[a] += d;
+    pl[b] += d;
+    if (a == pc || b == pc) continue;
+    p[f] = -d;
+    n[f] = -d;
+  }
+}
+
 void fvm_uniform(uint64_t seed, int64_t count, double *out) {
   std::mt19937_64 rng(seed);
   for (int64_t i = 0; i < count; ++i)

@@ -74,6 +74,32 @@ void fvm_assemble_pressure(const fvm_mesh *m, int pin, double *p, double *n,
 double fvm_assemble_momentum(const fvm_mesh *m, double gamma, double pe_max,
                              double cfl, double *p, double *n, double *pl);
 
+/* Momentum matrix of a lid-driven cavity for a given cell velocity field
+ * u (3 per cell) and face mass fluxes flux (per face, owner -> neighbour;
+ * NULL = from the linearly interpolated u): upwind convection, central
+ * diffusion d = mu*area/l_pn, walls no-slip, the y = 1 wall moving with
+ * (u_lid, 0, 0), under-relaxation urf (cfd_setup.f90:324-330, 473-518):
+ * pl = (-sum off-diagonals) / urf.  rhs (3 per cell, may be NULL) gets
+ * the wall terms and (1-urf) pl u.  Returns the face fluxes used in flux_out
+ * (may be NULL). */
+void fvm_assemble_momentum_field(const fvm_mesh *m, const double *u, const double *flux,
+                                 double rho, double mu, double u_lid, double urf,
+                                 double *p, double *n, double *pl, double *rhs,
+                                 double *flux_out);
+
+/* Pressure-correction matrix of cfd_setup.f90:604-634:
+ * d = rho * p_r * area * v / l_pn with p_r, v the w_fp-weighted face
+ * values of 1/a_P (a_P = the momentum diagonal `ap`) and of the cell
+ * volume; p = n = -d, pl = sum d; boundaries all-Neumann; cell `pin`
+ * (1-based, 0 none) pinned as in fvm_assemble_pressure. */
+void fvm_assemble_pressure_correction(const fvm_mesh *m, const double *ap, double rho,
+                                      int pin, double *p, double *n, double *pl);
+
+/* A cavity-like divergence-free velocity field (3 per cell): stream
+ * function psi = u_lid x^2 (1-x)^2 y^2 (1-y) (scaled so u(0.5,1) = u_lid),
+ * u = dpsi/dy, v = -dpsi/dx, modulated by sin(pi z); w = 0. */
+void fvm_cavity_field(const fvm_mesh *m, double u_lid, double *u);
+
 /* Uniform [-1,1) values from std::mt19937_64(seed) (53-bit mantissa). */
 void fvm_uniform(uint64_t seed, int64_t count, double *out);
 

@@ -40,9 +40,11 @@ struct Lane {
   double s, beta, alpha, pq;           // CG: s = r.z, beta, alpha
   double rho, beta0, gam, omeg;        // BiCGSTAB (alpha shared)
   double res0_n, ratio, reduc, l1;
+  double gs;                           // FCG: residual scale fed to the network
   int iter, n_iter, active, status;
 };
-enum : int { kLaneRunning = 0, kLaneConverged = 1, kLaneMaxIter = 2, kLaneNaN = 3 };
+enum : int { kLaneRunning = 0, kLaneConverged = 1, kLaneMaxIter = 2, kLaneNaN = 3,
+             kLaneStall = 4 };
 
 template <typename T>
 struct Rows {
@@ -806,6 +808,103 @@ __global__ void k_bi_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
         L.beta0 = L.rho;
       }
     }
+  }
+}
+
+// ================ flexible CG, FCG(1), for a nonlinear preconditioner ==========
+// z = M(r); beta = -(z.q_old)/(p_old.q_old); p = z + beta p; q = A p;
+// alpha = (p.r)/(p.q); x += alpha p; r -= alpha q.  One system, V = 1.
+
+// gs = sum |r_i| rsd_i / N: the residual scale the network normalises by.
+template <typename T>
+__global__ void k_fcg_scale(SegMap sm, const T* __restrict__ r, const float* __restrict__ rsd,
+                            double* __restrict__ part, Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  if (!lanes[s].active) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[1] = {0.0};
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride)
+    acc[0] += fabs((double)r[i]) * rsd[i];
+  double tot[1];
+  if (seg_commit<1>(sm, b, s, part, acc, tot) && threadIdx.x == 0)
+    lanes[s].gs = tot[0] / (double)(c1 - c0);
+}
+
+template <typename T>
+__global__ void k_fcg_beta(SegMap sm, const T* __restrict__ z, const T* __restrict__ q,
+                           double* __restrict__ part, Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  if (!lanes[s].active) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[1] = {0.0};
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride)
+    acc[0] += prod(z[i], q[i]);
+  double tot[1];
+  if (seg_commit<1>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+    Lane& L = lanes[s];
+    L.beta = L.pq > 0.0 ? -tot[0] / L.pq : 0.0;
+  }
+}
+
+template <typename T>
+__global__ void k_fcg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
+                           const T* __restrict__ r, double* __restrict__ part,
+                           Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  if (!lanes[s].active) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[2] = {0.0, 0.0};
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+    T y[1];
+    row_apply<T, 1>(R, i, p, y);
+    q[i] = y[0];
+    acc[0] += prod(p[i], y[0]);
+    acc[1] += prod(p[i], r[i]);
+  }
+  double tot[2];
+  if (seg_commit<2>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+    Lane& L = lanes[s];
+    if (!(tot[0] > 0.0) || !(tot[1] == tot[1])) {  // not SPD-like: hand over to PCG
+      L.alpha = 0.0;
+      lane_stop(L, kLaneStall, sm.n_active);
+    } else {
+      L.pq = tot[0];
+      L.alpha = tot[1] / tot[0];
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_fcg_update(SegMap sm, const float* __restrict__ rsd, T* __restrict__ phi,
+                             T* __restrict__ r, const T* __restrict__ p, const T* __restrict__ q,
+                             double* __restrict__ part, Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  if (!lanes[s].active) return;
+  const T alpha = (T)lanes[s].alpha;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[2] = {0.0, 0.0};
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+    phi[i] = add(phi[i], mul(alpha, p[i]));
+    const T rn = sub(r[i], mul(alpha, q[i]));
+    r[i] = rn;
+    acc[0] += fabs((double)rn);
+    acc[1] += fabs((double)rn) * rsd[i];
+  }
+  double tot[2];
+  if (seg_commit<2>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+    Lane& L = lanes[s];
+    L.iter += 1;
+    L.l1 = tot[0];
+    L.gs = tot[1] / (double)(c1 - c0);
+    const double ratio = tot[0] / (L.res0_n + kSmall);
+    L.ratio = ratio;
+    if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);
+    else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);
+    else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
   }
 }
 

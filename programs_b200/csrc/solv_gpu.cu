@@ -22,6 +22,7 @@
 
 #include "../../include/solv_gpu.h"
 #include "kernels.cuh"
+#include "gnn.cuh"
 
 using sg::Lane;
 using sg::Rows;
@@ -100,6 +101,15 @@ struct solv_gpu_ctx {
   int launches = 0;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // learned preconditioner (gnn.cuh)
+  DevBuf g_param, g_grad, g_m, g_v, g_wcat;  // FP32 master, grads, Adam moments, BF16 packed
+  DevBuf g_rsd, g_frs, g_fdeg, g_gw;         // per-matrix features
+  DevBuf g_h0, g_h1, g_u, g_r, g_out, g_jsum;
+  DevBuf g_train;                            // training activations
+  bool g_feat_valid = false, g_wcat_valid = false, g_has_params = false;
+  int g_adam_t = 0;
+  int fallbacks = 0;
 };
 
 namespace {
@@ -334,6 +344,7 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
   c->n_slots = total;
   c->n_slice = ns;
   c->f32_valid = false;
+  c->g_feat_valid = false;
   cudaStream_t st = c->stream;
   CUDA_TRY(c, c->old_of_new.ensure(N * sizeof(int)));
   CUDA_TRY(c, c->slice_ptr.ensure((ns + 1) * sizeof(int)));
@@ -378,6 +389,7 @@ int matrix_values_dev(solv_gpu_ctx* c, const double* p, const double* n, const d
       N, c->old_of_new.as<int>(), pl, c->diag.as<double>());
   CUDA_TRY(c, cudaGetLastError());
   c->f32_valid = false;
+  c->g_feat_valid = false;
   return SOLV_GPU_OK;
 }
 
@@ -397,6 +409,83 @@ int ensure_f32_matrix(solv_gpu_ctx* c) {
   CUDA_TRY(c, cudaGetLastError());
   c->f32_valid = true;
   return SOLV_GPU_OK;
+}
+
+// ---- learned preconditioner ------------------------------------------------------
+gnn::Feat gnn_feat(solv_gpu_ctx* c) {
+  gnn::Feat F;
+  F.rsd = c->g_rsd.as<float>();
+  F.frs = c->g_frs.as<float>();
+  F.fdeg = c->g_fdeg.as<float>();
+  F.gw = c->g_gw.as<float>();
+  return F;
+}
+
+int gnn_grid_warps(solv_gpu_ctx* c, long long n_threads) {
+  long long g = (n_threads + 255) / 256;
+  return (int)std::max(1LL, std::min(g, (long long)c->n_sm * 16));
+}
+
+// Features of the current matrix, packed BF16 weights and inference buffers.
+int gnn_prepare(solv_gpu_ctx* c) {
+  if (!c->g_has_params)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "learned preconditioner: no parameters set");
+  if (c->n_seg != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "learned preconditioner: one system only");
+  int rc = ensure_f32_matrix(c);
+  if (rc) return rc;
+  const int N = c->N;
+  const void* before[4] = {c->g_h0.p, c->g_h1.p, c->g_u.p, c->g_wcat.p};
+  if (!c->g_feat_valid) {
+    CUDA_TRY(c, c->g_rsd.ensure(N * sizeof(float)));
+    CUDA_TRY(c, c->g_frs.ensure(N * sizeof(float)));
+    CUDA_TRY(c, c->g_fdeg.ensure(N * sizeof(float)));
+    CUDA_TRY(c, c->g_gw.ensure(c->n_slots * sizeof(float)));
+    gnn::k_gnn_features<<<grid_for(c, N), c->block, 0, c->stream>>>(
+        N, rows<double>(c), c->g_rsd.as<float>(), c->g_frs.as<float>(), c->g_fdeg.as<float>(),
+        c->g_gw.as<float>());
+    CUDA_TRY(c, cudaGetLastError());
+    c->g_feat_valid = true;
+  }
+  if (!c->g_wcat_valid) {
+    const int nw = gnn::NL * 2 * gnn::H * gnn::H;
+    CUDA_TRY(c, c->g_wcat.ensure(nw * sizeof(__nv_bfloat16)));
+    gnn::k_gnn_pack<<<(nw + 255) / 256, 256, 0, c->stream>>>(c->g_param.as<float>(),
+                                                             c->g_wcat.as<__nv_bfloat16>());
+    CUDA_TRY(c, cudaGetLastError());
+    c->g_wcat_valid = true;
+  }
+  CUDA_TRY(c, c->g_h0.ensure((size_t)N * gnn::H * sizeof(__nv_bfloat16)));
+  CUDA_TRY(c, c->g_h1.ensure((size_t)N * gnn::H * sizeof(__nv_bfloat16)));
+  CUDA_TRY(c, c->g_u.ensure((size_t)N * sizeof(float)));
+  const void* after[4] = {c->g_h0.p, c->g_h1.p, c->g_u.p, c->g_wcat.p};
+  for (int k = 0; k < 4; ++k)
+    if (before[k] != after[k]) drop_graphs(c);
+  return SOLV_GPU_OK;
+}
+
+// z = M(r) with the network (inference path: BF16, tensor cores).
+template <typename T>
+void gnn_apply(solv_gpu_ctx* c, const T* r, T* z, const int* n_active) {
+  const int N = c->N;
+  gnn::Feat F = gnn_feat(c);
+  const float* P = c->g_param.as<float>();
+  const int gw = gnn_grid_warps(c, (long long)N * 32);
+  __nv_bfloat16* h0 = c->g_h0.as<__nv_bfloat16>();
+  __nv_bfloat16* h1 = c->g_h1.as<__nv_bfloat16>();
+  gnn::k_gnn_enc<T><<<gw, 256, 0, c->stream>>>(N, F, r, P, c->lanes.as<Lane>(), h0,
+                                                c->g_u.as<float>(), n_active);
+  const int tiles = (N + gnn::TC_CELLS - 1) / gnn::TC_CELLS;
+  const int tcb = std::max(1, std::min((tiles + gnn::TC_WARPS - 1) / gnn::TC_WARPS, c->n_sm * 8));
+  __nv_bfloat16 *hin = h0, *hout = h1;
+  for (int l = 0; l < gnn::NL; ++l) {
+    gnn::k_gnn_layer_tc<<<tcb, gnn::TC_WARPS * 32, 0, c->stream>>>(
+        N, rows<float>(c), F, hin, hout, c->g_wcat.as<__nv_bfloat16>() + l * 2 * gnn::H * gnn::H,
+        P + gnn::P_LAYER + l * gnn::LAYER_SZ + 2 * gnn::H * gnn::H, n_active);
+    std::swap(hin, hout);
+  }
+  gnn::k_gnn_dec_z<T><<<gw, 256, 0, c->stream>>>(N, F, hin, c->g_u.as<float>(), P,
+                                                  c->lanes.as<Lane>(), z, n_active);
+  c->launches += 2 + gnn::NL;
 }
 
 // ---- building blocks -----------------------------------------------------------
@@ -544,6 +633,23 @@ void bicg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
   c->launches += 5;
 }
 
+// One flexible-CG iteration with the learned preconditioner (one system).
+template <typename T>
+void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
+  SegMap sm = segmap(c);
+  double* part = c->part.as<double>();
+  Lane* lanes = c->lanes.as<Lane>();
+  const int G = c->seg.total_blk, B = c->block;
+  cudaStream_t st = c->stream;
+  gnn_apply<T>(c, w.r, w.z, sm.n_active);                                    // z = M(r)
+  sg::k_fcg_beta<T><<<G, B, 0, st>>>(sm, w.z, w.q, part, lanes);            // beta
+  sg::k_cg_p<T, 1, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes);   // p = z + beta p
+  sg::k_fcg_spmv<T><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, w.r, part, lanes);
+  sg::k_fcg_update<T><<<G, B, 0, st>>>(sm, c->g_rsd.as<float>(), w.phi, w.r, w.p, w.q, part,
+                                       lanes);
+  c->launches += 4;
+}
+
 // Run Krylov iterations until every lane stops (device counter), launching
 // `graph_iters` iterations per CUDA-graph launch.
 template <typename T, int V>
@@ -551,7 +657,8 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
   const int K = c->graph_iters;
   auto body = [&]() {
     if (solver == 0) cg_iteration<T, V>(c, imat, w);
-    else bicg_iteration<T, V>(c, imat, w);
+    else if (solver == 1) bicg_iteration<T, V>(c, imat, w);
+    else if constexpr (V == 1) fcg_iteration<T>(c, w);
   };
   cudaGraphExec_t exec = nullptr;
   if (K > 0) {
@@ -582,7 +689,8 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     int nl = (int)c->lvl_ptr.size() - 1;
     int sweep = imat > 0 ? 2 * nl : 1;
     if (solver == 0) per_launch_kernels = imat > 0 ? sweep + 4 : 3;
-    else per_launch_kernels = imat > 0 ? 2 * sweep + 5 : 5;
+    else if (solver == 1) per_launch_kernels = imat > 0 ? 2 * sweep + 5 : 5;
+    else per_launch_kernels = 5 + gnn::NL + 1;
     c->launches = l0;
   }
   while (done < n_iter) {
@@ -761,6 +869,8 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   }
   const double* rcur = w.r0;  // current FP64 residual
   int refinements = 0, gl_total = 0;
+  bool gnn_ok = true;
+  c->fallbacks = 0;
   std::vector<Lane> hl(nl);
   for (int k = 0; k < c->max_refine; ++k) {
     int na = 0, cap = 0;
@@ -791,21 +901,28 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
     CUDA_TRY(c, cudaMemsetAsync(f.v, 0, NV * sizeof(float), s));
     CUDA_TRY(c, cudaMemsetAsync(f.z, 0, NV * sizeof(float), s));
     SegMap sm = segmap(c);
-    if (solver == 0) {
+    // the learned preconditioner runs until it fails once; then plain PCG
+    const int inner = (solver == 2 && !gnn_ok) ? 0 : solver;
+    if (inner == 0) {
       if (imat <= 0) {
         sg::k_cg_rz<float, V, true><<<c->seg.total_blk, c->block, 0, s>>>(
             sm, f.c, f.r, f.z, c->part.as<double>(), c->lanes.as<Lane>());
         c->launches++;
       }
-    } else {
+    } else if (inner == 1) {
       sg::k_bi_rho<float, V><<<c->seg.total_blk, c->block, 0, s>>>(
           sm, f.r, f.r0, c->part.as<double>(), c->lanes.as<Lane>());
+      c->launches++;
+    } else {
+      if ((rc = gnn_prepare(c))) return rc;
+      sg::k_fcg_scale<float><<<c->seg.total_blk, c->block, 0, s>>>(
+          sm, f.r, c->g_rsd.as<float>(), c->part.as<double>(), c->lanes.as<Lane>());
       c->launches++;
     }
     c->launches++;
     CUDA_TRY(c, cudaGetLastError());
     int gl = 0;
-    if ((rc = iterate<float, V>(c, solver, imat, cap, f, gl))) return rc;
+    if ((rc = iterate<float, V>(c, inner, imat, cap, f, gl))) return rc;
     gl_total += gl;
     CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->lanes.p, nl * sizeof(Lane), cudaMemcpyDeviceToHost, s));
     // x += d in FP64, then the true residual r = b - A x in FP64
@@ -829,6 +946,11 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
       } else if (iters[l] >= n_iter) {
         active[l] = false;
         status_v[l] = sg::kLaneMaxIter;
+      } else if (inner == 2 && (hl[l].status == sg::kLaneStall || ratio[l] > 0.5 * prev[l])) {
+        // the learned preconditioner stalled (or lost positive curvature):
+        // plain PCG takes over from the current iterate
+        gnn_ok = false;
+        c->fallbacks++;
       } else {
         // a sweep that does not halve the residual twice running: FP32 has
         // reached its floor on this system
@@ -864,6 +986,7 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
     }
     st->status = status;
     st->refinements = refinements;
+    st->fallbacks = c->fallbacks;
     st->graph_launches += gl_total;
   }
   return status;
@@ -1307,6 +1430,198 @@ int solv_gpu_autotune(solv_gpu_ctx* c, int solver, int imat, int n_vc, solv_gpu_
   return SOLV_GPU_OK;
 }
 
+// ---- learned preconditioner: solve, inference, training ---------------------------
+int solv_gpu_fcg(solv_gpu_ctx* c, double reduc, int n_iter, double* phi, double* res0,
+                 double* res0_n, int not_r0, solv_gpu_stats* st) {
+  return solve_host(c, 2, 0, reduc, n_iter, 1, phi, res0, res0_n, not_r0, st);
+}
+int solv_gpu_fcg_dev(solv_gpu_ctx* c, double reduc, int n_iter, double* phi, double* res0,
+                     double* res0_n, int not_r0, solv_gpu_stats* st) {
+  return solve_common(c, 2, 0, reduc, n_iter, 1, phi, res0, res0_n, not_r0, st);
+}
+
+int solv_gpu_gnn_n_params(void) { return gnn::N_PARAM; }
+
+int solv_gpu_gnn_set_params(solv_gpu_ctx* c, const float* p, int n) {
+  if (!c || !p || n != gnn::N_PARAM) return set_err(c, SOLV_GPU_BAD_INPUT, "gnn: expected N_PARAM floats");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const size_t b = gnn::N_PARAM_PAD * sizeof(float);
+  CUDA_TRY(c, c->g_param.ensure(b));
+  CUDA_TRY(c, c->g_grad.ensure(b));
+  CUDA_TRY(c, c->g_m.ensure(b));
+  CUDA_TRY(c, c->g_v.ensure(b));
+  CUDA_TRY(c, cudaMemsetAsync(c->g_param.p, 0, b, c->stream));
+  CUDA_TRY(c, cudaMemcpyAsync(c->g_param.p, p, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->g_grad.p, 0, b, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->g_m.p, 0, b, c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(c->g_v.p, 0, b, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  c->g_has_params = true;
+  c->g_wcat_valid = false;
+  c->g_adam_t = 0;
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_gnn_get_params(solv_gpu_ctx* c, float* p, int n) {
+  if (!c || !p || n != gnn::N_PARAM || !c->g_has_params)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "gnn: no parameters / bad size");
+  CUDA_TRY(c, cudaMemcpy(p, c->g_param.p, n * sizeof(float), cudaMemcpyDeviceToHost));
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_gnn_get_grad(solv_gpu_ctx* c, float* g, int n) {
+  if (!c || !g || n != gnn::N_PARAM || !c->g_has_params)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "gnn: no parameters / bad size");
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  CUDA_TRY(c, cudaMemcpy(g, c->g_grad.p, n * sizeof(float), cudaMemcpyDeviceToHost));
+  return SOLV_GPU_OK;
+}
+
+int solv_gpu_gnn_zero_grad(solv_gpu_ctx* c) {
+  if (!c || !c->g_has_params) return set_err(c, SOLV_GPU_BAD_INPUT, "gnn: no parameters");
+  CUDA_TRY(c, cudaMemsetAsync(c->g_grad.p, 0, gnn::N_PARAM_PAD * sizeof(float), c->stream));
+  return SOLV_GPU_OK;
+}
+
+// Training activations: 15 FP32 arrays of N x 32 plus 4 of N.
+static int gnn_train_buffers(solv_gpu_ctx* c, float** B) {
+  const size_t nh = (size_t)c->N * gnn::H, n1 = (size_t)c->N;
+  CUDA_TRY(c, c->g_train.ensure((15 * nh + 4 * n1) * sizeof(float)));
+  float* base = c->g_train.as<float>();
+  for (int k = 0; k < 15; ++k) B[k] = base + k * nh;
+  for (int k = 0; k < 4; ++k) B[15 + k] = base + 15 * nh + k * n1;
+  return SOLV_GPU_OK;
+}
+enum { TB_H0 = 0, TB_AGG0 = 4, TB_PRE0 = 7, TB_DHA = 11, TB_DHB = 12, TB_DHS = 13, TB_DAGG = 14,
+       TB_U = 15, TB_OUT = 16, TB_G = 17, TB_R = 18 };
+
+// r (caller layout, device) -> internal FP32 residual and its scale (lane 0)
+static int gnn_load_residual(solv_gpu_ctx* c, const double* r_dev, float* rf) {
+  const int N = c->N;
+  sg::k_phi_in<float><<<grid_for(c, N), c->block, 0, c->stream>>>(N, 1, c->old_of_new.as<int>(),
+                                                                  r_dev, rf);
+  Lane L{};
+  L.active = 1;
+  CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, &L, sizeof(Lane), cudaMemcpyHostToDevice, c->stream));
+  sg::k_fcg_scale<float><<<c->seg.total_blk, c->block, 0, c->stream>>>(
+      segmap(c), rf, c->g_rsd.as<float>(), c->part.as<double>(), c->lanes.as<Lane>());
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
+}
+
+// Training-path forward (FP32 CUDA cores, BF16 rounding as inference).
+static void gnn_train_forward(solv_gpu_ctx* c, float** B) {
+  const int N = c->N;
+  gnn::Feat F = gnn_feat(c);
+  const float* P = c->g_param.as<float>();
+  const int gw = gnn_grid_warps(c, (long long)N * 32);
+  gnn::k_gnn_enc<float><<<gw, 256, 0, c->stream>>>(N, F, B[TB_R], P, c->lanes.as<Lane>(),
+                                                    c->g_h0.as<__nv_bfloat16>(), B[TB_U], nullptr);
+  gnn::k_gnn_enc_train<<<gw, 256, 0, c->stream>>>(N, F, B[TB_U], P, B[TB_H0], B[TB_PRE0]);
+  const int lb = std::max(1, std::min((N + 7) / 8, c->n_sm * 8));
+  for (int l = 0; l < gnn::NL; ++l)
+    gnn::k_gnn_layer_train<<<lb, 256, 0, c->stream>>>(
+        N, rows<float>(c), F, B[TB_H0 + l], B[TB_AGG0 + l], B[TB_PRE0 + 1 + l], B[TB_H0 + 1 + l],
+        P + gnn::P_LAYER + l * gnn::LAYER_SZ);
+  gnn::k_gnn_dec_out<float><<<gw, 256, 0, c->stream>>>(N, B[TB_H0 + 3], B[TB_U], P, B[TB_OUT]);
+}
+
+__global__ void k_gnn_scale_z(int n, const float* __restrict__ rsd, const float* __restrict__ out,
+                              const Lane* __restrict__ lanes, float* __restrict__ z) {
+  const double s = lanes[0].gs > 0 ? lanes[0].gs : 1.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    z[i] = (float)((double)out[i] * s * rsd[i]);
+}
+
+// z = M(r) for a caller-layout residual: path 0 = inference (BF16 tensor
+// cores), path 1 = training path (FP32 CUDA cores).
+int solv_gpu_gnn_forward_dev(solv_gpu_ctx* c, const double* r_dev, double* z_dev, int path) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  int rc = gnn_prepare(c);
+  if (rc) return rc;
+  float* B[19];
+  if ((rc = gnn_train_buffers(c, B))) return rc;
+  if ((rc = gnn_load_residual(c, r_dev, B[TB_R]))) return rc;
+  const int N = c->N;
+  if (path == 0) {
+    gnn_apply<float>(c, B[TB_R], B[TB_G], nullptr);
+  } else {
+    gnn_train_forward(c, B);
+    k_gnn_scale_z<<<grid_for(c, N), c->block, 0, c->stream>>>(N, c->g_rsd.as<float>(), B[TB_OUT],
+                                                              c->lanes.as<Lane>(), B[TB_G]);
+  }
+  sg::k_phi_out<float><<<grid_for(c, N), c->block, 0, c->stream>>>(N, 1, c->old_of_new.as<int>(),
+                                                                  B[TB_G], z_dev);
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
+}
+
+// Forward + backward of the energy loss for one residual; gradients are
+// added to the accumulator (zeroed first unless `accumulate`).  loss = J/N.
+int solv_gpu_gnn_grad_dev(solv_gpu_ctx* c, const double* r_dev, double* loss, int accumulate) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  int rc = gnn_prepare(c);
+  if (rc) return rc;
+  float* B[19];
+  if ((rc = gnn_train_buffers(c, B))) return rc;
+  if (!accumulate) CUDA_TRY(c, cudaMemsetAsync(c->g_grad.p, 0, gnn::N_PARAM_PAD * sizeof(float), c->stream));
+  if ((rc = gnn_load_residual(c, r_dev, B[TB_R]))) return rc;
+  gnn_train_forward(c, B);
+  const int N = c->N;
+  gnn::Feat F = gnn_feat(c);
+  const float* P = c->g_param.as<float>();
+  float* G = c->g_grad.as<float>();
+  CUDA_TRY(c, c->g_jsum.ensure(sizeof(double)));
+  CUDA_TRY(c, cudaMemsetAsync(c->g_jsum.p, 0, sizeof(double), c->stream));
+  gnn::k_gnn_loss_grad<<<grid_for(c, N), 256, 0, c->stream>>>(N, rows<float>(c), F, B[TB_OUT],
+                                                               B[TB_U], B[TB_G],
+                                                               c->g_jsum.as<double>());
+  const int gw = gnn_grid_warps(c, (long long)N * 32);
+  gnn::k_gnn_dec_back<<<gw, 256, 0, c->stream>>>(N, B[TB_H0 + 3], B[TB_U], B[TB_G], 1.0f / N, P,
+                                                 B[TB_DHA], G);
+  float* dcur = B[TB_DHA];
+  const int lb = std::max(1, std::min((N + 7) / 8, c->n_sm * 8));
+  for (int l = gnn::NL - 1; l >= 0; --l) {
+    const float* L = P + gnn::P_LAYER + l * gnn::LAYER_SZ;
+    gnn::k_gnn_layer_back1<<<lb, 256, 0, c->stream>>>(
+        N, B[TB_H0 + l], B[TB_AGG0 + l], B[TB_PRE0 + 1 + l], dcur, L, B[TB_DHS], B[TB_DAGG],
+        G + gnn::P_LAYER + l * gnn::LAYER_SZ);
+    float* dnext = dcur == B[TB_DHA] ? B[TB_DHB] : B[TB_DHA];
+    gnn::k_gnn_layer_back2<<<gw, 256, 0, c->stream>>>(N, rows<float>(c), F, B[TB_DHS], B[TB_DAGG],
+                                                      dnext);
+    dcur = dnext;
+  }
+  gnn::k_gnn_enc_back<<<gw, 256, 0, c->stream>>>(N, F, B[TB_U], B[TB_PRE0], dcur, G);
+  CUDA_TRY(c, cudaGetLastError());
+  double j = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&j, c->g_jsum.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (loss) *loss = j / N;
+  return SOLV_GPU_OK;
+}
+
+// Adam step on the accumulated gradient (times grad_scale), then zero it.
+int solv_gpu_gnn_adam(solv_gpu_ctx* c, float lr, float grad_scale) {
+  if (!c || !c->g_has_params) return set_err(c, SOLV_GPU_BAD_INPUT, "gnn: no parameters");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  c->g_adam_t++;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float bc1 = 1.0f - std::pow(b1, (float)c->g_adam_t);
+  const float bc2 = 1.0f - std::pow(b2, (float)c->g_adam_t);
+  gnn::k_adam<<<(gnn::N_PARAM + 255) / 256, 256, 0, c->stream>>>(
+      gnn::N_PARAM, c->g_param.as<float>(), c->g_grad.as<float>(), c->g_m.as<float>(),
+      c->g_v.as<float>(), lr, b1, b2, 1e-8f, bc1, bc2, grad_scale);
+  CUDA_TRY(c, cudaMemsetAsync(c->g_grad.p, 0, gnn::N_PARAM_PAD * sizeof(float), c->stream));
+  CUDA_TRY(c, cudaGetLastError());
+  c->g_wcat_valid = false;
+  return SOLV_GPU_OK;
+}
+
 // ---- batches of independent systems ------------------------------------------
 int solv_gpu_matrix_set_batch(solv_gpu_ctx* c, int n_sys, const int* cell_ptr, int n_face,
                               const int* ip, const int* in, const double* p, const double* n,
@@ -1405,6 +1720,11 @@ namespace {
 int solve_dispatch(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter, int V,
                    double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
                    solv_gpu_stats* st, int* oi, double* orat) {
+  if (solver == 2) {  // flexible CG with the learned preconditioner, FP32 inner
+    if (V != 1 || c->n_seg != 1)
+      return set_err(c, SOLV_GPU_BAD_INPUT, "learned preconditioner: one system, n_vc = 1");
+    return solve_mixed<1>(c, 2, 0, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+  }
   if (c->precision == 1) {
     switch (V) {
       case 1: return solve_mixed<1>(c, solver, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);

@@ -1,0 +1,164 @@
+"""Training and use of the learned preconditioner (the network in
+programs_b200/csrc/gnn.cuh, applied by solv_gpu_fcg).
+
+Training data are pressure-correction systems as the SIMPLE loop assembles
+them (spray-simulation/cfd_setup.f90:604-646: d = rho (V/a_P)_f area/l_pn,
+a_P the momentum diagonal of the current velocity field) on jittered hex
+meshes of a lid-driven cavity: jitter uniform in [0, 0.25], lid velocity in
+[0.1, 2].  Each mesh contributes several systems (different flow states);
+each system several residuals, taken from the Jacobi-PCG iterates the
+plain solver visits.  The loss is the energy J = 1/2 z'Az - z'r in the
+Jacobi-scaled space, minimised by z = A^-1 r, so no reference solutions
+are needed.  Forward, backward and the Adam step run on the GPU in the
+library's own kernels; this module only orchestrates.
+
+  python -m programs_b200.learn --size 64 --systems 2000 --out weights.npz
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from .mesh import Mesh, cavity_field, momentum_field, poisson_rhs, pressure_correction
+from .solver import GpuSolver
+
+H, NF, NL = 32, 4, 3
+P_WIN = 0
+P_LAYER = H * NF
+LAYER_SZ = 2 * H * H + H
+P_WOUT = P_LAYER + NL * LAYER_SZ
+P_C = P_WOUT + H
+N_PARAM = P_C + 1
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "gnn_pressure.npz")
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """Random hidden layers, zero correction: the untrained network is the
+    Jacobi step (w_out = 0, c = 1)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(N_PARAM, np.float32)
+    p[P_WIN:P_WIN + H * NF] = rng.normal(0, 0.5, H * NF)
+    for l in range(NL):
+        o = P_LAYER + l * LAYER_SZ
+        p[o:o + H * H] = rng.normal(0, 0.3 / np.sqrt(H), H * H)            # Ws
+        p[o + H * H:o + 2 * H * H] = rng.normal(0, 0.3 / np.sqrt(H), H * H)  # Wn
+    p[P_WOUT:P_WOUT + H] = 0.0
+    p[P_C] = 1.0
+    return p
+
+
+def save_params(path: str, p: np.ndarray, meta: dict) -> None:
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    np.savez(path, params=np.asarray(p, np.float32), n_param=N_PARAM,
+             layout="H32-NF4-NL3-v1", meta=json.dumps(meta))
+
+
+def load_params(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
+    d = np.load(path)
+    if int(d["n_param"]) != N_PARAM or str(d["layout"]) != "H32-NF4-NL3-v1":
+        raise ValueError(f"{path}: parameter layout does not match this build")
+    return np.asarray(d["params"], np.float32)
+
+
+def simple_systems(size: int, n_mesh: int, per_mesh: int, seed: int = 0):
+    """Yield (mesh, pressure-correction FaceMatrix, rhs) as the SIMPLE loop
+    would assemble them: per mesh, per_mesh flow states (lid velocity,
+    flow development)."""
+    rng = np.random.default_rng(seed)
+    for k in range(n_mesh):
+        jit = float(rng.uniform(0.0, 0.25))
+        m = Mesh.hex(size, jitter=jit, seed=seed * 1000 + k, permute=True)
+        m.renumber(Mesh.RCM)
+        for j in range(per_mesh):
+            lid = float(np.exp(rng.uniform(np.log(0.1), np.log(2.0))))
+            # flow development within the outer loop: scale of the field
+            dev = float(rng.uniform(0.2, 1.0))
+            u = cavity_field(m, lid * dev)
+            M, _, _ = momentum_field(m, u, u_lid=lid, mu=1e-3, urf=0.7)
+            P = pressure_correction(m, M.pl, pin=1)
+            b = poisson_rhs(P.n_cell, seed * 100000 + k * 1000 + j)
+            yield m, P, b
+
+
+def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=150):
+    """Residuals r_k = b - A x_k of Jacobi-PCG after k iterations."""
+    N = b_dev.shape[0]
+    phi = torch.zeros(N, dtype=torch.float64, device=b_dev.device)
+    res0 = torch.empty_like(b_dev)
+    y = torch.empty_like(b_dev)
+    out = [b_dev.clone()]
+    ks = sorted(rng.integers(1, max_k, n_samples - 1).tolist())
+    for k in ks:
+        phi.zero_()
+        res0.copy_(b_dev)
+        s.solv_cg_dev(0, 1e-300, int(k), 1, phi.data_ptr(), res0.data_ptr())
+        s.spmv_dev(phi.data_ptr(), y.data_ptr())
+        out.append(b_dev - y)
+    return out
+
+
+def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
+          init=None, log_every=50, device=0):
+    import torch
+    s = GpuSolver(device)
+    p = init_params(seed) if init is None else np.asarray(init, np.float32)
+    s.gnn_set_params(p)
+    rng = np.random.default_rng(seed + 7)
+    dev = torch.device("cuda", device)
+    hist = []
+    t0 = time.time()
+    step = 0
+    for ep in range(epochs):
+        last_mesh = None
+        for m, P, b in simple_systems(size, n_mesh, per_mesh, seed=seed + ep):
+            if m is not last_mesh:
+                s.matrix_set(P)
+                last_mesh = m
+            else:
+                s.matrix_values(P.p, P.n, P.pl)
+            b_dev = torch.from_numpy(b).to(dev)
+            rs = _residual_samples(s, b_dev, samples, rng, torch)
+            loss = 0.0
+            for k, r in enumerate(rs):
+                loss += s.gnn_grad_dev(r.data_ptr(), accumulate=k > 0)
+            s.gnn_adam(lr, 1.0 / len(rs))
+            step += 1
+            hist.append(loss / len(rs))
+            if log_every and step % log_every == 0:
+                print(json.dumps({"step": step, "loss": float(np.mean(hist[-log_every:])),
+                                  "t": round(time.time() - t0, 1)}), flush=True)
+    p = s.gnn_get_params()
+    s.close()
+    return p, hist
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--size", type=int, default=64)
+    ap.add_argument("--meshes", type=int, default=40)
+    ap.add_argument("--per-mesh", type=int, default=50)
+    ap.add_argument("--samples", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=1)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--resume", default=None)
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    a = ap.parse_args(argv)
+    init = load_params(a.resume) if a.resume else None
+    t = time.time()
+    p, hist = train(a.size, a.meshes, a.per_mesh, a.samples, a.epochs, a.lr, a.seed, init)
+    meta = {"size": a.size, "systems": a.meshes * a.per_mesh * a.epochs, "samples": a.samples,
+            "lr": a.lr, "seed": a.seed, "first_loss": float(np.mean(hist[:20])),
+            "last_loss": float(np.mean(hist[-20:])), "train_s": round(time.time() - t, 1)}
+    save_params(a.out, p, meta)
+    print(json.dumps(meta))
+
+
+if __name__ == "__main__":
+    main()

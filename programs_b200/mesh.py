@@ -42,6 +42,12 @@ def _lib():
         lib.fvm_assemble_momentum.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
                                               ctypes.c_double, _f64p, _f64p, _f64p]
         lib.fvm_uniform.argtypes = [ctypes.c_uint64, ctypes.c_int64, _f64p]
+        lib.fvm_cavity_field.argtypes = [ctypes.c_void_p, ctypes.c_double, _f64p]
+        lib.fvm_assemble_momentum_field.argtypes = [
+            ctypes.c_void_p, _f64p, _f64p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+            ctypes.c_double, _f64p, _f64p, _f64p, _f64p, _f64p]
+        lib.fvm_assemble_pressure_correction.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_double,
+                                                         ctypes.c_int, _f64p, _f64p, _f64p]
         lib._typed = True
     return lib
 
@@ -176,6 +182,41 @@ class Mesh:
         dt = self._lib.fvm_assemble_momentum(self._h, gamma, pe_max, cfl, _p(p, _f64p),
                                              _p(n, _f64p), _p(pl, _f64p))
         return FaceMatrix(N, ip, inb, p, n, pl), dt
+
+
+def cavity_field(mesh: "Mesh", u_lid: float) -> np.ndarray:
+    """A divergence-free cavity-like velocity field (n_cell, 3)."""
+    u = np.empty((mesh.n_cell, 3))
+    _lib().fvm_cavity_field(mesh._h, u_lid, _p(u, _f64p))
+    return u
+
+
+def momentum_field(mesh: "Mesh", u: np.ndarray, flux=None, rho=1.0, mu=1e-3, u_lid=1.0,
+                   urf=0.7):
+    """Momentum matrix for velocity field u (cfd_setup.f90:324-330, 517-518).
+    Returns (FaceMatrix, rhs (n_cell, 3), face fluxes)."""
+    ip, inb = mesh.faces()
+    F, N = ip.shape[0], mesh.n_cell
+    u = np.ascontiguousarray(u, np.float64)
+    p, n, pl = np.empty(F), np.empty(F), np.empty(N)
+    rhs = np.empty((N, 3))
+    fo = np.empty(F)
+    fl = None if flux is None else _p(np.ascontiguousarray(flux, np.float64), _f64p)
+    _lib().fvm_assemble_momentum_field(mesh._h, _p(u, _f64p), fl, rho, mu, u_lid, urf,
+                                       _p(p, _f64p), _p(n, _f64p), _p(pl, _f64p),
+                                       _p(rhs, _f64p), _p(fo, _f64p))
+    return FaceMatrix(N, ip, inb, p, n, pl), rhs, fo
+
+
+def pressure_correction(mesh: "Mesh", ap: np.ndarray, rho=1.0, pin=1) -> FaceMatrix:
+    """Pressure-correction matrix from the momentum diagonal (cfd_setup.f90:604-634)."""
+    ip, inb = mesh.faces()
+    F, N = ip.shape[0], mesh.n_cell
+    ap = np.ascontiguousarray(ap, np.float64)
+    p, n, pl = np.empty(F), np.empty(F), np.empty(N)
+    _lib().fvm_assemble_pressure_correction(mesh._h, _p(ap, _f64p), rho, pin, _p(p, _f64p),
+                                            _p(n, _f64p), _p(pl, _f64p))
+    return FaceMatrix(N, ip, inb, p, n, pl)
 
 
 def uniform(seed: int, count: int) -> np.ndarray:

@@ -39,14 +39,15 @@ class Stats(ctypes.Structure):
                 ("ratio", ctypes.c_double * MAX_VC), ("status", ctypes.c_int),
                 ("n_levels", ctypes.c_int), ("refinements", ctypes.c_int),
                 ("graph_launches", ctypes.c_int), ("kernel_launches", ctypes.c_int),
-                ("solve_ms", ctypes.c_double)]
+                ("solve_ms", ctypes.c_double), ("fallbacks", ctypes.c_int)]
 
     def as_dict(self):
         V = self.n_vc
         return {"iters": list(self.iters[:V]), "ratio": list(self.ratio[:V]),
                 "status": self.status, "n_levels": self.n_levels,
                 "refinements": self.refinements, "graph_launches": self.graph_launches,
-                "kernel_launches": self.kernel_launches, "solve_ms": self.solve_ms}
+                "kernel_launches": self.kernel_launches, "solve_ms": self.solve_ms,
+                "fallbacks": self.fallbacks}
 
 
 class Tune(ctypes.Structure):
@@ -64,6 +65,9 @@ EXPORTS = [
     "solv_gpu_bicg", "solv_gpu_cg_dev", "solv_gpu_bicg_dev", "solv_gpu_spmv_dev",
     "solv_gpu_matrix_set_batch", "solv_gpu_n_systems", "solv_gpu_cg_batch", "solv_gpu_bicg_batch",
     "solv_gpu_cg_batch_dev", "solv_gpu_bicg_batch_dev", "solv_gpu_autotune",
+    "solv_gpu_fcg", "solv_gpu_fcg_dev", "solv_gpu_gnn_n_params", "solv_gpu_gnn_set_params",
+    "solv_gpu_gnn_get_params", "solv_gpu_gnn_forward_dev", "solv_gpu_gnn_grad_dev",
+    "solv_gpu_gnn_get_grad", "solv_gpu_gnn_zero_grad", "solv_gpu_gnn_adam",
     "solv_gpu_create_", "solv_gpu_destroy_", "solv_gpu_matrix_set_", "solv_gpu_matrix_values_",
     "solv_gpu_res_", "solv_gpu_precond_", "solv_gpu_direct_", "solv_gpu_cg_", "solv_gpu_bicg_",
 ]
@@ -102,6 +106,19 @@ def lib():
     L.solv_gpu_n_systems.argtypes = [vp]
     L.solv_gpu_autotune.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                     ctypes.POINTER(Tune)]
+    L.solv_gpu_fcg.argtypes = [vp, ctypes.c_double, ctypes.c_int, _f64p, _f64p, _f64p,
+                               ctypes.c_int, ctypes.POINTER(Stats)]
+    L.solv_gpu_fcg_dev.argtypes = [vp, ctypes.c_double, ctypes.c_int, vp, vp, _f64p,
+                                   ctypes.c_int, ctypes.POINTER(Stats)]
+    L.solv_gpu_gnn_n_params.argtypes = []
+    _f32p = ctypes.POINTER(ctypes.c_float)
+    L.solv_gpu_gnn_set_params.argtypes = [vp, _f32p, ctypes.c_int]
+    L.solv_gpu_gnn_get_params.argtypes = [vp, _f32p, ctypes.c_int]
+    L.solv_gpu_gnn_get_grad.argtypes = [vp, _f32p, ctypes.c_int]
+    L.solv_gpu_gnn_zero_grad.argtypes = [vp]
+    L.solv_gpu_gnn_forward_dev.argtypes = [vp, vp, vp, ctypes.c_int]
+    L.solv_gpu_gnn_grad_dev.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    L.solv_gpu_gnn_adam.argtypes = [vp, ctypes.c_float, ctypes.c_float]
     for fn in (L.solv_gpu_cg_batch, L.solv_gpu_bicg_batch):
         fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _f64p,
                        _f64p, _f64p, ctypes.c_int, _i32p, _f64p, ctypes.POINTER(Stats)]
@@ -257,6 +274,60 @@ class GpuSolver:
     def solv_bicg_dev(self, imat, reduc, n_iter, n_vc, phi_ptr, res0_ptr, not_r0=False):
         return self._solve_dev(self._lib.solv_gpu_bicg_dev, imat, reduc, n_iter, n_vc, phi_ptr,
                                res0_ptr, not_r0)
+
+    # -- learned preconditioner --------------------------------------------------
+    def solv_fcg(self, reduc, n_iter, phi, res0, res0_n, not_r0=False):
+        """Flexible CG with the learned preconditioner (FP32 inner, FP64
+        refinement, plain PCG fallback); arguments as solv_cg minus imat."""
+        phi2 = self._as_phi(phi)
+        self._as_res0(res0)
+        st = Stats()
+        rc = self._lib.solv_gpu_fcg(self._h, float(reduc), int(n_iter), _p(phi2, _f64p),
+                                    _p(res0, _f64p), _p(res0_n, _f64p), int(bool(not_r0)),
+                                    ctypes.byref(st))
+        self._check(rc, allow=(OK, MAXITER))
+        return st.as_dict()
+
+    def solv_fcg_dev(self, reduc, n_iter, phi_ptr, res0_ptr, not_r0=False):
+        res0_n = np.zeros(1)
+        st = Stats()
+        rc = self._lib.solv_gpu_fcg_dev(self._h, float(reduc), int(n_iter), phi_ptr, res0_ptr,
+                                        _p(res0_n, _f64p), int(bool(not_r0)), ctypes.byref(st))
+        self._check(rc, allow=(OK, MAXITER))
+        return res0_n, st.as_dict()
+
+    @staticmethod
+    def gnn_n_params() -> int:
+        return int(lib().solv_gpu_gnn_n_params())
+
+    def gnn_set_params(self, params: np.ndarray) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        self._check(self._lib.solv_gpu_gnn_set_params(
+            self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.shape[0]))
+
+    def gnn_get_params(self) -> np.ndarray:
+        p = np.empty(self.gnn_n_params(), np.float32)
+        self._check(self._lib.solv_gpu_gnn_get_params(
+            self._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), p.shape[0]))
+        return p
+
+    def gnn_get_grad(self) -> np.ndarray:
+        g = np.empty(self.gnn_n_params(), np.float32)
+        self._check(self._lib.solv_gpu_gnn_get_grad(
+            self._h, g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), g.shape[0]))
+        return g
+
+    def gnn_forward_dev(self, r_ptr: int, z_ptr: int, path: int = 0) -> None:
+        self._check(self._lib.solv_gpu_gnn_forward_dev(self._h, r_ptr, z_ptr, path))
+
+    def gnn_grad_dev(self, r_ptr: int, accumulate: bool = False) -> float:
+        loss = ctypes.c_double()
+        self._check(self._lib.solv_gpu_gnn_grad_dev(self._h, r_ptr, ctypes.byref(loss),
+                                                    int(bool(accumulate))))
+        return loss.value
+
+    def gnn_adam(self, lr: float, grad_scale: float = 1.0) -> None:
+        self._check(self._lib.solv_gpu_gnn_adam(self._h, lr, grad_scale))
 
     def autotune(self, solver: str = "cg", imat: int = 0, n_vc: int = 1) -> dict:
         """Pick launch shapes for this matrix (left set on the context)."""
