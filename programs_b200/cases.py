@@ -56,7 +56,9 @@ def main(argv=None):
     ap.add_argument("what", choices=["solve", "spmv", "batch"])
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--system", default="pressure", choices=["pressure", "momentum"])
-    ap.add_argument("--solver", default="cg", choices=["cg", "bicg"])
+    ap.add_argument("--solver", default="cg", choices=["cg", "bicg", "fcg"])
+    ap.add_argument("--weights", default=None, help="learned-preconditioner weights (.npz)")
+    ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--imat", type=int, default=0)
     ap.add_argument("--precision", type=int, default=0)
     ap.add_argument("--n-vc", type=int, default=1)
@@ -97,6 +99,11 @@ def main(argv=None):
         A, b = make_system(a.size, a.system, renumber=a.renumber)
         s.matrix_set(A)
         dev = torch.device("cuda", 0)
+        if a.solver == "fcg":
+            from .learn import DEFAULT_WEIGHTS, load_params
+            s.gnn_set_params(load_params(a.weights or DEFAULT_WEIGHTS))
+        if a.autotune:
+            out["tune"] = s.autotune("cg" if a.solver != "bicg" else "bicg", a.imat, a.n_vc)
         if a.what == "spmv":
             x = torch.from_numpy(uniform(3, A.n_cell)).to(dev)
             y = torch.empty_like(x)
@@ -113,12 +120,16 @@ def main(argv=None):
                 phi.zero_()
                 res0.copy_(bd)
                 torch.cuda.synchronize()
-                fn = s.solv_cg_dev if a.solver == "cg" else s.solv_bicg_dev
-                rn, st = fn(a.imat, 1e-10, 100000, V, phi.data_ptr(), res0.data_ptr())
+                if a.solver == "fcg":
+                    rn, st = s.solv_fcg_dev(1e-10, 100000, phi.data_ptr(), res0.data_ptr())
+                else:
+                    fn = s.solv_cg_dev if a.solver == "cg" else s.solv_bicg_dev
+                    rn, st = fn(a.imat, 1e-10, 100000, V, phi.data_ptr(), res0.data_ptr())
                 ts.append(st["solve_ms"])
             out.update(n_cell=A.n_cell, levels=s.levels, solve_ms=min(ts), iters=st["iters"],
                        ratio=st["ratio"], refinements=st["refinements"],
-                       kernel_launches=st["kernel_launches"], status=st["status"])
+                       kernel_launches=st["kernel_launches"], status=st["status"],
+                       fallbacks=st["fallbacks"])
     s.close()
     print(json.dumps(out))
 

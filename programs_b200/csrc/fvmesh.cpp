@@ -54,8 +54,13 @@ struct fvm_mesh {
   std::vector<V3> xc;              // cell centres
   int n_cell = 0;
   int n_bface = 0;
+  // optional cache of the face geometry (9 doubles per face) and volumes,
+  // for repeated assembly on one mesh (fvm_mesh_cache_geometry)
+  std::vector<double> geo, vol_cache;
 
   void emit_faces() {
+    geo.clear();
+    vol_cache.clear();
     f_ip.clear();
     f_in.clear();
     f_loc.clear();
@@ -88,23 +93,30 @@ struct fvm_mesh {
   // grd_geom.f90:119-147 (3-d branch) and :161-198.
   void face_geom(size_t f, double &s, V3 &nrm, V3 &xf, double &l_pn,
                  double &w_fp) const {
+    if (!geo.empty()) {
+      const double *g = &geo[9 * f];
+      s = g[0];
+      nrm = {g[1], g[2], g[3]};
+      xf = {g[4], g[5], g[6]};
+      l_pn = g[7];
+      w_fp = g[8];
+      return;
+    }
     int c = f_ip[f];
     int k = f_loc[f];
     V3 v[4];
     for (int i = 0; i < 4; ++i) v[i] = vert[cell_vert[(size_t)c * 8 + kHexFaces[k][i]]];
-    V3 acc{0, 0, 0};
-    double area = 0.0;
-    V3 e_prev = v[1] - v[0];
-    for (int i = 2; i < 4; ++i) {
-      V3 e = v[i] - v[0];
-      V3 t = cross(e_prev, e) * 0.5;
-      double a = mag(t);
-      acc = acc + t * (1.0 / a);
-      area += a;
-      e_prev = e;
-    }
-    nrm = acc * (1.0 / 2.0);
-    s = area;
+    // Area vector of the quadrilateral: 1/2 sum v_i x v_{i+1}.  It does not
+    // depend on where a triangulation starts, so a face is the same seen
+    // from either cell and every cell's area vectors sum to zero.  The
+    // reference's fan triangles with averaged unit normals
+    // (grd_geom.f90:127-140) do not close on non-planar (jittered) faces,
+    // which puts a spurious O(jitter/h) gradient on a constant field.
+    V3 A{0, 0, 0};
+    for (int i = 0; i < 4; ++i) A = A + cross(v[i], v[(i + 1) & 3]);
+    A = A * 0.5;
+    s = mag(A);
+    nrm = A * (1.0 / s);
     xf = (v[0] + v[1] + v[2] + v[3]) * 0.25;
     V3 xp_aux = xf - nrm * dot(xf - xc[c], nrm);
     int nb = f_in[f];
@@ -291,9 +303,30 @@ void fvm_mesh_face_geom(const fvm_mesh *m, double *s, double *nrm, double *xf,
   }
 }
 
+void fvm_mesh_cache_geometry(fvm_mesh *m) {
+  const size_t F = m->f_ip.size();
+  std::vector<double> g(9 * F);
+  for (size_t f = 0; f < F; ++f) {
+    double s, l, w;
+    V3 nn, x;
+    m->face_geom(f, s, nn, x, l, w);
+    double *q = &g[9 * f];
+    q[0] = s; q[1] = nn.x; q[2] = nn.y; q[3] = nn.z; q[4] = x.x; q[5] = x.y; q[6] = x.z;
+    q[7] = l; q[8] = w;
+  }
+  std::vector<double> v(m->n_cell);
+  fvm_mesh_cell_geom(m, nullptr, v.data());
+  m->geo.swap(g);
+  m->vol_cache.swap(v);
+}
+
 void fvm_mesh_cell_geom(const fvm_mesh *m, double *xc, double *vol) {
   for (int c = 0; c < m->n_cell; ++c)
     if (xc) { xc[3 * c] = m->xc[c].x; xc[3 * c + 1] = m->xc[c].y; xc[3 * c + 2] = m->xc[c].z; }
+  if (vol && !m->vol_cache.empty()) {
+    std::copy(m->vol_cache.begin(), m->vol_cache.end(), vol);
+    return;
+  }
   if (vol) {
     // Volume of the cell whose faces are split into four triangles about
     // the face centre: tetrahedra from the cell centre to each triangle of
@@ -582,6 +615,102 @@ void fvm_assemble_pressure_correction(const fvm_mesh *m, const double *ap, doubl
     if (a == pc || b == pc) continue;
     p[f] = -d;
     n[f] = -d;
+  }
+}
+
+void fvm_gradient(const fvm_mesh *m, int ncomp, const double *phi, double *grad) {
+  const int N = m->n_cell;
+  const size_t F = m->f_ip.size();
+  std::vector<double> vol(N);
+  fvm_mesh_cell_geom(m, nullptr, vol.data());
+  std::fill(grad, grad + (size_t)3 * ncomp * N, 0.0);
+  for (size_t f = 0; f < F; ++f) {
+    double s, l, w;
+    V3 nn, x;
+    m->face_geom(f, s, nn, x, l, w);
+    const int a = m->f_ip[f], b = m->f_in[f];
+    for (int k = 0; k < ncomp; ++k) {
+      const double pa = phi[(size_t)a * ncomp + k];
+      const double pf = b >= 0 ? w * phi[(size_t)b * ncomp + k] + (1 - w) * pa : pa;
+      double *ga = grad + ((size_t)a * ncomp + k) * 3;
+      ga[0] += pf * s * nn.x;
+      ga[1] += pf * s * nn.y;
+      ga[2] += pf * s * nn.z;
+      if (b >= 0) {
+        double *gb = grad + ((size_t)b * ncomp + k) * 3;
+        gb[0] -= pf * s * nn.x;
+        gb[1] -= pf * s * nn.y;
+        gb[2] -= pf * s * nn.z;
+      }
+    }
+  }
+  for (int c = 0; c < N; ++c)
+    for (int k = 0; k < 3 * ncomp; ++k) grad[(size_t)c * 3 * ncomp + k] /= vol[c];
+}
+
+void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
+                   const double *ap, double rho, double *flux) {
+  const size_t F = m->f_ip.size();
+  std::vector<double> vol(m->n_cell);
+  fvm_mesh_cell_geom(m, nullptr, vol.data());
+  for (size_t f = 0; f < F; ++f) {
+    const int a = m->f_ip[f], b = m->f_in[f];
+    if (b < 0) {
+      flux[f] = 0.0;
+      continue;
+    }
+    double s, l, w;
+    V3 nn, x;
+    m->face_geom(f, s, nn, x, l, w);
+    V3 uf{w * u[3 * b] + (1 - w) * u[3 * a], w * u[3 * b + 1] + (1 - w) * u[3 * a + 1],
+          w * u[3 * b + 2] + (1 - w) * u[3 * a + 2]};
+    const double p_r = w / (ap[b] + 1e-20) + (1 - w) / (ap[a] + 1e-20);
+    const double v = w * vol[b] + (1 - w) * vol[a];
+    const double d = rho * p_r * s * v / l;
+    V3 gf{w * gradp[3 * b] + (1 - w) * gradp[3 * a], w * gradp[3 * b + 1] + (1 - w) * gradp[3 * a + 1],
+          w * gradp[3 * b + 2] + (1 - w) * gradp[3 * a + 2]};
+    const double dp = (p[b] - p[a]) - dot(gf, m->xc[b] - m->xc[a]);
+    flux[f] = rho * s * dot(uf, nn) - d * dp;
+  }
+}
+
+double fvm_mass_imbalance(const fvm_mesh *m, const double *flux, int pin, double *b) {
+  const int N = m->n_cell;
+  const size_t F = m->f_ip.size();
+  for (int c = 0; c < N; ++c) b[c] = 0.0;
+  for (size_t f = 0; f < F; ++f) {
+    const int a = m->f_ip[f], n = m->f_in[f];
+    if (n < 0) continue;
+    b[a] -= flux[f];
+    b[n] += flux[f];
+  }
+  if (pin > 0) b[pin - 1] = 0.0;
+  double t = 0.0;
+  for (int c = 0; c < N; ++c) t += std::fabs(b[c]);
+  return t;
+}
+
+void fvm_simple_correct(const fvm_mesh *m, const double *pp, const double *gradpp,
+                        const double *ap, double rho, double urf_p, double *u, double *p,
+                        double *flux) {
+  const int N = m->n_cell;
+  const size_t F = m->f_ip.size();
+  std::vector<double> vol(N);
+  fvm_mesh_cell_geom(m, nullptr, vol.data());
+  for (int c = 0; c < N; ++c) {
+    p[c] += urf_p * pp[c];
+    const double k = vol[c] / (ap[c] + 1e-20);
+    for (int d = 0; d < 3; ++d) u[3 * c + d] -= k * gradpp[3 * c + d];
+  }
+  for (size_t f = 0; f < F; ++f) {
+    const int a = m->f_ip[f], b = m->f_in[f];
+    if (b < 0) continue;
+    double s, l, w;
+    V3 nn, x;
+    m->face_geom(f, s, nn, x, l, w);
+    const double p_r = w / (ap[b] + 1e-20) + (1 - w) / (ap[a] + 1e-20);
+    const double v = w * vol[b] + (1 - w) * vol[a];
+    flux[f] -= rho * p_r * s * v / l * (pp[b] - pp[a]);
   }
 }
 

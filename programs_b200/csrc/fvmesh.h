@@ -46,6 +46,11 @@ void fvm_mesh_faces(const fvm_mesh *m, int *ip, int *in);
 void fvm_mesh_face_geom(const fvm_mesh *m, double *s, double *nrm, double *xf,
                         double *l_pn, double *w_fp);
 
+/* Keep the face geometry and cell volumes in memory (9 + 1 doubles per
+ * face / cell) so repeated assemblies on one mesh skip the geometry;
+ * dropped by renumbering. */
+void fvm_mesh_cache_geometry(fvm_mesh *m);
+
 /* Cell centres (3 per cell) and volumes (either may be NULL). */
 void fvm_mesh_cell_geom(const fvm_mesh *m, double *xc, double *vol);
 
@@ -99,6 +104,30 @@ void fvm_assemble_pressure_correction(const fvm_mesh *m, const double *ap, doubl
  * function psi = u_lid x^2 (1-x)^2 y^2 (1-y) (scaled so u(0.5,1) = u_lid),
  * u = dpsi/dy, v = -dpsi/dx, modulated by sin(pi z); w = 0. */
 void fvm_cavity_field(const fvm_mesh *m, double u_lid, double *u);
+
+/* -- SIMPLE outer-loop pieces (lid-driven cavity) ------------------------ */
+/* Green-Gauss gradient (solv_grad, cfd_setup.f90:765-866, one sweep):
+ * grad_i = sum_f phi_f area n / V_i, phi_f = w phi_N + (1-w) phi_P inside,
+ * phi_P on walls (zero normal gradient); `ncomp` components per cell,
+ * grad has 3*ncomp per cell. */
+void fvm_gradient(const fvm_mesh *m, int ncomp, const double *phi, double *grad);
+
+/* Face mass fluxes from the momentum-predicted velocity with Rhie-Chow
+ * pressure smoothing (cfd_setup.f90:615-634): F = rho area (u_f . n)
+ * - d ((p_N - p_P) - grad(p)_f . (x_N - x_P)), d = rho (V/a_P)_f area / l_pn;
+ * zero on walls. */
+void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
+                   const double *ap, double rho, double *flux);
+
+/* Mass imbalance right-hand side b_i = -sum of outflow of cell i; cell
+ * `pin` (1-based) gets 0.  Returns sum |b|. */
+double fvm_mass_imbalance(const fvm_mesh *m, const double *flux, int pin, double *b);
+
+/* SIMPLE corrections with the pressure correction pp:
+ * p += urf_p pp; u_i -= (V_i / a_P,i) grad(pp)_i; F -= d (pp_N - pp_P). */
+void fvm_simple_correct(const fvm_mesh *m, const double *pp, const double *gradpp,
+                        const double *ap, double rho, double urf_p, double *u, double *p,
+                        double *flux);
 
 /* Uniform [-1,1) values from std::mt19937_64(seed) (53-bit mantissa). */
 void fvm_uniform(uint64_t seed, int64_t count, double *out);

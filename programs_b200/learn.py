@@ -75,6 +75,7 @@ def simple_systems(size: int, n_mesh: int, per_mesh: int, seed: int = 0):
         jit = float(rng.uniform(0.0, 0.25))
         m = Mesh.hex(size, jitter=jit, seed=seed * 1000 + k, permute=True)
         m.renumber(Mesh.RCM)
+        m.cache_geometry()
         for j in range(per_mesh):
             lid = float(np.exp(rng.uniform(np.log(0.1), np.log(2.0))))
             # flow development within the outer loop: scale of the field

@@ -43,6 +43,14 @@ def _lib():
                                               ctypes.c_double, _f64p, _f64p, _f64p]
         lib.fvm_uniform.argtypes = [ctypes.c_uint64, ctypes.c_int64, _f64p]
         lib.fvm_cavity_field.argtypes = [ctypes.c_void_p, ctypes.c_double, _f64p]
+        lib.fvm_mesh_cache_geometry.argtypes = [ctypes.c_void_p]
+        lib.fvm_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p]
+        lib.fvm_face_flux.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, ctypes.c_double,
+                                      _f64p]
+        lib.fvm_mass_imbalance.restype = ctypes.c_double
+        lib.fvm_mass_imbalance.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int, _f64p]
+        lib.fvm_simple_correct.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, ctypes.c_double,
+                                           ctypes.c_double, _f64p, _f64p, _f64p]
         lib.fvm_assemble_momentum_field.argtypes = [
             ctypes.c_void_p, _f64p, _f64p, ctypes.c_double, ctypes.c_double, ctypes.c_double,
             ctypes.c_double, _f64p, _f64p, _f64p, _f64p, _f64p]
@@ -158,6 +166,10 @@ class Mesh:
             raise ValueError("renumber failed")
         return perm
 
+    def cache_geometry(self) -> None:
+        """Keep face geometry and volumes for repeated assembly on this mesh."""
+        self._lib.fvm_mesh_cache_geometry(self._h)
+
     def permute(self, perm: np.ndarray) -> None:
         """Apply a given permutation (new 1-based index of old cell i)."""
         perm = np.ascontiguousarray(perm, np.int32)
@@ -217,6 +229,43 @@ def pressure_correction(mesh: "Mesh", ap: np.ndarray, rho=1.0, pin=1) -> FaceMat
     _lib().fvm_assemble_pressure_correction(mesh._h, _p(ap, _f64p), rho, pin, _p(p, _f64p),
                                             _p(n, _f64p), _p(pl, _f64p))
     return FaceMatrix(N, ip, inb, p, n, pl)
+
+
+def _c(a):
+    return np.ascontiguousarray(a, np.float64)
+
+
+def gradient(mesh: "Mesh", phi: np.ndarray) -> np.ndarray:
+    """Green-Gauss gradient of a cell field (n_cell,) or (n_cell, k)."""
+    phi = _c(phi)
+    k = 1 if phi.ndim == 1 else phi.shape[1]
+    g = np.empty((mesh.n_cell, k, 3)) if k > 1 else np.empty((mesh.n_cell, 3))
+    _lib().fvm_gradient(mesh._h, k, _p(phi, _f64p), _p(g, _f64p))
+    return g
+
+
+def face_flux(mesh: "Mesh", u, p, gradp, ap, rho=1.0) -> np.ndarray:
+    f = np.empty(mesh.n_face)
+    u, p, gradp, ap = _c(u), _c(p), _c(gradp), _c(ap)
+    _lib().fvm_face_flux(mesh._h, _p(u, _f64p), _p(p, _f64p), _p(gradp, _f64p), _p(ap, _f64p),
+                         rho, _p(f, _f64p))
+    return f
+
+
+def mass_imbalance(mesh: "Mesh", flux, pin=1):
+    b = np.empty(mesh.n_cell)
+    flux = _c(flux)
+    t = _lib().fvm_mass_imbalance(mesh._h, _p(flux, _f64p), pin, _p(b, _f64p))
+    return b, t
+
+
+def simple_correct(mesh: "Mesh", pp, gradpp, ap, rho, urf_p, u, p, flux) -> None:
+    """In place: p += urf_p pp; u -= V/a_P grad pp; flux -= d (pp_N - pp_P)."""
+    for a in (u, p, flux):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    pp, gradpp, ap = _c(pp), _c(gradpp), _c(ap)
+    _lib().fvm_simple_correct(mesh._h, _p(pp, _f64p), _p(gradpp, _f64p), _p(ap, _f64p), rho,
+                              urf_p, _p(u, _f64p), _p(p, _f64p), _p(flux, _f64p))
 
 
 def uniform(seed: int, count: int) -> np.ndarray:

@@ -1,0 +1,135 @@
+"""SIMPLE outer loop for the 3-D lid-driven cavity, with the linear solves
+on the GPU through the C-ABI -- the split the reference has, assembly on
+the host (spray-simulation/cfd_solve.f90:131-179 calling cfd_setup_eqn and
+cfd_setup_pp) and the solver swapped for the B200 one.
+
+Per outer iteration:
+  grad p (Green-Gauss)                              solv_grad, cfd_setup.f90:765
+  momentum: upwind + diffusion, -grad p V, urf_u    cfd_setup.f90:178-518
+  u* = solve (BiCGSTAB + DILU, u, v, w in one call) cfd_setup.f90:528
+  face flux with Rhie-Chow pressure smoothing       cfd_setup.f90:615-634
+  pressure correction: d = rho (V/a_P)_f area/l_pn  cfd_setup.f90:604-646
+  p' = solve (CG, or FCG with the learned preconditioner)   :662
+  p += urf_p p', u -= V/a_P grad p', F -= d dp'     cfd_setup.f90:689-729
+
+  python -m programs_b200.simple --size 32 --outer 200 [--learned]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from .mesh import (Mesh, face_flux, gradient, mass_imbalance, momentum_field,
+                   pressure_correction, simple_correct)
+from .solver import GpuSolver, OPT_PRECISION
+
+
+def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15, seed=0,
+        p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None, p_imat=1,
+        m_precision=0, device=0, log_every=0):
+    """Returns (u (N,3), p (N,), history, timings).  learned: weights array
+    (FCG with the learned preconditioner for the pressure correction) or
+    None (plain FP64 PCG with imat p_imat)."""
+    rho = 1.0
+    mu = rho * u_lid * 1.0 / re
+    m = Mesh.hex(size, jitter=jitter, seed=seed, permute=True)
+    m.renumber(Mesh.RCM)
+    m.cache_geometry()
+    N = m.n_cell
+    _, vol = m.cell_geom()
+    u = np.zeros((N, 3))
+    p = np.zeros(N)
+    F = None
+    sm = GpuSolver(device)
+    sp = GpuSolver(device)
+    sm.set_option(OPT_PRECISION, m_precision)
+    if learned is not None:
+        sp.gnn_set_params(learned)
+    hist = []
+    t_solve_m = t_solve_p = t_asm = 0.0
+    t0 = time.time()
+    for k in range(n_outer):
+        ta = time.time()
+        gradp = gradient(m, p)
+        M, rhs, Fm = momentum_field(m, u, flux=F, rho=rho, mu=mu, u_lid=u_lid, urf=urf_u)
+        if F is None:
+            F = Fm
+        rhs -= gradp * vol[:, None]
+        t_asm += time.time() - ta
+        ts = time.time()
+        if k == 0:
+            sm.matrix_set(M)
+        else:
+            sm.matrix_values(M.p, M.n, M.pl)
+        phi = np.ascontiguousarray(u)
+        res0 = np.asfortranarray(rhs)
+        rn_m = np.zeros(3)
+        stm = sm.solv_bicg(2, m_reduc, m_iter, phi, res0, rn_m)
+        u = phi
+        t_solve_m += time.time() - ts
+        ta = time.time()
+        F = face_flux(m, u, p, gradp, M.pl, rho)
+        P = pressure_correction(m, M.pl, rho=rho, pin=1)
+        b, imb = mass_imbalance(m, F, pin=1)
+        t_asm += time.time() - ta
+        ts = time.time()
+        if k == 0:
+            sp.matrix_set(P)
+        else:
+            sp.matrix_values(P.p, P.n, P.pl)
+        pp = np.zeros((N, 1))
+        res0 = np.asfortranarray(b.reshape(-1, 1))
+        rn_p = np.zeros(1)
+        if learned is not None:
+            stp = sp.solv_fcg(p_reduc, p_iter, pp, res0, rn_p, not_r0=True)
+        else:
+            stp = sp.solv_cg(p_imat, p_reduc, p_iter, pp, res0, rn_p, not_r0=True)
+        t_solve_p += time.time() - ts
+        ta = time.time()
+        gradpp = gradient(m, pp[:, 0])
+        simple_correct(m, pp[:, 0].copy(), gradpp, M.pl, rho, urf_p, u, p, F)
+        t_asm += time.time() - ta
+        rec = {"it": k, "mass": float(imb), "mom_res0": rn_m.tolist(), "p_iters": stp["iters"][0],
+               "m_iters": stm["iters"], "fallbacks": stp.get("fallbacks", 0)}
+        hist.append(rec)
+        if log_every and (k % log_every == 0 or k == n_outer - 1):
+            print(json.dumps(rec), flush=True)
+    sm.close()
+    sp.close()
+    timing = {"total_s": time.time() - t0, "assembly_s": t_asm, "momentum_solve_s": t_solve_m,
+              "pressure_solve_s": t_solve_p, "n_cell": N}
+    return u, p, hist, timing
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--size", type=int, default=32)
+    ap.add_argument("--outer", type=int, default=200)
+    ap.add_argument("--re", type=float, default=1000.0)
+    ap.add_argument("--learned", action="store_true", help="also run learned + mixed FCG and compare")
+    ap.add_argument("--weights", default=None)
+    ap.add_argument("--log-every", type=int, default=20)
+    a = ap.parse_args(argv)
+    u0, p0, h0, t0 = run(a.size, a.outer, a.re, log_every=a.log_every)
+    out = {"size": a.size, "outer": a.outer, "plain": t0, "final_mass_plain": h0[-1]["mass"],
+           "p_iters_plain": int(np.sum([h["p_iters"] for h in h0]))}
+    if a.learned:
+        from .learn import DEFAULT_WEIGHTS, load_params
+        w = load_params(a.weights or DEFAULT_WEIGHTS)
+        u1, p1, h1, t1 = run(a.size, a.outer, a.re, learned=w, log_every=a.log_every)
+        out.update(learned=t1, p_iters_learned=int(np.sum([h["p_iters"] for h in h1])),
+                   fallbacks=int(np.sum([h["fallbacks"] for h in h1])),
+                   rel_l2_u=rel_l2(u1[:, 0], u0[:, 0]), rel_l2_v=rel_l2(u1[:, 1], u0[:, 1]),
+                   rel_l2_w=rel_l2(u1[:, 2], u0[:, 2]), rel_l2_p=rel_l2(p1, p0))
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

@@ -37,9 +37,9 @@ def test_geometry_closes():
     np.add.at(acc, ip - 1, nrm * s[:, None])
     inner = inb > 0
     np.add.at(acc, inb[inner] - 1, -(nrm * s[:, None])[inner])
-    # the reference averages unit normals of the fan triangles (grd_geom.f90:130-140),
-    # so non-planar faces do not close exactly: within 15% of a face area here
-    assert np.abs(acc).max() < 0.15 / 36
+    # exact polygon area vectors close every cell (the reference's averaged
+    # fan normals, grd_geom.f90:127-140, would not on jittered faces)
+    assert np.abs(acc).max() < 1e-14
 
 
 @pytest.mark.parametrize("method", [Mesh.RCM, Mesh.SFC])
