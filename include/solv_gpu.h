@@ -67,6 +67,9 @@ extern "C" {
 #define SOLV_OPT_MAX_REFINE 6   /* cap on refinement sweeps (FP32 mode)    */
 #define SOLV_OPT_INNER_MAX_ITER 7 /* cap on FP32 iterations per refinement
                                    sweep (default 2000)                    */
+#define SOLV_OPT_RELIABLE_DELTA 8 /* FP32 CG: replace the recursive residual
+                                   by the FP64 one each time it has dropped
+                                   by this factor (default 0.1)            */
 
 typedef struct solv_gpu_ctx solv_gpu_ctx;
 
@@ -142,16 +145,18 @@ int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
                       int repeat, float *ms_per_call);
 
 /* -- learned preconditioner ---------------------------------------------- */
-/* No counterpart in the reference.  Flexible CG, FCG(1), whose
- * preconditioner is a 3-layer, width-32 message-passing network over the
- * face graph (BF16 weights, per-cell MLPs on the tensor cores, FP32
- * accumulate), run as the FP32 inner solver of the FP64 refinement loop of
- * SOLV_OPT_PRECISION=1.  If a sweep with the network stalls (the residual
- * does not halve, or p.Ap <= 0), plain Jacobi-PCG takes over from the
- * current iterate for the rest of the solve (stats.fallbacks); the FP64
- * residual test |b - A x|_1 / |r0|_1 < reduc decides convergence either
- * way.  Same argument meaning as solv_gpu_cg with imat ignored, n_vc = 1,
- * one system; the matrix must be symmetric (the pressure system). */
+/* No counterpart in the reference.  Flexible CG, FCG(1), in FP32 with
+ * FP64 reliable updates, preconditioned by M^-1 = D^-1/2 S (I + E) S D^-1/2:
+ * a 3-layer, width-32 message-passing network over the face graph (BF16
+ * weights, per-cell MLPs on the tensor cores, FP32 accumulate) reads the
+ * cell diagonal, the face coefficients and the initial residual once per
+ * solve and emits the per-cell scales S and the symmetric face weights E
+ * (|E| < 1 by construction, so M^-1 is symmetric positive definite).  If
+ * the iteration loses positive curvature or produces NaN, plain Jacobi-PCG
+ * takes over from the current iterate (stats.fallbacks); the FP64 residual
+ * test |b - A x|_1 / |r0|_1 < reduc decides convergence either way.  Same
+ * argument meaning as solv_gpu_cg with imat ignored, n_vc = 1, one system;
+ * the matrix must be symmetric (the pressure system). */
 int solv_gpu_fcg(solv_gpu_ctx *ctx, double reduc, int n_iter, double *phi,
                  double *res0, double *res0_n, int not_r0,
                  solv_gpu_stats *stats);
@@ -162,14 +167,18 @@ int solv_gpu_fcg_dev(solv_gpu_ctx *ctx, double reduc, int n_iter,
 int solv_gpu_gnn_n_params(void);
 int solv_gpu_gnn_set_params(solv_gpu_ctx *ctx, const float *params, int n);
 int solv_gpu_gnn_get_params(solv_gpu_ctx *ctx, float *params, int n);
-/* z = M(r) on the current matrix; r_dev / z_dev caller order, device.
+/* z = M^-1 r with the preconditioner the network builds from r0 (the
+ * solve's initial residual); r0_dev, r_dev, z_dev caller order, device.
  * path 0: inference kernels (BF16, tensor cores); 1: training kernels. */
-int solv_gpu_gnn_forward_dev(solv_gpu_ctx *ctx, const double *r_dev,
-                             double *z_dev, int path);
-/* Training: forward + backward of J = 1/2 z'Az - z'r in the Jacobi-scaled
- * space (minimised by z = A^-1 r) for one residual; gradients add up in an
+int solv_gpu_gnn_forward_dev(solv_gpu_ctx *ctx, const double *r0_dev,
+                             const double *r_dev, double *z_dev, int path);
+/* Training: forward + backward of the energy J = 1/2 z'Âz - z'u, z = K u,
+ * in the Jacobi-scaled space (minimised by K u = Â^-1 u) for the
+ * preconditioner built from r0, averaged over n_samples residuals (each
+ * n_cell long, consecutive, caller order, device); gradients add up in an
  * FP32 accumulator (zeroed first unless accumulate); loss = J / n_cell. */
-int solv_gpu_gnn_grad_dev(solv_gpu_ctx *ctx, const double *r_dev,
+int solv_gpu_gnn_grad_dev(solv_gpu_ctx *ctx, const double *r0_dev,
+                          const double *samples_dev, int n_samples,
                           double *loss, int accumulate);
 int solv_gpu_gnn_get_grad(solv_gpu_ctx *ctx, float *grad, int n);
 int solv_gpu_gnn_zero_grad(solv_gpu_ctx *ctx);

@@ -1,13 +1,13 @@
-"""CPU reference of the learned preconditioner's network and loss
-(TEST INFRASTRUCTURE ONLY: the checker for programs_b200/csrc/gnn.cuh).
+"""CPU reference of the learned preconditioner (TEST INFRASTRUCTURE ONLY:
+the checker for programs_b200/csrc/gnn.cuh).
 
-The reference code base has no learned preconditioner, so this is a
-restatement of the network as specified in gnn.cuh, in float64 on the CPU,
-with BF16 rounding emulated at exactly the points the GPU rounds (weights,
-stored hidden states, aggregated messages) and straight-through gradients
-there, as the GPU backward kernels use.  Gradients come from torch autograd
-on the CPU, an implementation independent of the hand-written backward
-kernels they check.
+The reference code base has no learned preconditioner, so this restates
+the network and preconditioner as specified in gnn.cuh, in float64 on the
+CPU, with BF16 rounding emulated at exactly the points the GPU rounds
+(weights, stored hidden states, aggregated messages) and straight-through
+gradients there, as the GPU backward kernels use.  Gradients come from
+torch autograd on the CPU, an implementation independent of the
+hand-written backward kernels they check.
 """
 from __future__ import annotations
 
@@ -18,9 +18,14 @@ H, NF, NL = 32, 4, 3
 P_WIN = 0
 P_LAYER = H * NF
 LAYER_SZ = 2 * H * H + H
-P_WOUT = P_LAYER + NL * LAYER_SZ
-P_C = P_WOUT + H
-N_PARAM = P_C + 1
+P_WA = P_LAYER + NL * LAYER_SZ
+P_BA = P_WA + H
+P_WE = P_BA + 1
+P_BE = P_WE + H
+N_PARAM = P_BE + 1
+GAMMA = 0.95
+
+ROUND = True  # False: exact float64 network (finite-difference checks)
 
 
 def bf16_round(x: torch.Tensor) -> torch.Tensor:
@@ -31,9 +36,6 @@ def bf16_round(x: torch.Tensor) -> torch.Tensor:
     r = ((bits + 0x7FFF + lsb) & 0xFFFF0000)
     r = torch.where(r >= 2 ** 31, r - 2 ** 32, r).to(torch.int32)
     return r.view(torch.float32).to(x.dtype)
-
-
-ROUND = True  # False: exact float64 network (finite-difference checks)
 
 
 def bf(x: torch.Tensor) -> torch.Tensor:
@@ -63,16 +65,21 @@ def features(A):
             rows, cols, w)
 
 
-def forward(A, r, params, grad=False):
-    """z = M(r) and the per-cell energy loss J/N; returns (z, loss, params_tensor)."""
+def _scaled(r, rsd):
+    """u = r rsd / s (float32 as the GPU), s = mean |r| rsd."""
+    r32 = np.asarray(r, np.float64).astype(np.float32)
+    s = float(np.sum(np.abs(r32.astype(np.float64)) * rsd.astype(np.float64)) / r32.shape[0])
+    return (r32 * rsd * np.float32(1.0 / s)).astype(np.float32), s
+
+
+def build(A, r0, params, grad=False):
+    """The preconditioner the network builds from r0: (s, gE per directed
+    edge, edge arrays, params tensor, features)."""
     rsd, frs, fdeg, rows, cols, w = features(A)
     N = A.n_cell
-    r32 = np.asarray(r, np.float64).astype(np.float32)
-    s = float(np.sum(np.abs(r32.astype(np.float64)) * rsd.astype(np.float64)) / N)
-    inv_s = np.float32(1.0 / s)
-    u = (r32 * rsd * inv_s).astype(np.float32)
+    u0, _ = _scaled(r0, rsd)
     P = torch.tensor(np.asarray(params, np.float64), requires_grad=grad)
-    ut = torch.tensor(u, dtype=torch.float64)
+    ut = torch.tensor(u0, dtype=torch.float64)
     x = torch.stack([ut, torch.tensor(frs, dtype=torch.float64),
                      torch.tensor(fdeg, dtype=torch.float64), torch.ones(N, dtype=torch.float64)], 1)
     rows_t, cols_t = torch.tensor(rows), torch.tensor(cols)
@@ -93,14 +100,46 @@ def forward(A, r, params, grad=False):
         agg = bf(adj(h))
         pre = h @ Ws.T + agg @ Wn.T + b
         h = bf(h + torch.relu(pre))
-    out = bf(P[P_C]) * ut + h @ bf(P[P_WOUT:P_WOUT + H])
-    aout = out - adj(out[:, None])[:, 0]
-    J = (0.5 * out @ aout - out @ ut) / N
-    z = out.detach().numpy() * s * rsd.astype(np.float64)
-    return z, J, P
+    pa = h @ bf(P[P_WA:P_WA + H]) + bf(P[P_BA])
+    s = torch.sqrt(torch.nn.functional.softplus(pa) / np.log(2.0))
+    he = h @ bf(P[P_WE:P_WE + H])
+    pre_e = 0.5 * (he[rows_t] + he[cols_t]) + bf(P[P_BE])
+    gE = GAMMA * torch.tanh(pre_e) * wt
+    return s, gE, rows_t, cols_t, wt, P, rsd
 
 
-def loss_and_grad(A, r, params):
-    _, J, P = forward(A, r, params, grad=True)
+def _apply(q, gE, rows_t, cols_t, v):
+    """q (v q + E (q v)) with E given per directed edge."""
+    y = q * v
+    t = y.clone()
+    t.index_add_(0, rows_t, gE * y[cols_t])
+    return q * t
+
+
+def precondition(A, r0, r, params):
+    """z = M^-1 r in the caller's space (float64 result)."""
+    s, gE, rows_t, cols_t, wt, _, rsd = build(A, r0, params)
+    q = s.detach() * torch.tensor(rsd, dtype=torch.float64)
+    rt = torch.tensor(np.asarray(r, np.float64).astype(np.float32), dtype=torch.float64)
+    return _apply(q, gE.detach(), rows_t, cols_t, rt).numpy()
+
+
+def loss(A, r0, samples, params, grad=False):
+    """Mean over samples of J/N, J = 1/2 z.Â z - z.u, z = K u (scaled space)."""
+    s, gE, rows_t, cols_t, wt, P, rsd = build(A, r0, params, grad=grad)
+    N = A.n_cell
+    J = 0.0
+    for r in samples:
+        u, _ = _scaled(r, rsd)
+        ut = torch.tensor(u, dtype=torch.float64)
+        z = _apply(s, gE, rows_t, cols_t, ut)
+        az = z.clone()
+        az.index_add_(0, rows_t, -wt * z[cols_t])
+        J = J + (0.5 * z @ az - z @ ut) / N
+    return J / len(samples), P
+
+
+def loss_and_grad(A, r0, samples, params):
+    J, P = loss(A, r0, samples, params, grad=True)
     J.backward()
     return float(J.detach()), P.grad.numpy().copy()

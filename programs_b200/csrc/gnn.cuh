@@ -1,26 +1,34 @@
 // gnn.cuh -- learned preconditioner: a message-passing network over the
-// face graph of the pressure matrix, applied to the residual inside
-// flexible CG.
+// face graph of the (symmetric) pressure matrix that builds, once per solve,
+// a symmetric positive definite preconditioner applied in flexible CG.
 //
 // Scaled system: D = diag(A), Â = D^-1/2 A D^-1/2 (unit diagonal), edge
-// weight w_ij = -Â_ij.  Per application, with u_i = r_i / (sqrt(d_i) s),
-// s = sum_i |r_i|/sqrt(d_i) / N (scale of the residual):
-//   h0_i   = relu(W_in x_i),        x_i = [u_i, rowsum_i/d_i, deg_i/6, 1]
-//   agg_i  = sum_j w_ij h^l_j                       (gather over the row)
+// weight w_ij = -Â_ij (w_ij = w_ji).  Network (width 32, 3 layers), inputs
+// per cell x_i = [u0_i, rowsum_i/d_i, deg_i/6, 1] with u0 the initial
+// residual scaled by D^-1/2 and by its mean magnitude:
+//   h0_i      = relu(W_in x_i)
+//   agg_i     = sum_j w_ij h^l_j                          (gather over the row)
 //   h^{l+1}_i = h^l_i + relu(W_s h^l_i + W_n agg_i + b^l),  l = 0, 1, 2
-//   out_i  = c u_i + w_out . h3_i
-//   z_i    = s out_i / sqrt(d_i)
-// so z scales with r, and with the network's correction zeroed
-// (w_out = 0, c = 1) z is the Jacobi step D^-1 r.  Width 32, 3 layers.
+// Heads (per cell, then per face):
+//   s_i   = sqrt(softplus(w_a . h3_i + b_a) / softplus(0)) (diagonal scale > 0)
+//   e_ij  = gamma tanh((w_e . h3_i + w_e . h3_j)/2 + b_e)  (symmetric in i, j)
+// Preconditioner, linear in the residual:
+//   M^-1 = D^-1/2 S (I + E) S D^-1/2,  S = diag(s),  E_ij = e_ij w_ij
+// E is symmetric and, since sum_j w_ij <= 1 on these M-matrices and
+// gamma < 1, I + E is diagonally dominant: M^-1 is symmetric positive
+// definite for any weights, so CG keeps its optimality.  With w_a = w_e = 0,
+// b_a = b_e = 0 it is exactly the Jacobi step D^-1.
+// Applying it costs one gather over the rows per Krylov iteration:
+//   z_i = q_i (q_i r_i + sum_j gE_ij q_j r_j),  q = S D^-1/2 r,  gE = E.
 //
 // Inference: weights and hidden states in BF16, the per-cell MLP of each
 // layer ([h | agg] (64) x W (64x32)) on the tensor cores with FP32
 // accumulate (mma.sync m16n8k16, 16 cells per warp).
 // Training: FP32 CUDA-core kernels that round weights and stored hidden
-// states to BF16 exactly where inference does, save the activations, and
-// back-propagate the energy loss J = 1/2 out^T Â out - out^T u (its
-// minimiser is out = Â^-1 u, i.e. z = A^-1 r); gradients are accumulated
-// in FP32 and applied by Adam.
+// states to BF16 where inference does; the loss is the energy of the
+// preconditioned step in the scaled space, J = 1/2 z.Â z - z.u with z = K u
+// (K = S (I+E) S), minimised by K u = Â^-1 u, averaged over residual
+// samples u of the same system.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -32,13 +40,16 @@ constexpr int H = 32;  // width
 constexpr int NF = 4;  // input features
 constexpr int NL = 3;  // message-passing layers
 // parameter vector (FP32 master copy)
-constexpr int P_WIN = 0;                       // [H][NF]
-constexpr int P_LAYER = H * NF;                // per layer: Ws[H][H], Wn[H][H], b[H]
+constexpr int P_WIN = 0;                         // [H][NF]
+constexpr int P_LAYER = H * NF;                  // per layer: Ws[H][H], Wn[H][H], b[H]
 constexpr int LAYER_SZ = 2 * H * H + H;
-constexpr int P_WOUT = P_LAYER + NL * LAYER_SZ;  // [H]
-constexpr int P_C = P_WOUT + H;                  // scalar skip weight
-constexpr int N_PARAM = P_C + 1;
+constexpr int P_WA = P_LAYER + NL * LAYER_SZ;    // [H] diagonal-scale head
+constexpr int P_BA = P_WA + H;                   // scalar
+constexpr int P_WE = P_BA + 1;                   // [H] face head
+constexpr int P_BE = P_WE + H;                   // scalar
+constexpr int N_PARAM = P_BE + 1;
 constexpr int N_PARAM_PAD = (N_PARAM + 7) & ~7;
+constexpr float kGamma = 0.95f;
 
 // Per-matrix features, internal cell order.
 struct Feat {
@@ -49,6 +60,8 @@ struct Feat {
 };
 
 __device__ __forceinline__ float bf(float x) { return __bfloat162float(__float2bfloat16(x)); }
+__device__ __forceinline__ float softplus(float x) { return x > 20.f ? x : log1pf(expf(x)); }
+__device__ __forceinline__ float sigmoid(float x) { return 1.0f / (1.0f + expf(-x)); }
 
 // ---- features ------------------------------------------------------------------
 __global__ void k_gnn_features(int n, sg::Rows<double> R, float* __restrict__ rsd,
@@ -91,13 +104,12 @@ __global__ void k_gnn_pack(const float* __restrict__ P, __nv_bfloat16* __restric
   wcat[t] = __float2bfloat16(w);
 }
 
-// ---- inference ---------------------------------------------------------------
-// Encoder: one warp per cell, lane = channel.  u from r (any precision).
+// ---- network ------------------------------------------------------------------
+// Encoder: one warp per cell, lane = channel; u = r rsd / gs (gs in lane 0).
 template <typename T>
 __global__ void k_gnn_enc(int n, Feat F, const T* __restrict__ r, const float* __restrict__ P,
                           const sg::Lane* __restrict__ lanes, __nv_bfloat16* __restrict__ h0,
-                          float* __restrict__ u_out, const int* __restrict__ n_active) {
-  if (n_active && *n_active == 0) return;
+                          float* __restrict__ u_out) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
   const double scale = lanes[0].gs > 0 ? lanes[0].gs : 1.0;  // sum |r| rsd / N
@@ -137,8 +149,7 @@ constexpr int TC_WARPS = 4;
 __global__ void __launch_bounds__(TC_WARPS * 32)
 k_gnn_layer_tc(int n, sg::Rows<float> R, Feat F, const __nv_bfloat16* __restrict__ hin,
                __nv_bfloat16* __restrict__ hout, const __nv_bfloat16* __restrict__ wcat,
-               const float* __restrict__ bias, const int* __restrict__ n_active) {
-  if (n_active && *n_active == 0) return;
+               const float* __restrict__ bias) {
   __shared__ __nv_bfloat16 sB[2 * H][H + 8];
   __shared__ __nv_bfloat16 sA[TC_WARPS][TC_CELLS][2 * H + 8];
   __shared__ float sbias[H];
@@ -205,6 +216,74 @@ k_gnn_layer_tc(int n, sg::Rows<float> R, Feat F, const __nv_bfloat16* __restrict
   }
 }
 
+// Heads, per cell (one warp per cell): pa = w_a.h3 + b_a, s = sqrt(softplus(pa)),
+// he = w_e.h3; q = s * qscale_i (qscale = rsd for the preconditioner, NULL = 1).
+template <typename HT>
+__global__ void k_gnn_heads(int n, const HT* __restrict__ h3, const float* __restrict__ P,
+                            const float* __restrict__ qscale, float* __restrict__ pa_out,
+                            float* __restrict__ s_out, float* __restrict__ he_out) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const float wa = bf(P[P_WA + lane]), we = bf(P[P_WE + lane]), ba = bf(P[P_BA]);
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    const float h = (float)h3[(size_t)i * H + lane];
+    float a = wa * h, e = we * h;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      e += __shfl_xor_sync(0xffffffffu, e, o);
+    }
+    if (lane == 0) {
+      const float pa = a + ba;
+      const float s = sqrtf(softplus(pa) / softplus(0.0f));  // exactly 1 untrained
+      if (pa_out) pa_out[i] = pa;
+      s_out[i] = qscale ? s * qscale[i] : s;
+      he_out[i] = e;
+    }
+  }
+}
+
+// Face weights per sliced-ELL slot: gE = gamma tanh((he_i + he_j)/2 + b_e) w_ij.
+__global__ void k_gnn_edges(int n, sg::Rows<float> R, Feat F, const float* __restrict__ he,
+                            const float* __restrict__ P, float* __restrict__ epre,
+                            float* __restrict__ gE) {
+  const float be = bf(P[P_BE]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    sg::RowIt<float> it(R, i);
+    const float hi = he[i];
+    for (int k = 0; k < it.w; ++k) {
+      const int e = it.base + k * sg::kWarp;
+      const int j = R.col[e];
+      float g = 0.0f;
+      if (j >= 0) {
+        const float pre = 0.5f * (hi + he[j]) + be;
+        if (epre) epre[e] = pre;
+        g = kGamma * tanhf(pre) * F.gw[e];
+      }
+      gE[e] = g;
+    }
+  }
+}
+
+// z = q (q r + E (q r)): the preconditioner application (one row gather).
+template <typename T>
+__global__ void k_gnn_apply(int n, sg::Rows<float> R, const float* __restrict__ gE,
+                            const float* __restrict__ q, const T* __restrict__ r,
+                            T* __restrict__ z, const int* __restrict__ n_active) {
+  if (n_active && *n_active == 0) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    sg::RowIt<float> it(R, i);
+    const float qi = q[i];
+    float t = qi * (float)r[i];
+    for (int k = 0; k < it.w; ++k) {
+      const int e = it.base + k * sg::kWarp;
+      const int j = R.col[e];
+      if (j >= 0) t += gE[e] * q[j] * (float)r[j];
+    }
+    z[i] = (T)(qi * t);
+  }
+}
+
 // ---- training (FP32 CUDA cores, BF16 rounding where inference rounds) ------------
 // Encoder with saved pre-activations.  Thread per (cell, channel).
 __global__ void k_gnn_enc_train(int n, Feat F, const float* __restrict__ u,
@@ -264,57 +343,21 @@ k_gnn_layer_train(int n, sg::Rows<float> R, Feat F, const float* __restrict__ hi
   }
 }
 
-// Decoder (training and inference share it): out = c u + w_out . h3; one
-// warp per cell.  Training passes float h3; inference BF16.
-template <typename HT>
-__global__ void k_gnn_dec_out(int n, const HT* __restrict__ h3, const float* __restrict__ u,
-                              const float* __restrict__ P, float* __restrict__ out) {
-  const int lane = threadIdx.x & 31;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  const float wo = bf(P[P_WOUT + lane]), c = bf(P[P_C]);
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
-    float v = wo * (float)h3[(size_t)i * H + lane];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) out[i] = c * u[i] + v;
-  }
-}
-
-// Inference decoder: out as above, then z_i = s out_i / sqrt(d_i).
-template <typename T>
-__global__ void k_gnn_dec_z(int n, Feat F, const __nv_bfloat16* __restrict__ h3,
-                            const float* __restrict__ u, const float* __restrict__ P,
-                            const sg::Lane* __restrict__ lanes, T* __restrict__ z,
-                            const int* __restrict__ n_active) {
-  if (n_active && *n_active == 0) return;
-  const int lane = threadIdx.x & 31;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  const float wo = bf(P[P_WOUT + lane]), c = bf(P[P_C]);
-  const double scale = lanes[0].gs > 0 ? lanes[0].gs : 1.0;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
-    float v = wo * __bfloat162float(h3[(size_t)i * H + lane]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) z[i] = (T)((double)(c * u[i] + v) * scale * F.rsd[i]);
-  }
-}
-
-// Energy loss pieces: g = Â out - u (= dJ/dout) and J = 1/2 out.Â out - out.u
-// (block partials, summed on the host side by the caller's reduction).
-__global__ void k_gnn_loss_grad(int n, sg::Rows<float> R, Feat F, const float* __restrict__ out,
+// Energy loss of one sample: g = Â z - u (= dJ/dz), J = 1/2 z.Â z - z.u.
+__global__ void k_gnn_loss_grad(int n, sg::Rows<float> R, Feat F, const float* __restrict__ z,
                                 const float* __restrict__ u, float* __restrict__ g,
                                 double* __restrict__ jsum) {
   double acc = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     sg::RowIt<float> it(R, i);
-    float aout = out[i];  // unit diagonal
+    float az = z[i];  // unit diagonal
     for (int k = 0; k < it.w; ++k) {
       const int e = it.base + k * sg::kWarp;
       const int j = R.col[e];
-      if (j >= 0) aout -= F.gw[e] * out[j];
+      if (j >= 0) az -= F.gw[e] * z[j];
     }
-    g[i] = aout - u[i];
-    acc += 0.5 * (double)out[i] * aout - (double)out[i] * u[i];
+    g[i] = az - u[i];
+    acc += 0.5 * (double)z[i] * az - (double)z[i] * u[i];
   }
   acc = sg::warp_sum(acc);
   __shared__ double sh[32];
@@ -327,23 +370,73 @@ __global__ void k_gnn_loss_grad(int n, sg::Rows<float> R, Feat F, const float* _
   }
 }
 
-// Decoder backward: dout (= g * scale) -> dW_out, dc, dh3.
-__global__ void k_gnn_dec_back(int n, const float* __restrict__ h3, const float* __restrict__ u,
-                               const float* __restrict__ dout, float gsc,
-                               const float* __restrict__ P, float* __restrict__ dh3,
-                               float* __restrict__ G) {
+// Backward through z = S (I + E) S u for one sample (S = diag(s)):
+//   y = s u, dt = s g, t = y + E y, dy = dt + E dt,
+//   ds_i  += g_i t_i + dy_i u_i
+//   esum_i += sum_j (dt_i y_j + dt_j y_i) gamma w_ij sech^2(pre_ij)
+// (esum_i is the derivative w.r.t. the face pre-activations touching i).
+__global__ void k_gnn_apply_back1(int n, const float* __restrict__ s, const float* __restrict__ u,
+                                  const float* __restrict__ g, float* __restrict__ y,
+                                  float* __restrict__ dt) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    y[i] = s[i] * u[i];
+    dt[i] = s[i] * g[i];
+  }
+}
+__global__ void k_gnn_apply_back2(int n, sg::Rows<float> R, Feat F, const float* __restrict__ gE,
+                                  const float* __restrict__ epre, const float* __restrict__ u,
+                                  const float* __restrict__ g, const float* __restrict__ y,
+                                  const float* __restrict__ dt, float* __restrict__ ds,
+                                  float* __restrict__ esum) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    sg::RowIt<float> it(R, i);
+    float t = y[i], edt = 0.0f, es = 0.0f;
+    const float dti = dt[i], yi = y[i];
+    for (int k = 0; k < it.w; ++k) {
+      const int e = it.base + k * sg::kWarp;
+      const int j = R.col[e];
+      if (j >= 0) {
+        t += gE[e] * y[j];
+        edt += gE[e] * dt[j];
+        const float th = tanhf(epre[e]);
+        es += (dti * y[j] + dt[j] * yi) * kGamma * F.gw[e] * (1.0f - th * th);
+      }
+    }
+    ds[i] += g[i] * t + (dti + edt) * u[i];
+    esum[i] += es;
+  }
+}
+
+// Heads backward (one warp per cell): from ds (w.r.t. s) and esum,
+// dpa = ds sigmoid(pa) / (2 s), dhe = esum / 2, dh3 = dpa w_a + dhe w_e,
+// and the head parameter gradients.  gsc scales everything (1/(N samples)).
+__global__ void k_gnn_heads_back(int n, const float* __restrict__ h3, const float* __restrict__ pa,
+                                 const float* __restrict__ s, const float* __restrict__ ds,
+                                 const float* __restrict__ esum, float gsc,
+                                 const float* __restrict__ P, float* __restrict__ dh3,
+                                 float* __restrict__ G) {
   const int lane = threadIdx.x & 31;
   const int warps = (gridDim.x * blockDim.x) >> 5;
-  const float wo = bf(P[P_WOUT + lane]);
-  float gw = 0.0f, gc = 0.0f;
+  const float wa = bf(P[P_WA + lane]), we = bf(P[P_WE + lane]);
+  float gwa = 0.f, gwe = 0.f, gba = 0.f, gbe = 0.f;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
-    const float d = dout[i] * gsc;
-    gw += d * h3[(size_t)i * H + lane];
-    if (lane == 0) gc += d * u[i];
-    dh3[(size_t)i * H + lane] = d * wo;
+    const float dpa = ds[i] * gsc * sigmoid(pa[i]) / (2.0f * s[i] * softplus(0.0f));
+    const float dhe = 0.5f * esum[i] * gsc;
+    const float h = h3[(size_t)i * H + lane];
+    dh3[(size_t)i * H + lane] = dpa * wa + dhe * we;
+    gwa += dpa * h;
+    gwe += dhe * h;
+    if (lane == 0) {
+      gba += dpa;
+      gbe += dhe;  // d/d b_e = sum over faces = 1/2 sum_i esum_i
+    }
   }
-  atomicAdd(&G[P_WOUT + lane], gw);
-  if (lane == 0) atomicAdd(&G[P_C], gc);
+  atomicAdd(&G[P_WA + lane], gwa);
+  atomicAdd(&G[P_WE + lane], gwe);
+  if (lane == 0) {
+    atomicAdd(&G[P_BA], gba);
+    atomicAdd(&G[P_BE], gbe);
+  }
 }
 
 // Layer backward, step 1 (per cell): dpre = dh_out * [pre > 0];

@@ -41,6 +41,7 @@ struct Lane {
   double rho, beta0, gam, omeg;        // BiCGSTAB (alpha shared)
   double res0_n, ratio, reduc, l1;
   double gs;                           // FCG: residual scale fed to the network
+  double s_prev;                       // CG: r.z of the previous iteration
   int iter, n_iter, active, status;
 };
 enum : int { kLaneRunning = 0, kLaneConverged = 1, kLaneMaxIter = 2, kLaneNaN = 3,
@@ -490,6 +491,7 @@ __global__ void k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict_
       Lane& L = lanes[s * V + v];
       if (!L.active) continue;
       double beta = 1.0 / L.s;   // :44
+      L.s_prev = L.s;
       L.s = tot[v];              // :47
       L.beta = beta * L.s;       // :50
     }
@@ -611,6 +613,7 @@ __global__ void k_cg_update(SegMap sm, const T* __restrict__ c, T* __restrict__ 
       else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
       if (JAC && L.active) {
         double beta = 1.0 / L.s;
+        L.s_prev = L.s;
         L.s = tot[V + v];
         L.beta = beta * L.s;
       }
@@ -808,6 +811,86 @@ __global__ void k_bi_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
         L.beta0 = L.rho;
       }
     }
+  }
+}
+
+// ================ reliable updates for the mixed-precision CG =================
+// After the FP64 residual has replaced the FP32 recursive one, the Jacobi
+// form's fused s = r.(c r) (computed from the old residual in k_cg_update)
+// is recomputed from the new residual, with beta = s_new / s_prev, so the
+// search direction carries on instead of restarting.
+template <typename T, int V>
+__global__ void k_cg_replace_rz(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
+                                double* __restrict__ part, Lane* __restrict__ lanes) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) any |= lanes[s * V + v].active != 0;
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = 0.0;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      const T ri = r[(size_t)i * V + v];
+      acc[v] += prod(ri, mul(ri, c[i]));
+    }
+  }
+  double tot[V];
+  if (seg_commit<V>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      Lane& L = lanes[s * V + v];
+      if (!L.active) continue;
+      L.s = tot[v];
+      L.beta = L.s_prev > 0.0 ? (1.0 / L.s_prev) * L.s : 0.0;
+    }
+  }
+}
+
+// d (FP32 correction since the last update) -> x (FP64) for every lane
+// flagged in mask, and d = 0.
+template <int V>
+__global__ void k_mp_flush(SegMap sm, const int* __restrict__ mask, double* __restrict__ x,
+                           float* __restrict__ d) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool on[V];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) { on[v] = mask[s * V + v] != 0; any |= on[v]; }
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      if (on[v]) {
+        const size_t k = (size_t)i * V + v;
+        x[k] += (double)d[k];
+        d[k] = 0.0f;
+      }
+  }
+}
+
+// r_f = (float) r for the lanes in mask
+template <int V>
+__global__ void k_mp_replace(SegMap sm, const int* __restrict__ mask, const double* __restrict__ r,
+                             float* __restrict__ rf) {
+  const int b = blockIdx.x, s = sm.blk_seg[b];
+  bool on[V];
+  bool any = false;
+#pragma unroll
+  for (int v = 0; v < V; ++v) { on[v] = mask[s * V + v] != 0; any |= on[v]; }
+  if (!any) return;
+  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
+  const int stride = sm.seg_nblk[s] * blockDim.x;
+  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      if (on[v]) rf[(size_t)i * V + v] = (float)r[(size_t)i * V + v];
   }
 }
 

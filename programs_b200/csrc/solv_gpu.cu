@@ -69,6 +69,7 @@ struct solv_gpu_ctx {
   int grid_per_sm = 8;
   int max_refine = 30;
   int inner_max_iter = 2000;
+  double reliable_delta = 0.1;
 
   // matrix (caller sizes)
   bool has_matrix = false;
@@ -105,7 +106,7 @@ struct solv_gpu_ctx {
   // learned preconditioner (gnn.cuh)
   DevBuf g_param, g_grad, g_m, g_v, g_wcat;  // FP32 master, grads, Adam moments, BF16 packed
   DevBuf g_rsd, g_frs, g_fdeg, g_gw;         // per-matrix features
-  DevBuf g_h0, g_h1, g_u, g_r, g_out, g_jsum;
+  DevBuf g_h0, g_h1, g_u, g_r, g_out, g_jsum, g_q, g_he, g_ge;
   DevBuf g_train;                            // training activations
   bool g_feat_valid = false, g_wcat_valid = false, g_has_params = false;
   int g_adam_t = 0;
@@ -434,7 +435,7 @@ int gnn_prepare(solv_gpu_ctx* c) {
   int rc = ensure_f32_matrix(c);
   if (rc) return rc;
   const int N = c->N;
-  const void* before[4] = {c->g_h0.p, c->g_h1.p, c->g_u.p, c->g_wcat.p};
+  const void* before[6] = {c->g_h0.p, c->g_h1.p, c->g_u.p, c->g_wcat.p, c->g_q.p, c->g_ge.p};
   if (!c->g_feat_valid) {
     CUDA_TRY(c, c->g_rsd.ensure(N * sizeof(float)));
     CUDA_TRY(c, c->g_frs.ensure(N * sizeof(float)));
@@ -457,35 +458,42 @@ int gnn_prepare(solv_gpu_ctx* c) {
   CUDA_TRY(c, c->g_h0.ensure((size_t)N * gnn::H * sizeof(__nv_bfloat16)));
   CUDA_TRY(c, c->g_h1.ensure((size_t)N * gnn::H * sizeof(__nv_bfloat16)));
   CUDA_TRY(c, c->g_u.ensure((size_t)N * sizeof(float)));
-  const void* after[4] = {c->g_h0.p, c->g_h1.p, c->g_u.p, c->g_wcat.p};
-  for (int k = 0; k < 4; ++k)
+  CUDA_TRY(c, c->g_q.ensure((size_t)N * sizeof(float)));
+  CUDA_TRY(c, c->g_he.ensure((size_t)N * sizeof(float)));
+  CUDA_TRY(c, c->g_ge.ensure((size_t)c->n_slots * sizeof(float)));
+  const void* after[6] = {c->g_h0.p, c->g_h1.p, c->g_u.p, c->g_wcat.p, c->g_q.p, c->g_ge.p};
+  for (int k = 0; k < 6; ++k)
     if (before[k] != after[k]) drop_graphs(c);
   return SOLV_GPU_OK;
 }
 
-// z = M(r) with the network (inference path: BF16, tensor cores).
+// Build the preconditioner for this solve from the initial residual r0
+// (internal order; its scale gs already in lane 0): the network on the
+// tensor cores, then the heads (q = s / sqrt(d)) and the face weights gE.
 template <typename T>
-void gnn_apply(solv_gpu_ctx* c, const T* r, T* z, const int* n_active) {
+void gnn_build(solv_gpu_ctx* c, const T* r0) {
   const int N = c->N;
   gnn::Feat F = gnn_feat(c);
   const float* P = c->g_param.as<float>();
   const int gw = gnn_grid_warps(c, (long long)N * 32);
   __nv_bfloat16* h0 = c->g_h0.as<__nv_bfloat16>();
   __nv_bfloat16* h1 = c->g_h1.as<__nv_bfloat16>();
-  gnn::k_gnn_enc<T><<<gw, 256, 0, c->stream>>>(N, F, r, P, c->lanes.as<Lane>(), h0,
-                                                c->g_u.as<float>(), n_active);
+  gnn::k_gnn_enc<T><<<gw, 256, 0, c->stream>>>(N, F, r0, P, c->lanes.as<Lane>(), h0,
+                                                c->g_u.as<float>());
   const int tiles = (N + gnn::TC_CELLS - 1) / gnn::TC_CELLS;
   const int tcb = std::max(1, std::min((tiles + gnn::TC_WARPS - 1) / gnn::TC_WARPS, c->n_sm * 8));
   __nv_bfloat16 *hin = h0, *hout = h1;
   for (int l = 0; l < gnn::NL; ++l) {
     gnn::k_gnn_layer_tc<<<tcb, gnn::TC_WARPS * 32, 0, c->stream>>>(
         N, rows<float>(c), F, hin, hout, c->g_wcat.as<__nv_bfloat16>() + l * 2 * gnn::H * gnn::H,
-        P + gnn::P_LAYER + l * gnn::LAYER_SZ + 2 * gnn::H * gnn::H, n_active);
+        P + gnn::P_LAYER + l * gnn::LAYER_SZ + 2 * gnn::H * gnn::H);
     std::swap(hin, hout);
   }
-  gnn::k_gnn_dec_z<T><<<gw, 256, 0, c->stream>>>(N, F, hin, c->g_u.as<float>(), P,
-                                                  c->lanes.as<Lane>(), z, n_active);
-  c->launches += 2 + gnn::NL;
+  gnn::k_gnn_heads<__nv_bfloat16><<<gw, 256, 0, c->stream>>>(
+      N, hin, P, c->g_rsd.as<float>(), nullptr, c->g_q.as<float>(), c->g_he.as<float>());
+  gnn::k_gnn_edges<<<grid_for(c, N), c->block, 0, c->stream>>>(
+      N, rows<float>(c), F, c->g_he.as<float>(), P, nullptr, c->g_ge.as<float>());
+  c->launches += 3 + gnn::NL;
 }
 
 // ---- building blocks -----------------------------------------------------------
@@ -641,13 +649,15 @@ void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
   Lane* lanes = c->lanes.as<Lane>();
   const int G = c->seg.total_blk, B = c->block;
   cudaStream_t st = c->stream;
-  gnn_apply<T>(c, w.r, w.z, sm.n_active);                                    // z = M(r)
+  gnn::k_gnn_apply<T><<<grid_for(c, c->N), B, 0, st>>>(c->N, rows<float>(c), c->g_ge.as<float>(),
+                                                        c->g_q.as<float>(), w.r, w.z,
+                                                        sm.n_active);      // z = M^-1 r
   sg::k_fcg_beta<T><<<G, B, 0, st>>>(sm, w.z, w.q, part, lanes);            // beta
   sg::k_cg_p<T, 1, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes);   // p = z + beta p
   sg::k_fcg_spmv<T><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, w.r, part, lanes);
   sg::k_fcg_update<T><<<G, B, 0, st>>>(sm, c->g_rsd.as<float>(), w.phi, w.r, w.p, w.q, part,
                                        lanes);
-  c->launches += 4;
+  c->launches += 5;
 }
 
 // Run Krylov iterations until every lane stops (device counter), launching
@@ -690,7 +700,7 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     int sweep = imat > 0 ? 2 * nl : 1;
     if (solver == 0) per_launch_kernels = imat > 0 ? sweep + 4 : 3;
     else if (solver == 1) per_launch_kernels = imat > 0 ? 2 * sweep + 5 : 5;
-    else per_launch_kernels = 5 + gnn::NL + 1;
+    else per_launch_kernels = 5;
     c->launches = l0;
   }
   while (done < n_iter) {
@@ -917,6 +927,7 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
       if ((rc = gnn_prepare(c))) return rc;
       sg::k_fcg_scale<float><<<c->seg.total_blk, c->block, 0, s>>>(
           sm, f.r, c->g_rsd.as<float>(), c->part.as<double>(), c->lanes.as<Lane>());
+      gnn_build<float>(c, f.r);
       c->launches++;
     }
     c->launches++;
@@ -986,6 +997,211 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
     }
     st->status = status;
     st->refinements = refinements;
+    st->fallbacks = c->fallbacks;
+    st->graph_launches += gl_total;
+  }
+  return status;
+}
+
+// Mixed-precision CG / FCG with reliable updates: the Krylov iteration runs
+// in FP32 without restarts; whenever a lane's FP32 recursive residual has
+// dropped by `reliable_delta` since the last update (or claims
+// convergence), the FP32 correction is added to the FP64 solution, the
+// FP64 residual b - A x replaces the FP32 one, and the search direction
+// carries on.  Only the FP64 residual decides convergence.
+template <int V>
+int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
+                         double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
+                         solv_gpu_stats* st, int* out_iters, double* out_ratio) {
+  WS<double> w;
+  WS<float> f;
+  int rc = ensure_ws<double>(c, V, w);
+  if (rc) return rc;
+  if ((rc = ensure_ws<float>(c, V, f))) return rc;
+  {
+    void* old = c->valf.p;
+    if ((rc = ensure_f32_matrix(c))) return rc;
+    if (old != c->valf.p) drop_graphs(c);
+  }
+  const int N = c->N;
+  const int nl = c->n_seg * V;
+  const long long NV = (long long)N * V;
+  cudaStream_t s = c->stream;
+  const int* o2n = c->old_of_new.as<int>();
+  CUDA_TRY(c, c->mp_mask.ensure(nl * sizeof(int)));
+  double* b = w.q;
+  sg::k_phi_in<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, phi_dev, w.phi);
+  sg::k_col_in<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, res0_dev, b);
+  CUDA_TRY(c, cudaMemcpyAsync(w.r0, b, NV * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  c->launches += 2;
+  if (not_r0) {
+    CUDA_TRY(c, cudaMemcpyAsync(w.v, w.phi, NV * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(c, cudaMemsetAsync(w.phi, 0, NV * sizeof(double), s));
+  }
+  if ((rc = run_res(c, V, w.phi, w.r0, not_r0))) return rc;
+  sg::k_col_out<<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.r0, res0_dev);
+  c->launches++;
+  std::vector<double> l1(nl);
+  CUDA_TRY(c, cudaMemcpyAsync(l1.data(), c->l1.p, nl * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  double mx = -HUGE_VAL;
+  for (int l = 0; l < nl; ++l) {
+    res0_n[l] = l1[l];
+    mx = std::max(mx, l1[l]);
+  }
+  if (st) st->n_vc = V;
+  if (mx < sg::kSmall) {
+    if (st) st->status = SOLV_GPU_ZERO_RHS;
+    if (out_iters) std::fill(out_iters, out_iters + nl, 0);
+    if (out_ratio) std::fill(out_ratio, out_ratio + nl, 0.0);
+    return SOLV_GPU_OK;
+  }
+  launch_precond(c, imat, w.c, w.cr);
+  sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.c, f.c);
+  sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.cr, f.cr);
+  sg::k_mp_start<V><<<grid_for(c, NV), c->block, 0, s>>>(NV, w.r0, f.r, f.r0, f.phi);
+  CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
+  CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
+  CUDA_TRY(c, cudaMemsetAsync(f.z, 0, NV * sizeof(float), s));
+  c->launches += 3;
+
+  std::vector<Lane> hl(nl);
+  std::vector<double> ratio(nl), l1_last(nl);
+  std::vector<int> final_(nl, 0), status_v(nl, sg::kLaneRunning), stalls(nl, 0), mask(nl, 0);
+  int na = 0;
+  for (int l = 0; l < nl; ++l) {
+    Lane L{};
+    L.s = sg::kLarge; L.alpha = 1.0; L.beta0 = 1.0; L.gam = 1.0;
+    L.res0_n = res0_n[l];
+    L.l1 = l1[l];
+    L.reduc = reduc;
+    L.n_iter = n_iter;
+    ratio[l] = l1[l] / (res0_n[l] + sg::kSmall);
+    L.active = !(ratio[l] < reduc) && n_iter > 0;
+    if (!L.active) {
+      final_[l] = 1;
+      status_v[l] = n_iter > 0 ? sg::kLaneConverged : sg::kLaneMaxIter;
+    }
+    L.status = sg::kLaneRunning;
+    l1_last[l] = l1[l];
+    na += L.active;
+    hl[l] = L;
+  }
+  CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
+  SegMap sm = segmap(c);
+  const int G = c->seg.total_blk, B = c->block;
+  if (solver == 2) {  // the learned preconditioner of this solve, from r0
+    if ((rc = gnn_prepare(c))) return rc;
+    sg::k_fcg_scale<float><<<G, B, 0, s>>>(sm, f.r, c->g_rsd.as<float>(), c->part.as<double>(),
+                                          c->lanes.as<Lane>());
+    gnn_build<float>(c, f.r);
+    c->launches++;
+  } else if (imat <= 0) {
+    sg::k_cg_rz<float, V, true><<<G, B, 0, s>>>(sm, f.c, f.r, f.z, c->part.as<double>(),
+                                                c->lanes.as<Lane>());
+    c->launches++;
+  }
+  CUDA_TRY(c, cudaGetLastError());
+  const double delta = c->reliable_delta;
+  int updates = 0, gl_total = 0, launched = 0;
+  int cur = solver;  // the learned preconditioner hands over to Jacobi-PCG once it stalls
+  c->fallbacks = 0;
+  const int K = std::max(1, c->graph_iters);
+  while (na > 0) {
+    int gl = 0;
+    if ((rc = iterate<float, V>(c, cur, imat, K, f, gl))) return rc;  // K iterations at most
+    gl_total += gl;
+    launched += K;
+    CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->lanes.p, nl * sizeof(Lane), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(c, cudaStreamSynchronize(s));
+    bool need = false;
+    for (int l = 0; l < nl; ++l) {
+      if (final_[l]) continue;
+      if (!hl[l].active || hl[l].l1 < delta * l1_last[l]) need = true;
+      if (cur == 2 && hl[l].status == sg::kLaneStall) {
+        cur = 0;  // no positive curvature from the network: plain PCG from here
+        c->fallbacks++;
+      }
+    }
+    if (!need && launched <= n_iter + K) continue;
+    // reliable update of every lane still in play
+    for (int l = 0; l < nl; ++l) mask[l] = !final_[l];
+    CUDA_TRY(c, cudaMemcpyAsync(c->mp_mask.p, mask.data(), nl * sizeof(int), cudaMemcpyHostToDevice, s));
+    sg::k_mp_flush<V><<<G, B, 0, s>>>(sm, c->mp_mask.as<int>(), w.phi, f.phi);
+    CUDA_TRY(c, cudaMemcpyAsync(w.r, b, NV * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if ((rc = run_res(c, V, w.phi, w.r, 0))) return rc;
+    sg::k_mp_replace<V><<<G, B, 0, s>>>(sm, c->mp_mask.as<int>(), w.r, f.r);
+    c->launches += 3;
+    ++updates;
+    CUDA_TRY(c, cudaMemcpyAsync(l1.data(), c->l1.p, nl * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(c, cudaStreamSynchronize(s));
+    na = 0;
+    for (int l = 0; l < nl; ++l) {
+      if (final_[l]) {
+        hl[l].active = 0;
+        continue;
+      }
+      Lane& L = hl[l];
+      ratio[l] = l1[l] / (res0_n[l] + sg::kSmall);
+      L.l1 = l1[l];
+      L.status = sg::kLaneRunning;
+      L.active = 1;
+      if (!(ratio[l] == ratio[l]) || std::isinf(ratio[l]) || hl[l].status == sg::kLaneNaN) {
+        final_[l] = 1;
+        status_v[l] = sg::kLaneNaN;
+      } else if (ratio[l] < reduc) {
+        final_[l] = 1;
+        status_v[l] = sg::kLaneConverged;
+      } else if (L.iter >= n_iter || launched > n_iter + K) {
+        final_[l] = 1;
+        status_v[l] = sg::kLaneMaxIter;
+      } else {
+        // the FP64 residual stopped improving between updates: FP32 floor
+        stalls[l] = l1[l] > 0.9 * l1_last[l] ? stalls[l] + 1 : 0;
+        if (stalls[l] >= 3) {
+          final_[l] = 1;
+          status_v[l] = sg::kLaneMaxIter;
+        }
+      }
+      if (final_[l]) L.active = 0;
+      l1_last[l] = l1[l];
+      na += L.active;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
+    if (na == 0) break;
+    if (cur == 2) {
+      // M^-1 is fixed for the solve; FCG's beta uses the stored q of the
+      // last step, so nothing to recompute
+    } else if (imat <= 0) {
+      sg::k_cg_replace_rz<float, V><<<G, B, 0, s>>>(sm, f.c, f.r, c->part.as<double>(),
+                                                    c->lanes.as<Lane>());
+      c->launches++;
+    }
+    CUDA_TRY(c, cudaGetLastError());
+  }
+  if (not_r0) {
+    sg::k_add<<<grid_for(c, NV), c->block, 0, s>>>(NV, w.phi, w.v);
+    c->launches++;
+  }
+  sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.phi, phi_dev);
+  c->launches++;
+  CUDA_TRY(c, cudaGetLastError());
+  int status = SOLV_GPU_OK;
+  for (int l = 0; l < nl; ++l) {
+    if (status_v[l] == sg::kLaneNaN) status = SOLV_GPU_NAN;
+    else if (status_v[l] != sg::kLaneConverged && status == SOLV_GPU_OK) status = SOLV_GPU_MAXITER;
+    if (out_iters) out_iters[l] = hl[l].iter;
+    if (out_ratio) out_ratio[l] = ratio[l];
+  }
+  if (st) {
+    for (int v = 0; v < V && v < nl; ++v) {
+      st->iters[v] = hl[v].iter;
+      st->ratio[v] = ratio[v];
+    }
+    st->status = status;
+    st->refinements = updates;
     st->fallbacks = c->fallbacks;
     st->graph_launches += gl_total;
   }
@@ -1094,6 +1310,10 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
     case SOLV_OPT_MAX_REFINE:
       if (value < 1 || value > 1000) return set_err(c, SOLV_GPU_BAD_INPUT, "max refine in 1..1000");
       c->max_refine = (int)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_RELIABLE_DELTA:
+      if (!(value > 0 && value < 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "reliable delta in (0,1)");
+      c->reliable_delta = value;
       return SOLV_GPU_OK;
     case SOLV_OPT_INNER_MAX_ITER:
       if (value < 1 || value > 1e7) return set_err(c, SOLV_GPU_BAD_INPUT, "inner max iter in 1..1e7");
@@ -1483,19 +1703,22 @@ int solv_gpu_gnn_zero_grad(solv_gpu_ctx* c) {
   return SOLV_GPU_OK;
 }
 
-// Training activations: 15 FP32 arrays of N x 32 plus 4 of N.
+// Training buffers: 15 FP32 arrays of N x 32, 14 of N, 2 per slot.
+enum { TB_H0 = 0, TB_AGG0 = 4, TB_PRE0 = 7, TB_DHA = 11, TB_DHB = 12, TB_DHS = 13, TB_DAGG = 14,
+       TB_R0 = 15, TB_U0, TB_PA, TB_S, TB_HE, TB_RS, TB_US, TB_ZS, TB_GS, TB_Y, TB_DT, TB_DS,
+       TB_ES, TB_Q, TB_EPRE, TB_GE, TB_COUNT };
 static int gnn_train_buffers(solv_gpu_ctx* c, float** B) {
-  const size_t nh = (size_t)c->N * gnn::H, n1 = (size_t)c->N;
-  CUDA_TRY(c, c->g_train.ensure((15 * nh + 4 * n1) * sizeof(float)));
-  float* base = c->g_train.as<float>();
-  for (int k = 0; k < 15; ++k) B[k] = base + k * nh;
-  for (int k = 0; k < 4; ++k) B[15 + k] = base + 15 * nh + k * n1;
+  const size_t nh = (size_t)c->N * gnn::H, n1 = (size_t)c->N, ns = (size_t)c->n_slots;
+  CUDA_TRY(c, c->g_train.ensure((15 * nh + 14 * n1 + 2 * ns) * sizeof(float)));
+  float* p = c->g_train.as<float>();
+  for (int k = 0; k < 15; ++k, p += nh) B[k] = p;
+  for (int k = TB_R0; k <= TB_Q; ++k, p += n1) B[k] = p;
+  B[TB_EPRE] = p;
+  B[TB_GE] = p + ns;
   return SOLV_GPU_OK;
 }
-enum { TB_H0 = 0, TB_AGG0 = 4, TB_PRE0 = 7, TB_DHA = 11, TB_DHB = 12, TB_DHS = 13, TB_DAGG = 14,
-       TB_U = 15, TB_OUT = 16, TB_G = 17, TB_R = 18 };
 
-// r (caller layout, device) -> internal FP32 residual and its scale (lane 0)
+// r (caller layout, device) -> internal FP32 and its scale gs in lane 0
 static int gnn_load_residual(solv_gpu_ctx* c, const double* r_dev, float* rf) {
   const int N = c->N;
   sg::k_phi_in<float><<<grid_for(c, N), c->block, 0, c->stream>>>(N, 1, c->old_of_new.as<int>(),
@@ -1509,81 +1732,127 @@ static int gnn_load_residual(solv_gpu_ctx* c, const double* r_dev, float* rf) {
   return SOLV_GPU_OK;
 }
 
-// Training-path forward (FP32 CUDA cores, BF16 rounding as inference).
-static void gnn_train_forward(solv_gpu_ctx* c, float** B) {
+__global__ void k_gnn_scaled_u(int n, const float* __restrict__ rsd, const float* __restrict__ r,
+                               const Lane* __restrict__ lanes, float* __restrict__ u) {
+  const double s = lanes[0].gs > 0 ? lanes[0].gs : 1.0;
+  const float inv = (float)(1.0 / s);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    u[i] = r[i] * rsd[i] * inv;
+}
+__global__ void k_gnn_mul(int n, const float* __restrict__ a, const float* __restrict__ b,
+                          float* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = a[i] * b[i];
+}
+
+// Training-path forward from the feature residual r0 (FP32 CUDA cores, BF16
+// rounding as inference): activations, heads (s in the scaled space), faces.
+static int gnn_train_forward(solv_gpu_ctx* c, const double* r0_dev, float** B) {
+  int rc = gnn_load_residual(c, r0_dev, B[TB_R0]);
+  if (rc) return rc;
   const int N = c->N;
   gnn::Feat F = gnn_feat(c);
   const float* P = c->g_param.as<float>();
   const int gw = gnn_grid_warps(c, (long long)N * 32);
-  gnn::k_gnn_enc<float><<<gw, 256, 0, c->stream>>>(N, F, B[TB_R], P, c->lanes.as<Lane>(),
-                                                    c->g_h0.as<__nv_bfloat16>(), B[TB_U], nullptr);
-  gnn::k_gnn_enc_train<<<gw, 256, 0, c->stream>>>(N, F, B[TB_U], P, B[TB_H0], B[TB_PRE0]);
+  gnn::k_gnn_enc<float><<<gw, 256, 0, c->stream>>>(N, F, B[TB_R0], P, c->lanes.as<Lane>(),
+                                                    c->g_h0.as<__nv_bfloat16>(), B[TB_U0]);
+  gnn::k_gnn_enc_train<<<gw, 256, 0, c->stream>>>(N, F, B[TB_U0], P, B[TB_H0], B[TB_PRE0]);
   const int lb = std::max(1, std::min((N + 7) / 8, c->n_sm * 8));
   for (int l = 0; l < gnn::NL; ++l)
     gnn::k_gnn_layer_train<<<lb, 256, 0, c->stream>>>(
         N, rows<float>(c), F, B[TB_H0 + l], B[TB_AGG0 + l], B[TB_PRE0 + 1 + l], B[TB_H0 + 1 + l],
         P + gnn::P_LAYER + l * gnn::LAYER_SZ);
-  gnn::k_gnn_dec_out<float><<<gw, 256, 0, c->stream>>>(N, B[TB_H0 + 3], B[TB_U], P, B[TB_OUT]);
+  gnn::k_gnn_heads<float><<<gw, 256, 0, c->stream>>>(N, B[TB_H0 + 3], P, nullptr, B[TB_PA],
+                                                     B[TB_S], B[TB_HE]);
+  gnn::k_gnn_edges<<<grid_for(c, N), c->block, 0, c->stream>>>(N, rows<float>(c), F, B[TB_HE], P,
+                                                               B[TB_EPRE], B[TB_GE]);
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
 }
 
-__global__ void k_gnn_scale_z(int n, const float* __restrict__ rsd, const float* __restrict__ out,
-                              const Lane* __restrict__ lanes, float* __restrict__ z) {
-  const double s = lanes[0].gs > 0 ? lanes[0].gs : 1.0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    z[i] = (float)((double)out[i] * s * rsd[i]);
-}
-
-// z = M(r) for a caller-layout residual: path 0 = inference (BF16 tensor
-// cores), path 1 = training path (FP32 CUDA cores).
-int solv_gpu_gnn_forward_dev(solv_gpu_ctx* c, const double* r_dev, double* z_dev, int path) {
+// z = M^-1 r with the preconditioner built from r0 (caller layout, device):
+// path 0 = inference kernels (BF16, tensor cores), 1 = training kernels.
+int solv_gpu_gnn_forward_dev(solv_gpu_ctx* c, const double* r0_dev, const double* r_dev,
+                             double* z_dev, int path) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (!r0_dev || !r_dev || !z_dev) return set_err(c, SOLV_GPU_BAD_INPUT, "gnn forward: null pointer");
   CUDA_TRY(c, cudaSetDevice(c->dev));
   int rc = gnn_prepare(c);
   if (rc) return rc;
-  float* B[19];
+  float* B[TB_COUNT];
   if ((rc = gnn_train_buffers(c, B))) return rc;
-  if ((rc = gnn_load_residual(c, r_dev, B[TB_R]))) return rc;
   const int N = c->N;
+  const int* o2n = c->old_of_new.as<int>();
+  const float *q, *ge;
   if (path == 0) {
-    gnn_apply<float>(c, B[TB_R], B[TB_G], nullptr);
+    if ((rc = gnn_load_residual(c, r0_dev, B[TB_R0]))) return rc;
+    gnn_build<float>(c, B[TB_R0]);
+    q = c->g_q.as<float>();
+    ge = c->g_ge.as<float>();
   } else {
-    gnn_train_forward(c, B);
-    k_gnn_scale_z<<<grid_for(c, N), c->block, 0, c->stream>>>(N, c->g_rsd.as<float>(), B[TB_OUT],
-                                                              c->lanes.as<Lane>(), B[TB_G]);
+    if ((rc = gnn_train_forward(c, r0_dev, B))) return rc;
+    k_gnn_mul<<<grid_for(c, N), c->block, 0, c->stream>>>(N, B[TB_S], c->g_rsd.as<float>(),
+                                                           B[TB_Q]);
+    q = B[TB_Q];
+    ge = B[TB_GE];
   }
-  sg::k_phi_out<float><<<grid_for(c, N), c->block, 0, c->stream>>>(N, 1, c->old_of_new.as<int>(),
-                                                                  B[TB_G], z_dev);
+  sg::k_phi_in<float><<<grid_for(c, N), c->block, 0, c->stream>>>(N, 1, o2n, r_dev, B[TB_RS]);
+  gnn::k_gnn_apply<float><<<grid_for(c, N), c->block, 0, c->stream>>>(N, rows<float>(c), ge, q,
+                                                                      B[TB_RS], B[TB_ZS], nullptr);
+  sg::k_phi_out<float><<<grid_for(c, N), c->block, 0, c->stream>>>(N, 1, o2n, B[TB_ZS], z_dev);
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   CUDA_TRY(c, cudaGetLastError());
   return SOLV_GPU_OK;
 }
 
-// Forward + backward of the energy loss for one residual; gradients are
-// added to the accumulator (zeroed first unless `accumulate`).  loss = J/N.
-int solv_gpu_gnn_grad_dev(solv_gpu_ctx* c, const double* r_dev, double* loss, int accumulate) {
+// Forward + backward of the energy loss J = 1/2 z.Â z - z.u, z = K u, for
+// the preconditioner built from r0 and the n_samples residual samples r_k
+// (each n_cell long, caller layout, consecutive; each normalised to unit
+// mean magnitude).  Gradients add up in the FP32 accumulator (zeroed first
+// unless accumulate); loss = mean over samples of J / n_cell.
+int solv_gpu_gnn_grad_dev(solv_gpu_ctx* c, const double* r0_dev, const double* samples_dev,
+                          int n_samples, double* loss, int accumulate) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (!r0_dev || !samples_dev || n_samples < 1)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "gnn grad: bad arguments");
   CUDA_TRY(c, cudaSetDevice(c->dev));
   int rc = gnn_prepare(c);
   if (rc) return rc;
-  float* B[19];
+  float* B[TB_COUNT];
   if ((rc = gnn_train_buffers(c, B))) return rc;
   if (!accumulate) CUDA_TRY(c, cudaMemsetAsync(c->g_grad.p, 0, gnn::N_PARAM_PAD * sizeof(float), c->stream));
-  if ((rc = gnn_load_residual(c, r_dev, B[TB_R]))) return rc;
-  gnn_train_forward(c, B);
+  if ((rc = gnn_train_forward(c, r0_dev, B))) return rc;
   const int N = c->N;
   gnn::Feat F = gnn_feat(c);
   const float* P = c->g_param.as<float>();
   float* G = c->g_grad.as<float>();
+  const int* o2n = c->old_of_new.as<int>();
   CUDA_TRY(c, c->g_jsum.ensure(sizeof(double)));
   CUDA_TRY(c, cudaMemsetAsync(c->g_jsum.p, 0, sizeof(double), c->stream));
-  gnn::k_gnn_loss_grad<<<grid_for(c, N), 256, 0, c->stream>>>(N, rows<float>(c), F, B[TB_OUT],
-                                                               B[TB_U], B[TB_G],
-                                                               c->g_jsum.as<double>());
+  CUDA_TRY(c, cudaMemsetAsync(B[TB_DS], 0, N * sizeof(float), c->stream));
+  CUDA_TRY(c, cudaMemsetAsync(B[TB_ES], 0, N * sizeof(float), c->stream));
+  for (int k = 0; k < n_samples; ++k) {
+    if ((rc = gnn_load_residual(c, samples_dev + (size_t)k * N, B[TB_RS]))) return rc;
+    // gnn_load_residual permuted the sample in; normalise it
+    k_gnn_scaled_u<<<grid_for(c, N), c->block, 0, c->stream>>>(N, c->g_rsd.as<float>(), B[TB_RS],
+                                                              c->lanes.as<Lane>(), B[TB_US]);
+    gnn::k_gnn_apply<float><<<grid_for(c, N), c->block, 0, c->stream>>>(
+        N, rows<float>(c), B[TB_GE], B[TB_S], B[TB_US], B[TB_ZS], nullptr);
+    gnn::k_gnn_loss_grad<<<grid_for(c, N), 256, 0, c->stream>>>(
+        N, rows<float>(c), F, B[TB_ZS], B[TB_US], B[TB_GS], c->g_jsum.as<double>());
+    gnn::k_gnn_apply_back1<<<grid_for(c, N), c->block, 0, c->stream>>>(N, B[TB_S], B[TB_US],
+                                                                      B[TB_GS], B[TB_Y], B[TB_DT]);
+    gnn::k_gnn_apply_back2<<<grid_for(c, N), c->block, 0, c->stream>>>(
+        N, rows<float>(c), F, B[TB_GE], B[TB_EPRE], B[TB_US], B[TB_GS], B[TB_Y], B[TB_DT],
+        B[TB_DS], B[TB_ES]);
+  }
+  (void)o2n;
   const int gw = gnn_grid_warps(c, (long long)N * 32);
-  gnn::k_gnn_dec_back<<<gw, 256, 0, c->stream>>>(N, B[TB_H0 + 3], B[TB_U], B[TB_G], 1.0f / N, P,
-                                                 B[TB_DHA], G);
+  const float gsc = 1.0f / ((float)N * (float)n_samples);
+  gnn::k_gnn_heads_back<<<gw, 256, 0, c->stream>>>(N, B[TB_H0 + 3], B[TB_PA], B[TB_S], B[TB_DS],
+                                                   B[TB_ES], gsc, P, B[TB_DHA], G);
   float* dcur = B[TB_DHA];
   const int lb = std::max(1, std::min((N + 7) / 8, c->n_sm * 8));
   for (int l = gnn::NL - 1; l >= 0; --l) {
@@ -1596,12 +1865,12 @@ int solv_gpu_gnn_grad_dev(solv_gpu_ctx* c, const double* r_dev, double* loss, in
                                                       dnext);
     dcur = dnext;
   }
-  gnn::k_gnn_enc_back<<<gw, 256, 0, c->stream>>>(N, F, B[TB_U], B[TB_PRE0], dcur, G);
+  gnn::k_gnn_enc_back<<<gw, 256, 0, c->stream>>>(N, F, B[TB_U0], B[TB_PRE0], dcur, G);
   CUDA_TRY(c, cudaGetLastError());
   double j = 0;
   CUDA_TRY(c, cudaMemcpyAsync(&j, c->g_jsum.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-  if (loss) *loss = j / N;
+  if (loss) *loss = j / N / n_samples;
   return SOLV_GPU_OK;
 }
 
@@ -1723,7 +1992,16 @@ int solve_dispatch(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_it
   if (solver == 2) {  // flexible CG with the learned preconditioner, FP32 inner
     if (V != 1 || c->n_seg != 1)
       return set_err(c, SOLV_GPU_BAD_INPUT, "learned preconditioner: one system, n_vc = 1");
-    return solve_mixed<1>(c, 2, 0, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+    return solve_mixed_reliable<1>(c, 2, 0, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+  }
+  if (c->precision == 1 && solver == 0) {
+    switch (V) {
+      case 1: return solve_mixed_reliable<1>(c, 0, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+      case 2: return solve_mixed_reliable<2>(c, 0, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+      case 3: return solve_mixed_reliable<3>(c, 0, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+      case 4: return solve_mixed_reliable<4>(c, 0, imat, reduc, n_iter, phi_dev, res0_dev, res0_n, not_r0, st, oi, orat);
+    }
+    return set_err(c, SOLV_GPU_BAD_INPUT, "n_vc must be 1..4");
   }
   if (c->precision == 1) {
     switch (V) {

@@ -30,17 +30,20 @@ H, NF, NL = 32, 4, 3
 P_WIN = 0
 P_LAYER = H * NF
 LAYER_SZ = 2 * H * H + H
-P_WOUT = P_LAYER + NL * LAYER_SZ
-P_C = P_WOUT + H
-N_PARAM = P_C + 1
+P_WA = P_LAYER + NL * LAYER_SZ  # diagonal-scale head
+P_BA = P_WA + H
+P_WE = P_BA + 1                 # face head
+P_BE = P_WE + H
+N_PARAM = P_BE + 1
+LAYOUT = "H32-NF4-NL3-spd-v2"
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "gnn_pressure.npz")
 
 
 def init_params(seed: int = 0) -> np.ndarray:
-    """Random hidden layers, zero correction: the untrained network is the
-    Jacobi step (w_out = 0, c = 1)."""
+    """Random hidden layers, zero heads: the untrained preconditioner is the
+    Jacobi step (s = sqrt(softplus(0)/softplus(0)) = 1, E = 0)."""
     rng = np.random.default_rng(seed)
     p = np.zeros(N_PARAM, np.float32)
     p[P_WIN:P_WIN + H * NF] = rng.normal(0, 0.5, H * NF)
@@ -48,20 +51,18 @@ def init_params(seed: int = 0) -> np.ndarray:
         o = P_LAYER + l * LAYER_SZ
         p[o:o + H * H] = rng.normal(0, 0.3 / np.sqrt(H), H * H)            # Ws
         p[o + H * H:o + 2 * H * H] = rng.normal(0, 0.3 / np.sqrt(H), H * H)  # Wn
-    p[P_WOUT:P_WOUT + H] = 0.0
-    p[P_C] = 1.0
     return p
 
 
 def save_params(path: str, p: np.ndarray, meta: dict) -> None:
     os.makedirs(os.path.dirname(path), exist_ok=True)
-    np.savez(path, params=np.asarray(p, np.float32), n_param=N_PARAM,
-             layout="H32-NF4-NL3-v1", meta=json.dumps(meta))
+    np.savez(path, params=np.asarray(p, np.float32), n_param=N_PARAM, layout=LAYOUT,
+             meta=json.dumps(meta))
 
 
 def load_params(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
     d = np.load(path)
-    if int(d["n_param"]) != N_PARAM or str(d["layout"]) != "H32-NF4-NL3-v1":
+    if int(d["n_param"]) != N_PARAM or str(d["layout"]) != LAYOUT:
         raise ValueError(f"{path}: parameter layout does not match this build")
     return np.asarray(d["params"], np.float32)
 
@@ -87,20 +88,22 @@ def simple_systems(size: int, n_mesh: int, per_mesh: int, seed: int = 0):
             yield m, P, b
 
 
-def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=150):
-    """Residuals r_k = b - A x_k of Jacobi-PCG after k iterations."""
+def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=400):
+    """[b, r_k1, r_k2, ...]: residuals b - A x_k of Jacobi-PCG after k
+    iterations (the residuals the solver visits), as one (n, N) tensor."""
     N = b_dev.shape[0]
     phi = torch.zeros(N, dtype=torch.float64, device=b_dev.device)
     res0 = torch.empty_like(b_dev)
     y = torch.empty_like(b_dev)
-    out = [b_dev.clone()]
-    ks = sorted(rng.integers(1, max_k, n_samples - 1).tolist())
-    for k in ks:
+    out = torch.empty((n_samples, N), dtype=torch.float64, device=b_dev.device)
+    out[0].copy_(b_dev)
+    ks = sorted(np.exp(rng.uniform(0, np.log(max_k), n_samples - 1)).astype(int).tolist())
+    for m, k in enumerate(ks, start=1):
         phi.zero_()
         res0.copy_(b_dev)
-        s.solv_cg_dev(0, 1e-300, int(k), 1, phi.data_ptr(), res0.data_ptr())
+        s.solv_cg_dev(0, 1e-300, int(max(k, 1)), 1, phi.data_ptr(), res0.data_ptr())
         s.spmv_dev(phi.data_ptr(), y.data_ptr())
-        out.append(b_dev - y)
+        out[m].copy_(b_dev - y)
     return out
 
 
@@ -125,12 +128,10 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
                 s.matrix_values(P.p, P.n, P.pl)
             b_dev = torch.from_numpy(b).to(dev)
             rs = _residual_samples(s, b_dev, samples, rng, torch)
-            loss = 0.0
-            for k, r in enumerate(rs):
-                loss += s.gnn_grad_dev(r.data_ptr(), accumulate=k > 0)
-            s.gnn_adam(lr, 1.0 / len(rs))
+            loss = s.gnn_grad_dev(b_dev.data_ptr(), rs.data_ptr(), rs.shape[0])
+            s.gnn_adam(lr, 1.0)
             step += 1
-            hist.append(loss / len(rs))
+            hist.append(loss)
             if log_every and step % log_every == 0:
                 print(json.dumps({"step": step, "loss": float(np.mean(hist[-log_every:])),
                                   "t": round(time.time() - t0, 1)}), flush=True)

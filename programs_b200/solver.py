@@ -116,8 +116,9 @@ def lib():
     L.solv_gpu_gnn_get_params.argtypes = [vp, _f32p, ctypes.c_int]
     L.solv_gpu_gnn_get_grad.argtypes = [vp, _f32p, ctypes.c_int]
     L.solv_gpu_gnn_zero_grad.argtypes = [vp]
-    L.solv_gpu_gnn_forward_dev.argtypes = [vp, vp, vp, ctypes.c_int]
-    L.solv_gpu_gnn_grad_dev.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    L.solv_gpu_gnn_forward_dev.argtypes = [vp, vp, vp, vp, ctypes.c_int]
+    L.solv_gpu_gnn_grad_dev.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.c_int]
     L.solv_gpu_gnn_adam.argtypes = [vp, ctypes.c_float, ctypes.c_float]
     for fn in (L.solv_gpu_cg_batch, L.solv_gpu_bicg_batch):
         fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _f64p,
@@ -317,13 +318,15 @@ class GpuSolver:
             self._h, g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), g.shape[0]))
         return g
 
-    def gnn_forward_dev(self, r_ptr: int, z_ptr: int, path: int = 0) -> None:
-        self._check(self._lib.solv_gpu_gnn_forward_dev(self._h, r_ptr, z_ptr, path))
+    def gnn_forward_dev(self, r0_ptr: int, r_ptr: int, z_ptr: int, path: int = 0) -> None:
+        """z = M^-1 r, the preconditioner built from r0 (device pointers, caller order)."""
+        self._check(self._lib.solv_gpu_gnn_forward_dev(self._h, r0_ptr, r_ptr, z_ptr, path))
 
-    def gnn_grad_dev(self, r_ptr: int, accumulate: bool = False) -> float:
+    def gnn_grad_dev(self, r0_ptr: int, samples_ptr: int, n_samples: int,
+                     accumulate: bool = False) -> float:
         loss = ctypes.c_double()
-        self._check(self._lib.solv_gpu_gnn_grad_dev(self._h, r_ptr, ctypes.byref(loss),
-                                                    int(bool(accumulate))))
+        self._check(self._lib.solv_gpu_gnn_grad_dev(self._h, r0_ptr, samples_ptr, n_samples,
+                                                    ctypes.byref(loss), int(bool(accumulate))))
         return loss.value
 
     def gnn_adam(self, lr: float, grad_scale: float = 1.0) -> None:

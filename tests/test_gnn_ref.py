@@ -5,6 +5,7 @@ import re
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 from oracle import gnn_ref
 from programs_b200 import learn
@@ -25,17 +26,39 @@ def _system(n=6, seed=1):
     return pressure_correction(m, M.pl, pin=1)
 
 
+def _active(seed=1):
+    p = learn.init_params(seed).astype(np.float64)
+    rng = np.random.default_rng(seed)
+    p[learn.P_WA:learn.P_WA + 32] = rng.normal(0, 0.3, 32)
+    p[learn.P_WE:learn.P_WE + 32] = rng.normal(0, 0.3, 32)
+    p[learn.P_BE] = 0.2
+    return p
+
+
 def test_layout_matches_cuda_header():
     src = open(os.path.join(ROOT, "programs_b200", "csrc", "gnn.cuh")).read()
     assert re.search(r"constexpr int H = 32;", src) and re.search(r"constexpr int NL = 3;", src)
-    assert learn.N_PARAM == gnn_ref.N_PARAM == 128 + 3 * (2 * 32 * 32 + 32) + 33
+    assert re.search(r"kGamma = 0\.95f", src) and gnn_ref.GAMMA == 0.95
+    assert learn.N_PARAM == gnn_ref.N_PARAM == 128 + 3 * (2 * 32 * 32 + 32) + 66
+    assert (learn.P_WA, learn.P_BA, learn.P_WE, learn.P_BE) == (
+        gnn_ref.P_WA, gnn_ref.P_BA, gnn_ref.P_WE, gnn_ref.P_BE)
 
 
 def test_untrained_network_is_the_jacobi_step():
     A = _system()
     r = uniform(3, A.n_cell)
-    z, _, _ = gnn_ref.forward(A, r, learn.init_params(0))
-    assert np.allclose(z, r / A.pl, rtol=2e-6)
+    z = gnn_ref.precondition(A, r, r, learn.init_params(0))
+    assert np.allclose(z, r.astype(np.float32) / A.pl, rtol=1e-6)
+
+
+def test_preconditioner_is_symmetric_positive_definite():
+    A = _system(5, seed=2)
+    p = _active(4)
+    N = A.n_cell
+    r0 = uniform(1, N)
+    M = np.stack([gnn_ref.precondition(A, r0, e, p) for e in np.eye(N)], axis=1)
+    assert np.allclose(M, M.T, rtol=1e-6, atol=1e-9)
+    assert np.linalg.eigvalsh(0.5 * (M + M.T)).min() > 0
 
 
 def test_bf16_rounding_is_round_to_nearest_even():
@@ -50,26 +73,27 @@ def test_reference_gradient_matches_finite_differences():
     gnn_ref.ROUND = False
     try:
         A = _system(5, seed=2)
-        r = uniform(4, A.n_cell)
-        p = learn.init_params(1).astype(np.float64)
+        r0 = uniform(4, A.n_cell)
+        samples = [r0, uniform(5, A.n_cell)]
+        p = _active(1)
+        J0, g = gnn_ref.loss_and_grad(A, r0, samples, p)
         rng = np.random.default_rng(0)
-        p[learn.P_WOUT:learn.P_WOUT + 32] = rng.normal(0, 0.3, 32)  # open the correction path
-        J0, g = gnn_ref.loss_and_grad(A, r, p)
-        idx = rng.choice(learn.N_PARAM, 25, replace=False)
+        idx = np.concatenate([rng.choice(learn.N_PARAM, 20, replace=False),
+                              [learn.P_BA, learn.P_BE, learn.P_WA, learn.P_WE + 3]])
         for k in idx:
             e = 1e-6
             pp, pm = p.copy(), p.copy()
             pp[k] += e
             pm[k] -= e
-            fd = (float(gnn_ref.forward(A, r, pp)[1]) - float(gnn_ref.forward(A, r, pm)[1])) / (2 * e)
-            assert abs(fd - g[k]) <= 1e-6 + 1e-4 * abs(g[k])
+            fd = (float(gnn_ref.loss(A, r0, samples, pp)[0]) -
+                  float(gnn_ref.loss(A, r0, samples, pm)[0])) / (2 * e)
+            assert abs(fd - g[k]) <= 1e-7 + 1e-4 * abs(g[k]), k
     finally:
         gnn_ref.ROUND = True
 
 
 def test_energy_loss_minimiser_is_the_solution():
-    """J(out) = 1/2 out.Â out - out.u is minimised by out = Â^-1 u."""
-    import scipy.sparse as sp
+    """J(z) = 1/2 z.Â z - z.u is minimised by z = Â^-1 u."""
     import scipy.sparse.linalg as spla
     A = _system(5, seed=3)
     rsd = 1.0 / np.sqrt(A.pl)
@@ -77,6 +101,6 @@ def test_energy_loss_minimiser_is_the_solution():
     u = uniform(5, A.n_cell)
     x = spla.spsolve(S.tocsc(), u)
     J = lambda o: 0.5 * o @ (S @ o) - o @ u
-    for _ in range(5):
-        d = np.random.default_rng(_).normal(size=A.n_cell) * 1e-3
+    for k in range(5):
+        d = np.random.default_rng(k).normal(size=A.n_cell) * 1e-3
         assert J(x + d) > J(x)

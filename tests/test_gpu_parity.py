@@ -123,7 +123,8 @@ def test_solve_matches_oracle(gpu, case, solver, imat):
     st = getattr(gpu, "solv_" + solver)(imat, 1e-10, 3000, phi, res0, rn)
     assert st["status"] == OK
     pressure = name.startswith("p")
-    if (solver == "bicg" and pressure) or (imat == 1 and not pressure):
+    unpaired = (solver == "bicg" and pressure) or (imat == 1 and not pressure)
+    if unpaired:
         # Pairings the reference never makes (cfd_setup.f90:528 runs
         # BiCGSTAB+DILU on momentum, :662 CG+DIC on pressure).  BiCGSTAB on
         # the SPD pressure matrix and DIC (n^2, solv_precond.f90:19) on the
@@ -137,10 +138,10 @@ def test_solve_matches_oracle(gpu, case, solver, imat):
         assert _rel(phi, ref[0]) <= SOL_TOL
     assert np.array_equal(res0, ref[1])
     assert np.allclose(rn, ref[2], rtol=NORM_TOL)
-    # tree-ordered dot products: counts agree to a couple of iterations, or a
-    # few percent where the preconditioner does not fit the matrix (DIC on
-    # the non-symmetric momentum matrix converges erratically)
-    assert abs(st["iters"][0] - int(ref[3][0])) <= max(2, 0.06 * int(ref[3][0]))
+    # tree-ordered dot products: counts agree to a couple of iterations in the
+    # reference's own pairings, and to 15% in the erratic unpaired ones
+    tol = 0.15 if unpaired else 0.02
+    assert abs(st["iters"][0] - int(ref[3][0])) <= max(2, tol * int(ref[3][0]))
     assert st["ratio"][0] < 1e-10
 
 
