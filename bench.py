@@ -1,24 +1,30 @@
 """Benchmark: seconds per pressure solve to a 1e-10 relative residual on a
-256^3 jittered, permuted hex mesh (16.7M cells, 50.1M interior faces),
-plus the SpMV HBM roofline.
+256^3 jittered, permuted hex mesh (16.8M cells, 50.1M interior faces):
+the learned + mixed-precision solve against plain FP64 PCG, plus the
+matrix-product HBM rooflines.
 
-One step = one full Krylov solve (the spray-simulation solv_cg call with
-reduc=1e-10) of the pressure-correction Poisson system: jitter +-15%,
-cells randomly permuted (seed 0) and then renumbered by the framework
-(reverse Cuthill-McKee), coefficients area/l_pn, all-Neumann boundaries,
-cell 1 pinned, rhs uniform[-1,1] with its mean removed, phi0 = 0.
+One step = one full solve of the pressure-correction Poisson system
+(jitter +-15%, cells randomly permuted (seed 0) then renumbered by the
+framework (reverse Cuthill-McKee), coefficients area/l_pn, all-Neumann
+boundaries, cell 1 pinned, rhs uniform[-1,1] with its mean removed,
+phi0 = 0) with the spray-simulation stopping rule |r|_1/|r0|_1 < 1e-10.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
-                  [--size 256] [--method pcg|pcg-mixed] [--imat 0]
+                  [--size 256] [--method learned|mixed|plain]
 
-The b200 arm times K solves with CUDA events on the solver's stream
-(inputs resident in HBM; every input is larger than the 126 MB L2), then
-the same solves through the host C-ABI (pinned host buffers, copies
-included) for `e2e`.  The reference arm times the CPU oracle -- the
-line-faithful C restatement of the Fortran solver -- on a bounded sample
-of iterations of the same system and scales to a full solve.
+Methods (all through the library's C-ABI, same context, same system):
+  learned -- flexible CG with the learned preconditioner, FP32 inner
+             iteration with FP64 reliable updates (solv_gpu_fcg); `value`
+  mixed   -- Jacobi PCG, FP32 inner iteration with FP64 reliable updates
+  plain   -- Jacobi PCG in FP64 (solv_gpu_cg, the reference algorithm)
+Each is timed with CUDA events on the solver's stream (inputs resident in
+HBM; every array is larger than the 126 MB L2, so no flush is needed); the
+measured method is then timed end to end through the host C-ABI with
+pinned host buffers (`e2e`).  The reference arm times the CPU oracle -- the
+line-faithful C restatement of the Fortran solver -- on a bounded sample of
+iterations of the same system, scaled to the full solve.
 Multi-GPU: the path does not shard (replicas only): each rank solves its
-own system, timing is max over ranks.
+own system; timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -35,13 +41,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Full-solve iteration count of the default workload (256^3, Jacobi PCG,
-# reduc 1e-10), recorded from the GPU solver; the oracle matches the GPU
-# count to +-2 iterations (tests/test_gpu_parity.py).  Used only by the
-# reference arm, which cannot afford to run the ~20-minute CPU solve.
-FULL_ITERS = {(256, "pcg", 0): 2616, (64, "pcg", 0): 715}
+# Full-solve iteration counts of plain FP64 Jacobi PCG (reduc 1e-10) on the
+# default systems, recorded from the GPU solver (the oracle matches the GPU
+# count to +-2 iterations, tests/test_gpu_parity.py).  Only the reference
+# arm uses them: it cannot afford the ~20-minute single-core CPU solve.
+FULL_ITERS = {256: 2616, 128: 1448, 64: 715}
 
 PEAK_FALLBACK_GBS = 6650.0
+METRIC = "s/solve to 1e-10 rel resid (learned+mixed vs plain FP64 PCG); SpMV HBM GB/s"
 
 
 def _env_int(k, d):
@@ -70,11 +77,18 @@ def build_system(size: int, seed: int = 0):
     return A, b
 
 
-def spmv_bytes(A, k=1, fp=8):
+def spmv_bytes(A, fp=8, k=1):
     """Algorithmic bytes of one matrix product: F*(8+fp*k) + 3*fp*N
     (index pair + k coefficients per interior face; diag, x, y per cell)."""
     F = int((A.inb > 0).sum())
     return F * (8 + fp * k) + 3 * fp * A.n_cell
+
+
+def apply_bytes(A):
+    """Algorithmic bytes of one application of the learned preconditioner:
+    per face an index pair and one FP32 weight, per cell q, r, z (FP32)."""
+    F = int((A.inb > 0).sum())
+    return F * 12 + 12 * A.n_cell
 
 
 class ClockSampler:
@@ -86,6 +100,7 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.out = ""
 
     def __enter__(self):
         try:
@@ -98,7 +113,6 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
-        self.out = ""
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -128,9 +142,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def _traffic_from_profile(size):
-    """DRAM bytes per SpMV launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"spmv_fp64_pressure_{size}.txt")
+def _traffic_from_profile(name):
+    """DRAM bytes per launch from a committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -142,49 +156,55 @@ def _traffic_from_profile(size):
     return None
 
 
-def cpu_baseline(A, b, imat, iters_full, budget_s=15.0):
-    """Oracle (single core, the reference is serial) on a bounded sample."""
+def cpu_baseline(A, b, iters_full, budget_s=15.0):
+    """Oracle plain PCG (single core: the reference is serial) on a bounded sample."""
     from oracle.oracle import Oracle
     o = Oracle.from_matrix(A)
     rhs = b.reshape(-1, 1)
     t = time.perf_counter()
-    o.solv_cg(imat, 1e-10, 2, np.zeros((A.n_cell, 1)), rhs)
-    t2 = time.perf_counter() - t
-    s = max(2, min(200, int(budget_s / max(t2 / 2, 1e-6))))
+    o.solv_cg(0, 1e-10, 2, np.zeros((A.n_cell, 1)), rhs)
+    per = (time.perf_counter() - t) / 2
+    s = max(2, min(200, int(budget_s / max(per, 1e-6))))
     t = time.perf_counter()
-    o.solv_cg(imat, 1e-10, s, np.zeros((A.n_cell, 1)), rhs)
+    o.solv_cg(0, 1e-10, s, np.zeros((A.n_cell, 1)), rhs)
     dt = time.perf_counter() - t
-    per_iter = dt / s
-    return per_iter * iters_full, s, dt
+    return dt / s * iters_full, s, dt
+
+
+def _config(args, A):
+    return {"workload": f"pressure Poisson {args.size}^3 jittered hex, solve to 1e-10 L1-relative",
+            "n_cell": A.n_cell, "n_face_interior": int((A.inb > 0).sum()),
+            "method": args.method, "baseline_method": "plain FP64 Jacobi PCG",
+            "ordering": "RCM", "l2": "inputs larger than L2 (no flush needed)",
+            "parallelism": "replicas"}
 
 
 def run_reference(args, rank):
     if rank != 0:
         return
     A, b = build_system(args.size, seed=0)
-    key = (args.size, "pcg", args.imat)
-    iters = FULL_ITERS.get(key)
+    iters = FULL_ITERS.get(args.size)
     if iters is None:
         print(json.dumps({"impl": "reference", "unavailable":
-                          f"no recorded full-solve iteration count for {key}"}))
+                          f"no recorded full-solve iteration count for size {args.size}"}))
         return
     from oracle.oracle import Oracle
     o = Oracle.from_matrix(A)
     rhs = b.reshape(-1, 1)
     t = time.perf_counter()
-    o.solv_cg(args.imat, 1e-10, 2, np.zeros((A.n_cell, 1)), rhs)
+    o.solv_cg(0, 1e-10, 2, np.zeros((A.n_cell, 1)), rhs)
     per = (time.perf_counter() - t) / 2
     sample = max(2, min(100, int(20.0 / max(per, 1e-6))))
     for _ in range(args.warmup):
-        o.solv_cg(args.imat, 1e-10, 1, np.zeros((A.n_cell, 1)), rhs)
+        o.solv_cg(0, 1e-10, 1, np.zeros((A.n_cell, 1)), rhs)
     times = []
     for _ in range(args.steps):
         t = time.perf_counter()
-        o.solv_cg(args.imat, 1e-10, sample, np.zeros((A.n_cell, 1)), rhs)
+        o.solv_cg(0, 1e-10, sample, np.zeros((A.n_cell, 1)), rhs)
         times.append((time.perf_counter() - t) / sample * iters)
     v = statistics.mean(times)
-    desc = (f"{sample} PCG iterations of the {args.size}^3 system per step, scaled by the "
-            f"{iters}-iteration full solve")
+    desc = (f"{sample} PCG iterations of the {args.size}^3 system per step (single core; the "
+            f"reference is serial), scaled by the {iters}-iteration full solve")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "s/solve",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -197,16 +217,6 @@ def run_reference(args, rank):
     }))
 
 
-METRIC = "s/solve to 1e-10 rel resid (learned+mixed vs plain FP64 PCG); SpMV HBM GB/s"
-
-
-def _config(args, A):
-    return {"workload": f"pressure Poisson {args.size}^3 jittered hex, PCG to 1e-10 L1-relative",
-            "n_cell": A.n_cell, "n_face_interior": int((A.inb > 0).sum()),
-            "method": args.method, "imat": args.imat, "ordering": "RCM",
-            "l2": "inputs larger than L2 (no flush needed)", "parallelism": "replicas"}
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -214,9 +224,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=256)
-    ap.add_argument("--method", default="pcg", choices=["pcg"])
-    ap.add_argument("--imat", type=int, default=0)
+    ap.add_argument("--method", default="learned", choices=["learned", "mixed", "plain"])
+    ap.add_argument("--weights", default=None)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
     args = ap.parse_args()
 
     rank = _env_int("RANK", 0)
@@ -227,7 +238,8 @@ def main():
         return
 
     import torch
-    from programs_b200.solver import GpuSolver
+    from programs_b200.learn import DEFAULT_WEIGHTS, load_params
+    from programs_b200.solver import GpuSolver, OPT_PRECISION
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
@@ -237,107 +249,137 @@ def main():
 
     t0 = time.perf_counter()
     A, b = build_system(args.size, seed=rank)
-    setup_s = time.perf_counter() - t0
     N = A.n_cell
     s = GpuSolver(local)
     stream = torch.cuda.Stream()
     s.set_stream(stream.cuda_stream)
     s.matrix_set(A)
+    setup_s = time.perf_counter() - t0
+    if args.method == "learned":
+        s.gnn_set_params(load_params(args.weights or DEFAULT_WEIGHTS))
     dev = torch.device("cuda", local)
     b_dev = torch.from_numpy(b).to(dev).reshape(N, 1)
     phi = torch.zeros(N, 1, dtype=torch.float64, device=dev)
     res0 = torch.empty(N, 1, dtype=torch.float64, device=dev)
+    tune = None
+    if not args.no_tune:
+        s.set_option(OPT_PRECISION, 1 if args.method != "plain" else 0)
+        tune = s.autotune("cg", 0, 1)
     torch.cuda.synchronize()
 
-    def solve():
+    def solve(method):
+        s.set_option(OPT_PRECISION, 0 if method == "plain" else 1)
         with torch.cuda.stream(stream):
             phi.zero_()
             res0.copy_(b_dev)
-        return s.solv_cg_dev(args.imat, 1e-10, 100000, 1, phi.data_ptr(), res0.data_ptr())
+        if method == "learned":
+            return s.solv_fcg_dev(1e-10, 100000, phi.data_ptr(), res0.data_ptr())
+        return s.solv_cg_dev(0, 1e-10, 100000, 1, phi.data_ptr(), res0.data_ptr())
 
-    for _ in range(max(args.warmup, 1)):
-        rn, st = solve()
-    iters = st["iters"][0]
-    launches = 0
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    def timed(method, steps, warmup, clocks=False):
+        for _ in range(max(warmup, 1)):
+            rn, st = solve(method)
+        launches = 0
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = ClockSampler(local) if clocks else None
+        if clk:
+            clk.__enter__()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
-            rn, st = solve()
+        for _ in range(steps):
+            rn, st = solve(method)
             launches += st["kernel_launches"] + 2
         e1.record(stream)
         torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    ms_per_step = ms / args.steps
-    value = ms_per_step / 1e3 / world  # seconds per solve, whole job
+        if clk:
+            clk.__exit__()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / steps, st, launches, (clk.summary() if clk else None)
 
-    # solution check: true residual of the last solve
+    ms_step, st, launches, clocks = timed(args.method, args.steps, args.warmup, clocks=True)
     x = phi.double().cpu().numpy().reshape(-1)
-    r_true = b - (A.to_scipy() @ x) if N <= 2_500_000 else None
+    r_true = b - (A.to_scipy() @ x)
+    true_rel = float(np.abs(r_true).sum() / np.abs(b).sum())
+    ms_plain, st_plain, _, _ = (timed("plain", 2, 1) if args.method != "plain"
+                                else (ms_step, st, 0, None))
+    x_plain = phi.double().cpu().numpy().reshape(-1)
+    ms_mixed, st_mixed, _, _ = (timed("mixed", 2, 1) if args.method != "mixed"
+                                else (ms_step, st, 0, None))
+    # solution agreement of the measured method with plain FP64 PCG
+    rel_vs_plain = float(np.linalg.norm(x - x_plain) / np.linalg.norm(x_plain))
 
-    # e2e: host C-ABI call, pinned host buffers, copies inside the timed region
+    # e2e: the measured method through the host C-ABI, pinned host buffers,
+    # both copies inside the timed region
     phi_h = torch.zeros(N, 1, dtype=torch.float64).pin_memory().numpy()
     res_h = torch.zeros(N, 1, dtype=torch.float64).pin_memory().numpy()
-    res_h_f = np.asfortranarray(res_h)
+    s.set_option(OPT_PRECISION, 0 if args.method == "plain" else 1)
     e2e = []
     for k in range(args.steps + 1):
         phi_h[:] = 0.0
-        res_h_f[:, 0] = b
+        res_h[:, 0] = b
         rn_h = np.zeros(1)
         torch.cuda.synchronize()
         t = time.perf_counter()
-        s.solv_cg(args.imat, 1e-10, 100000, phi_h, res_h_f, rn_h)
+        if args.method == "learned":
+            s.solv_fcg(1e-10, 100000, phi_h, res_h, rn_h)
+        else:
+            s.solv_cg(0, 1e-10, 100000, phi_h, res_h, rn_h)
         dt = time.perf_counter() - t
         if k > 0:
             e2e.append(dt)
-    e2e_v = statistics.mean(e2e) / world
 
-    # roofline of the dominant kernel (the matrix product), CUDA events on the
-    # solver's stream around back-to-back launches
-    x_dev = torch.from_numpy(np.random.default_rng(1).uniform(-1, 1, N)).to(dev)
-    y_dev = torch.empty_like(x_dev)
-    torch.cuda.synchronize()
-    s.spmv_dev(x_dev.data_ptr(), y_dev.data_ptr(), repeat=3)
-    spmv_ms = s.spmv_dev(x_dev.data_ptr(), y_dev.data_ptr(), repeat=20)
-    alg = spmv_bytes(A, k=1, fp=8)
+    # rooflines: kernels of the solve timed live on the solver's stream
     peak, peak_kind = _peaks()
-    achieved = alg / (spmv_ms * 1e-3) / 1e9
-    traffic = _traffic_from_profile(args.size)
+    kt = {"spmv_fp64": s.kernel_time(0, 20), "spmv_fp32": s.kernel_time(1, 20)}
+    alg = {"spmv_fp64": spmv_bytes(A, 8), "spmv_fp32": spmv_bytes(A, 4)}
+    if args.method == "learned":
+        kt["precond_apply"] = s.kernel_time(2, 20)
+        alg["precond_apply"] = apply_bytes(A)
+    gbs = {k: alg[k] / (kt[k] * 1e-3) / 1e9 for k in kt}
+    dominant = "spmv_fp64" if args.method == "plain" else "spmv_fp32"
+    traffic = _traffic_from_profile(f"{dominant}_pressure_{args.size}.txt")
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, sample, dt = cpu_baseline(A, b, args.imat, iters)
+        v, sample, dt = cpu_baseline(A, b, st_plain["iters"][0])
         cpu = {"value": v, "unit": "s/solve", "cores": 1, "kind": "port",
-               "sample": f"{sample} oracle PCG iterations ({dt:.1f} s) of this system, "
-                         f"scaled to the {iters}-iteration solve"}
+               "sample": f"{sample} oracle PCG iterations ({dt:.1f} s, single core) of this "
+                         f"system, scaled to the {st_plain['iters'][0]}-iteration plain solve"}
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "s/solve", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "metric": METRIC, "value": ms_step / 1e3 / world, "unit": "s/solve", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "config": _config(args, A),
-            "iterations": iters, "final_ratio": st["ratio"][0],
-            "true_rel_resid_l1": (float(np.abs(r_true).sum() / np.abs(b).sum())
-                                  if r_true is not None else None),
-            "e2e": {"value": e2e_v, "unit": "s/solve", "h2d_bytes_per_step": 2 * N * 8,
-                    "d2h_bytes_per_step": 2 * N * 8 + 8},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "SpMV (sliced-ELL face gather)",
-                         "alg_bytes_per_launch": alg, "launch_ms": spmv_ms,
+            "dtype": "f64 (outer) / f32 (inner) / bf16 (network)" if args.method != "plain"
+                     else "f64",
+            "data": "synthetic", "config": _config(args, A),
+            "iterations": st["iters"][0], "reliable_updates": st["refinements"],
+            "fallbacks": st["fallbacks"], "true_rel_resid_l1": true_rel,
+            "rel_diff_vs_plain_fp64": rel_vs_plain,
+            "plain_fp64_pcg": {"s_per_solve": ms_plain / 1e3, "iterations": st_plain["iters"][0]},
+            "mixed_pcg": {"s_per_solve": ms_mixed / 1e3, "iterations": st_mixed["iters"][0]},
+            "speedup_vs_plain_fp64": ms_plain / ms_step,
+            "e2e": {"value": statistics.mean(e2e) / world, "unit": "s/solve",
+                    "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8 + 8},
+            "roofline": {"bound": "hbm", "achieved": gbs[dominant], "peak": peak, "unit": "GB/s",
+                         "frac": gbs[dominant] / peak, "traffic": traffic,
+                         "kernel": f"{dominant} (sliced-ELL face gather)",
+                         "alg_bytes_per_launch": alg[dominant], "launch_ms": kt[dominant],
                          "peak_kind": peak_kind},
+            "spmv_gbs": {k: round(v, 1) for k, v in gbs.items()},
+            "spmv_frac_of_peak": {k: round(v / peak, 3) for k, v in gbs.items()},
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "gpu_launches": launches,
+            "autotune": tune,
             "setup_s": setup_s,
         }
         print(json.dumps(line))

@@ -143,6 +143,13 @@ int solv_gpu_bicg_dev(solv_gpu_ctx *ctx, int imat, double reduc, int n_iter,
                       double *res0_n, int not_r0, solv_gpu_stats *stats);
 int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
                       int repeat, float *ms_per_call);
+/* Device time per launch (CUDA events on the context's stream, `repeat`
+ * back-to-back launches on workspace vectors) of a kernel of the solve
+ * path: which 0 = FP64 matrix product, 1 = FP32 matrix product, 2 = the
+ * learned preconditioner's application (FP32).  No counterpart in the
+ * reference; used for roofline reporting. */
+int solv_gpu_kernel_time(solv_gpu_ctx *ctx, int which, int repeat,
+                         float *ms_per_launch);
 
 /* -- learned preconditioner ---------------------------------------------- */
 /* No counterpart in the reference.  Flexible CG, FCG(1), in FP32 with

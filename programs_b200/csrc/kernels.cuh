@@ -158,22 +158,60 @@ struct RowIt {
   }
 };
 
-// y = A x for V interleaved components; y_i = pl_i x_i + sum in face order.
+// y = A x for V interleaved components.
+// FP64: y_i = pl_i x_i + sum in face order (the reference's arithmetic).
+// FP32: difference form y_i = rs_i x_i + sum_j a_ij (x_j - x_i), where the
+// FP32 "diagonal" holds the row sum rs_i = pl_i + sum_j a_ij (formed in
+// FP64).  For the smooth vectors late Krylov iterations produce, x_j - x_i
+// is exact and small, so the product keeps its relative accuracy instead of
+// losing log10(cond) digits to cancellation; same bytes moved.
 template <typename T, int V>
 __device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
                                           const T* __restrict__ x, T (&y)[V]) {
   RowIt<T> it(R, i);
   const T d = R.diag[i];
+  if constexpr (sizeof(T) == 4) {
+    T xi[V];
 #pragma unroll
-  for (int v = 0; v < V; ++v) y[v] = mul(d, x[(size_t)i * V + v]);
-  for (int k = 0; k < it.w; ++k) {
-    const int e = it.base + k * kWarp;
-    const int j = __ldg(&R.col[e]);
-    if (j >= 0) {
-      const T a = R.val[e];
-#pragma unroll
-      for (int v = 0; v < V; ++v) y[v] = add(y[v], mul(a, x[(size_t)j * V + v]));
+    for (int v = 0; v < V; ++v) {
+      xi[v] = x[(size_t)i * V + v];
+      y[v] = d * xi[v];
     }
+    for (int k = 0; k < it.w; ++k) {
+      const int e = it.base + k * kWarp;
+      const int j = __ldg(&R.col[e]);
+      if (j >= 0) {
+        const T a = R.val[e];
+#pragma unroll
+        for (int v = 0; v < V; ++v) y[v] = fmaf(a, x[(size_t)j * V + v] - xi[v], y[v]);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int v = 0; v < V; ++v) y[v] = mul(d, x[(size_t)i * V + v]);
+    for (int k = 0; k < it.w; ++k) {
+      const int e = it.base + k * kWarp;
+      const int j = __ldg(&R.col[e]);
+      if (j >= 0) {
+        const T a = R.val[e];
+#pragma unroll
+        for (int v = 0; v < V; ++v) y[v] = add(y[v], mul(a, x[(size_t)j * V + v]));
+      }
+    }
+  }
+}
+
+// FP32 row-sum "diagonal" for the difference-form product: rs_i = pl_i +
+// sum_j a_ij, formed in FP64 then rounded once.
+__global__ void k_rowsum_diag(int n, Rows<double> R, float* __restrict__ rs) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    RowIt<double> it(R, i);
+    double s = R.diag[i];
+    for (int k = 0; k < it.w; ++k) {
+      const int e = it.base + k * kWarp;
+      if (R.col[e] >= 0) s += R.val[e];
+    }
+    rs[i] = (float)s;
   }
 }
 

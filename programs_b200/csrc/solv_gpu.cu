@@ -405,8 +405,8 @@ int ensure_f32_matrix(solv_gpu_ctx* c) {
     sg::k_convert<double, float><<<grid_for(c, c->n_slots), c->block, 0, c->stream>>>(
         c->n_slots, c->sval.as<double>(), c->svalf.as<float>());
   }
-  sg::k_convert<double, float><<<grid_for(c, c->N), c->block, 0, c->stream>>>(
-      c->N, c->diag.as<double>(), c->diagf.as<float>());
+  sg::k_rowsum_diag<<<grid_for(c, c->N), c->block, 0, c->stream>>>(c->N, rows<double>(c),
+                                                                   c->diagf.as<float>());
   CUDA_TRY(c, cudaGetLastError());
   c->f32_valid = true;
   return SOLV_GPU_OK;
@@ -1116,13 +1116,21 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->lanes.p, nl * sizeof(Lane), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(c, cudaStreamSynchronize(s));
     bool need = false;
+    bool fell_back = false;
+    std::vector<char> trig(nl, 0);
     for (int l = 0; l < nl; ++l) {
       if (final_[l]) continue;
-      if (!hl[l].active || hl[l].l1 < delta * l1_last[l]) need = true;
+      if (!hl[l].active || hl[l].l1 < delta * l1_last[l]) need = trig[l] = 1;
       if (cur == 2 && hl[l].status == sg::kLaneStall) {
         cur = 0;  // no positive curvature from the network: plain PCG from here
+        fell_back = true;
         c->fallbacks++;
       }
+    }
+    if (fell_back) {  // restart the search direction (it may hold NaN)
+      CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
+      CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
+      for (int l = 0; l < nl; ++l) hl[l].s_prev = 0.0;
     }
     if (!need && launched <= n_iter + K) continue;
     // reliable update of every lane still in play
@@ -1156,8 +1164,9 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
       } else if (L.iter >= n_iter || launched > n_iter + K) {
         final_[l] = 1;
         status_v[l] = sg::kLaneMaxIter;
-      } else {
-        // the FP64 residual stopped improving between updates: FP32 floor
+      } else if (trig[l]) {
+        // this lane asked for the update but its FP64 residual did not
+        // improve on the last one it asked for: FP32 floor
         stalls[l] = l1[l] > 0.9 * l1_last[l] ? stalls[l] + 1 : 0;
         if (stalls[l] >= 3) {
           final_[l] = 1;
@@ -1165,7 +1174,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
         }
       }
       if (final_[l]) L.active = 0;
-      l1_last[l] = l1[l];
+      if (trig[l]) l1_last[l] = l1[l];  // lanes along for the ride keep their window
       na += L.active;
     }
     CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
@@ -1472,6 +1481,62 @@ int solv_gpu_spmv_dev(solv_gpu_ctx* c, const double* x_dev, double* y_dev, int r
   return SOLV_GPU_OK;
 }
 
+// Device time of one kernel of the solve path, timed with events on the
+// context's stream over `repeat` back-to-back launches on workspace vectors:
+// which 0 = FP64 matrix product, 1 = FP32 matrix product, 2 = the learned
+// preconditioner's application (FP32; needs parameters, builds M^-1 from a
+// constant residual first).
+int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_launch) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  if (which < 0 || which > 2 || repeat < 1 || !ms_per_launch)
+    return set_err(c, SOLV_GPU_BAD_INPUT, "kernel_time: bad arguments");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  const int N = c->N;
+  cudaStream_t s = c->stream;
+  int rc;
+  if (which == 0) {
+    WS<double> w;
+    if ((rc = ensure_ws<double>(c, 1, w))) return rc;
+    CUDA_TRY(c, cudaMemsetAsync(w.p, 0, N * sizeof(double), s));
+    sg::k_spmv<double, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
+    CUDA_TRY(c, cudaEventRecord(c->ev0, s));
+    for (int k = 0; k < repeat; ++k)
+      sg::k_spmv<double, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
+    CUDA_TRY(c, cudaEventRecord(c->ev1, s));
+  } else {
+    WS<float> f;
+    if ((rc = ensure_ws<float>(c, 1, f))) return rc;
+    if ((rc = ensure_f32_matrix(c))) return rc;
+    CUDA_TRY(c, cudaMemsetAsync(f.p, 0, N * sizeof(float), s));
+    if (which == 2) {
+      if ((rc = gnn_prepare(c))) return rc;
+      Lane L{};
+      L.active = 1;
+      L.gs = 1.0;
+      CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, &L, sizeof(Lane), cudaMemcpyHostToDevice, s));
+      gnn_build<float>(c, f.p);
+    }
+    auto launch = [&]() {
+      if (which == 1)
+        sg::k_spmv<float, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<float>(c), f.p, f.q);
+      else
+        gnn::k_gnn_apply<float><<<grid_for(c, N), c->block, 0, s>>>(
+            N, rows<float>(c), c->g_ge.as<float>(), c->g_q.as<float>(), f.p, f.q, nullptr);
+    };
+    launch();
+    CUDA_TRY(c, cudaEventRecord(c->ev0, s));
+    for (int k = 0; k < repeat; ++k) launch();
+    CUDA_TRY(c, cudaEventRecord(c->ev1, s));
+  }
+  CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+  CUDA_TRY(c, cudaGetLastError());
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  *ms_per_launch = ms / repeat;
+  return SOLV_GPU_OK;
+}
+
 int solv_gpu_spmv(solv_gpu_ctx* c, const double* x, double* y) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
@@ -1499,6 +1564,7 @@ static int solve_common(solv_gpu_ctx* c, int solver, int imat, double reduc, int
   if (!phi_dev || !res0_dev || !res0_n) return set_err(c, SOLV_GPU_BAD_INPUT, "null pointer");
   if (c->n_seg > 1 && !batch)
     return set_err(c, SOLV_GPU_BAD_INPUT, "a batch of systems is set: use the _batch entry points");
+  c->err.clear();
   if (st) {
     std::memset(st, 0, sizeof(*st));
     st->n_levels = (int)c->lvl_ptr.size() - 1;

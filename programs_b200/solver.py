@@ -68,6 +68,7 @@ EXPORTS = [
     "solv_gpu_fcg", "solv_gpu_fcg_dev", "solv_gpu_gnn_n_params", "solv_gpu_gnn_set_params",
     "solv_gpu_gnn_get_params", "solv_gpu_gnn_forward_dev", "solv_gpu_gnn_grad_dev",
     "solv_gpu_gnn_get_grad", "solv_gpu_gnn_zero_grad", "solv_gpu_gnn_adam",
+    "solv_gpu_kernel_time",
     "solv_gpu_create_", "solv_gpu_destroy_", "solv_gpu_matrix_set_", "solv_gpu_matrix_values_",
     "solv_gpu_res_", "solv_gpu_precond_", "solv_gpu_direct_", "solv_gpu_cg_", "solv_gpu_bicg_",
 ]
@@ -120,6 +121,8 @@ def lib():
     L.solv_gpu_gnn_grad_dev.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                         ctypes.c_int]
     L.solv_gpu_gnn_adam.argtypes = [vp, ctypes.c_float, ctypes.c_float]
+    L.solv_gpu_kernel_time.argtypes = [vp, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_float)]
     for fn in (L.solv_gpu_cg_batch, L.solv_gpu_bicg_batch):
         fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _f64p,
                        _f64p, _f64p, ctypes.c_int, _i32p, _f64p, ctypes.POINTER(Stats)]
@@ -404,6 +407,12 @@ class GpuSolver:
         d.update(res0_n=rn.reshape(-1, n_vc), iters_all=iters.reshape(-1, n_vc),
                  ratio_all=ratio.reshape(-1, n_vc))
         return d
+
+    def kernel_time(self, which: int, repeat: int = 20) -> float:
+        """ms per launch: 0 FP64 SpMV, 1 FP32 SpMV, 2 learned-preconditioner apply."""
+        ms = ctypes.c_float()
+        self._check(self._lib.solv_gpu_kernel_time(self._h, which, repeat, ctypes.byref(ms)))
+        return ms.value
 
     def spmv_dev(self, x_ptr: int, y_ptr: int, repeat: int = 1) -> float:
         ms = ctypes.c_float()
