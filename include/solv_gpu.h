@@ -52,6 +52,8 @@ extern "C" {
 #define SOLV_GPU_NO_MATRIX 7    /* no solv_gpu_matrix_set yet              */
 #define SOLV_GPU_ZERO_RHS 8     /* maxval(res0_n) < small: returned early
                                    exactly as solv_cg.f90:21 does          */
+#define SOLV_GPU_TOO_LARGE 9    /* beyond the fixed scratch of
+                                   solv_gpu_res_noalloc (n_vc > 4)         */
 
 #define SOLV_GPU_MAX_VC 4
 
@@ -238,6 +240,33 @@ int solv_gpu_bicg_batch_dev(solv_gpu_ctx *ctx, int imat, double reduc,
                             int n_iter, int n_vc, double *phi_dev,
                             double *res0_dev, double *res0_n, int not_r0,
                             int *iters, double *ratio, solv_gpu_stats *stats);
+
+/* -- residual without any allocation -------------------------------------- */
+/* No counterpart in the reference: an entry point for callers that cannot
+ * allocate device memory (their memory pool belongs to another runtime, or
+ * a long-running service forbids allocation once started).
+ * Computes solv_res (r = b - A phi, res0_n = sum |r| per component,
+ * solv_res.f90:5-30) straight from caller-owned DEVICE arrays: the face
+ * list ip/in/p/n (n_face, 1-based, in = 0 on boundary faces) and pl
+ * (n_cell), phi (cell-major), res0 (column-major; in: b, out: r) and
+ * res0_n (device, n_vc doubles).  Needs no context; runs on `stream` (a
+ * cudaStream_t, NULL for the default stream) on the current device and
+ * returns when the result is there.  It calls no cudaMalloc / cudaFree:
+ * its scratch is one fixed file-scope device array (about 19 KB per GPU
+ * that loads the library, held until exit); the first call on a device
+ * looks its address up (cudaGetSymbolAddress) -- make that first call
+ * before any stream capture.  Calls overlapping on the GPU share that
+ * scratch and race.  The scratch's counters are cleared by every call;
+ * nothing the caller passes must start at zero (res0_n is overwritten).
+ * Limits: n_vc <= 4 (SOLV_GPU_TOO_LARGE beyond).
+ * Face contributions are added with atomics, so r agrees with solv_res to
+ * rounding, not bit for bit.  Returns SOLV_GPU_BAD_INPUT if a face index is
+ * out of range. */
+int solv_gpu_res_noalloc(int n_cell, int n_face, const int *ip_dev,
+                         const int *in_dev, const double *p_dev,
+                         const double *n_dev, const double *pl_dev, int n_vc,
+                         const double *phi_dev, double *res0_dev,
+                         double *res0_n_dev, int not_r0, void *stream);
 
 /* -- Fortran bindings (gfortran mangling, everything by reference) ------ */
 /* ctx is passed as an integer(c_intptr_t) holding the context address.
