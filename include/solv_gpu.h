@@ -72,6 +72,22 @@ extern "C" {
 #define SOLV_OPT_RELIABLE_DELTA 8 /* FP32 CG: replace the recursive residual
                                    by the FP64 one each time it has dropped
                                    by this factor (default 0.1)            */
+#define SOLV_OPT_GNN_LOSS 9     /* training loss of the learned
+                                   preconditioner: 0 = energy of z,
+                                   1 = energy after the best step along z
+                                   (scale-free, default), both for the
+                                   network's operator alone; 2 = the
+                                   scale-free loss of the V-cycle with the
+                                   network as finest-level smoother        */
+#define SOLV_OPT_MG_LEVELS 10   /* learned preconditioner: coarse levels of
+                                   the aggregation hierarchy at most (default
+                                   12; 0 = the network's one-level operator
+                                   alone)                                  */
+#define SOLV_OPT_MG_SMOOTHER 11 /* finest-level smoother of the hierarchy:
+                                   1 = the network's operator (default),
+                                   0 = damped Jacobi (no network)          */
+#define SOLV_OPT_MG_OMEGA 12    /* smoother damping (default 0.8)          */
+#define SOLV_OPT_MG_ALPHA 13    /* coarse-correction scale (default 2)     */
 
 typedef struct solv_gpu_ctx solv_gpu_ctx;
 
@@ -88,6 +104,8 @@ typedef struct {
   double solve_ms;               /* device time of the solve (events)      */
   int fallbacks;                 /* learned preconditioner handed over to
                                     plain PCG (solv_gpu_fcg)               */
+  int mg_levels;                 /* coarse levels of the aggregation
+                                    hierarchy used (solv_gpu_fcg)          */
 } solv_gpu_stats;
 
 /* -- context ------------------------------------------------------------ */
@@ -155,12 +173,18 @@ int solv_gpu_kernel_time(solv_gpu_ctx *ctx, int which, int repeat,
 
 /* -- learned preconditioner ---------------------------------------------- */
 /* No counterpart in the reference.  Flexible CG, FCG(1), in FP32 with
- * FP64 reliable updates, preconditioned by M^-1 = D^-1/2 S (I + E) S D^-1/2:
- * a 3-layer, width-32 message-passing network over the face graph (BF16
- * weights, per-cell MLPs on the tensor cores, FP32 accumulate) reads the
- * cell diagonal, the face coefficients and the initial residual once per
- * solve and emits the per-cell scales S and the symmetric face weights E
- * (|E| < 1 by construction, so M^-1 is symmetric positive definite).  If
+ * FP64 reliable updates.  A 3-layer, width-32 message-passing network over
+ * the face graph (BF16 weights, per-cell MLPs on the tensor cores, FP32
+ * accumulate) reads the cell diagonal, the face coefficients and the
+ * initial residual once per solve and emits the per-cell scales S and the
+ * symmetric face weights E of K = D^-1/2 S (I + E) S D^-1/2 (|E| < 1 by
+ * construction, so K is symmetric positive definite).  K is the finest-
+ * level smoother of a symmetric V-cycle over an aggregation hierarchy
+ * (about 8 cells per aggregate, Galerkin coarse matrices, damped Jacobi on
+ * the coarse levels, dense inverse on the coarsest), and the V-cycle is the
+ * preconditioner (SOLV_OPT_MG_*; the hierarchy is built on the host at the
+ * first such solve after solv_gpu_matrix_set, from the coefficients then;
+ * SOLV_OPT_MG_LEVELS 0 uses K alone).  If
  * the iteration loses positive curvature or produces NaN, plain Jacobi-PCG
  * takes over from the current iterate (stats.fallbacks); the FP64 residual
  * test |b - A x|_1 / |r0|_1 < reduc decides convergence either way.  Same
@@ -172,6 +196,12 @@ int solv_gpu_fcg(solv_gpu_ctx *ctx, double reduc, int n_iter, double *phi,
 int solv_gpu_fcg_dev(solv_gpu_ctx *ctx, double reduc, int n_iter,
                      double *phi_dev, double *res0_dev, double *res0_n,
                      int not_r0, solv_gpu_stats *stats);
+/* Aggregation of the hierarchy: for each cell of level - 1 (caller order
+ * for level 1, i.e. the caller's cells), the index of its aggregate on
+ * `level` (1..levels); n = that finer level's size, *n_coarse = the size of
+ * `level`.  Builds the hierarchy if needed. */
+int solv_gpu_mg_aggregates(solv_gpu_ctx *ctx, int level, int *agg, int n,
+                           int *n_coarse);
 /* Network parameters (FP32 master copy, solv_gpu_gnn_n_params() floats). */
 int solv_gpu_gnn_n_params(void);
 int solv_gpu_gnn_set_params(solv_gpu_ctx *ctx, const float *params, int n);

@@ -124,8 +124,10 @@ def precondition(A, r0, r, params):
     return _apply(q, gE.detach(), rows_t, cols_t, rt).numpy()
 
 
-def loss(A, r0, samples, params, grad=False):
-    """Mean over samples of J/N, J = 1/2 z.Â z - z.u, z = K u (scaled space)."""
+def loss(A, r0, samples, params, grad=False, kind=1):
+    """Mean over samples of L/N with z = K u (scaled space):
+    kind 0: L = 1/2 z.Â z - z.u (energy of z);
+    kind 1: L = -(z.u)^2 / (z.Â z) (energy after the best step along z)."""
     s, gE, rows_t, cols_t, wt, P, rsd = build(A, r0, params, grad=grad)
     N = A.n_cell
     J = 0.0
@@ -135,11 +137,83 @@ def loss(A, r0, samples, params, grad=False):
         z = _apply(s, gE, rows_t, cols_t, ut)
         az = z.clone()
         az.index_add_(0, rows_t, -wt * z[cols_t])
-        J = J + (0.5 * z @ az - z @ ut) / N
+        if kind == 0:
+            J = J + (0.5 * z @ az - z @ ut) / N
+        else:
+            J = J - (z @ ut) ** 2 / (z @ az) / N
     return J / len(samples), P
 
 
-def loss_and_grad(A, r0, samples, params):
-    J, P = loss(A, r0, samples, params, grad=True)
+def loss_and_grad(A, r0, samples, params, kind=1):
+    J, P = loss(A, r0, samples, params, grad=True, kind=kind)
+    J.backward()
+    return float(J.detach()), P.grad.numpy().copy()
+
+
+def _sparse(M):
+    M = M.tocoo()
+    idx = torch.tensor(np.vstack([M.row, M.col]), dtype=torch.int64)
+    return torch.sparse_coo_tensor(idx, torch.tensor(M.data, dtype=torch.float64), M.shape,
+                                   check_invariants=True).coalesce()
+
+
+def hierarchy(A, aggs):
+    """Galerkin levels A_{l+1} = P_l^T A_l P_l of the piecewise-constant
+    prolongations given by aggs[l] (level-l cell -> level-(l+1) aggregate)."""
+    import scipy.sparse as sp
+    mats, Ps = [A.to_scipy().tocsr()], []
+    for a in aggs:
+        a = np.asarray(a)
+        P = sp.csr_matrix((np.ones(len(a)), (np.arange(len(a)), a)), shape=(len(a), int(a.max()) + 1))
+        Ps.append(P)
+        mats.append((P.T @ mats[-1] @ P).tocsr())
+    return mats, Ps
+
+
+def vcycle(mats, Ps, b, smooth0, omega, alpha, l=0):
+    """One symmetric V-cycle on level l: w S b pre-smoothing from zero,
+    coarse correction scaled by alpha, w S post-smoothing; S = smooth0 on
+    level 0, D^-1 below; the coarsest level solved exactly (torch, float64)."""
+    A = mats[l]
+    if l == len(mats) - 1:
+        return torch.linalg.solve(torch.tensor(A.toarray()), b)
+    At = _sparse(A)
+    if l == 0:
+        S = smooth0
+    else:
+        dinv = torch.tensor(1.0 / A.diagonal())
+        S = lambda v: dinv * v
+    mv = lambda v: torch.sparse.mm(At, v[:, None])[:, 0]
+    Pt = _sparse(Ps[l])
+    x = omega * S(b)
+    t = b - mv(x)
+    xc = vcycle(mats, Ps, torch.sparse.mm(Pt.t(), t[:, None])[:, 0], smooth0, omega, alpha, l + 1)
+    x = x + alpha * torch.sparse.mm(Pt, xc[:, None])[:, 0]
+    return x + omega * S(b - mv(x))
+
+
+def loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=False):
+    """Mean over samples of L/N, L = -(z.b)^2/(z.A z) with z the V-cycle
+    applied to b = r / gs, the network's operator K = D^-1/2 S (I+E) S D^-1/2
+    smoothing level 0 (the loss the GPU trains with through the V-cycle)."""
+    s, gE, rows_t, cols_t, wt, P, rsd = build(A, r0, params, grad=grad)
+    rsd_t = torch.tensor(rsd, dtype=torch.float64)
+    K = lambda v: rsd_t * _apply(s, gE, rows_t, cols_t, rsd_t * v)
+    mats, Ps = hierarchy(A, aggs)
+    At = _sparse(mats[0])
+    N = A.n_cell
+    J = 0.0
+    for r in samples:
+        _, gs = _scaled(r, rsd)
+        b = torch.tensor(np.asarray(r, np.float64).astype(np.float32).astype(np.float64) / gs,
+                         dtype=torch.float64)
+        z = vcycle(mats, Ps, b, K, omega, alpha)
+        az = torch.sparse.mm(At, z[:, None])[:, 0]
+        J = J - (z @ b) ** 2 / (z @ az) / N
+    return J / len(samples), P
+
+
+def loss_mg_and_grad(A, r0, samples, params, aggs, omega, alpha):
+    J, P = loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=True)
     J.backward()
     return float(J.detach()), P.grad.numpy().copy()

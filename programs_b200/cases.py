@@ -18,7 +18,8 @@ import time
 import numpy as np
 
 from .mesh import Mesh, poisson_rhs, uniform
-from .solver import GpuSolver, OPT_GRAPH_ITERS, OPT_PRECISION
+from .solver import (GpuSolver, OPT_GRAPH_ITERS, OPT_MG_ALPHA, OPT_MG_LEVELS, OPT_MG_OMEGA,
+                     OPT_MG_SMOOTHER, OPT_PRECISION)
 
 
 def make_system(size, system="pressure", seed=0, renumber="rcm"):
@@ -68,12 +69,20 @@ def main(argv=None):
     ap.add_argument("--n-sys", type=int, default=64)
     ap.add_argument("--min", type=int, default=8000)
     ap.add_argument("--max", type=int, default=500000)
+    ap.add_argument("--mg-levels", type=int, default=12, help="fcg: coarse levels (0 = one-level)")
+    ap.add_argument("--smoother", type=int, default=1, help="fcg: 1 network, 0 Jacobi")
+    ap.add_argument("--omega", type=float, default=0.8)
+    ap.add_argument("--alpha", type=float, default=2.0)
     a = ap.parse_args(argv)
 
     import torch
     s = GpuSolver(0)
     s.set_option(OPT_GRAPH_ITERS, a.graph_iters)
     s.set_option(OPT_PRECISION, a.precision)
+    s.set_option(OPT_MG_LEVELS, a.mg_levels)
+    s.set_option(OPT_MG_SMOOTHER, a.smoother)
+    s.set_option(OPT_MG_OMEGA, a.omega)
+    s.set_option(OPT_MG_ALPHA, a.alpha)
     out = {"case": a.what}
     if a.what == "batch":
         mats, rhs = batch_meshes(a.n_sys, a.min, a.max)
@@ -115,21 +124,24 @@ def main(argv=None):
             bd = torch.from_numpy(np.asfortranarray(B).ravel(order="F")).to(dev)
             phi = torch.zeros(A.n_cell * V, dtype=torch.float64, device=dev)
             res0 = torch.empty_like(bd)
-            ts = []
+            ts, walls = [], []
             for _ in range(a.repeat):
                 phi.zero_()
                 res0.copy_(bd)
                 torch.cuda.synchronize()
+                t0 = time.perf_counter()
                 if a.solver == "fcg":
                     rn, st = s.solv_fcg_dev(1e-10, 100000, phi.data_ptr(), res0.data_ptr())
                 else:
                     fn = s.solv_cg_dev if a.solver == "cg" else s.solv_bicg_dev
                     rn, st = fn(a.imat, 1e-10, 100000, V, phi.data_ptr(), res0.data_ptr())
+                walls.append(time.perf_counter() - t0)
                 ts.append(st["solve_ms"])
             out.update(n_cell=A.n_cell, levels=s.levels, solve_ms=min(ts), iters=st["iters"],
                        ratio=st["ratio"], refinements=st["refinements"],
                        kernel_launches=st["kernel_launches"], status=st["status"],
-                       fallbacks=st["fallbacks"])
+                       fallbacks=st["fallbacks"], mg_levels=st["mg_levels"],
+                       first_call_s=walls[0])
     s.close()
     print(json.dumps(out))
 

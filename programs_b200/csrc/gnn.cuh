@@ -370,6 +370,57 @@ __global__ void k_gnn_loss_grad(int n, sg::Rows<float> R, Feat F, const float* _
   }
 }
 
+// Scale-free variant of the loss: the energy after the best step along z,
+// L = -(z.u)^2 / (z.Â z), whose gradient is 2 a (a Â z - u) with
+// a = z.u / z.Â z -- CG does not see the scale of M^-1, and neither does L.
+// Pass 1: Âz and the sums z.Âz, z.u; pass 2 (this kernel): g from them.
+__global__ void k_gnn_az_sums(int n, sg::Rows<float> R, Feat F, const float* __restrict__ z,
+                              const float* __restrict__ u, float* __restrict__ az_out,
+                              double* __restrict__ sums) {
+  double a0 = 0.0, a1 = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    sg::RowIt<float> it(R, i);
+    float az = z[i];
+    for (int k = 0; k < it.w; ++k) {
+      const int e = it.base + k * sg::kWarp;
+      const int j = R.col[e];
+      if (j >= 0) az -= F.gw[e] * z[j];
+    }
+    az_out[i] = az;
+    a0 += (double)z[i] * az;
+    a1 += (double)z[i] * u[i];
+  }
+  a0 = sg::warp_sum(a0);
+  a1 = sg::warp_sum(a1);
+  __shared__ double sh[2][32];
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = a0;
+    sh[1][threadIdx.x >> 5] = a1;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const bool in = threadIdx.x < (blockDim.x + 31) / 32;
+    double v0 = in ? sh[0][threadIdx.x] : 0.0, v1 = in ? sh[1][threadIdx.x] : 0.0;
+    v0 = sg::warp_sum(v0);
+    v1 = sg::warp_sum(v1);
+    if (threadIdx.x == 0) {
+      atomicAdd(&sums[0], v0);
+      atomicAdd(&sums[1], v1);
+    }
+  }
+}
+// g = 2 a (a Â z - u), a = z.u / z.Âz; adds L = -(z.u)^2/(z.Âz) to jsum
+// (once, from thread 0 of block 0).
+__global__ void k_gnn_scalefree_grad(int n, const float* __restrict__ az,
+                                     const float* __restrict__ u, const double* __restrict__ sums,
+                                     float* __restrict__ g, double* __restrict__ jsum) {
+  const double zaz = sums[0] > 0.0 ? sums[0] : 1e-300, zu = sums[1];
+  const double a = zu / zaz;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    g[i] = (float)(2.0 * a * (a * (double)az[i] - (double)u[i]));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *jsum += -zu * zu / zaz;
+}
+
 // Backward through z = S (I + E) S u for one sample (S = diag(s)):
 //   y = s u, dt = s g, t = y + E y, dy = dt + E dt,
 //   ds_i  += g_i t_i + dy_i u_i

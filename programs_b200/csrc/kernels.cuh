@@ -499,11 +499,14 @@ __global__ void k_lane_init(Lane* lanes, int nl, int n_iter, double reduc, int* 
 }
 
 // s = r.z with z = M^-1 r (Jacobi: z = c r, computed here); then
-// beta = (1/s_old) s, s_old = s  (solv_cg.f90:44-50)
-template <typename T, int V, bool JAC>
+// beta = (1/s_old) s, s_old = s  (solv_cg.f90:44-50).
+// FLEX (the FP32 inner iteration, not the reference's): beta = -(z.q)/(p.q)
+// with q = A p of the previous step, the flexible-CG formula that
+// A-orthogonalises the new direction against the last one explicitly.
+template <typename T, int V, bool JAC, bool FLEX = false>
 __global__ void k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
                         const T* __restrict__ z, double* __restrict__ part,
-                        Lane* __restrict__ lanes) {
+                        Lane* __restrict__ lanes, const T* __restrict__ q = nullptr) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   bool any = false;
 #pragma unroll
@@ -519,7 +522,7 @@ __global__ void k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict_
     for (int v = 0; v < V; ++v) {
       const T ri = r[(size_t)i * V + v];
       const T zi = JAC ? mul(ri, c[i]) : z[(size_t)i * V + v];
-      acc[v] += prod(ri, zi);
+      acc[v] += FLEX ? prod(zi, q[(size_t)i * V + v]) : prod(ri, zi);
     }
   }
   double tot[V];
@@ -528,6 +531,10 @@ __global__ void k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict_
     for (int v = 0; v < V; ++v) {
       Lane& L = lanes[s * V + v];
       if (!L.active) continue;
+      if (FLEX) {
+        L.beta = L.pq > 0.0 ? -tot[v] / L.pq : 0.0;
+        continue;
+      }
       double beta = 1.0 / L.s;   // :44
       L.s_prev = L.s;
       L.s = tot[v];              // :47
@@ -536,11 +543,13 @@ __global__ void k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict_
   }
 }
 
-// p = z + beta p  (solv_cg.f90:53)
-template <typename T, int V, bool JAC>
+// p = z + beta p  (solv_cg.f90:53).  FLEX: also s = p.r, so that the step
+// alpha = (p.r)/(p.q) of k_cg_spmv makes the new residual orthogonal to p
+// in the arithmetic actually done (flexible CG).
+template <typename T, int V, bool JAC, bool FLEX = false>
 __global__ void k_cg_p(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
                        const T* __restrict__ z, T* __restrict__ p,
-                       const Lane* __restrict__ lanes) {
+                       Lane* __restrict__ lanes, double* __restrict__ part = nullptr) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   bool act[V];
   T beta[V];
@@ -554,13 +563,27 @@ __global__ void k_cg_p(SegMap sm, const T* __restrict__ c, const T* __restrict__
   if (!any) return;
   const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
   const int stride = sm.seg_nblk[s] * blockDim.x;
+  double acc[V];
+#pragma unroll
+  for (int v = 0; v < V; ++v) acc[v] = 0.0;
   for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       if (!act[v]) continue;
       const size_t k = (size_t)i * V + v;
-      const T zi = JAC ? mul(r[k], c[i]) : z[k];
-      p[k] = add(zi, mul(beta[v], p[k]));
+      const T ri = (JAC || FLEX) ? r[k] : T(0);
+      const T zi = JAC ? mul(ri, c[i]) : z[k];
+      const T pn = add(zi, mul(beta[v], p[k]));
+      p[k] = pn;
+      if (FLEX) acc[v] += prod(pn, ri);
+    }
+  }
+  if constexpr (FLEX) {
+    double tot[V];
+    if (seg_commit<V>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        if (act[v]) lanes[s * V + v].s = tot[v];
     }
   }
 }
@@ -601,8 +624,9 @@ __global__ void k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __re
 }
 
 // phi += alpha p; r -= alpha q; L1 = sum|r|; stop test (solv_cg.f90:73-82).
-// With JAC, also s_next = r.(c r) and beta for the next iteration.
-template <typename T, int V, bool JAC>
+// With JAC, also s_next = r.(c r) and beta for the next iteration; with
+// JAC and FLEX, beta = -(z.q)/(p.q) instead, z = c r of the new residual.
+template <typename T, int V, bool JAC, bool FLEX = false>
 __global__ void k_cg_update(SegMap sm, const T* __restrict__ c, T* __restrict__ phi,
                             T* __restrict__ r, const T* __restrict__ p,
                             const T* __restrict__ q, double* __restrict__ part,
@@ -633,7 +657,7 @@ __global__ void k_cg_update(SegMap sm, const T* __restrict__ c, T* __restrict__ 
       const T rn = sub(r[k], mul(alpha[v], q[k]));
       r[k] = rn;
       acc[v] += (double)fabs(rn);
-      if (JAC) acc[V + v] += prod(rn, mul(rn, c[i]));
+      if (JAC) acc[V + v] += FLEX ? prod(mul(rn, c[i]), q[k]) : prod(rn, mul(rn, c[i]));
     }
   }
   double tot[NR];
@@ -649,7 +673,9 @@ __global__ void k_cg_update(SegMap sm, const T* __restrict__ c, T* __restrict__ 
       if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);
       else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);  // :82
       else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
-      if (JAC && L.active) {
+      if (JAC && FLEX && L.active) {
+        L.beta = L.pq > 0.0 ? -tot[V + v] / L.pq : 0.0;
+      } else if (JAC && L.active) {
         double beta = 1.0 / L.s;
         L.s_prev = L.s;
         L.s = tot[V + v];
@@ -853,42 +879,6 @@ __global__ void k_bi_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
 }
 
 // ================ reliable updates for the mixed-precision CG =================
-// After the FP64 residual has replaced the FP32 recursive one, the Jacobi
-// form's fused s = r.(c r) (computed from the old residual in k_cg_update)
-// is recomputed from the new residual, with beta = s_new / s_prev, so the
-// search direction carries on instead of restarting.
-template <typename T, int V>
-__global__ void k_cg_replace_rz(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
-                                double* __restrict__ part, Lane* __restrict__ lanes) {
-  const int b = blockIdx.x, s = sm.blk_seg[b];
-  bool any = false;
-#pragma unroll
-  for (int v = 0; v < V; ++v) any |= lanes[s * V + v].active != 0;
-  if (!any) return;
-  const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
-  const int stride = sm.seg_nblk[s] * blockDim.x;
-  double acc[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) acc[v] = 0.0;
-  for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      const T ri = r[(size_t)i * V + v];
-      acc[v] += prod(ri, mul(ri, c[i]));
-    }
-  }
-  double tot[V];
-  if (seg_commit<V>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
-#pragma unroll
-    for (int v = 0; v < V; ++v) {
-      Lane& L = lanes[s * V + v];
-      if (!L.active) continue;
-      L.s = tot[v];
-      L.beta = L.s_prev > 0.0 ? (1.0 / L.s_prev) * L.s : 0.0;
-    }
-  }
-}
-
 // d (FP32 correction since the last update) -> x (FP64) for every lane
 // flagged in mask, and d = 0.
 template <int V>
@@ -999,28 +989,26 @@ __global__ void k_fcg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __r
 }
 
 template <typename T>
-__global__ void k_fcg_update(SegMap sm, const float* __restrict__ rsd, T* __restrict__ phi,
-                             T* __restrict__ r, const T* __restrict__ p, const T* __restrict__ q,
+__global__ void k_fcg_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
+                             const T* __restrict__ p, const T* __restrict__ q,
                              double* __restrict__ part, Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   if (!lanes[s].active) return;
   const T alpha = (T)lanes[s].alpha;
   const int c0 = sm.seg_c0[s], c1 = sm.seg_c1[s];
   const int stride = sm.seg_nblk[s] * blockDim.x;
-  double acc[2] = {0.0, 0.0};
+  double acc[1] = {0.0};
   for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
     phi[i] = add(phi[i], mul(alpha, p[i]));
     const T rn = sub(r[i], mul(alpha, q[i]));
     r[i] = rn;
     acc[0] += fabs((double)rn);
-    acc[1] += fabs((double)rn) * rsd[i];
   }
-  double tot[2];
-  if (seg_commit<2>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
+  double tot[1];
+  if (seg_commit<1>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
     Lane& L = lanes[s];
     L.iter += 1;
     L.l1 = tot[0];
-    L.gs = tot[1] / (double)(c1 - c0);
     const double ratio = tot[0] / (L.res0_n + kSmall);
     L.ratio = ratio;
     if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -23,6 +24,7 @@
 #include "../../include/solv_gpu.h"
 #include "kernels.cuh"
 #include "gnn.cuh"
+#include "mg.cuh"
 
 using sg::Lane;
 using sg::Rows;
@@ -45,6 +47,27 @@ struct DevBuf {
     return e;
   }
   template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// One coarse level of the aggregation hierarchy (mg.cuh); level l's
+// aggregation arrays map level l-1 cells to level l cells.
+struct MgLevel {
+  int n = 0;
+  long long n_slots = 0;
+  DevBuf slice_ptr, slice_w, col, val, rs, dinv;
+  DevBuf gptr, gsrc;                  // coarse slot <- finer slots
+  DevBuf agg_ptr, agg_cells, agg_of;  // members (finer numbering); finer cell -> cell
+  DevBuf x, b, t, y;                  // V-cycle vectors
+  Rows<float> rows() const {
+    Rows<float> R;
+    R.slice_ptr = slice_ptr.as<int>();
+    R.slice_w = slice_w.as<uint8_t>();
+    R.col = col.as<int>();
+    R.val = val.as<float>();
+    R.sval = val.as<float>();
+    R.diag = rs.as<float>();
+    return R;
+  }
 };
 
 // Host-side description of the segment (system) -> block map.
@@ -70,6 +93,7 @@ struct solv_gpu_ctx {
   int max_refine = 30;
   int inner_max_iter = 2000;
   double reliable_delta = 0.1;
+  int gnn_loss = 1;  // training loss: 0 energy, 1 scale-free (best-step energy)
 
   // matrix (caller sizes)
   bool has_matrix = false;
@@ -111,6 +135,18 @@ struct solv_gpu_ctx {
   bool g_feat_valid = false, g_wcat_valid = false, g_has_params = false;
   int g_adam_t = 0;
   int fallbacks = 0;
+
+  // aggregation multigrid around the learned preconditioner (mg.cuh)
+  int mg_max_levels = mg::kMaxLevels;  // coarse levels at most; 0 = one-level preconditioner
+  int mg_smoother = 1;                 // level-0 smoother: 1 the network's operator, 0 Jacobi
+  double mg_omega = 0.8;               // smoother damping (1.0 loses the V-cycle)
+  double mg_alpha = 2.0;               // coarse-correction scale (unsmoothed
+                                       // aggregation under-corrects smooth error)
+  bool mg_valid = false;               // hierarchy built for the current structure
+  std::vector<std::unique_ptr<MgLevel>> mg;  // coarse levels 1..L
+  DevBuf mg_x0, mg_t0, mg_dinv0, mg_dense, mg_ainv;
+  DevBuf mg_train;                     // training through the V-cycle: 8 vectors
+  double mg_setup_s = 0.0;
 };
 
 namespace {
@@ -346,6 +382,8 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
   c->n_slice = ns;
   c->f32_valid = false;
   c->g_feat_valid = false;
+  c->mg_valid = false;
+  c->mg.clear();
   cudaStream_t st = c->stream;
   CUDA_TRY(c, c->old_of_new.ensure(N * sizeof(int)));
   CUDA_TRY(c, c->slice_ptr.ensure((ns + 1) * sizeof(int)));
@@ -496,6 +534,211 @@ void gnn_build(solv_gpu_ctx* c, const T* r0) {
   c->launches += 3 + gnn::NL;
 }
 
+// ---- aggregation multigrid (mg.cuh) -----------------------------------------------
+template <typename V>
+cudaError_t upload(DevBuf& d, const std::vector<V>& h, cudaStream_t s) {
+  cudaError_t e = d.ensure(std::max<size_t>(h.size(), 1) * sizeof(V));
+  if (e != cudaSuccess || h.empty()) return e;
+  return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, s);
+}
+
+// Build the hierarchy for the current structure from the coefficients
+// present now (host aggregation; once per structure).  A hierarchy that
+// cannot reach kCoarsest cells (coarsening stalls) is not used: the solve
+// then runs with the one-level preconditioner.
+int mg_setup(solv_gpu_ctx* c) {
+  if (c->mg_valid) return SOLV_GPU_OK;
+  auto t0 = std::chrono::steady_clock::now();
+  int rc = ensure_f32_matrix(c);
+  if (rc) return rc;
+  drop_graphs(c);
+  c->mg.clear();
+  cudaStream_t s = c->stream;
+  // level 0 from the device
+  int n = c->N;
+  const int ns0 = c->n_slice;
+  std::vector<int> sp(ns0 + 1), col(c->n_slots);
+  std::vector<uint8_t> sw(ns0);
+  std::vector<float> val(c->n_slots), rs(n);
+  CUDA_TRY(c, cudaMemcpyAsync(sp.data(), c->slice_ptr.p, (ns0 + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaMemcpyAsync(sw.data(), c->slice_w.p, ns0, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaMemcpyAsync(col.data(), c->col.p, c->n_slots * sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaMemcpyAsync(val.data(), c->valf.p, c->n_slots * sizeof(float), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  std::vector<std::unique_ptr<MgLevel>> levels;
+  bool ok = n > mg::kCoarsest;
+  while (ok && n > mg::kCoarsest) {
+    if ((int)levels.size() >= std::min(c->mg_max_levels, mg::kMaxLevels)) { ok = false; break; }
+    mg::Graph g = mg::graph_of(n, sp, sw, col, val);
+    std::vector<int> agg;
+    const int nc = mg::aggregate(g, 3, agg);
+    if (nc > 0.75 * n) { ok = false; break; }  // coarsening stalled
+    mg::CoarseHost C;
+    if (!mg::build_coarse(n, sp, sw, col, agg, nc, C)) { ok = false; break; }
+    // coarse coefficients on the host too (the next aggregation's strengths)
+    std::vector<float> cval(C.n_slots, 0.0f);
+    for (long long e = 0; e < C.n_slots; ++e) {
+      double a = 0.0;
+      for (int k = C.gptr[e]; k < C.gptr[e + 1]; ++k) a += val[C.gsrc[k]];
+      cval[e] = (float)a;
+    }
+    auto L = std::make_unique<MgLevel>();
+    L->n = nc;
+    L->n_slots = C.n_slots;
+    CUDA_TRY(c, upload(L->slice_ptr, C.slice_ptr, s));
+    CUDA_TRY(c, upload(L->slice_w, C.slice_w, s));
+    CUDA_TRY(c, upload(L->col, C.col, s));
+    CUDA_TRY(c, upload(L->gptr, C.gptr, s));
+    CUDA_TRY(c, upload(L->gsrc, C.gsrc, s));
+    CUDA_TRY(c, upload(L->agg_ptr, C.agg_ptr, s));
+    CUDA_TRY(c, upload(L->agg_cells, C.agg_cells, s));
+    CUDA_TRY(c, upload(L->agg_of, C.agg_of, s));
+    const size_t vb = (size_t)nc * sizeof(float);
+    CUDA_TRY(c, L->val.ensure(std::max<long long>(C.n_slots, 1) * sizeof(float)));
+    CUDA_TRY(c, L->rs.ensure(vb));
+    CUDA_TRY(c, L->dinv.ensure(vb));
+    CUDA_TRY(c, L->x.ensure(vb));
+    CUDA_TRY(c, L->b.ensure(vb));
+    CUDA_TRY(c, L->t.ensure(vb));
+    CUDA_TRY(c, L->y.ensure(vb));
+    CUDA_TRY(c, cudaStreamSynchronize(s));  // host arrays die below
+    levels.push_back(std::move(L));
+    sp.swap(C.slice_ptr);
+    sw.swap(C.slice_w);
+    col.swap(C.col);
+    val.swap(cval);
+    n = nc;
+  }
+  c->mg_valid = true;
+  if (!ok || levels.empty()) {
+    c->mg.clear();
+    c->mg_setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return SOLV_GPU_OK;
+  }
+  c->mg = std::move(levels);
+  const int nL = c->mg.back()->n;
+  CUDA_TRY(c, c->mg_x0.ensure((size_t)c->N * sizeof(float)));
+  CUDA_TRY(c, c->mg_t0.ensure((size_t)c->N * sizeof(float)));
+  CUDA_TRY(c, c->mg_dinv0.ensure((size_t)c->N * sizeof(float)));
+  CUDA_TRY(c, c->mg_dense.ensure((size_t)nL * nL * sizeof(double)));
+  CUDA_TRY(c, c->mg_ainv.ensure((size_t)nL * nL * sizeof(float)));
+  c->mg_setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return SOLV_GPU_OK;
+}
+
+// Coefficients of every coarse level for the current values (each solve):
+// Galerkin sums level by level, inverse diagonals, the coarsest inverse.
+int mg_values(solv_gpu_ctx* c) {
+  int rc = ensure_f32_matrix(c);
+  if (rc) return rc;
+  cudaStream_t s = c->stream;
+  const int B = c->block;
+  mg::k_mg_dinv<<<grid_for(c, c->N), B, 0, s>>>(c->N, rows<float>(c), c->mg_dinv0.as<float>());
+  const float* vprev = c->valf.as<float>();
+  const float* rsprev = c->diagf.as<float>();
+  for (auto& L : c->mg) {
+    mg::k_mg_gather_slots<<<grid_for(c, L->n_slots), B, 0, s>>>(
+        L->n_slots, L->gptr.as<int>(), L->gsrc.as<int>(), vprev, L->val.as<float>());
+    mg::k_mg_rowsum<<<grid_for(c, L->n), B, 0, s>>>(L->n, L->agg_ptr.as<int>(),
+                                                    L->agg_cells.as<int>(), rsprev, L->rs.as<float>());
+    mg::k_mg_dinv<<<grid_for(c, L->n), B, 0, s>>>(L->n, L->rows(), L->dinv.as<float>());
+    vprev = L->val.as<float>();
+    rsprev = L->rs.as<float>();
+  }
+  MgLevel& C = *c->mg.back();
+  mg::k_mg_dense<<<grid_for(c, C.n), B, 0, s>>>(C.n, C.rows(), c->mg_dense.as<double>());
+  mg::k_mg_invert<<<1, 1024, 0, s>>>(C.n, c->mg_dense.as<double>(), c->mg_ainv.as<float>());
+  c->launches += 2 + 3 * (int)c->mg.size() + 2;
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
+}
+
+// The V-cycle below level 0: level 1's right-hand side mg[0]->b in, its
+// correction mg[0]->y out.  Returns the number of kernels launched.
+int mg_coarse_cycle(solv_gpu_ctx* c, const int* na) {
+  cudaStream_t s = c->stream;
+  const int B = c->block;
+  const float w = (float)c->mg_omega, a = (float)c->mg_alpha;
+  const int L = (int)c->mg.size();
+  int k = 0;
+  for (int l = 0; l + 1 < L; ++l) {
+    MgLevel& F = *c->mg[l];
+    MgLevel& C = *c->mg[l + 1];
+    mg::k_mg_pre<<<grid_for(c, F.n), B, 0, s>>>(F.n, F.rows(), F.dinv.as<float>(), w,
+                                                F.b.as<float>(), F.x.as<float>(),
+                                                F.t.as<float>(), na);
+    mg::k_mg_restrict<<<grid_for(c, C.n), B, 0, s>>>(C.n, C.agg_ptr.as<int>(),
+                                                     C.agg_cells.as<int>(), F.t.as<float>(),
+                                                     C.b.as<float>(), na);
+    k += 2;
+  }
+  {
+    MgLevel& C = *c->mg[L - 1];
+    mg::k_mg_coarse_solve<<<1, mg::kCoarseBlock, 0, s>>>(C.n, c->mg_ainv.as<float>(),
+                                                         C.b.as<float>(), C.y.as<float>(), na);
+    k += 1;
+  }
+  for (int l = L - 2; l >= 0; --l) {
+    MgLevel& F = *c->mg[l];
+    MgLevel& C = *c->mg[l + 1];
+    mg::k_mg_prolong<<<grid_for(c, F.n), B, 0, s>>>(F.n, C.agg_of.as<int>(), a, C.y.as<float>(),
+                                                    F.x.as<float>(), na);
+    mg::k_mg_post<float><<<grid_for(c, F.n), B, 0, s>>>(F.n, F.rows(), F.dinv.as<float>(), w,
+                                                        F.b.as<float>(), F.x.as<float>(),
+                                                        F.y.as<float>(), na);
+    k += 2;
+  }
+  return k;
+}
+
+// z = one symmetric V-cycle applied to r (FP32, level 0 = the context's
+// matrix).  The network's operator (q, gE) smooths level 0 when net, damped
+// Jacobi otherwise.  x0 and t0 hold, afterwards, the level-0 iterate before
+// post-smoothing and its residual.  Returns the number of kernels launched.
+template <typename TZ>
+int mg_vcycle(solv_gpu_ctx* c, const float* r, TZ* z, bool net, const float* q, const float* ge,
+              float* x0, float* t0, const int* na) {
+  cudaStream_t s = c->stream;
+  const int B = c->block;
+  const float w = (float)c->mg_omega, a = (float)c->mg_alpha;
+  const int N = c->N;
+  Rows<float> R0 = rows<float>(c);
+  const float* d0 = c->mg_dinv0.as<float>();
+  MgLevel& L1 = *c->mg[0];
+  int k = 0;
+  if (net) {
+    mg::k_mg_net<false, float><<<grid_for(c, N), B, 0, s>>>(N, R0, ge, q, w, r, nullptr, x0, na);
+    mg::k_mg_resid<<<grid_for(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
+    k += 2;
+  } else {
+    mg::k_mg_pre<<<grid_for(c, N), B, 0, s>>>(N, R0, d0, w, r, x0, t0, na);
+    k += 1;
+  }
+  mg::k_mg_restrict<<<grid_for(c, L1.n), B, 0, s>>>(L1.n, L1.agg_ptr.as<int>(),
+                                                    L1.agg_cells.as<int>(), t0, L1.b.as<float>(),
+                                                    na);
+  k += 1 + mg_coarse_cycle(c, na);
+  mg::k_mg_prolong<<<grid_for(c, N), B, 0, s>>>(N, L1.agg_of.as<int>(), a, L1.y.as<float>(), x0,
+                                                na);
+  k += 1;
+  if (net) {
+    mg::k_mg_resid<<<grid_for(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
+    mg::k_mg_net<true, TZ><<<grid_for(c, N), B, 0, s>>>(N, R0, ge, q, w, t0, x0, z, na);
+    k += 2;
+  } else {
+    mg::k_mg_post<TZ><<<grid_for(c, N), B, 0, s>>>(N, R0, d0, w, r, x0, z, na);
+    k += 1;
+  }
+  return k;
+}
+
+// Kernels in one V-cycle (launch statistics of graph replays).
+int mg_kernels(const solv_gpu_ctx* c) {
+  const int L = (int)c->mg.size();
+  const int fine = c->mg_smoother == 1 ? 5 : 3;  // smoothing, residual, prolongation
+  return fine + 1 + 2 * (L - 1) + 1 + 2 * (L - 1);
+}
+
 // ---- building blocks -----------------------------------------------------------
 template <int V>
 void launch_res(solv_gpu_ctx* c, const double* phi, double* r, int not_r0) {
@@ -590,9 +833,14 @@ int ensure_ws(solv_gpu_ctx* c, int V, WS<T>& w) {
   return SOLV_GPU_OK;
 }
 
-// One CG iteration (solv_cg.f90:37-84) on workspace w.
+// One CG iteration (solv_cg.f90:37-84) on workspace w.  The FP32 inner
+// iteration of the mixed-precision solve takes the flexible-CG step and
+// direction formulas (FLEX in kernels.cuh): FP32 products lose the
+// orthogonality the classic formulas rely on, and on a 256^3 pressure system
+// the classic ones needed several times the FP64 iteration count.
 template <typename T, int V>
 void cg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
+  constexpr bool FLEX = std::is_same<T, float>::value;
   SegMap sm = segmap(c);
   double* part = c->part.as<double>();
   Lane* lanes = c->lanes.as<Lane>();
@@ -600,15 +848,17 @@ void cg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
   cudaStream_t st = c->stream;
   if (imat > 0) {
     launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active);
-    sg::k_cg_rz<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, part, lanes);
-    sg::k_cg_p<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes);
+    sg::k_cg_rz<T, V, false, FLEX><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, part, lanes, w.q);
+    sg::k_cg_p<T, V, false, FLEX><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes, part);
     sg::k_cg_spmv<T, V><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, part, lanes);
-    sg::k_cg_update<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.p, w.q, part, lanes);
+    sg::k_cg_update<T, V, false, FLEX><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.p, w.q, part,
+                                                        lanes);
     c->launches += 4;
   } else {
-    sg::k_cg_p<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes);
+    sg::k_cg_p<T, V, true, FLEX><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes, part);
     sg::k_cg_spmv<T, V><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, part, lanes);
-    sg::k_cg_update<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.p, w.q, part, lanes);
+    sg::k_cg_update<T, V, true, FLEX><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.p, w.q, part,
+                                                       lanes);
     c->launches += 3;
   }
 }
@@ -641,7 +891,9 @@ void bicg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
   c->launches += 5;
 }
 
-// One flexible-CG iteration with the learned preconditioner (one system).
+// One flexible-CG iteration with the learned preconditioner (one system):
+// z from one V-cycle of the aggregation hierarchy when one is built, else
+// from the network's one-level operator.
 template <typename T>
 void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
   SegMap sm = segmap(c);
@@ -649,14 +901,22 @@ void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
   Lane* lanes = c->lanes.as<Lane>();
   const int G = c->seg.total_blk, B = c->block;
   cudaStream_t st = c->stream;
-  gnn::k_gnn_apply<T><<<grid_for(c, c->N), B, 0, st>>>(c->N, rows<float>(c), c->g_ge.as<float>(),
-                                                        c->g_q.as<float>(), w.r, w.z,
-                                                        sm.n_active);      // z = M^-1 r
+  int nk = 1;
+  if constexpr (std::is_same<T, float>::value) {
+    if (!c->mg.empty())  // z = V-cycle(r)
+      nk = mg_vcycle<T>(c, w.r, w.z, c->mg_smoother == 1, c->g_q.as<float>(),
+                        c->g_ge.as<float>(), c->mg_x0.as<float>(), c->mg_t0.as<float>(),
+                        sm.n_active);
+  }
+  if (c->mg.empty())
+    gnn::k_gnn_apply<T><<<grid_for(c, c->N), B, 0, st>>>(c->N, rows<float>(c),
+                                                          c->g_ge.as<float>(), c->g_q.as<float>(),
+                                                          w.r, w.z, sm.n_active);  // z = M^-1 r
+  c->launches += nk - 1;
   sg::k_fcg_beta<T><<<G, B, 0, st>>>(sm, w.z, w.q, part, lanes);            // beta
   sg::k_cg_p<T, 1, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes);   // p = z + beta p
   sg::k_fcg_spmv<T><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, w.r, part, lanes);
-  sg::k_fcg_update<T><<<G, B, 0, st>>>(sm, c->g_rsd.as<float>(), w.phi, w.r, w.p, w.q, part,
-                                       lanes);
+  sg::k_fcg_update<T><<<G, B, 0, st>>>(sm, w.phi, w.r, w.p, w.q, part, lanes);
   c->launches += 5;
 }
 
@@ -700,7 +960,7 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     int sweep = imat > 0 ? 2 * nl : 1;
     if (solver == 0) per_launch_kernels = imat > 0 ? sweep + 4 : 3;
     else if (solver == 1) per_launch_kernels = imat > 0 ? 2 * sweep + 5 : 5;
-    else per_launch_kernels = 5;
+    else per_launch_kernels = 4 + (c->mg.empty() ? 1 : mg_kernels(c));
     c->launches = l0;
   }
   while (done < n_iter) {
@@ -1092,11 +1352,15 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
   SegMap sm = segmap(c);
   const int G = c->seg.total_blk, B = c->block;
   if (solver == 2) {  // the learned preconditioner of this solve, from r0
-    if ((rc = gnn_prepare(c))) return rc;
-    sg::k_fcg_scale<float><<<G, B, 0, s>>>(sm, f.r, c->g_rsd.as<float>(), c->part.as<double>(),
-                                          c->lanes.as<Lane>());
-    gnn_build<float>(c, f.r);
-    c->launches++;
+    if (c->mg_max_levels > 0 && (rc = mg_setup(c))) return rc;  // may build no levels
+    if (c->mg.empty() || c->mg_smoother == 1) {
+      if ((rc = gnn_prepare(c))) return rc;
+      sg::k_fcg_scale<float><<<G, B, 0, s>>>(sm, f.r, c->g_rsd.as<float>(),
+                                            c->part.as<double>(), c->lanes.as<Lane>());
+      gnn_build<float>(c, f.r);
+      c->launches++;
+    }
+    if (!c->mg.empty() && (rc = mg_values(c))) return rc;
   } else if (imat <= 0) {
     sg::k_cg_rz<float, V, true><<<G, B, 0, s>>>(sm, f.c, f.r, f.z, c->part.as<double>(),
                                                 c->lanes.as<Lane>());
@@ -1130,7 +1394,6 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     if (fell_back) {  // restart the search direction (it may hold NaN)
       CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
       CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
-      for (int l = 0; l < nl; ++l) hl[l].s_prev = 0.0;
     }
     if (!need && launched <= n_iter + K) continue;
     // reliable update of every lane still in play
@@ -1180,14 +1443,9 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
     CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
     if (na == 0) break;
-    if (cur == 2) {
-      // M^-1 is fixed for the solve; FCG's beta uses the stored q of the
-      // last step, so nothing to recompute
-    } else if (imat <= 0) {
-      sg::k_cg_replace_rz<float, V><<<G, B, 0, s>>>(sm, f.c, f.r, c->part.as<double>(),
-                                                    c->lanes.as<Lane>());
-      c->launches++;
-    }
+    // Nothing to recompute: the flexible formulas take beta from the last
+    // step's q (the replaced residual differs from the recursive one far
+    // below beta's own accuracy) and alpha from p.r of the next step.
     CUDA_TRY(c, cudaGetLastError());
   }
   if (not_r0) {
@@ -1212,6 +1470,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     st->status = status;
     st->refinements = updates;
     st->fallbacks = c->fallbacks;
+    st->mg_levels = solver == 2 ? (int)c->mg.size() : 0;
     st->graph_launches += gl_total;
   }
   return status;
@@ -1320,9 +1579,37 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
       if (value < 1 || value > 1000) return set_err(c, SOLV_GPU_BAD_INPUT, "max refine in 1..1000");
       c->max_refine = (int)value;
       return SOLV_GPU_OK;
+    case SOLV_OPT_GNN_LOSS:
+      if (value != 0 && value != 1 && value != 2)
+        return set_err(c, SOLV_GPU_BAD_INPUT, "gnn loss is 0, 1 or 2");
+      c->gnn_loss = (int)value;
+      return SOLV_GPU_OK;
     case SOLV_OPT_RELIABLE_DELTA:
       if (!(value > 0 && value < 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "reliable delta in (0,1)");
       c->reliable_delta = value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_MG_LEVELS:
+      if (value < 0 || value > mg::kMaxLevels)
+        return set_err(c, SOLV_GPU_BAD_INPUT, "multigrid levels in 0..12");
+      c->mg_max_levels = (int)value;
+      c->mg_valid = false;
+      c->mg.clear();
+      drop_graphs(c);
+      return SOLV_GPU_OK;
+    case SOLV_OPT_MG_SMOOTHER:
+      if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "multigrid smoother is 0 or 1");
+      c->mg_smoother = (int)value;
+      drop_graphs(c);
+      return SOLV_GPU_OK;
+    case SOLV_OPT_MG_OMEGA:
+      if (!(value > 0 && value < 2)) return set_err(c, SOLV_GPU_BAD_INPUT, "smoother damping in (0,2)");
+      c->mg_omega = value;
+      drop_graphs(c);
+      return SOLV_GPU_OK;
+    case SOLV_OPT_MG_ALPHA:
+      if (!(value > 0 && value <= 4)) return set_err(c, SOLV_GPU_BAD_INPUT, "coarse-correction scale in (0,4]");
+      c->mg_alpha = value;
+      drop_graphs(c);
       return SOLV_GPU_OK;
     case SOLV_OPT_INNER_MAX_ITER:
       if (value < 1 || value > 1e7) return set_err(c, SOLV_GPU_BAD_INPUT, "inner max iter in 1..1e7");
@@ -1726,6 +2013,31 @@ int solv_gpu_fcg_dev(solv_gpu_ctx* c, double reduc, int n_iter, double* phi, dou
   return solve_common(c, 2, 0, reduc, n_iter, 1, phi, res0, res0_n, not_r0, st);
 }
 
+int solv_gpu_mg_aggregates(solv_gpu_ctx* c, int level, int* agg, int n, int* n_coarse) {
+  if (!c || !agg || !n_coarse) return set_err(c, SOLV_GPU_BAD_INPUT, "mg aggregates: null pointer");
+  if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  int rc = mg_setup(c);
+  if (rc) return rc;
+  if (level < 1 || level > (int)c->mg.size())
+    return set_err(c, SOLV_GPU_BAD_INPUT, "mg aggregates: no such level");
+  const int nf = level == 1 ? c->N : c->mg[level - 2]->n;
+  if (n != nf) return set_err(c, SOLV_GPU_BAD_INPUT, "mg aggregates: n must be the finer level's size");
+  std::vector<int> a(nf);
+  CUDA_TRY(c, cudaMemcpyAsync(a.data(), c->mg[level - 1]->agg_of.p, nf * sizeof(int),
+                              cudaMemcpyDeviceToHost, c->stream));
+  std::vector<int> o2n;
+  if (level == 1) {
+    o2n.resize(nf);
+    CUDA_TRY(c, cudaMemcpyAsync(o2n.data(), c->old_of_new.p, nf * sizeof(int),
+                                cudaMemcpyDeviceToHost, c->stream));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < nf; ++i) agg[level == 1 ? o2n[i] : i] = a[i];
+  *n_coarse = c->mg[level - 1]->n;
+  return SOLV_GPU_OK;
+}
+
 int solv_gpu_gnn_n_params(void) { return gnn::N_PARAM; }
 
 int solv_gpu_gnn_set_params(solv_gpu_ctx* c, const float* p, int n) {
@@ -1872,6 +2184,61 @@ int solv_gpu_gnn_forward_dev(solv_gpu_ctx* c, const double* r0_dev, const double
   return SOLV_GPU_OK;
 }
 
+// One sample of the loss through the V-cycle (the smoother of level 0 is the
+// training-path network: s in B[TB_S] as q = s rsd in B[TB_Q], faces in
+// B[TB_GE]): forward V-cycle, loss L = -(z.b)^2/(z.Az) and its gradient,
+// then the adjoint of the V-cycle, which gives the gradient with respect to
+// each of the two smoother applications; the scaled-space backward kernels
+// turn those into the gradients of s and of the face pre-activations.
+static int mg_train_sample(solv_gpu_ctx* c, float** B) {
+  const int N = c->N;
+  const int G = grid_for(c, N), Bk = c->block;
+  cudaStream_t s = c->stream;
+  Rows<float> R0 = rows<float>(c);
+  gnn::Feat F = gnn_feat(c);
+  const float w = (float)c->mg_omega, a = (float)c->mg_alpha;
+  const float* rsd = c->g_rsd.as<float>();
+  const float* q = B[TB_Q];
+  const float* ge = B[TB_GE];
+  float* T = c->mg_train.as<float>();
+  float *b = T, *z = T + N, *az = T + 2 * (size_t)N, *gz = T + 3 * (size_t)N;
+  float *uh = T + 4 * (size_t)N, *gh = T + 5 * (size_t)N, *tmp = T + 6 * (size_t)N;
+  float* gx = T + 7 * (size_t)N;
+  float* x0 = c->mg_x0.as<float>();
+  float* t0 = c->mg_t0.as<float>();
+  MgLevel& L1 = *c->mg[0];
+  double* sums = c->g_jsum.as<double>() + 1;
+  auto back = [&](const float* u, const float* g) {
+    gnn::k_gnn_apply_back1<<<G, Bk, 0, s>>>(N, B[TB_S], u, g, B[TB_Y], B[TB_DT]);
+    gnn::k_gnn_apply_back2<<<G, Bk, 0, s>>>(N, R0, F, ge, B[TB_EPRE], u, g, B[TB_Y], B[TB_DT],
+                                            B[TB_DS], B[TB_ES]);
+  };
+  mg::k_mg_normalise<<<G, Bk, 0, s>>>(N, B[TB_RS], c->lanes.as<Lane>(), b);
+  mg_vcycle<float>(c, b, z, true, q, ge, x0, t0, nullptr);  // t0 = b - A x before post-smoothing
+  CUDA_TRY(c, cudaMemsetAsync(sums, 0, 2 * sizeof(double), s));
+  mg::k_mg_loss_sums<<<G, 256, 0, s>>>(N, R0, z, b, az, sums);
+  mg::k_mg_loss_grad<<<G, Bk, 0, s>>>(N, az, b, sums, gz, c->g_jsum.as<double>());
+  // post-smoother z = x + w K t: its input t0, its output gradient gz
+  mg::k_mg_scaled_pair<<<G, Bk, 0, s>>>(N, rsd, w, t0, gz, uh, gh);
+  back(uh, gh);
+  // adjoint to x (before post-smoothing): gx = gz - A (w K gz)
+  mg::k_mg_net<false, float><<<G, Bk, 0, s>>>(N, R0, ge, q, w, gz, nullptr, tmp, nullptr);
+  mg::k_mg_resid<<<G, Bk, 0, s>>>(N, R0, gz, tmp, gx, nullptr);
+  // through the coarse correction x += a P C P^T (b - A x): gx -= A (a P C P^T gx)
+  mg::k_mg_restrict<<<grid_for(c, L1.n), Bk, 0, s>>>(L1.n, L1.agg_ptr.as<int>(),
+                                                     L1.agg_cells.as<int>(), gx, L1.b.as<float>(),
+                                                     nullptr);
+  mg_coarse_cycle(c, nullptr);
+  CUDA_TRY(c, cudaMemsetAsync(tmp, 0, (size_t)N * sizeof(float), s));
+  mg::k_mg_prolong<<<G, Bk, 0, s>>>(N, L1.agg_of.as<int>(), a, L1.y.as<float>(), tmp, nullptr);
+  mg::k_mg_resid<<<G, Bk, 0, s>>>(N, R0, gx, tmp, az, nullptr);  // az = adjoint at x = w K b
+  // pre-smoother x = w K b: its input b, its output gradient az
+  mg::k_mg_scaled_pair<<<G, Bk, 0, s>>>(N, rsd, w, b, az, uh, gh);
+  back(uh, gh);
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
+}
+
 // Forward + backward of the energy loss J = 1/2 z.Â z - z.u, z = K u, for
 // the preconditioner built from r0 and the n_samples residual samples r_k
 // (each n_cell long, caller layout, consecutive; each normalised to unit
@@ -1895,19 +2262,42 @@ int solv_gpu_gnn_grad_dev(solv_gpu_ctx* c, const double* r0_dev, const double* s
   const float* P = c->g_param.as<float>();
   float* G = c->g_grad.as<float>();
   const int* o2n = c->old_of_new.as<int>();
-  CUDA_TRY(c, c->g_jsum.ensure(sizeof(double)));
+  CUDA_TRY(c, c->g_jsum.ensure(3 * sizeof(double)));
   CUDA_TRY(c, cudaMemsetAsync(c->g_jsum.p, 0, sizeof(double), c->stream));
   CUDA_TRY(c, cudaMemsetAsync(B[TB_DS], 0, N * sizeof(float), c->stream));
   CUDA_TRY(c, cudaMemsetAsync(B[TB_ES], 0, N * sizeof(float), c->stream));
+  if (c->gnn_loss == 2) {  // through the V-cycle: hierarchy and smoother in the original space
+    if ((rc = mg_setup(c))) return rc;
+    if (c->mg.empty())
+      return set_err(c, SOLV_GPU_BAD_INPUT, "gnn grad: the multigrid loss needs a hierarchy "
+                                            "(system too small, or coarsening stalled)");
+    if ((rc = mg_values(c))) return rc;
+    CUDA_TRY(c, c->mg_train.ensure((size_t)8 * N * sizeof(float)));
+    k_gnn_mul<<<grid_for(c, N), c->block, 0, c->stream>>>(N, B[TB_S], c->g_rsd.as<float>(),
+                                                           B[TB_Q]);
+  }
   for (int k = 0; k < n_samples; ++k) {
     if ((rc = gnn_load_residual(c, samples_dev + (size_t)k * N, B[TB_RS]))) return rc;
+    if (c->gnn_loss == 2) {
+      if ((rc = mg_train_sample(c, B))) return rc;
+      continue;
+    }
     // gnn_load_residual permuted the sample in; normalise it
     k_gnn_scaled_u<<<grid_for(c, N), c->block, 0, c->stream>>>(N, c->g_rsd.as<float>(), B[TB_RS],
                                                               c->lanes.as<Lane>(), B[TB_US]);
     gnn::k_gnn_apply<float><<<grid_for(c, N), c->block, 0, c->stream>>>(
         N, rows<float>(c), B[TB_GE], B[TB_S], B[TB_US], B[TB_ZS], nullptr);
-    gnn::k_gnn_loss_grad<<<grid_for(c, N), 256, 0, c->stream>>>(
-        N, rows<float>(c), F, B[TB_ZS], B[TB_US], B[TB_GS], c->g_jsum.as<double>());
+    if (c->gnn_loss == 0) {
+      gnn::k_gnn_loss_grad<<<grid_for(c, N), 256, 0, c->stream>>>(
+          N, rows<float>(c), F, B[TB_ZS], B[TB_US], B[TB_GS], c->g_jsum.as<double>());
+    } else {  // scale-free: energy after the best step along z
+      double* sums = c->g_jsum.as<double>() + 1;
+      CUDA_TRY(c, cudaMemsetAsync(sums, 0, 2 * sizeof(double), c->stream));
+      gnn::k_gnn_az_sums<<<grid_for(c, N), 256, 0, c->stream>>>(N, rows<float>(c), F, B[TB_ZS],
+                                                                B[TB_US], B[TB_GS], sums);
+      gnn::k_gnn_scalefree_grad<<<grid_for(c, N), 256, 0, c->stream>>>(
+          N, B[TB_GS], B[TB_US], sums, B[TB_GS], c->g_jsum.as<double>());
+    }
     gnn::k_gnn_apply_back1<<<grid_for(c, N), c->block, 0, c->stream>>>(N, B[TB_S], B[TB_US],
                                                                       B[TB_GS], B[TB_Y], B[TB_DT]);
     gnn::k_gnn_apply_back2<<<grid_for(c, N), c->block, 0, c->stream>>>(

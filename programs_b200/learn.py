@@ -7,9 +7,14 @@ a_P the momentum diagonal of the current velocity field) on jittered hex
 meshes of a lid-driven cavity: jitter uniform in [0, 0.25], lid velocity in
 [0.1, 2].  Each mesh contributes several systems (different flow states);
 each system several residuals, taken from the Jacobi-PCG iterates the
-plain solver visits.  The loss is the energy J = 1/2 z'Az - z'r in the
-Jacobi-scaled space, minimised by z = A^-1 r, so no reference solutions
-are needed.  Forward, backward and the Adam step run on the GPU in the
+plain solver visits.  The losses need no reference solutions: with z the
+preconditioned residual, the energy J = 1/2 z'Az - z'r (loss 0, minimised
+by z = A^-1 r) or the scale-free -(z'r)^2/(z'Az) (the energy after the
+best step along z, which is what one CG step takes, free in the overall
+scale of z as flexible CG is), for z = K r with the network's operator K
+alone (losses 0 and 1) or for z = V(r), the V-cycle of the aggregation
+hierarchy with K as its finest-level smoother (loss 2, the default: the
+preconditioner solv_gpu_fcg applies), differentiated through the V-cycle.  Forward, backward and the Adam step run on the GPU in the
 library's own kernels; this module only orchestrates.
 
   python -m programs_b200.learn --size 64 --systems 2000 --out weights.npz
@@ -108,9 +113,11 @@ def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=400):
 
 
 def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
-          init=None, log_every=50, device=0):
+          init=None, log_every=50, device=0, loss=2):
     import torch
+    from .solver import OPT_GNN_LOSS
     s = GpuSolver(device)
+    s.set_option(OPT_GNN_LOSS, loss)
     p = init_params(seed) if init is None else np.asarray(init, np.float32)
     s.gnn_set_params(p)
     rng = np.random.default_rng(seed + 7)
@@ -128,10 +135,10 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
                 s.matrix_values(P.p, P.n, P.pl)
             b_dev = torch.from_numpy(b).to(dev)
             rs = _residual_samples(s, b_dev, samples, rng, torch)
-            loss = s.gnn_grad_dev(b_dev.data_ptr(), rs.data_ptr(), rs.shape[0])
+            val = s.gnn_grad_dev(b_dev.data_ptr(), rs.data_ptr(), rs.shape[0])
             s.gnn_adam(lr, 1.0)
             step += 1
-            hist.append(loss)
+            hist.append(val)
             if log_every and step % log_every == 0:
                 print(json.dumps({"step": step, "loss": float(np.mean(hist[-log_every:])),
                                   "t": round(time.time() - t0, 1)}), flush=True)
@@ -150,12 +157,16 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--resume", default=None)
+    ap.add_argument("--loss", type=int, default=2,
+                    help="0 energy, 1 scale-free (network alone), 2 scale-free through the V-cycle")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     a = ap.parse_args(argv)
     init = load_params(a.resume) if a.resume else None
     t = time.time()
-    p, hist = train(a.size, a.meshes, a.per_mesh, a.samples, a.epochs, a.lr, a.seed, init)
-    meta = {"size": a.size, "systems": a.meshes * a.per_mesh * a.epochs, "samples": a.samples,
+    p, hist = train(a.size, a.meshes, a.per_mesh, a.samples, a.epochs, a.lr, a.seed, init,
+                    loss=a.loss)
+    meta = {"size": a.size, "loss": a.loss, "systems": a.meshes * a.per_mesh * a.epochs,
+            "samples": a.samples,
             "lr": a.lr, "seed": a.seed, "first_loss": float(np.mean(hist[:20])),
             "last_loss": float(np.mean(hist[-20:])), "train_s": round(time.time() - t, 1)}
     save_params(a.out, p, meta)

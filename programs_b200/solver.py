@@ -29,6 +29,8 @@ OK, MAXITER, NAN, BAD_INPUT, DEVICE_ERROR, NO_MATRIX, ZERO_RHS = 0, 1, 3, 4, 5, 
 MAX_VC = 4
 OPT_PRECISION, OPT_INNER_REDUC, OPT_GRAPH_ITERS, OPT_BLOCK, OPT_GRID_PER_SM, OPT_MAX_REFINE = (
     1, 2, 3, 4, 5, 6)
+OPT_INNER_MAX_ITER, OPT_RELIABLE_DELTA, OPT_GNN_LOSS = 7, 8, 9
+OPT_MG_LEVELS, OPT_MG_SMOOTHER, OPT_MG_OMEGA, OPT_MG_ALPHA = 10, 11, 12, 13
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -39,7 +41,8 @@ class Stats(ctypes.Structure):
                 ("ratio", ctypes.c_double * MAX_VC), ("status", ctypes.c_int),
                 ("n_levels", ctypes.c_int), ("refinements", ctypes.c_int),
                 ("graph_launches", ctypes.c_int), ("kernel_launches", ctypes.c_int),
-                ("solve_ms", ctypes.c_double), ("fallbacks", ctypes.c_int)]
+                ("solve_ms", ctypes.c_double), ("fallbacks", ctypes.c_int),
+                ("mg_levels", ctypes.c_int)]
 
     def as_dict(self):
         V = self.n_vc
@@ -47,7 +50,7 @@ class Stats(ctypes.Structure):
                 "status": self.status, "n_levels": self.n_levels,
                 "refinements": self.refinements, "graph_launches": self.graph_launches,
                 "kernel_launches": self.kernel_launches, "solve_ms": self.solve_ms,
-                "fallbacks": self.fallbacks}
+                "fallbacks": self.fallbacks, "mg_levels": self.mg_levels}
 
 
 class Tune(ctypes.Structure):
@@ -68,7 +71,7 @@ EXPORTS = [
     "solv_gpu_fcg", "solv_gpu_fcg_dev", "solv_gpu_gnn_n_params", "solv_gpu_gnn_set_params",
     "solv_gpu_gnn_get_params", "solv_gpu_gnn_forward_dev", "solv_gpu_gnn_grad_dev",
     "solv_gpu_gnn_get_grad", "solv_gpu_gnn_zero_grad", "solv_gpu_gnn_adam",
-    "solv_gpu_kernel_time",
+    "solv_gpu_kernel_time", "solv_gpu_mg_aggregates",
     "solv_gpu_create_", "solv_gpu_destroy_", "solv_gpu_matrix_set_", "solv_gpu_matrix_values_",
     "solv_gpu_res_", "solv_gpu_precond_", "solv_gpu_direct_", "solv_gpu_cg_", "solv_gpu_bicg_",
 ]
@@ -123,6 +126,7 @@ def lib():
     L.solv_gpu_gnn_adam.argtypes = [vp, ctypes.c_float, ctypes.c_float]
     L.solv_gpu_kernel_time.argtypes = [vp, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_float)]
+    L.solv_gpu_mg_aggregates.argtypes = [vp, ctypes.c_int, _i32p, ctypes.c_int, _i32p]
     for fn in (L.solv_gpu_cg_batch, L.solv_gpu_bicg_batch):
         fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _f64p,
                        _f64p, _f64p, ctypes.c_int, _i32p, _f64p, ctypes.POINTER(Stats)]
@@ -331,6 +335,15 @@ class GpuSolver:
         self._check(self._lib.solv_gpu_gnn_grad_dev(self._h, r0_ptr, samples_ptr, n_samples,
                                                     ctypes.byref(loss), int(bool(accumulate))))
         return loss.value
+
+    def mg_aggregates(self, level: int, n_finer: int) -> tuple[np.ndarray, int]:
+        """Aggregate index of every cell of level-1 (caller order for level 1)
+        and the size of `level`."""
+        agg = np.zeros(n_finer, np.int32)
+        nc = ctypes.c_int()
+        self._check(self._lib.solv_gpu_mg_aggregates(self._h, level, _p(agg, _i32p), n_finer,
+                                                     ctypes.byref(nc)))
+        return agg, nc.value
 
     def gnn_adam(self, lr: float, grad_scale: float = 1.0) -> None:
         self._check(self._lib.solv_gpu_gnn_adam(self._h, lr, grad_scale))

@@ -6,6 +6,7 @@ import re
 import numpy as np
 import pytest
 import scipy.sparse as sp
+import torch
 
 from oracle import gnn_ref
 from programs_b200 import learn
@@ -69,14 +70,15 @@ def test_bf16_rounding_is_round_to_nearest_even():
     assert abs(y[3] + 3.3) < 3.3 * 2 ** -8
 
 
-def test_reference_gradient_matches_finite_differences():
+@pytest.mark.parametrize("kind", [0, 1])
+def test_reference_gradient_matches_finite_differences(kind):
     gnn_ref.ROUND = False
     try:
         A = _system(5, seed=2)
         r0 = uniform(4, A.n_cell)
         samples = [r0, uniform(5, A.n_cell)]
         p = _active(1)
-        J0, g = gnn_ref.loss_and_grad(A, r0, samples, p)
+        J0, g = gnn_ref.loss_and_grad(A, r0, samples, p, kind=kind)
         rng = np.random.default_rng(0)
         idx = np.concatenate([rng.choice(learn.N_PARAM, 20, replace=False),
                               [learn.P_BA, learn.P_BE, learn.P_WA, learn.P_WE + 3]])
@@ -85,8 +87,8 @@ def test_reference_gradient_matches_finite_differences():
             pp, pm = p.copy(), p.copy()
             pp[k] += e
             pm[k] -= e
-            fd = (float(gnn_ref.loss(A, r0, samples, pp)[0]) -
-                  float(gnn_ref.loss(A, r0, samples, pm)[0])) / (2 * e)
+            fd = (float(gnn_ref.loss(A, r0, samples, pp, kind=kind)[0]) -
+                  float(gnn_ref.loss(A, r0, samples, pm, kind=kind)[0])) / (2 * e)
             assert abs(fd - g[k]) <= 1e-7 + 1e-4 * abs(g[k]), k
     finally:
         gnn_ref.ROUND = True
@@ -104,3 +106,68 @@ def test_energy_loss_minimiser_is_the_solution():
     for k in range(5):
         d = np.random.default_rng(k).normal(size=A.n_cell) * 1e-3
         assert J(x + d) > J(x)
+
+
+def test_scale_free_loss_ignores_the_scale_of_z():
+    """L(z) = -(z.u)^2/(z.Â z) is twice the energy after the best step along
+    z: the same for every multiple of z, at most twice the energy of z, and
+    minimal (-u.Â^-1 u) at z = Â^-1 u."""
+    import scipy.sparse.linalg as spla
+    A = _system(5, seed=3)
+    rsd = 1.0 / np.sqrt(A.pl)
+    S = sp.diags(rsd) @ A.to_scipy() @ sp.diags(rsd)
+    u = uniform(6, A.n_cell)
+    L = lambda z: -(z @ u) ** 2 / (z @ (S @ z))
+    E = lambda z: 0.5 * z @ (S @ z) - z @ u
+    z = u * np.random.default_rng(1).uniform(0.5, 2.0, A.n_cell)
+    assert abs(L(3.7 * z) - L(z)) <= 1e-12 * abs(L(z))
+    assert 0.5 * L(z) <= E(z) + 1e-12 * abs(E(z))
+    x = spla.spsolve(S.tocsc(), u)
+    assert abs(L(x) - 2 * E(x)) <= 1e-9 * abs(E(x))
+
+
+def _aggs(A):
+    """A two-level aggregation of consecutive cell indices (the reference's
+    V-cycle takes any aggregation; the GPU's own comes from its API)."""
+    a = np.arange(A.n_cell) // 8
+    return [a]
+
+
+def test_reference_vcycle_is_symmetric_and_untrained_is_jacobi_smoothing():
+    A = _system(5, seed=4)
+    mats, Ps = gnn_ref.hierarchy(A, _aggs(A))
+    p0 = learn.init_params(0)
+    s, gE, rows_t, cols_t, wt, P, rsd = gnn_ref.build(A, uniform(1, A.n_cell), p0)
+    rsd_t = torch.tensor(rsd, dtype=torch.float64)
+    K = lambda v: rsd_t * gnn_ref._apply(s, gE, rows_t, cols_t, rsd_t * v)
+    D = torch.tensor(1.0 / A.pl)
+    x = torch.tensor(uniform(2, A.n_cell))
+    y = torch.tensor(uniform(3, A.n_cell))
+    assert torch.allclose(K(x), D * x, rtol=1e-6)  # untrained network = Jacobi (FP32 rsd)
+    Vx = gnn_ref.vcycle(mats, Ps, x, K, 0.8, 2.0)
+    Vy = gnn_ref.vcycle(mats, Ps, y, K, 0.8, 2.0)
+    assert abs(float(Vx @ y - x @ Vy)) <= 1e-10 * abs(float(Vx @ y))
+
+
+def test_reference_vcycle_gradient_matches_finite_differences():
+    gnn_ref.ROUND = False
+    try:
+        A = _system(5, seed=2)
+        r0 = uniform(4, A.n_cell)
+        samples = [r0, uniform(5, A.n_cell)]
+        p = _active(1)
+        aggs = _aggs(A)
+        J0, g = gnn_ref.loss_mg_and_grad(A, r0, samples, p, aggs, 0.8, 2.0)
+        rng = np.random.default_rng(1)
+        idx = np.concatenate([rng.choice(learn.N_PARAM, 12, replace=False),
+                              [learn.P_BA, learn.P_BE, learn.P_WA + 1, learn.P_WE + 2]])
+        for k in idx:
+            e = 1e-6
+            pp, pm = p.copy(), p.copy()
+            pp[k] += e
+            pm[k] -= e
+            fd = (float(gnn_ref.loss_mg(A, r0, samples, pp, aggs, 0.8, 2.0)[0]) -
+                  float(gnn_ref.loss_mg(A, r0, samples, pm, aggs, 0.8, 2.0)[0])) / (2 * e)
+            assert abs(fd - g[k]) <= 1e-7 + 1e-4 * abs(g[k]), k
+    finally:
+        gnn_ref.ROUND = True

@@ -17,6 +17,10 @@ from programs_b200.solver import OK, OPT_PRECISION
 pytestmark = pytest.mark.gpu
 
 SOL_TOL = 1e-8
+# Two different iterations that both stop at |r|_1/|r0|_1 < 1e-10 differ by
+# up to about cond(A) x 1e-10; the FP32-inner solves of a batch of uneven
+# meshes are held to that (their own FP64 residual is checked exactly).
+MIX_BATCH_TOL = 1e-7
 
 
 def _rel(a, b):
@@ -102,7 +106,10 @@ def test_batch_pressure_matches_separate_solves(gpu, precision, imat):
         sl = slice(cell_ptr[k], cell_ptr[k + 1])
         ref = Oracle.from_matrix(A).solv_cg(imat, 1e-10, 3000, np.zeros((A.n_cell, 1)),
                                             b[sl].reshape(-1, 1))
-        assert _rel(phi[sl], ref[0]) <= SOL_TOL
+        assert _rel(phi[sl], ref[0]) <= (SOL_TOL if precision == 0 else MIX_BATCH_TOL)
+        if precision == 1:
+            r = b[sl] - A.to_scipy() @ phi[sl, 0]
+            assert np.abs(r).sum() / np.abs(b[sl]).sum() < 1e-10
         assert np.array_equal(res0[sl], ref[1])
         assert np.isclose(st["res0_n"][k, 0], ref[2][0], rtol=1e-12)
         if precision == 0:

@@ -8,7 +8,12 @@
 * flexible CG: the untrained network (= the Jacobi step) reproduces PCG;
   any network converges to the FP64 oracle's solution (the FP64 residual
   decides); a broken network hands over to plain PCG;
-* training lowers the loss and the FCG iteration count (the gain test).
+* training lowers the loss and the FCG iteration count (the gain test);
+* multigrid: with the network's operator as the finest-level smoother of the
+  aggregation V-cycle, the untrained network equals Jacobi smoothing, the
+  iteration count no longer grows like plain PCG's, a broken network still
+  hands over to PCG, and the trained network's smoother is measured against
+  Jacobi smoothing.
 """
 import os
 
@@ -19,9 +24,16 @@ from oracle import gnn_ref
 from oracle.oracle import Oracle
 from programs_b200 import learn
 from programs_b200.mesh import Mesh, cavity_field, momentum_field, pressure_correction, uniform
-from programs_b200.solver import OK
+from programs_b200.solver import (OK, OPT_MG_LEVELS, OPT_MG_SMOOTHER, OPT_PRECISION)
 
 pytestmark = pytest.mark.gpu
+
+# Two different iterations that both stop at |r|_1/|r0|_1 < 1e-10 (the
+# learned FCG and the oracle's PCG) differ by up to about cond(A) x 1e-10,
+# some 1e-8 on these systems; solves to 1e-10 are held to that, and
+# test_learned_solution_agrees_with_the_oracle_when_both_converge holds
+# the learned solve to 1e-8 against the oracle with both run to 1e-12.
+AGREE_1E10 = 1e-7
 
 
 def _system(n=10, seed=1, lid=1.0, jitter=0.2):
@@ -76,19 +88,24 @@ def test_forward_kernels_match_reference(gpu):
     assert _rel(z0, z1) < 2e-2          # tensor-core accumulation order vs CUDA cores
 
 
-def test_gradient_kernels_match_autograd(gpu):
+@pytest.mark.parametrize("kind", [0, 1])
+def test_gradient_kernels_match_autograd(gpu, kind):
     import torch
     A = _system(8, seed=2)
     gpu.matrix_set(A)
     p = _active_params(3)
     gpu.gnn_set_params(p)
+    gpu.set_option(9, kind)  # SOLV_OPT_GNN_LOSS
     r0 = uniform(5, A.n_cell)
     samples = [r0, uniform(6, A.n_cell), uniform(7, A.n_cell)]
     sd = torch.from_numpy(np.stack(samples)).cuda()
     r0d = _dev(r0)
-    loss_g = gpu.gnn_grad_dev(r0d.data_ptr(), sd.data_ptr(), len(samples))
+    try:
+        loss_g = gpu.gnn_grad_dev(r0d.data_ptr(), sd.data_ptr(), len(samples))
+    finally:
+        gpu.set_option(9, 1)
     g_g = gpu.gnn_get_grad()
-    loss_c, g_c = gnn_ref.loss_and_grad(A, r0, samples, p)
+    loss_c, g_c = gnn_ref.loss_and_grad(A, r0, samples, p, kind=kind)
     assert abs(loss_g - loss_c) <= 1e-3 * abs(loss_c)
     blocks = [("w_in", 0, learn.P_LAYER)]
     for l in range(3):
@@ -101,15 +118,51 @@ def test_gradient_kernels_match_autograd(gpu):
         assert _rel(g_g[a:b], g_c[a:b]) < 3e-2, name
 
 
-def _solve_fcg(gpu, A, b):
+@pytest.fixture
+def one_level(gpu):
+    """The network's operator alone as the preconditioner (no hierarchy)."""
+    gpu.set_option(OPT_MG_LEVELS, 0)
+    yield gpu
+    gpu.set_option(OPT_MG_LEVELS, 12)
+
+
+def test_multigrid_gradient_kernels_match_reference(gpu):
+    """Training through the V-cycle (loss 2): the GPU's forward V-cycle,
+    loss and adjoint give the gradient torch autograd gives on the CPU
+    reference V-cycle over the same aggregation."""
+    import torch
+    A = _system(12, seed=3)
+    gpu.matrix_set(A)
+    p = _active_params(4)
+    gpu.gnn_set_params(p)
+    agg, nc = gpu.mg_aggregates(1, A.n_cell)
+    assert nc <= 256  # one coarse level, solved exactly, as in the reference
+    r0 = uniform(8, A.n_cell)
+    samples = [r0, uniform(9, A.n_cell)]
+    sd = torch.from_numpy(np.stack(samples)).cuda()
+    gpu.set_option(9, 2)  # SOLV_OPT_GNN_LOSS: through the V-cycle
+    try:
+        loss_g = gpu.gnn_grad_dev(_dev(r0).data_ptr(), sd.data_ptr(), len(samples))
+    finally:
+        gpu.set_option(9, 1)
+    g_g = gpu.gnn_get_grad()
+    loss_c, g_c = gnn_ref.loss_mg_and_grad(A, r0, samples, p, [agg], 0.8, 2.0)
+    assert abs(loss_g - loss_c) <= 1e-3 * abs(loss_c)
+    for name, a, b in [("w_in", 0, learn.P_LAYER), ("layers", learn.P_LAYER, learn.P_WA),
+                       ("w_a", learn.P_WA, learn.P_BA), ("w_e", learn.P_WE, learn.P_BE)]:
+        assert _rel(g_g[a:b], g_c[a:b]) < 3e-2, name
+
+
+def _solve_fcg(gpu, A, b, reduc=1e-10):
     phi = np.zeros((A.n_cell, 1))
     res0 = np.asfortranarray(b.reshape(-1, 1).copy())
     rn = np.zeros(1)
-    st = gpu.solv_fcg(1e-10, 20000, phi, res0, rn)
+    st = gpu.solv_fcg(reduc, 20000, phi, res0, rn)
     return phi, st, rn
 
 
-def test_untrained_network_reproduces_pcg(gpu):
+def test_untrained_network_reproduces_pcg(one_level):
+    gpu = one_level
     A = _system(12, seed=4)
     gpu.matrix_set(A)
     gpu.gnn_set_params(learn.init_params(0))
@@ -117,13 +170,26 @@ def test_untrained_network_reproduces_pcg(gpu):
     phi, st, rn = _solve_fcg(gpu, A, b)
     ref = Oracle.from_matrix(A).solv_cg(0, 1e-10, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
     assert st["status"] == OK and st["fallbacks"] == 0
-    assert _rel(phi, ref[0]) <= 1e-8
-    # FCG(1) with the fixed SPD Jacobi preconditioner is PCG; FP32 with
-    # reliable updates may cost a few iterations
-    assert st["iters"][0] <= 1.15 * int(ref[3][0])
+    assert _rel(phi, ref[0]) <= AGREE_1E10
+    # FCG(1) with the fixed SPD Jacobi preconditioner is Jacobi-PCG: the
+    # same FP32 iteration with reliable updates as the mixed-precision CG
+    # (which computes z = c r instead of z = q (q r)); FP32 iteration counts
+    # at a 1e-10 target move with rounding (181 against 153 on this system),
+    # and FP32 itself may cost some over FP64
+    gpu.set_option(OPT_PRECISION, 1)
+    try:
+        phi_m = np.zeros((A.n_cell, 1))
+        st_m = gpu.solv_cg(0, 1e-10, 20000, phi_m, np.asfortranarray(b.reshape(-1, 1).copy()),
+                           np.zeros(1))
+    finally:
+        gpu.set_option(OPT_PRECISION, 0)
+    assert st_m["status"] == OK
+    assert abs(st["iters"][0] - st_m["iters"][0]) <= 0.25 * st_m["iters"][0] + 2
+    assert st["iters"][0] <= 1.5 * int(ref[3][0])
 
 
-def test_broken_network_falls_back_to_pcg(gpu):
+def test_broken_network_falls_back_to_pcg(one_level):
+    gpu = one_level
     A = _system(10, seed=5)
     gpu.matrix_set(A)
     p = learn.init_params(0)
@@ -133,15 +199,16 @@ def test_broken_network_falls_back_to_pcg(gpu):
     phi, st, rn = _solve_fcg(gpu, A, b)
     ref = Oracle.from_matrix(A).solv_cg(0, 1e-10, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
     assert st["status"] == OK and st["fallbacks"] >= 1
-    assert _rel(phi, ref[0]) <= 1e-8
+    assert _rel(phi, ref[0]) <= AGREE_1E10
 
 
-def test_training_gains_over_the_untrained_network(gpu):
+def test_training_gains_over_the_untrained_network(one_level):
+    gpu = one_level
     """A short training run lowers the energy loss and the FCG iteration
     count below the untrained network's (which is Jacobi-PCG)."""
     p0 = learn.init_params(0)
     p, hist = learn.train(size=12, n_mesh=4, per_mesh=12, samples=4, epochs=3, lr=3e-3, seed=0,
-                          init=p0, log_every=0)
+                          init=p0, log_every=0, loss=1)
     assert np.mean(hist[-10:]) < np.mean(hist[:10])
     A = _system(14, seed=11, lid=0.7, jitter=0.12)
     gpu.matrix_set(A)
@@ -151,7 +218,7 @@ def test_training_gains_over_the_untrained_network(gpu):
     gpu.gnn_set_params(p)
     phi, st1, _ = _solve_fcg(gpu, A, b)
     ref = Oracle.from_matrix(A).solv_cg(0, 1e-10, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
-    assert _rel(phi, ref[0]) <= 1e-8
+    assert _rel(phi, ref[0]) <= AGREE_1E10
     assert st1["iters"][0] < 0.9 * st0["iters"][0], (st0["iters"], st1["iters"])
 
 
@@ -164,7 +231,128 @@ def test_committed_weights_solve_to_the_oracle_solution(gpu):
     phi, st, rn = _solve_fcg(gpu, A, b)
     ref = Oracle.from_matrix(A).solv_cg(0, 1e-10, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
     assert st["status"] == OK
-    assert _rel(phi, ref[0]) <= 1e-8
+    assert _rel(phi, ref[0]) <= AGREE_1E10
     S = A.to_scipy()
     assert np.abs(b - S @ phi[:, 0]).sum() / rn[0] < 1e-10
     assert st["iters"][0] < int(ref[3][0])  # fewer iterations than Jacobi-PCG
+
+
+def _ref_iters(A, b):
+    ref = Oracle.from_matrix(A).solv_cg(0, 1e-10, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
+    return ref[0], int(ref[3][0])
+
+
+def test_multigrid_untrained_network_equals_jacobi_smoothing(gpu):
+    A = _system(20, seed=6)
+    gpu.matrix_set(A)
+    gpu.gnn_set_params(learn.init_params(0))
+    b = _rhs(A, 10)
+    _, st_net, _ = _solve_fcg(gpu, A, b)
+    gpu.set_option(OPT_MG_SMOOTHER, 0)
+    try:
+        phi, st_jac, rn = _solve_fcg(gpu, A, b)
+    finally:
+        gpu.set_option(OPT_MG_SMOOTHER, 1)
+    x_ref, it_ref = _ref_iters(A, b)
+    assert st_net["status"] == OK and st_jac["status"] == OK
+    assert st_net["mg_levels"] >= 1 and st_jac["mg_levels"] == st_net["mg_levels"]
+    assert _rel(phi, x_ref) <= AGREE_1E10
+    assert abs(st_net["iters"][0] - st_jac["iters"][0]) <= 0.2 * st_jac["iters"][0] + 2
+    assert st_jac["iters"][0] < 0.5 * it_ref
+
+
+def test_multigrid_iterations_do_not_grow_like_pcg(gpu):
+    """Plain PCG needs about twice the iterations when the cell size halves;
+    the V-cycle preconditioned FCG needs far fewer, growing much less."""
+    gpu.gnn_set_params(learn.init_params(0))
+    its, refs = [], []
+    for n in (16, 32):
+        A = _system(n, seed=7)
+        gpu.matrix_set(A)
+        b = _rhs(A, 11)
+        phi, st, rn = _solve_fcg(gpu, A, b)
+        x_ref, it_ref = _ref_iters(A, b)
+        assert st["status"] == OK and st["fallbacks"] == 0
+        assert _rel(phi, x_ref) <= AGREE_1E10
+        S = A.to_scipy()
+        assert np.abs(b - S @ phi[:, 0]).sum() / rn[0] < 1e-10
+        its.append(st["iters"][0])
+        refs.append(it_ref)
+    assert its[1] < 0.25 * refs[1], (its, refs)
+    assert its[1] / its[0] < 0.8 * refs[1] / refs[0], (its, refs)
+
+
+def test_multigrid_broken_network_falls_back_to_pcg(gpu):
+    A = _system(16, seed=8)
+    gpu.matrix_set(A)
+    p = learn.init_params(0)
+    p[learn.P_BA] = np.nan
+    gpu.gnn_set_params(p)
+    b = _rhs(A, 12)
+    phi, st, rn = _solve_fcg(gpu, A, b)
+    x_ref, _ = _ref_iters(A, b)
+    assert st["status"] == OK and st["fallbacks"] >= 1
+    assert _rel(phi, x_ref) <= AGREE_1E10
+
+
+@pytest.mark.skipif(not os.path.exists(learn.DEFAULT_WEIGHTS), reason="no trained weights")
+def test_multigrid_trained_smoother_against_jacobi(gpu):
+    """What the trained network gains as the finest-level smoother, against
+    the same V-cycle with Jacobi smoothing (iteration counts recorded; the
+    solve must reach the oracle's solution either way)."""
+    A = _system(32, seed=22, lid=1.1, jitter=0.2)
+    gpu.matrix_set(A)
+    b = _rhs(A, 13)
+    gpu.gnn_set_params(learn.load_params())
+    phi, st_net, _ = _solve_fcg(gpu, A, b)
+    gpu.set_option(OPT_MG_SMOOTHER, 0)
+    try:
+        _, st_jac, _ = _solve_fcg(gpu, A, b)
+    finally:
+        gpu.set_option(OPT_MG_SMOOTHER, 1)
+    x_ref, _ = _ref_iters(A, b)
+    assert st_net["status"] == OK and _rel(phi, x_ref) <= AGREE_1E10
+    print("multigrid iterations: network smoother", st_net["iters"][0],
+          "Jacobi smoother", st_jac["iters"][0])
+    assert st_net["iters"][0] <= 1.1 * st_jac["iters"][0] + 2
+
+
+@pytest.mark.skipif(not os.path.exists(learn.DEFAULT_WEIGHTS), reason="no trained weights")
+@pytest.mark.parametrize("levels", [0, 12])
+def test_learned_solution_agrees_with_the_oracle_when_both_converge(gpu, levels):
+    """Solution error against the FP64 oracle, both solved to 1e-12: the
+    learned + mixed-precision solve agrees to 1e-8 relative."""
+    A = _system(24, seed=23, lid=0.9, jitter=0.2)
+    gpu.matrix_set(A)
+    gpu.gnn_set_params(learn.load_params())
+    gpu.set_option(OPT_MG_LEVELS, levels)
+    try:
+        b = _rhs(A, 14)
+        phi, st, rn = _solve_fcg(gpu, A, b, reduc=1e-12)
+    finally:
+        gpu.set_option(OPT_MG_LEVELS, 12)
+    ref = Oracle.from_matrix(A).solv_cg(0, 1e-12, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
+    assert st["status"] == OK
+    assert _rel(phi, ref[0]) <= 1e-8
+
+
+def test_multigrid_training_gains_over_jacobi_smoothing(gpu):
+    """The gain test of the deployed preconditioner: a short training run
+    through the V-cycle lowers its loss, and the trained smoother needs
+    fewer FCG iterations than the same V-cycle with Jacobi smoothing (the
+    untrained network)."""
+    p0 = learn.init_params(0)
+    p, hist = learn.train(size=24, n_mesh=3, per_mesh=16, samples=4, epochs=2, lr=3e-3, seed=0,
+                          init=p0, log_every=0, loss=2)
+    assert np.mean(hist[-8:]) < np.mean(hist[:8])
+    A = _system(32, seed=12, lid=0.8, jitter=0.15)
+    gpu.matrix_set(A)
+    b = _rhs(A, 15)
+    gpu.gnn_set_params(p0)
+    _, st0, _ = _solve_fcg(gpu, A, b)
+    gpu.gnn_set_params(p)
+    phi, st1, rn = _solve_fcg(gpu, A, b)
+    x_ref, _ = _ref_iters(A, b)
+    assert st1["status"] == OK and _rel(phi, x_ref) <= AGREE_1E10
+    print("multigrid training: iterations untrained", st0["iters"][0], "trained", st1["iters"][0])
+    assert st1["iters"][0] < st0["iters"][0], (st0["iters"], st1["iters"])
