@@ -77,8 +77,9 @@ extern "C" {
                                    1 = energy after the best step along z
                                    (scale-free, default), both for the
                                    network's operator alone; 2 = the
-                                   scale-free loss of the V-cycle with the
-                                   network as finest-level smoother        */
+                                   V-cycle with the network as finest-level
+                                   smoother, -log((z.b)^2/(z.Az)) per
+                                   sample                                  */
 #define SOLV_OPT_MG_LEVELS 10   /* learned preconditioner: coarse levels of
                                    the aggregation hierarchy at most (default
                                    12; 0 = the network's one-level operator
@@ -166,8 +167,10 @@ int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
 /* Device time per launch (CUDA events on the context's stream, `repeat`
  * back-to-back launches on workspace vectors) of a kernel of the solve
  * path: which 0 = FP64 matrix product, 1 = FP32 matrix product, 2 = the
- * learned preconditioner's application (FP32).  No counterpart in the
- * reference; used for roofline reporting. */
+ * learned preconditioner's one-level application (FP32), 3 = one V-cycle
+ * of the multigrid preconditioner (FP32, all its kernels, with the current
+ * SOLV_OPT_MG_* settings).  No counterpart in the reference; used for
+ * roofline reporting. */
 int solv_gpu_kernel_time(solv_gpu_ctx *ctx, int which, int repeat,
                          float *ms_per_launch);
 

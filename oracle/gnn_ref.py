@@ -193,9 +193,10 @@ def vcycle(mats, Ps, b, smooth0, omega, alpha, l=0):
 
 
 def loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=False):
-    """Mean over samples of L/N, L = -(z.b)^2/(z.A z) with z the V-cycle
-    applied to b = r / gs, the network's operator K = D^-1/2 S (I+E) S D^-1/2
-    smoothing level 0 (the loss the GPU trains with through the V-cycle)."""
+    """Mean over samples of L/N, L = -log((z.b)^2/(z.A z)) with z the
+    V-cycle applied to b = r / gs, the network's operator
+    K = D^-1/2 S (I+E) S D^-1/2 smoothing level 0 (the loss the GPU trains
+    with through the V-cycle)."""
     s, gE, rows_t, cols_t, wt, P, rsd = build(A, r0, params, grad=grad)
     rsd_t = torch.tensor(rsd, dtype=torch.float64)
     K = lambda v: rsd_t * _apply(s, gE, rows_t, cols_t, rsd_t * v)
@@ -209,7 +210,7 @@ def loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=False):
                          dtype=torch.float64)
         z = vcycle(mats, Ps, b, K, omega, alpha)
         az = torch.sparse.mm(At, z[:, None])[:, 0]
-        J = J - (z @ b) ** 2 / (z @ az) / N
+        J = J - torch.log((z @ b) ** 2 / (z @ az)) / N
     return J / len(samples), P
 
 

@@ -36,6 +36,7 @@
 #include <cmath>
 #include <cstdint>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -92,37 +93,70 @@ inline void members(const std::vector<int>& agg, int nc, std::vector<int>& ptr,
   for (int i = 0; i < (int)agg.size(); ++i) cells[pos[agg[i]]++] = i;
 }
 
+// Run f(begin, end, thread) over [0, n) in contiguous chunks on up to 16
+// host threads (one for small n).  Callers write disjoint outputs per index,
+// so results do not depend on the number of threads.
+template <typename F>
+inline void parallel_rows(int n, F f) {
+  const unsigned hc = std::thread::hardware_concurrency();
+  int T = (int)std::max(1u, std::min(hc ? hc : 1u, 16u));
+  if (n < 65536) T = 1;
+  const int chunk = (n + T - 1) / T;
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; ++t) {
+    const int b = t * chunk, e = std::min(n, b + chunk);
+    if (b < e) th.emplace_back(f, b, e, t);
+  }
+  f(0, std::min(n, chunk), 0);
+  for (auto& x : th) x.join();
+}
+
 // Graph of the aggregates: strengths of the couplings between two
-// aggregates summed, couplings inside an aggregate dropped.
+// aggregates summed (in member order, then row order), couplings inside an
+// aggregate dropped; each row lists its neighbours in order of first
+// appearance.
 inline Graph coarsen(const Graph& g, const std::vector<int>& agg, int nc) {
   std::vector<int> mp, mc;
   members(agg, nc, mp, mc);
   Graph out;
   out.n = nc;
   out.ptr.assign(nc + 1, 0);
-  std::vector<std::pair<int, float>> row;
-  for (int I = 0; I < nc; ++I) {
-    row.clear();
-    for (int m = mp[I]; m < mp[I + 1]; ++m) {
-      const int i = mc[m];
-      for (long long k = g.ptr[i]; k < g.ptr[i + 1]; ++k) {
-        const int J = agg[g.adj[k]];
-        if (J != I) row.emplace_back(J, g.w[k]);
+  const int T = 16;
+  std::vector<std::vector<int>> tadj(T);
+  std::vector<std::vector<float>> tw(T);
+  std::vector<int> deg(nc, 0), first(T, 0);
+  parallel_rows(nc, [&](int b, int e, int t) {
+    std::vector<int> mark(nc, -1), pos(nc, 0);
+    auto& A = tadj[t];
+    auto& W = tw[t];
+    first[t] = b;
+    for (int I = b; I < e; ++I) {
+      const size_t r0 = A.size();
+      for (int m = mp[I]; m < mp[I + 1]; ++m) {
+        const int i = mc[m];
+        for (long long k = g.ptr[i]; k < g.ptr[i + 1]; ++k) {
+          const int J = agg[g.adj[k]];
+          if (J == I) continue;
+          if (mark[J] != I) {
+            mark[J] = I;
+            pos[J] = (int)(A.size() - r0);
+            A.push_back(J);
+            W.push_back(g.w[k]);
+          } else {
+            W[r0 + pos[J]] += g.w[k];
+          }
+        }
       }
+      deg[I] = (int)(A.size() - r0);
     }
-    std::sort(row.begin(), row.end(),
-              [](const std::pair<int, float>& a, const std::pair<int, float>& b) {
-                return a.first < b.first;
-              });
-    for (size_t k = 0; k < row.size();) {
-      size_t e = k;
-      float s = 0.0f;
-      while (e < row.size() && row[e].first == row[k].first) s += row[e++].second;
-      out.adj.push_back(row[k].first);
-      out.w.push_back(s);
-      k = e;
-    }
-    out.ptr[I + 1] = (long long)out.adj.size();
+  });
+  for (int I = 0; I < nc; ++I) out.ptr[I + 1] = out.ptr[I] + deg[I];
+  out.adj.resize(out.ptr[nc]);
+  out.w.resize(out.ptr[nc]);
+  for (int t = 0; t < T; ++t) {
+    if (tadj[t].empty()) continue;
+    std::copy(tadj[t].begin(), tadj[t].end(), out.adj.begin() + out.ptr[first[t]]);
+    std::copy(tw[t].begin(), tw[t].end(), out.w.begin() + out.ptr[first[t]]);
   }
   return out;
 }
@@ -189,36 +223,43 @@ struct CoarseHost {
 };
 
 // Fine level given by its sliced-ELL arrays (n cells) and aggregation agg.
+// Coarse row I lists its neighbours J in order of first appearance over
+// I's members and their slots; slot (I, J) sums the finer slots listed for
+// it, in the same order.
 inline bool build_coarse(int n, const std::vector<int>& sp, const std::vector<uint8_t>& sw,
                          const std::vector<int>& col, const std::vector<int>& agg, int nc,
                          CoarseHost& C) {
   C.n = nc;
   C.agg_of = agg;
   members(agg, nc, C.agg_ptr, C.agg_cells);
-  // coarse rows: (J, finer slot) pairs grouped by J
-  std::vector<std::vector<std::pair<int, int>>> rows(nc);
-  std::vector<int> deg(nc, 0);
-  std::vector<std::pair<int, int>> tmp;
-  for (int I = 0; I < nc; ++I) {
-    tmp.clear();
-    for (int m = C.agg_ptr[I]; m < C.agg_ptr[I + 1]; ++m) {
-      const int i = C.agg_cells[m];
+  const std::vector<int>& mp = C.agg_ptr;
+  const std::vector<int>& mc = C.agg_cells;
+  // walk the finer slots of coarse row I: visit(J, finer slot, k of J)
+  auto walk = [&](int I, std::vector<int>& mark, std::vector<int>& pos, auto&& visit) {
+    int d = 0;
+    for (int m = mp[I]; m < mp[I + 1]; ++m) {
+      const int i = mc[m];
       const int s = i >> 5, l = i & 31;
       for (int k = 0; k < sw[s]; ++k) {
         const long long e = (long long)sp[s] + (long long)k * 32 + l;
         const int j = col[e];
         if (j < 0) continue;
         const int J = agg[j];
-        if (J != I) tmp.emplace_back(J, (int)e);
+        if (J == I) continue;
+        if (mark[J] != I) {
+          mark[J] = I;
+          pos[J] = d++;
+        }
+        visit(J, (int)e, pos[J]);
       }
     }
-    std::sort(tmp.begin(), tmp.end());
-    rows[I] = tmp;
-    int d = 0;
-    for (size_t k = 0; k < tmp.size(); ++k)
-      if (k == 0 || tmp[k].first != tmp[k - 1].first) ++d;
-    deg[I] = d;
-  }
+    return d;
+  };
+  std::vector<int> deg(nc, 0);
+  parallel_rows(nc, [&](int b, int e, int) {
+    std::vector<int> mark(nc, -1), pos(nc, 0);
+    for (int I = b; I < e; ++I) deg[I] = walk(I, mark, pos, [](int, int, int) {});
+  });
   const int ns = (nc + 31) / 32;
   C.slice_ptr.assign(ns + 1, 0);
   C.slice_w.assign(ns, 0);
@@ -237,32 +278,31 @@ inline bool build_coarse(int n, const std::vector<int>& sp, const std::vector<ui
   C.n_slots = total;
   C.col.assign(total, -1);
   std::vector<int> cnt(total, 0);
-  // first pass: column and count per slot
-  for (int I = 0; I < nc; ++I) {
-    const int s = I >> 5, l = I & 31;
-    const auto& r = rows[I];
-    int k = -1;
-    for (size_t q = 0; q < r.size(); ++q) {
-      if (q == 0 || r[q].first != r[q - 1].first) ++k;
-      const long long e = (long long)C.slice_ptr[s] + (long long)k * 32 + l;
-      C.col[e] = r[q].first;
-      cnt[e]++;
+  parallel_rows(nc, [&](int b, int e, int) {
+    std::vector<int> mark(nc, -1), pos(nc, 0);
+    for (int I = b; I < e; ++I) {
+      const long long base = (long long)C.slice_ptr[I >> 5] + (I & 31);
+      walk(I, mark, pos, [&](int J, int, int k) {
+        C.col[base + (long long)k * 32] = J;
+        cnt[base + (long long)k * 32]++;
+      });
     }
-  }
+  });
   C.gptr.assign(total + 1, 0);
   for (long long e = 0; e < total; ++e) C.gptr[e + 1] = C.gptr[e] + cnt[e];
   C.gsrc.assign(C.gptr[total], 0);
-  std::vector<int> fill(C.gptr.begin(), C.gptr.end() - 1);
-  for (int I = 0; I < nc; ++I) {
-    const int s = I >> 5, l = I & 31;
-    const auto& r = rows[I];
-    int k = -1;
-    for (size_t q = 0; q < r.size(); ++q) {
-      if (q == 0 || r[q].first != r[q - 1].first) ++k;
-      const long long e = (long long)C.slice_ptr[s] + (long long)k * 32 + l;
-      C.gsrc[fill[e]++] = r[q].second;
+  parallel_rows(nc, [&](int b, int e, int) {
+    std::vector<int> mark(nc, -1), pos(nc, 0);
+    for (int I = b; I < e; ++I) {
+      const long long base = (long long)C.slice_ptr[I >> 5] + (I & 31);
+      std::vector<int> fill;
+      walk(I, mark, pos, [&](int, int ef, int k) {
+        if ((int)fill.size() <= k) fill.resize(k + 1, 0);
+        const long long ec = base + (long long)k * 32;
+        C.gsrc[C.gptr[ec] + fill[k]++] = ef;
+      });
     }
-  }
+  });
   (void)n;
   return true;
 }
@@ -273,17 +313,31 @@ inline Graph graph_of(int n, const std::vector<int>& sp, const std::vector<uint8
   Graph g;
   g.n = n;
   g.ptr.assign(n + 1, 0);
-  for (int i = 0; i < n; ++i) {
-    const int s = i >> 5, l = i & 31;
-    for (int k = 0; k < sw[s]; ++k) {
-      const long long e = (long long)sp[s] + (long long)k * 32 + l;
-      if (col[e] >= 0) {
-        g.adj.push_back(col[e]);
-        g.w.push_back(std::fabs(val[e]));
+  std::vector<int> deg(n, 0);
+  parallel_rows(n, [&](int b, int e, int) {
+    for (int i = b; i < e; ++i) {
+      const int s = i >> 5, l = i & 31;
+      int d = 0;
+      for (int k = 0; k < sw[s]; ++k) d += col[(long long)sp[s] + (long long)k * 32 + l] >= 0;
+      deg[i] = d;
+    }
+  });
+  for (int i = 0; i < n; ++i) g.ptr[i + 1] = g.ptr[i] + deg[i];
+  g.adj.resize(g.ptr[n]);
+  g.w.resize(g.ptr[n]);
+  parallel_rows(n, [&](int b, int e, int) {
+    for (int i = b; i < e; ++i) {
+      const int s = i >> 5, l = i & 31;
+      long long o = g.ptr[i];
+      for (int k = 0; k < sw[s]; ++k) {
+        const long long q = (long long)sp[s] + (long long)k * 32 + l;
+        if (col[q] >= 0) {
+          g.adj[o] = col[q];
+          g.w[o++] = std::fabs(val[q]);
+        }
       }
     }
-    g.ptr[i + 1] = (long long)g.adj.size();
-  }
+  });
   return g;
 }
 
@@ -490,9 +544,11 @@ k_mg_coarse_solve(int n, const float* __restrict__ Ainv, const float* __restrict
 }
 
 // ---- device: training the network through the V-cycle ----------------------------
-// Loss per sample b (original space, z = V(b)): L = -(z.b)^2 / (z.A z), twice
-// the energy after the best step along z -- what one CG step with this
-// preconditioner achieves, and free of z's overall scale.
+// Loss per sample b (original space, z = V(b)): L = -log((z.b)^2 / (z.A z)).
+// (z.b)^2/(z.Az) is twice the energy one CG step along z removes -- free of
+// z's overall scale; the logarithm makes every sample count alike whatever
+// its own energy, which varies by orders of magnitude between smooth and
+// rough residuals.
 
 // b = r / gs (the sample at unit mean scaled magnitude; gs in lane 0)
 __global__ void k_mg_normalise(int n, const float* __restrict__ r, const sg::Lane* __restrict__ lanes,
@@ -531,16 +587,16 @@ k_mg_loss_sums(int n, sg::Rows<float> R, const float* __restrict__ z, const floa
   }
 }
 
-// g = dL/dz = 2 a (a A z - b), a = (z.b)/(z.Az); jsum += L (once)
+// g = dL/dz = 2 (A z / (z.Az) - b / (z.b)); jsum += L (once)
 __global__ void k_mg_loss_grad(int n, const float* __restrict__ az, const float* __restrict__ b,
                                const double* __restrict__ sums, float* __restrict__ g,
                                double* __restrict__ jsum) {
-  const double zaz = sums[1];
-  const double a = zaz > 0.0 ? sums[0] / zaz : 0.0;
-  const float fa = (float)a, f2a = (float)(2.0 * a);
+  const double zb = sums[0], zaz = sums[1];
+  const bool ok = zaz > 0.0 && zb != 0.0;
+  const float ca = ok ? (float)(2.0 / zaz) : 0.0f, cb = ok ? (float)(2.0 / zb) : 0.0f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    g[i] = f2a * (fa * az[i] - b[i]);
-  if (blockIdx.x == 0 && threadIdx.x == 0 && zaz > 0.0) *jsum += -sums[0] * sums[0] / zaz;
+    g[i] = ca * az[i] - cb * b[i];
+  if (blockIdx.x == 0 && threadIdx.x == 0 && ok) *jsum += -log(zb * zb / zaz);
 }
 
 // One application x -> w K x of the smoother, K = D^-1/2 S (I+E) S D^-1/2,

@@ -143,6 +143,7 @@ struct solv_gpu_ctx {
   double mg_alpha = 2.0;               // coarse-correction scale (unsmoothed
                                        // aggregation under-corrects smooth error)
   bool mg_valid = false;               // hierarchy built for the current structure
+  int mg_built_max = 0;                // mg_max_levels the hierarchy was built with
   std::vector<std::unique_ptr<MgLevel>> mg;  // coarse levels 1..L
   DevBuf mg_x0, mg_t0, mg_dinv0, mg_dense, mg_ainv;
   DevBuf mg_train;                     // training through the V-cycle: 8 vectors
@@ -547,7 +548,8 @@ cudaError_t upload(DevBuf& d, const std::vector<V>& h, cudaStream_t s) {
 // cannot reach kCoarsest cells (coarsening stalls) is not used: the solve
 // then runs with the one-level preconditioner.
 int mg_setup(solv_gpu_ctx* c) {
-  if (c->mg_valid) return SOLV_GPU_OK;
+  if (c->mg_valid && c->mg_built_max == c->mg_max_levels) return SOLV_GPU_OK;
+  c->mg_built_max = c->mg_max_levels;
   auto t0 = std::chrono::steady_clock::now();
   int rc = ensure_f32_matrix(c);
   if (rc) return rc;
@@ -732,6 +734,9 @@ int mg_vcycle(solv_gpu_ctx* c, const float* r, TZ* z, bool net, const float* q, 
   return k;
 }
 
+// The solve uses the hierarchy (built, and not switched off).
+bool mg_on(const solv_gpu_ctx* c) { return c->mg_max_levels > 0 && !c->mg.empty(); }
+
 // Kernels in one V-cycle (launch statistics of graph replays).
 int mg_kernels(const solv_gpu_ctx* c) {
   const int L = (int)c->mg.size();
@@ -903,12 +908,12 @@ void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
   cudaStream_t st = c->stream;
   int nk = 1;
   if constexpr (std::is_same<T, float>::value) {
-    if (!c->mg.empty())  // z = V-cycle(r)
+    if (mg_on(c))  // z = V-cycle(r)
       nk = mg_vcycle<T>(c, w.r, w.z, c->mg_smoother == 1, c->g_q.as<float>(),
                         c->g_ge.as<float>(), c->mg_x0.as<float>(), c->mg_t0.as<float>(),
                         sm.n_active);
   }
-  if (c->mg.empty())
+  if (!mg_on(c))
     gnn::k_gnn_apply<T><<<grid_for(c, c->N), B, 0, st>>>(c->N, rows<float>(c),
                                                           c->g_ge.as<float>(), c->g_q.as<float>(),
                                                           w.r, w.z, sm.n_active);  // z = M^-1 r
@@ -960,7 +965,7 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     int sweep = imat > 0 ? 2 * nl : 1;
     if (solver == 0) per_launch_kernels = imat > 0 ? sweep + 4 : 3;
     else if (solver == 1) per_launch_kernels = imat > 0 ? 2 * sweep + 5 : 5;
-    else per_launch_kernels = 4 + (c->mg.empty() ? 1 : mg_kernels(c));
+    else per_launch_kernels = 4 + (mg_on(c) ? mg_kernels(c) : 1);
     c->launches = l0;
   }
   while (done < n_iter) {
@@ -1353,14 +1358,14 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
   const int G = c->seg.total_blk, B = c->block;
   if (solver == 2) {  // the learned preconditioner of this solve, from r0
     if (c->mg_max_levels > 0 && (rc = mg_setup(c))) return rc;  // may build no levels
-    if (c->mg.empty() || c->mg_smoother == 1) {
+    if (!mg_on(c) || c->mg_smoother == 1) {
       if ((rc = gnn_prepare(c))) return rc;
       sg::k_fcg_scale<float><<<G, B, 0, s>>>(sm, f.r, c->g_rsd.as<float>(),
                                             c->part.as<double>(), c->lanes.as<Lane>());
       gnn_build<float>(c, f.r);
       c->launches++;
     }
-    if (!c->mg.empty() && (rc = mg_values(c))) return rc;
+    if (mg_on(c) && (rc = mg_values(c))) return rc;
   } else if (imat <= 0) {
     sg::k_cg_rz<float, V, true><<<G, B, 0, s>>>(sm, f.c, f.r, f.z, c->part.as<double>(),
                                                 c->lanes.as<Lane>());
@@ -1470,7 +1475,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     st->status = status;
     st->refinements = updates;
     st->fallbacks = c->fallbacks;
-    st->mg_levels = solver == 2 ? (int)c->mg.size() : 0;
+    st->mg_levels = solver == 2 && mg_on(c) ? (int)c->mg.size() : 0;
     st->graph_launches += gl_total;
   }
   return status;
@@ -1588,28 +1593,34 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
       if (!(value > 0 && value < 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "reliable delta in (0,1)");
       c->reliable_delta = value;
       return SOLV_GPU_OK;
-    case SOLV_OPT_MG_LEVELS:
+    case SOLV_OPT_MG_LEVELS:  // 0 keeps a built hierarchy aside; another maximum rebuilds it
       if (value < 0 || value > mg::kMaxLevels)
         return set_err(c, SOLV_GPU_BAD_INPUT, "multigrid levels in 0..12");
-      c->mg_max_levels = (int)value;
-      c->mg_valid = false;
-      c->mg.clear();
-      drop_graphs(c);
+      if ((int)value != c->mg_max_levels) {
+        c->mg_max_levels = (int)value;
+        drop_graphs(c);
+      }
       return SOLV_GPU_OK;
     case SOLV_OPT_MG_SMOOTHER:
       if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "multigrid smoother is 0 or 1");
-      c->mg_smoother = (int)value;
-      drop_graphs(c);
+      if ((int)value != c->mg_smoother) {
+        c->mg_smoother = (int)value;
+        drop_graphs(c);
+      }
       return SOLV_GPU_OK;
     case SOLV_OPT_MG_OMEGA:
       if (!(value > 0 && value < 2)) return set_err(c, SOLV_GPU_BAD_INPUT, "smoother damping in (0,2)");
-      c->mg_omega = value;
-      drop_graphs(c);
+      if (value != c->mg_omega) {
+        c->mg_omega = value;
+        drop_graphs(c);
+      }
       return SOLV_GPU_OK;
     case SOLV_OPT_MG_ALPHA:
       if (!(value > 0 && value <= 4)) return set_err(c, SOLV_GPU_BAD_INPUT, "coarse-correction scale in (0,4]");
-      c->mg_alpha = value;
-      drop_graphs(c);
+      if (value != c->mg_alpha) {
+        c->mg_alpha = value;
+        drop_graphs(c);
+      }
       return SOLV_GPU_OK;
     case SOLV_OPT_INNER_MAX_ITER:
       if (value < 1 || value > 1e7) return set_err(c, SOLV_GPU_BAD_INPUT, "inner max iter in 1..1e7");
@@ -1776,7 +1787,7 @@ int solv_gpu_spmv_dev(solv_gpu_ctx* c, const double* x_dev, double* y_dev, int r
 int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_launch) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
-  if (which < 0 || which > 2 || repeat < 1 || !ms_per_launch)
+  if (which < 0 || which > 3 || repeat < 1 || !ms_per_launch)
     return set_err(c, SOLV_GPU_BAD_INPUT, "kernel_time: bad arguments");
   CUDA_TRY(c, cudaSetDevice(c->dev));
   const int N = c->N;
@@ -1796,7 +1807,13 @@ int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_l
     if ((rc = ensure_ws<float>(c, 1, f))) return rc;
     if ((rc = ensure_f32_matrix(c))) return rc;
     CUDA_TRY(c, cudaMemsetAsync(f.p, 0, N * sizeof(float), s));
-    if (which == 2) {
+    if (which == 3) {
+      if (c->mg_max_levels <= 0) return set_err(c, SOLV_GPU_BAD_INPUT, "kernel_time: multigrid is off");
+      if ((rc = mg_setup(c))) return rc;
+      if (!mg_on(c)) return set_err(c, SOLV_GPU_BAD_INPUT, "kernel_time: no hierarchy for this matrix");
+      if ((rc = mg_values(c))) return rc;
+    }
+    if (which == 2 || (which == 3 && c->mg_smoother == 1)) {
       if ((rc = gnn_prepare(c))) return rc;
       Lane L{};
       L.active = 1;
@@ -1807,9 +1824,12 @@ int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_l
     auto launch = [&]() {
       if (which == 1)
         sg::k_spmv<float, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<float>(c), f.p, f.q);
-      else
+      else if (which == 2)
         gnn::k_gnn_apply<float><<<grid_for(c, N), c->block, 0, s>>>(
             N, rows<float>(c), c->g_ge.as<float>(), c->g_q.as<float>(), f.p, f.q, nullptr);
+      else
+        mg_vcycle<float>(c, f.p, f.q, c->mg_smoother == 1, c->g_q.as<float>(),
+                         c->g_ge.as<float>(), c->mg_x0.as<float>(), c->mg_t0.as<float>(), nullptr);
     };
     launch();
     CUDA_TRY(c, cudaEventRecord(c->ev0, s));

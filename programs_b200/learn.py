@@ -12,9 +12,10 @@ preconditioned residual, the energy J = 1/2 z'Az - z'r (loss 0, minimised
 by z = A^-1 r) or the scale-free -(z'r)^2/(z'Az) (the energy after the
 best step along z, which is what one CG step takes, free in the overall
 scale of z as flexible CG is), for z = K r with the network's operator K
-alone (losses 0 and 1) or for z = V(r), the V-cycle of the aggregation
-hierarchy with K as its finest-level smoother (loss 2, the default: the
-preconditioner solv_gpu_fcg applies), differentiated through the V-cycle.  Forward, backward and the Adam step run on the GPU in the
+alone (losses 0 and 1) or, as -log((z'r)^2/(z'Az)) so that every sample
+counts alike, for z = V(r), the V-cycle of the aggregation hierarchy with
+K as its finest-level smoother (loss 2, the default: the preconditioner
+solv_gpu_fcg applies), differentiated through the V-cycle.  Forward, backward and the Adam step run on the GPU in the
 library's own kernels; this module only orchestrates.
 
   python -m programs_b200.learn --size 64 --systems 2000 --out weights.npz
