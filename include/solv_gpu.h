@@ -64,8 +64,10 @@ extern "C" {
                                    sweep (FP32 mode), default 1e-6         */
 #define SOLV_OPT_GRAPH_ITERS 3  /* Krylov iterations per CUDA-graph launch
                                    (0 = no graphs, plain launches)         */
-#define SOLV_OPT_BLOCK 4        /* threads per block for the cell kernels  */
-#define SOLV_OPT_GRID_PER_SM 5  /* resident blocks per SM for reductions   */
+#define SOLV_OPT_BLOCK 4        /* threads per block for the cell kernels
+                                   (64..256, multiple of 32)               */
+#define SOLV_OPT_GRID_PER_SM 5  /* resident blocks per SM for reductions
+                                   (at most 2048 threads per SM are used)  */
 #define SOLV_OPT_MAX_REFINE 6   /* cap on refinement sweeps (FP32 mode)    */
 #define SOLV_OPT_INNER_MAX_ITER 7 /* cap on FP32 iterations per refinement
                                    sweep (default 2000)                    */

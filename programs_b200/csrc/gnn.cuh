@@ -32,6 +32,8 @@
 #pragma once
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace gnn {
@@ -151,7 +153,7 @@ k_gnn_layer_tc(int n, sg::Rows<float> R, Feat F, const __nv_bfloat16* __restrict
                __nv_bfloat16* __restrict__ hout, const __nv_bfloat16* __restrict__ wcat,
                const float* __restrict__ bias) {
   __shared__ __nv_bfloat16 sB[2 * H][H + 8];
-  __shared__ __nv_bfloat16 sA[TC_WARPS][TC_CELLS][2 * H + 8];
+  __shared__ __align__(16) __nv_bfloat16 sA[TC_WARPS][TC_CELLS][2 * H + 8];
   __shared__ float sbias[H];
   for (int t = threadIdx.x; t < 2 * H * H; t += blockDim.x) sB[t / H][t % H] = wcat[t];
   if (threadIdx.x < H) sbias[threadIdx.x] = bf(bias[threadIdx.x]);
@@ -161,22 +163,42 @@ k_gnn_layer_tc(int n, sg::Rows<float> R, Feat F, const __nv_bfloat16* __restrict
   const int tiles = (n + TC_CELLS - 1) / TC_CELLS;
   for (int tile = blockIdx.x * TC_WARPS + w; tile < tiles; tile += gridDim.x * TC_WARPS) {
     const int c0 = tile * TC_CELLS;
-    for (int cc = 0; cc < TC_CELLS; ++cc) {
+    // gather: four lanes per cell row (8 channels each, one 16-byte load per
+    // row), 8 cells of the tile at a time; per channel the neighbours add up
+    // in row order, as in the training kernels
+    const int sub = lane >> 2, cb = (lane & 3) * 8;
+    for (int cc0 = 0; cc0 < TC_CELLS; cc0 += 8) {
+      const int cc = cc0 + sub;
       const int i = c0 + cc;
-      __nv_bfloat16 hv = __float2bfloat16(0.0f), av = hv;
+      uint4 hv = make_uint4(0u, 0u, 0u, 0u);
+      float af[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) af[t] = 0.0f;
       if (i < n) {
-        hv = hin[(size_t)i * H + lane];
+        hv = *reinterpret_cast<const uint4*>(hin + (size_t)i * H + cb);
         sg::RowIt<float> it(R, i);
-        float agg = 0.0f;
         for (int k = 0; k < it.w; ++k) {
           const int e = it.base + k * sg::kWarp;
           const int j = R.col[e];
-          if (j >= 0) agg += F.gw[e] * __bfloat162float(hin[(size_t)j * H + lane]);
+          if (j >= 0) {
+            const float wgt = F.gw[e];
+            const uint4 v = *reinterpret_cast<const uint4*>(hin + (size_t)j * H + cb);
+            const __nv_bfloat162* p2 = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+              const float2 f = __bfloat1622float2(p2[t]);
+              af[2 * t] += wgt * f.x;
+              af[2 * t + 1] += wgt * f.y;
+            }
+          }
         }
-        av = __float2bfloat16(agg);
       }
-      sA[w][cc][lane] = hv;
-      sA[w][cc][H + lane] = av;
+      uint4 av;
+      __nv_bfloat162* a2 = reinterpret_cast<__nv_bfloat162*>(&av);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) a2[t] = __floats2bfloat162_rn(af[2 * t], af[2 * t + 1]);
+      *reinterpret_cast<uint4*>(&sA[w][cc][cb]) = hv;
+      *reinterpret_cast<uint4*>(&sA[w][cc][H + cb]) = av;
     }
     __syncwarp();
     float acc[4][4];
@@ -222,24 +244,46 @@ template <typename HT>
 __global__ void k_gnn_heads(int n, const HT* __restrict__ h3, const float* __restrict__ P,
                             const float* __restrict__ qscale, float* __restrict__ pa_out,
                             float* __restrict__ s_out, float* __restrict__ he_out) {
-  const int lane = threadIdx.x & 31;
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  const float wa = bf(P[P_WA + lane]), we = bf(P[P_WE + lane]), ba = bf(P[P_BA]);
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
-    const float h = (float)h3[(size_t)i * H + lane];
-    float a = wa * h, e = we * h;
+  // one thread per cell; the 32 hidden channels of a cell are one
+  // contiguous row (64 bytes in BF16: four 16-byte loads)
+  __shared__ float swa[H], swe[H];
+  if (threadIdx.x < H) {
+    swa[threadIdx.x] = bf(P[P_WA + threadIdx.x]);
+    swe[threadIdx.x] = bf(P[P_WE + threadIdx.x]);
+  }
+  __syncthreads();
+  const float ba = bf(P[P_BA]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float a = 0.0f, e = 0.0f;
+    if constexpr (std::is_same<HT, __nv_bfloat16>::value) {
+      const uint4* row = reinterpret_cast<const uint4*>(h3 + (size_t)i * H);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      e += __shfl_xor_sync(0xffffffffu, e, o);
+      for (int q = 0; q < 4; ++q) {
+        const uint4 v = row[q];
+        const __nv_bfloat162* p2 = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const float2 f = __bfloat1622float2(p2[t]);
+          const int c = q * 8 + 2 * t;
+          a = fmaf(swa[c], f.x, a);
+          a = fmaf(swa[c + 1], f.y, a);
+          e = fmaf(swe[c], f.x, e);
+          e = fmaf(swe[c + 1], f.y, e);
+        }
+      }
+    } else {
+#pragma unroll 8
+      for (int c = 0; c < H; ++c) {
+        const float h = (float)h3[(size_t)i * H + c];
+        a = fmaf(swa[c], h, a);
+        e = fmaf(swe[c], h, e);
+      }
     }
-    if (lane == 0) {
-      const float pa = a + ba;
-      const float s = sqrtf(softplus(pa) / softplus(0.0f));  // exactly 1 untrained
-      if (pa_out) pa_out[i] = pa;
-      s_out[i] = qscale ? s * qscale[i] : s;
-      he_out[i] = e;
-    }
+    const float pa = a + ba;
+    const float s = sqrtf(softplus(pa) / softplus(0.0f));  // exactly 1 untrained
+    if (pa_out) pa_out[i] = pa;
+    s_out[i] = qscale ? s * qscale[i] : s;
+    he_out[i] = e;
   }
 }
 

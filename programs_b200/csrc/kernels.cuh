@@ -147,6 +147,16 @@ __device__ __forceinline__ void lane_stop(Lane& L, int status, int* n_active) {
   }
 }
 
+// Kernels on the reduction grid (SegMap) are meant to run every block of the
+// grid at once: the grid holds at most 2048 threads per SM (blocks of at
+// most 256 threads), and the register budget of the one-component kernels
+// is capped at 32 so that all of them are resident -- a block left for a
+// second wave would run the tail of every reduction at a fraction of the
+// occupancy.  Several components (V > 1) get 64 registers and run in two
+// full waves.
+constexpr int kMaxBlock = 256;
+#define SG_BOUNDS(V) __launch_bounds__(sg::kMaxBlock, ((V) == 1 ? 8 : 4))
+
 // Row walk helpers ---------------------------------------------------------
 template <typename T>
 struct RowIt {
@@ -293,7 +303,7 @@ __global__ void k_convert(long long n, const Tsrc* __restrict__ a, Tdst* __restr
 // ---- residual: solv_res.f90:12-29 ----------------------------------------
 // r_i = ((b_i - pl_i phi_i) - a_1 phi_j1) - ...; L1 norm per component.
 template <int V>
-__global__ void k_res(Rows<double> R, SegMap sm, const double* __restrict__ phi,
+__global__ void SG_BOUNDS(V) k_res(Rows<double> R, SegMap sm, const double* __restrict__ phi,
                       double* __restrict__ r, int not_r0, double* __restrict__ part,
                       double* __restrict__ l1_out) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
@@ -359,7 +369,7 @@ __global__ void k_add(long long n, double* __restrict__ x, const double* __restr
 // phi += (double) d for the (system, component) lanes flagged in mask
 // (FP64 solution accumulation)
 template <int V>
-__global__ void k_mp_accum(SegMap sm, const int* __restrict__ mask, double* __restrict__ phi,
+__global__ void SG_BOUNDS(V) k_mp_accum(SegMap sm, const int* __restrict__ mask, double* __restrict__ phi,
                            const float* __restrict__ d) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   bool on[V];
@@ -504,7 +514,7 @@ __global__ void k_lane_init(Lane* lanes, int nl, int n_iter, double reduc, int* 
 // with q = A p of the previous step, the flexible-CG formula that
 // A-orthogonalises the new direction against the last one explicitly.
 template <typename T, int V, bool JAC, bool FLEX = false>
-__global__ void k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
+__global__ void SG_BOUNDS(V) k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
                         const T* __restrict__ z, double* __restrict__ part,
                         Lane* __restrict__ lanes, const T* __restrict__ q = nullptr) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
@@ -547,7 +557,7 @@ __global__ void k_cg_rz(SegMap sm, const T* __restrict__ c, const T* __restrict_
 // alpha = (p.r)/(p.q) of k_cg_spmv makes the new residual orthogonal to p
 // in the arithmetic actually done (flexible CG).
 template <typename T, int V, bool JAC, bool FLEX = false>
-__global__ void k_cg_p(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
+__global__ void SG_BOUNDS(V) k_cg_p(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
                        const T* __restrict__ z, T* __restrict__ p,
                        Lane* __restrict__ lanes, double* __restrict__ part = nullptr) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
@@ -590,7 +600,7 @@ __global__ void k_cg_p(SegMap sm, const T* __restrict__ c, const T* __restrict__
 
 // q = A p and p.q; alpha = s / (p.q + small)   (solv_cg.f90:56-68)
 template <typename T, int V>
-__global__ void k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
+__global__ void SG_BOUNDS(V) k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
                           double* __restrict__ part, Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   bool any = false;
@@ -627,7 +637,7 @@ __global__ void k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __re
 // With JAC, also s_next = r.(c r) and beta for the next iteration; with
 // JAC and FLEX, beta = -(z.q)/(p.q) instead, z = c r of the new residual.
 template <typename T, int V, bool JAC, bool FLEX = false>
-__global__ void k_cg_update(SegMap sm, const T* __restrict__ c, T* __restrict__ phi,
+__global__ void SG_BOUNDS(V) k_cg_update(SegMap sm, const T* __restrict__ c, T* __restrict__ phi,
                             T* __restrict__ r, const T* __restrict__ p,
                             const T* __restrict__ q, double* __restrict__ part,
                             Lane* __restrict__ lanes) {
@@ -688,7 +698,7 @@ __global__ void k_cg_update(SegMap sm, const T* __restrict__ c, T* __restrict__ 
 // ===================== BiCGSTAB: solv_bicg.f90:27-118 ======================
 // rho = r.r0; omeg = rho*gam/(alpha*beta0+small); beta0 = rho  (:48-50)
 template <typename T, int V>
-__global__ void k_bi_rho(SegMap sm, const T* __restrict__ r, const T* __restrict__ r0,
+__global__ void SG_BOUNDS(V) k_bi_rho(SegMap sm, const T* __restrict__ r, const T* __restrict__ r0,
                          double* __restrict__ part, Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   bool any = false;
@@ -719,7 +729,7 @@ __global__ void k_bi_rho(SegMap sm, const T* __restrict__ r, const T* __restrict
 
 // p = r + omeg (p - alpha u); with JAC also z = c p  (:54-58)
 template <typename T, int V, bool JAC>
-__global__ void k_bi_p(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
+__global__ void SG_BOUNDS(V) k_bi_p(SegMap sm, const T* __restrict__ c, const T* __restrict__ r,
                        T* __restrict__ p, const T* __restrict__ u, T* __restrict__ z,
                        const Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
@@ -751,7 +761,7 @@ __global__ void k_bi_p(SegMap sm, const T* __restrict__ c, const T* __restrict__
 // y = A z, and dots: MODE 0 -> y.r0 (gam = rho/(y.r0+small), :72-73)
 //                    MODE 1 -> y.r, y.y (alpha = (y.r)/(y.y+small), :98-100)
 template <typename T, int V, int MODE>
-__global__ void k_bi_spmv(Rows<T> R, SegMap sm, const T* __restrict__ z, T* __restrict__ y,
+__global__ void SG_BOUNDS(V) k_bi_spmv(Rows<T> R, SegMap sm, const T* __restrict__ z, T* __restrict__ y,
                           const T* __restrict__ w, double* __restrict__ part,
                           Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
@@ -792,7 +802,7 @@ __global__ void k_bi_spmv(Rows<T> R, SegMap sm, const T* __restrict__ z, T* __re
 
 // phi += gam z; r -= gam u; with JAC also z = c r   (:77-84)
 template <typename T, int V, bool JAC>
-__global__ void k_bi_half(SegMap sm, const T* __restrict__ c, T* __restrict__ phi,
+__global__ void SG_BOUNDS(V) k_bi_half(SegMap sm, const T* __restrict__ c, T* __restrict__ phi,
                           T* __restrict__ r, T* __restrict__ z, const T* __restrict__ u,
                           const Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
@@ -824,7 +834,7 @@ __global__ void k_bi_half(SegMap sm, const T* __restrict__ c, T* __restrict__ ph
 // phi += alpha z; r -= alpha v; L1; stop test; rho_next = r.r0 with the
 // omeg / beta0 update of the next iteration's head (:105-116, :48-50).
 template <typename T, int V>
-__global__ void k_bi_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
+__global__ void SG_BOUNDS(V) k_bi_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
                             const T* __restrict__ z, const T* __restrict__ vv,
                             const T* __restrict__ r0, double* __restrict__ part,
                             Lane* __restrict__ lanes) {
@@ -882,7 +892,7 @@ __global__ void k_bi_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
 // d (FP32 correction since the last update) -> x (FP64) for every lane
 // flagged in mask, and d = 0.
 template <int V>
-__global__ void k_mp_flush(SegMap sm, const int* __restrict__ mask, double* __restrict__ x,
+__global__ void SG_BOUNDS(V) k_mp_flush(SegMap sm, const int* __restrict__ mask, double* __restrict__ x,
                            float* __restrict__ d) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   bool on[V];
@@ -905,7 +915,7 @@ __global__ void k_mp_flush(SegMap sm, const int* __restrict__ mask, double* __re
 
 // r_f = (float) r for the lanes in mask
 template <int V>
-__global__ void k_mp_replace(SegMap sm, const int* __restrict__ mask, const double* __restrict__ r,
+__global__ void SG_BOUNDS(V) k_mp_replace(SegMap sm, const int* __restrict__ mask, const double* __restrict__ r,
                              float* __restrict__ rf) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   bool on[V];
@@ -928,7 +938,7 @@ __global__ void k_mp_replace(SegMap sm, const int* __restrict__ mask, const doub
 
 // gs = sum |r_i| rsd_i / N: the residual scale the network normalises by.
 template <typename T>
-__global__ void k_fcg_scale(SegMap sm, const T* __restrict__ r, const float* __restrict__ rsd,
+__global__ void SG_BOUNDS(1) k_fcg_scale(SegMap sm, const T* __restrict__ r, const float* __restrict__ rsd,
                             double* __restrict__ part, Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   if (!lanes[s].active) return;
@@ -943,7 +953,7 @@ __global__ void k_fcg_scale(SegMap sm, const T* __restrict__ r, const float* __r
 }
 
 template <typename T>
-__global__ void k_fcg_beta(SegMap sm, const T* __restrict__ z, const T* __restrict__ q,
+__global__ void SG_BOUNDS(1) k_fcg_beta(SegMap sm, const T* __restrict__ z, const T* __restrict__ q,
                            double* __restrict__ part, Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
   if (!lanes[s].active) return;
@@ -960,7 +970,7 @@ __global__ void k_fcg_beta(SegMap sm, const T* __restrict__ z, const T* __restri
 }
 
 template <typename T>
-__global__ void k_fcg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
+__global__ void SG_BOUNDS(1) k_fcg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
                            const T* __restrict__ r, double* __restrict__ part,
                            Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
@@ -989,7 +999,7 @@ __global__ void k_fcg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __r
 }
 
 template <typename T>
-__global__ void k_fcg_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
+__global__ void SG_BOUNDS(1) k_fcg_update(SegMap sm, T* __restrict__ phi, T* __restrict__ r,
                              const T* __restrict__ p, const T* __restrict__ q,
                              double* __restrict__ part, Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];

@@ -193,7 +193,9 @@ int build_segments(solv_gpu_ctx* c, const std::vector<int>& seg_c0,
   const int ns = (int)seg_c0.size();
   long long total = 0;
   for (int k = 0; k < ns; ++k) total += seg_c1[k] - seg_c0[k];
-  const long long cap = (long long)c->n_sm * c->grid_per_sm;
+  // all blocks of the reduction grid resident: at most 2048 threads per SM
+  const long long per_sm = std::min(c->grid_per_sm, 2048 / c->block);
+  const long long cap = (long long)c->n_sm * std::max(1LL, per_sm);
   for (int k = 0; k < ns; ++k) {
     long long n = seg_c1[k] - seg_c0[k];
     long long want = (n + c->block - 1) / c->block;
@@ -528,7 +530,7 @@ void gnn_build(solv_gpu_ctx* c, const T* r0) {
         P + gnn::P_LAYER + l * gnn::LAYER_SZ + 2 * gnn::H * gnn::H);
     std::swap(hin, hout);
   }
-  gnn::k_gnn_heads<__nv_bfloat16><<<gw, 256, 0, c->stream>>>(
+  gnn::k_gnn_heads<__nv_bfloat16><<<grid_for(c, N), 256, 0, c->stream>>>(
       N, hin, P, c->g_rsd.as<float>(), nullptr, c->g_q.as<float>(), c->g_he.as<float>());
   gnn::k_gnn_edges<<<grid_for(c, N), c->block, 0, c->stream>>>(
       N, rows<float>(c), F, c->g_he.as<float>(), P, nullptr, c->g_ge.as<float>());
@@ -1568,7 +1570,8 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
       return SOLV_GPU_OK;
     case SOLV_OPT_BLOCK: {
       int b = (int)value;
-      if (b < 64 || b > 1024 || (b & 31)) return set_err(c, SOLV_GPU_BAD_INPUT, "block must be a multiple of 32 in 64..1024");
+      if (b < 64 || b > sg::kMaxBlock || (b & 31))
+        return set_err(c, SOLV_GPU_BAD_INPUT, "block must be a multiple of 32 in 64..256");
       c->block = b;
       if (c->has_matrix) return build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
       return SOLV_GPU_OK;
@@ -1975,8 +1978,8 @@ int solv_gpu_autotune(solv_gpu_ctx* c, int solver, int imat, int n_vc, solv_gpu_
     ms = (float)st.solve_ms;
     return SOLV_GPU_OK;
   };
-  const int blocks[] = {128, 256, 512};
-  const int gps[] = {2, 4, 8, 16};
+  const int blocks[] = {128, 256};
+  const int gps[] = {4, 8, 16};
   const int graphs[] = {8, 32};
   const int k_short = 4, k_long = 36;
   const int precision = c->precision;
@@ -1990,6 +1993,7 @@ int solv_gpu_autotune(solv_gpu_ctx* c, int solver, int imat, int n_vc, solv_gpu_
     drop_graphs(c);
     for (int bl : blocks)
       for (int g : gps) {
+        if (g * bl > 2048) continue;  // the reduction grid stays resident
         c->block = bl;
         c->grid_per_sm = g;
         int rc = build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
@@ -2160,7 +2164,7 @@ static int gnn_train_forward(solv_gpu_ctx* c, const double* r0_dev, float** B) {
     gnn::k_gnn_layer_train<<<lb, 256, 0, c->stream>>>(
         N, rows<float>(c), F, B[TB_H0 + l], B[TB_AGG0 + l], B[TB_PRE0 + 1 + l], B[TB_H0 + 1 + l],
         P + gnn::P_LAYER + l * gnn::LAYER_SZ);
-  gnn::k_gnn_heads<float><<<gw, 256, 0, c->stream>>>(N, B[TB_H0 + 3], P, nullptr, B[TB_PA],
+  gnn::k_gnn_heads<float><<<grid_for(c, N), 256, 0, c->stream>>>(N, B[TB_H0 + 3], P, nullptr, B[TB_PA],
                                                      B[TB_S], B[TB_HE]);
   gnn::k_gnn_edges<<<grid_for(c, N), c->block, 0, c->stream>>>(N, rows<float>(c), F, B[TB_HE], P,
                                                                B[TB_EPRE], B[TB_GE]);
