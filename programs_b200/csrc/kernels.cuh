@@ -175,6 +175,13 @@ struct RowIt {
 // FP64).  For the smooth vectors late Krylov iterations produce, x_j - x_i
 // is exact and small, so the product keeps its relative accuracy instead of
 // losing log10(cond) digits to cancellation; same bytes moved.
+// FP32 rows are walked kRowChunk slots at a time: the column indices, the
+// coefficients and the gathered x of a chunk are all loaded before any of
+// them is used, so a warp keeps several independent gathers in flight; the
+// sums still run slot by slot.  (FP64 keeps the plain walk: chunks would
+// spill under the reduction kernels' 32-register cap.)
+constexpr int kRowChunk = 4;
+
 template <typename T, int V>
 __device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
                                           const T* __restrict__ x, T (&y)[V]) {
@@ -187,14 +194,29 @@ __device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
       xi[v] = x[(size_t)i * V + v];
       y[v] = d * xi[v];
     }
-    for (int k = 0; k < it.w; ++k) {
-      const int e = it.base + k * kWarp;
-      const int j = __ldg(&R.col[e]);
-      if (j >= 0) {
-        const T a = R.val[e];
+    for (int k0 = 0; k0 < it.w; k0 += kRowChunk) {
+      int j[kRowChunk];
+      T a[kRowChunk], xv[kRowChunk][V];
 #pragma unroll
-        for (int v = 0; v < V; ++v) y[v] = fmaf(a, x[(size_t)j * V + v] - xi[v], y[v]);
+      for (int u = 0; u < kRowChunk; ++u) {
+        j[u] = -1;
+        a[u] = T(0);
+        if (k0 + u < it.w) {
+          const int e = it.base + (k0 + u) * kWarp;
+          j[u] = __ldg(&R.col[e]);
+          a[u] = R.val[e];
+        }
       }
+#pragma unroll
+      for (int u = 0; u < kRowChunk; ++u)
+#pragma unroll
+        for (int v = 0; v < V; ++v) xv[u][v] = j[u] >= 0 ? x[(size_t)j[u] * V + v] : xi[v];
+#pragma unroll
+      for (int u = 0; u < kRowChunk; ++u)
+        if (j[u] >= 0) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) y[v] = fmaf(a[u], xv[u][v] - xi[v], y[v]);
+        }
     }
   } else {
 #pragma unroll

@@ -450,10 +450,24 @@ __global__ void k_mg_pre(int n, sg::Rows<float> R, const float* __restrict__ din
     const float bi = b[i];
     const float xi = w * dinv[i] * bi;
     float y = R.diag[i] * xi;
-    for (int k = 0; k < it.w; ++k) {
-      const int e = it.base + k * sg::kWarp;
-      const int j = __ldg(&R.col[e]);
-      if (j >= 0) y = fmaf(R.val[e], w * dinv[j] * b[j] - xi, y);
+    for (int k0 = 0; k0 < it.w; k0 += sg::kRowChunk) {
+      int j[sg::kRowChunk];
+      float a[sg::kRowChunk], xj[sg::kRowChunk];
+#pragma unroll
+      for (int u = 0; u < sg::kRowChunk; ++u) {
+        j[u] = -1;
+        a[u] = 0.0f;
+        if (k0 + u < it.w) {
+          const int e = it.base + (k0 + u) * sg::kWarp;
+          j[u] = __ldg(&R.col[e]);
+          a[u] = R.val[e];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < sg::kRowChunk; ++u) xj[u] = j[u] >= 0 ? w * dinv[j[u]] * b[j[u]] : xi;
+#pragma unroll
+      for (int u = 0; u < sg::kRowChunk; ++u)
+        if (j[u] >= 0) y = fmaf(a[u], xj[u] - xi, y);
     }
     x[i] = xi;
     t[i] = bi - y;
@@ -497,10 +511,27 @@ __global__ void k_mg_net(int n, sg::Rows<float> R, const float* __restrict__ gE,
     sg::RowIt<float> it(R, i);
     const float qi = q[i];
     float t = qi * in[i];
-    for (int k = 0; k < it.w; ++k) {
-      const int e = it.base + k * sg::kWarp;
-      const int j = __ldg(&R.col[e]);
-      if (j >= 0) t = fmaf(gE[e] * q[j], in[j], t);
+    for (int k0 = 0; k0 < it.w; k0 += sg::kRowChunk) {
+      int j[sg::kRowChunk];
+      float g[sg::kRowChunk], qj[sg::kRowChunk], vj[sg::kRowChunk];
+#pragma unroll
+      for (int u = 0; u < sg::kRowChunk; ++u) {
+        j[u] = -1;
+        g[u] = 0.0f;
+        if (k0 + u < it.w) {
+          const int e = it.base + (k0 + u) * sg::kWarp;
+          j[u] = __ldg(&R.col[e]);
+          g[u] = gE[e];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < sg::kRowChunk; ++u) {
+        qj[u] = j[u] >= 0 ? q[j[u]] : 0.0f;
+        vj[u] = j[u] >= 0 ? in[j[u]] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < sg::kRowChunk; ++u)
+        if (j[u] >= 0) t = fmaf(g[u] * qj[u], vj[u], t);
     }
     const float v = w * qi * t;
     out[i] = (TO)(ADD ? base[i] + v : v);
