@@ -12,7 +12,10 @@ Per outer iteration:
   p' = solve (CG, or FCG with the learned preconditioner)   :662
   p += urf_p p', u -= V/a_P grad p', F -= d dp'     cfd_setup.f90:689-729
 
-  python -m programs_b200.simple --size 32 --outer 200 [--learned]
+  python -m programs_b200.simple --size 32 --outer 200 [--learned] [--device-assembly]
+
+With --device-assembly (run_device) every piece above runs on the GPU
+(programs_b200/fv.py, include/fv_gpu.h), bit-for-bit as on the host.
 """
 from __future__ import annotations
 
@@ -104,6 +107,104 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
     return u, p, hist, timing
 
 
+def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15,
+               seed=0, p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None,
+               p_imat=1, m_precision=0, device=0, log_every=0):
+    """The same outer loop with everything on the GPU: assembly, gradients,
+    fluxes and corrections by the fv_gpu kernels (bit-for-bit the host
+    functions), solves through the device-pointer entry points; only the
+    mass-imbalance norm comes back per iteration.  Same arguments and
+    returns as run(); timings are wall clock with the stream synchronised."""
+    import torch
+
+    from .fv import GpuFv
+    from .mesh import FaceMatrix
+    rho = 1.0
+    mu = rho * u_lid * 1.0 / re
+    m = Mesh.hex(size, jitter=jitter, seed=seed, permute=True)
+    m.renumber(Mesh.RCM)
+    m.cache_geometry()
+    N = m.n_cell
+    ip, inb = m.faces()
+    _, vol_h = m.cell_geom()
+    dev = torch.device("cuda", device)
+    stream = torch.cuda.Stream(device=dev)
+    fv = GpuFv(m, device)
+    fv._lib.fv_gpu_set_stream(fv._h, stream.cuda_stream)
+    sm = GpuSolver(device)
+    sp = GpuSolver(device)
+    for s_ in (sm, sp):
+        s_.set_stream(stream.cuda_stream)
+    sm.set_option(OPT_PRECISION, m_precision)
+    if learned is not None:
+        sp.gnn_set_params(learned)
+    # the structure once (values come from the device each iteration)
+    F_ = ip.shape[0]
+    shell = FaceMatrix(N, ip, inb, np.zeros(F_), np.zeros(F_), np.ones(N))
+    sm.matrix_set(shell)
+    sp.matrix_set(shell)
+    hist = []
+    t_asm = t_solve_m = t_solve_p = 0.0
+
+    def sync_time(t):
+        stream.synchronize()
+        return time.time() - t
+
+    with torch.cuda.stream(stream):
+        vol = torch.from_numpy(vol_h).to(dev)
+        u = torch.zeros(N, 3, dtype=torch.float64, device=dev)
+        p = torch.zeros(N, dtype=torch.float64, device=dev)
+        F = None
+        t0 = time.time()
+        for k in range(n_outer):
+            ta = time.time()
+            gradp = fv.gradient(p)
+            Mp, Mn, Mpl, rhs, Fm = fv.momentum_field(u, flux=F, rho=rho, mu=mu, u_lid=u_lid,
+                                                     urf=urf_u)
+            if F is None:
+                F = Fm
+            rhs -= gradp * vol[:, None]
+            t_asm += sync_time(ta)
+            ts = time.time()
+            sm.matrix_values_dev(Mp.data_ptr(), Mn.data_ptr(), Mpl.data_ptr())
+            res0 = rhs.t().contiguous()  # column-major res0(ip, ivc)
+            rn_m, stm = sm.solv_bicg_dev(2, m_reduc, m_iter, 3, u.data_ptr(), res0.data_ptr())
+            t_solve_m += sync_time(ts)
+            ta = time.time()
+            F = fv.face_flux(u, p, gradp, Mpl, rho)
+            Pp, Pn, Ppl = fv.pressure_correction(Mpl, rho=rho, pin=1)
+            b, imb = fv.mass_imbalance(F, pin=1)
+            t_asm += sync_time(ta)
+            ts = time.time()
+            sp.matrix_values_dev(Pp.data_ptr(), Pn.data_ptr(), Ppl.data_ptr())
+            pp = torch.zeros(N, dtype=torch.float64, device=dev)
+            if learned is not None:
+                rn_p, stp = sp.solv_fcg_dev(p_reduc, p_iter, pp.data_ptr(), b.data_ptr(),
+                                            not_r0=True)
+            else:
+                rn_p, stp = sp.solv_cg_dev(p_imat, p_reduc, p_iter, 1, pp.data_ptr(),
+                                           b.data_ptr(), not_r0=True)
+            t_solve_p += sync_time(ts)
+            ta = time.time()
+            gradpp = fv.gradient(pp)
+            fv.simple_correct(pp, gradpp, Mpl, rho, urf_p, u, p, F)
+            t_asm += sync_time(ta)
+            rec = {"it": k, "mass": float(imb), "mom_res0": list(map(float, rn_m)),
+                   "p_iters": stp["iters"][0], "m_iters": stm["iters"],
+                   "fallbacks": stp.get("fallbacks", 0)}
+            hist.append(rec)
+            if log_every and (k % log_every == 0 or k == n_outer - 1):
+                print(json.dumps(rec), flush=True)
+        total = sync_time(t0)
+    u_h, p_h = u.cpu().numpy(), p.cpu().numpy()
+    sm.close()
+    sp.close()
+    fv.close()
+    timing = {"total_s": total, "assembly_s": t_asm, "momentum_solve_s": t_solve_m,
+              "pressure_solve_s": t_solve_p, "n_cell": N}
+    return u_h, p_h, hist, timing
+
+
 def rel_l2(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
 
@@ -116,14 +217,17 @@ def main(argv=None):
     ap.add_argument("--learned", action="store_true", help="also run learned + mixed FCG and compare")
     ap.add_argument("--weights", default=None)
     ap.add_argument("--log-every", type=int, default=20)
+    ap.add_argument("--device-assembly", action="store_true",
+                    help="assembly, gradients and corrections on the GPU too")
     a = ap.parse_args(argv)
-    u0, p0, h0, t0 = run(a.size, a.outer, a.re, log_every=a.log_every)
+    loop = run_device if a.device_assembly else run
+    u0, p0, h0, t0 = loop(a.size, a.outer, a.re, log_every=a.log_every)
     out = {"size": a.size, "outer": a.outer, "plain": t0, "final_mass_plain": h0[-1]["mass"],
            "p_iters_plain": int(np.sum([h["p_iters"] for h in h0]))}
     if a.learned:
         from .learn import DEFAULT_WEIGHTS, load_params
         w = load_params(a.weights or DEFAULT_WEIGHTS)
-        u1, p1, h1, t1 = run(a.size, a.outer, a.re, learned=w, log_every=a.log_every)
+        u1, p1, h1, t1 = loop(a.size, a.outer, a.re, learned=w, log_every=a.log_every)
         out.update(learned=t1, p_iters_learned=int(np.sum([h["p_iters"] for h in h1])),
                    fallbacks=int(np.sum([h["fallbacks"] for h in h1])),
                    rel_l2_u=rel_l2(u1[:, 0], u0[:, 0]), rel_l2_v=rel_l2(u1[:, 1], u0[:, 1]),

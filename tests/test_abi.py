@@ -16,7 +16,7 @@ def _built(built):
 def _declared(header):
     src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(solv_gpu_\w+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b((?:solv_gpu|fv_gpu)_\w+)\s*\(", src)))
 
 
 def test_every_declared_symbol_is_exported():
@@ -27,6 +27,15 @@ def test_every_declared_symbol_is_exported():
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
     assert set(names) <= set(EXPORTS) | set(names)
+
+
+def test_every_fv_symbol_is_exported():
+    from programs_b200.solver import lib
+    L = lib()
+    names = _declared("fv_gpu.h")
+    assert len(names) == 9
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
 
 
 def test_status_strings_and_no_device_path():
