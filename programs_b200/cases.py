@@ -3,6 +3,7 @@
   python -m programs_b200.cases solve  --size 128 --system pressure --solver cg --imat 0
   python -m programs_b200.cases spmv   --size 128 --repeat 20
   python -m programs_b200.cases batch  --n-sys 64 --min 8000 --max 500000
+  python -m programs_b200.cases kernel --size 160 --which 1 --repeat 5
 
 The systems are the seeded synthetic ones of the benchmarks: jittered
 (+-15%), randomly permuted hex meshes renumbered by the framework, the
@@ -54,7 +55,9 @@ def batch_meshes(n_sys, lo, hi, seed=1):
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("what", choices=["solve", "spmv", "batch"])
+    ap.add_argument("what", choices=["solve", "spmv", "batch", "kernel"])
+    ap.add_argument("--which", type=int, default=1,
+                    help="kernel: 0 FP64 SpMV, 1 FP32 SpMV, 2 network operator, 3 V-cycle")
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--system", default="pressure", choices=["pressure", "momentum"])
     ap.add_argument("--solver", default="cg", choices=["cg", "bicg", "fcg"])
@@ -113,7 +116,10 @@ def main(argv=None):
             s.gnn_set_params(load_params(a.weights or DEFAULT_WEIGHTS))
         if a.autotune:
             out["tune"] = s.autotune("cg" if a.solver != "bicg" else "bicg", a.imat, a.n_vc)
-        if a.what == "spmv":
+        if a.what == "kernel":
+            ms = s.kernel_time(a.which, a.repeat)
+            out.update(n_cell=A.n_cell, which=a.which, ms_per_launch=ms)
+        elif a.what == "spmv":
             x = torch.from_numpy(uniform(3, A.n_cell)).to(dev)
             y = torch.empty_like(x)
             ms = s.spmv_dev(x.data_ptr(), y.data_ptr(), repeat=a.repeat)
