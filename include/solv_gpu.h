@@ -88,7 +88,9 @@ extern "C" {
                                    alone)                                  */
 #define SOLV_OPT_MG_SMOOTHER 11 /* finest-level smoother of the hierarchy:
                                    1 = the network's operator (default),
-                                   0 = damped Jacobi (no network)          */
+                                   2 = its diagonal alone: Jacobi with the
+                                   network's per-cell weights (as cheap as
+                                   Jacobi), 0 = damped Jacobi (no network) */
 #define SOLV_OPT_MG_OMEGA 12    /* smoother damping (default 0.8)          */
 #define SOLV_OPT_MG_ALPHA 13    /* coarse-correction scale (default 2)     */
 

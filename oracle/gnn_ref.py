@@ -192,12 +192,14 @@ def vcycle(mats, Ps, b, smooth0, omega, alpha, l=0):
     return x + omega * S(b - mv(x))
 
 
-def loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=False):
+def loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=False, diag=False):
     """Mean over samples of L/N, L = -log((z.b)^2/(z.A z)) with z the
     V-cycle applied to b = r / gs, the network's operator
     K = D^-1/2 S (I+E) S D^-1/2 smoothing level 0 (the loss the GPU trains
     with through the V-cycle)."""
     s, gE, rows_t, cols_t, wt, P, rsd = build(A, r0, params, grad=grad)
+    if diag:  # smoother 2: the per-cell scales alone (learned Jacobi weights)
+        gE = gE * 0.0
     rsd_t = torch.tensor(rsd, dtype=torch.float64)
     K = lambda v: rsd_t * _apply(s, gE, rows_t, cols_t, rsd_t * v)
     mats, Ps = hierarchy(A, aggs)
@@ -214,7 +216,7 @@ def loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=False):
     return J / len(samples), P
 
 
-def loss_mg_and_grad(A, r0, samples, params, aggs, omega, alpha):
-    J, P = loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=True)
+def loss_mg_and_grad(A, r0, samples, params, aggs, omega, alpha, diag=False):
+    J, P = loss_mg(A, r0, samples, params, aggs, omega, alpha, grad=True, diag=diag)
     J.backward()
     return float(J.detach()), P.grad.numpy().copy()

@@ -14,7 +14,9 @@
 //                     two aggregates summed, row sums summed),
 //   V-cycle on b:  x = w K b;  t = b - A x;  x += a P V(P^T t);
 //                  x += w K (b - A x),
-//   K              = the network's operator on level 0 (or D^-1), D^-1 below,
+//   K              = the network's operator on level 0 (or its diagonal
+//                     S^2 D^-1 alone -- learned Jacobi weights, fused like
+//                     Jacobi -- or D^-1), D^-1 below,
 //   coarsest level = at most kCoarsest cells, solved with its dense inverse.
 //
 // With a symmetric positive definite K on level 0 and Jacobi below, the
@@ -536,6 +538,12 @@ __global__ void k_mg_net(int n, sg::Rows<float> R, const float* __restrict__ gE,
     const float v = w * qi * t;
     out[i] = (TO)(ADD ? base[i] + v : v);
   }
+}
+
+// dq = q^2: the network's per-cell scale as a Jacobi weight (smoother 2)
+__global__ void k_mg_square(int n, const float* __restrict__ q, float* __restrict__ dq) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    dq[i] = q[i] * q[i];
 }
 
 // bc[I] = sum of t over I's members (restriction P^T)

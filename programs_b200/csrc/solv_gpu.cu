@@ -138,7 +138,8 @@ struct solv_gpu_ctx {
 
   // aggregation multigrid around the learned preconditioner (mg.cuh)
   int mg_max_levels = mg::kMaxLevels;  // coarse levels at most; 0 = one-level preconditioner
-  int mg_smoother = 1;                 // level-0 smoother: 1 the network's operator, 0 Jacobi
+  int mg_smoother = 1;                 // level-0 smoother: 1 the network's operator K,
+                                       // 2 its diagonal (learned Jacobi weights), 0 Jacobi
   double mg_omega = 0.8;               // smoother damping (1.0 loses the V-cycle)
   double mg_alpha = 2.0;               // coarse-correction scale (unsmoothed
                                        // aggregation under-corrects smooth error)
@@ -147,6 +148,8 @@ struct solv_gpu_ctx {
   std::vector<std::unique_ptr<MgLevel>> mg;  // coarse levels 1..L
   DevBuf mg_x0, mg_t0, mg_dinv0, mg_dense, mg_ainv;
   DevBuf mg_train;                     // training through the V-cycle: 8 vectors
+  DevBuf mg_dq;                        // smoother 2: the network's per-cell weights q^2
+  DevBuf g_zero;                       // smoother 2 training: face weights held at zero
   double mg_setup_s = 0.0;
 };
 
@@ -624,6 +627,7 @@ int mg_setup(solv_gpu_ctx* c) {
   CUDA_TRY(c, c->mg_x0.ensure((size_t)c->N * sizeof(float)));
   CUDA_TRY(c, c->mg_t0.ensure((size_t)c->N * sizeof(float)));
   CUDA_TRY(c, c->mg_dinv0.ensure((size_t)c->N * sizeof(float)));
+  CUDA_TRY(c, c->mg_dq.ensure((size_t)c->N * sizeof(float)));
   CUDA_TRY(c, c->mg_dense.ensure((size_t)nL * nL * sizeof(double)));
   CUDA_TRY(c, c->mg_ainv.ensure((size_t)nL * nL * sizeof(float)));
   c->mg_setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -696,18 +700,21 @@ int mg_coarse_cycle(solv_gpu_ctx* c, const int* na) {
 }
 
 // z = one symmetric V-cycle applied to r (FP32, level 0 = the context's
-// matrix).  The network's operator (q, gE) smooths level 0 when net, damped
-// Jacobi otherwise.  x0 and t0 hold, afterwards, the level-0 iterate before
-// post-smoothing and its residual.  Returns the number of kernels launched.
+// matrix).  Level 0 is smoothed by the network's operator (q, gE) for
+// mode 1, by Jacobi with the network's per-cell weights q^2 for mode 2 and
+// by damped Jacobi for mode 0.  x0 and t0 hold, afterwards, the level-0
+// iterate before post-smoothing and its residual.  Returns the number of
+// kernels launched.
 template <typename TZ>
-int mg_vcycle(solv_gpu_ctx* c, const float* r, TZ* z, bool net, const float* q, const float* ge,
+int mg_vcycle(solv_gpu_ctx* c, const float* r, TZ* z, int mode, const float* q, const float* ge,
               float* x0, float* t0, const int* na) {
+  const bool net = mode == 1;
   cudaStream_t s = c->stream;
   const int B = c->block;
   const float w = (float)c->mg_omega, a = (float)c->mg_alpha;
   const int N = c->N;
   Rows<float> R0 = rows<float>(c);
-  const float* d0 = c->mg_dinv0.as<float>();
+  const float* d0 = mode == 2 ? c->mg_dq.as<float>() : c->mg_dinv0.as<float>();
   MgLevel& L1 = *c->mg[0];
   int k = 0;
   if (net) {
@@ -911,7 +918,7 @@ void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
   int nk = 1;
   if constexpr (std::is_same<T, float>::value) {
     if (mg_on(c))  // z = V-cycle(r)
-      nk = mg_vcycle<T>(c, w.r, w.z, c->mg_smoother == 1, c->g_q.as<float>(),
+      nk = mg_vcycle<T>(c, w.r, w.z, c->mg_smoother, c->g_q.as<float>(),
                         c->g_ge.as<float>(), c->mg_x0.as<float>(), c->mg_t0.as<float>(),
                         sm.n_active);
   }
@@ -1360,12 +1367,16 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
   const int G = c->seg.total_blk, B = c->block;
   if (solver == 2) {  // the learned preconditioner of this solve, from r0
     if (c->mg_max_levels > 0 && (rc = mg_setup(c))) return rc;  // may build no levels
-    if (!mg_on(c) || c->mg_smoother == 1) {
+    if (!mg_on(c) || c->mg_smoother >= 1) {
       if ((rc = gnn_prepare(c))) return rc;
       sg::k_fcg_scale<float><<<G, B, 0, s>>>(sm, f.r, c->g_rsd.as<float>(),
                                             c->part.as<double>(), c->lanes.as<Lane>());
       gnn_build<float>(c, f.r);
       c->launches++;
+      if (mg_on(c) && c->mg_smoother == 2) {  // learned Jacobi weights q^2
+        mg::k_mg_square<<<grid_for(c, N), B, 0, s>>>(N, c->g_q.as<float>(), c->mg_dq.as<float>());
+        c->launches++;
+      }
     }
     if (mg_on(c) && (rc = mg_values(c))) return rc;
   } else if (imat <= 0) {
@@ -1605,7 +1616,8 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
       }
       return SOLV_GPU_OK;
     case SOLV_OPT_MG_SMOOTHER:
-      if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "multigrid smoother is 0 or 1");
+      if (value != 0 && value != 1 && value != 2)
+        return set_err(c, SOLV_GPU_BAD_INPUT, "multigrid smoother is 0, 1 or 2");
       if ((int)value != c->mg_smoother) {
         c->mg_smoother = (int)value;
         drop_graphs(c);
@@ -1816,13 +1828,16 @@ int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_l
       if (!mg_on(c)) return set_err(c, SOLV_GPU_BAD_INPUT, "kernel_time: no hierarchy for this matrix");
       if ((rc = mg_values(c))) return rc;
     }
-    if (which == 2 || (which == 3 && c->mg_smoother == 1)) {
+    if (which == 2 || (which == 3 && c->mg_smoother >= 1)) {
       if ((rc = gnn_prepare(c))) return rc;
       Lane L{};
       L.active = 1;
       L.gs = 1.0;
       CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, &L, sizeof(Lane), cudaMemcpyHostToDevice, s));
       gnn_build<float>(c, f.p);
+      if (which == 3 && c->mg_smoother == 2)
+        mg::k_mg_square<<<grid_for(c, N), c->block, 0, s>>>(N, c->g_q.as<float>(),
+                                                           c->mg_dq.as<float>());
     }
     auto launch = [&]() {
       if (which == 1)
@@ -1831,7 +1846,7 @@ int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_l
         gnn::k_gnn_apply<float><<<grid_for(c, N), c->block, 0, s>>>(
             N, rows<float>(c), c->g_ge.as<float>(), c->g_q.as<float>(), f.p, f.q, nullptr);
       else
-        mg_vcycle<float>(c, f.p, f.q, c->mg_smoother == 1, c->g_q.as<float>(),
+        mg_vcycle<float>(c, f.p, f.q, c->mg_smoother, c->g_q.as<float>(),
                          c->g_ge.as<float>(), c->mg_x0.as<float>(), c->mg_t0.as<float>(), nullptr);
     };
     launch();
@@ -2223,7 +2238,8 @@ static int mg_train_sample(solv_gpu_ctx* c, float** B) {
   const float w = (float)c->mg_omega, a = (float)c->mg_alpha;
   const float* rsd = c->g_rsd.as<float>();
   const float* q = B[TB_Q];
-  const float* ge = B[TB_GE];
+  // smoother 2 trains the diagonal alone: the face weights stay zero
+  const float* ge = c->mg_smoother == 2 ? c->g_zero.as<float>() : B[TB_GE];
   float* T = c->mg_train.as<float>();
   float *b = T, *z = T + N, *az = T + 2 * (size_t)N, *gz = T + 3 * (size_t)N;
   float *uh = T + 4 * (size_t)N, *gh = T + 5 * (size_t)N, *tmp = T + 6 * (size_t)N;
@@ -2238,7 +2254,7 @@ static int mg_train_sample(solv_gpu_ctx* c, float** B) {
                                             B[TB_DS], B[TB_ES]);
   };
   mg::k_mg_normalise<<<G, Bk, 0, s>>>(N, B[TB_RS], c->lanes.as<Lane>(), b);
-  mg_vcycle<float>(c, b, z, true, q, ge, x0, t0, nullptr);  // t0 = b - A x before post-smoothing
+  mg_vcycle<float>(c, b, z, 1, q, ge, x0, t0, nullptr);  // t0 = b - A x before post-smoothing
   CUDA_TRY(c, cudaMemsetAsync(sums, 0, 2 * sizeof(double), s));
   mg::k_mg_loss_sums<<<G, 256, 0, s>>>(N, R0, z, b, az, sums);
   mg::k_mg_loss_grad<<<G, Bk, 0, s>>>(N, az, b, sums, gz, c->g_jsum.as<double>());
@@ -2291,10 +2307,18 @@ int solv_gpu_gnn_grad_dev(solv_gpu_ctx* c, const double* r0_dev, const double* s
   CUDA_TRY(c, cudaMemsetAsync(B[TB_DS], 0, N * sizeof(float), c->stream));
   CUDA_TRY(c, cudaMemsetAsync(B[TB_ES], 0, N * sizeof(float), c->stream));
   if (c->gnn_loss == 2) {  // through the V-cycle: hierarchy and smoother in the original space
+    if (c->mg_smoother == 0)
+      return set_err(c, SOLV_GPU_BAD_INPUT, "gnn grad: the multigrid loss needs the network "
+                                            "as smoother (SOLV_OPT_MG_SMOOTHER 1 or 2)");
     if ((rc = mg_setup(c))) return rc;
     if (c->mg.empty())
       return set_err(c, SOLV_GPU_BAD_INPUT, "gnn grad: the multigrid loss needs a hierarchy "
                                             "(system too small, or coarsening stalled)");
+    if (c->mg_smoother == 2) {
+      CUDA_TRY(c, c->g_zero.ensure(std::max<long long>(c->n_slots, 1) * sizeof(float)));
+      CUDA_TRY(c, cudaMemsetAsync(c->g_zero.p, 0, std::max<long long>(c->n_slots, 1) * sizeof(float),
+                                  c->stream));
+    }
     if ((rc = mg_values(c))) return rc;
     CUDA_TRY(c, c->mg_train.ensure((size_t)8 * N * sizeof(float)));
     k_gnn_mul<<<grid_for(c, N), c->block, 0, c->stream>>>(N, B[TB_S], c->g_rsd.as<float>(),
@@ -2331,6 +2355,8 @@ int solv_gpu_gnn_grad_dev(solv_gpu_ctx* c, const double* r0_dev, const double* s
   (void)o2n;
   const int gw = gnn_grid_warps(c, (long long)N * 32);
   const float gsc = 1.0f / ((float)N * (float)n_samples);
+  if (c->gnn_loss == 2 && c->mg_smoother == 2)  // the face weights are not used
+    CUDA_TRY(c, cudaMemsetAsync(B[TB_ES], 0, N * sizeof(float), c->stream));
   gnn::k_gnn_heads_back<<<gw, 256, 0, c->stream>>>(N, B[TB_H0 + 3], B[TB_PA], B[TB_S], B[TB_DS],
                                                    B[TB_ES], gsc, P, B[TB_DHA], G);
   float* dcur = B[TB_DHA];

@@ -45,6 +45,8 @@ LAYOUT = "H32-NF4-NL3-spd-v2"
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "gnn_pressure.npz")
+# trained for SOLV_OPT_MG_SMOOTHER 2 (the network's per-cell weights alone)
+DIAG_WEIGHTS = os.path.join(HERE, "weights", "gnn_pressure_diag.npz")
 
 
 def init_params(seed: int = 0) -> np.ndarray:
@@ -114,11 +116,14 @@ def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=400):
 
 
 def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
-          init=None, log_every=50, device=0, loss=2):
+          init=None, log_every=50, device=0, loss=2, smoother=1):
+    """smoother (loss 2): 1 trains the network's operator K as the V-cycle's
+    smoother, 2 its per-cell diagonal alone (learned Jacobi weights)."""
     import torch
-    from .solver import OPT_GNN_LOSS
+    from .solver import OPT_GNN_LOSS, OPT_MG_SMOOTHER
     s = GpuSolver(device)
     s.set_option(OPT_GNN_LOSS, loss)
+    s.set_option(OPT_MG_SMOOTHER, smoother)
     p = init_params(seed) if init is None else np.asarray(init, np.float32)
     s.gnn_set_params(p)
     rng = np.random.default_rng(seed + 7)
@@ -160,13 +165,15 @@ def main(argv=None):
     ap.add_argument("--resume", default=None)
     ap.add_argument("--loss", type=int, default=2,
                     help="0 energy, 1 scale-free (network alone), 2 scale-free through the V-cycle")
+    ap.add_argument("--smoother", type=int, default=1,
+                    help="loss 2: 1 the operator K, 2 its diagonal (learned Jacobi weights)")
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     a = ap.parse_args(argv)
     init = load_params(a.resume) if a.resume else None
     t = time.time()
     p, hist = train(a.size, a.meshes, a.per_mesh, a.samples, a.epochs, a.lr, a.seed, init,
-                    loss=a.loss)
-    meta = {"size": a.size, "loss": a.loss, "systems": a.meshes * a.per_mesh * a.epochs,
+                    loss=a.loss, smoother=a.smoother)
+    meta = {"size": a.size, "loss": a.loss, "smoother": a.smoother, "systems": a.meshes * a.per_mesh * a.epochs,
             "samples": a.samples,
             "lr": a.lr, "seed": a.seed, "first_loss": float(np.mean(hist[:20])),
             "last_loss": float(np.mean(hist[-20:])), "train_s": round(time.time() - t, 1)}

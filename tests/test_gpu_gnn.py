@@ -126,7 +126,8 @@ def one_level(gpu):
     gpu.set_option(OPT_MG_LEVELS, 12)
 
 
-def test_multigrid_gradient_kernels_match_reference(gpu):
+@pytest.mark.parametrize("smoother", [1, 2])
+def test_multigrid_gradient_kernels_match_reference(gpu, smoother):
     """Training through the V-cycle (loss 2): the GPU's forward V-cycle,
     loss and adjoint give the gradient torch autograd gives on the CPU
     reference V-cycle over the same aggregation."""
@@ -141,15 +142,23 @@ def test_multigrid_gradient_kernels_match_reference(gpu):
     samples = [r0, uniform(9, A.n_cell)]
     sd = torch.from_numpy(np.stack(samples)).cuda()
     gpu.set_option(9, 2)  # SOLV_OPT_GNN_LOSS: through the V-cycle
+    gpu.set_option(OPT_MG_SMOOTHER, smoother)
     try:
         loss_g = gpu.gnn_grad_dev(_dev(r0).data_ptr(), sd.data_ptr(), len(samples))
     finally:
         gpu.set_option(9, 1)
+        gpu.set_option(OPT_MG_SMOOTHER, 1)
     g_g = gpu.gnn_get_grad()
-    loss_c, g_c = gnn_ref.loss_mg_and_grad(A, r0, samples, p, [agg], 0.8, 2.0)
+    loss_c, g_c = gnn_ref.loss_mg_and_grad(A, r0, samples, p, [agg], 0.8, 2.0,
+                                           diag=smoother == 2)
     assert abs(loss_g - loss_c) <= 1e-3 * abs(loss_c)
-    for name, a, b in [("w_in", 0, learn.P_LAYER), ("layers", learn.P_LAYER, learn.P_WA),
-                       ("w_a", learn.P_WA, learn.P_BA), ("w_e", learn.P_WE, learn.P_BE)]:
+    blocks = [("w_in", 0, learn.P_LAYER), ("layers", learn.P_LAYER, learn.P_WA),
+              ("w_a", learn.P_WA, learn.P_BA)]
+    if smoother == 1:
+        blocks.append(("w_e", learn.P_WE, learn.P_BE))
+    else:  # the face weights take no part: no gradient reaches their head
+        assert np.all(g_g[learn.P_WE:learn.N_PARAM] == 0)
+    for name, a, b in blocks:
         assert _rel(g_g[a:b], g_c[a:b]) < 3e-2, name
 
 
@@ -259,6 +268,27 @@ def test_multigrid_untrained_network_equals_jacobi_smoothing(gpu):
     assert _rel(phi, x_ref) <= AGREE_1E10
     assert abs(st_net["iters"][0] - st_jac["iters"][0]) <= 0.2 * st_jac["iters"][0] + 2
     assert st_jac["iters"][0] < 0.5 * it_ref
+
+
+def test_multigrid_untrained_diagonal_equals_jacobi_smoothing(gpu):
+    """Smoother 2 with the untrained network uses q^2 = 1/d, the Jacobi
+    weights: the same V-cycle as smoother 0 up to FP32 rounding."""
+    A = _system(20, seed=6)
+    gpu.matrix_set(A)
+    gpu.gnn_set_params(learn.init_params(0))
+    b = _rhs(A, 10)
+    out = {}
+    try:
+        for sm in (0, 2):
+            gpu.set_option(OPT_MG_SMOOTHER, sm)
+            phi, st, rn = _solve_fcg(gpu, A, b)
+            assert st["status"] == OK and st["mg_levels"] >= 1
+            out[sm] = st["iters"][0]
+    finally:
+        gpu.set_option(OPT_MG_SMOOTHER, 1)
+    x_ref, _ = _ref_iters(A, b)
+    assert _rel(phi, x_ref) <= AGREE_1E10
+    assert abs(out[2] - out[0]) <= 0.1 * out[0] + 2, out
 
 
 def test_multigrid_iterations_do_not_grow_like_pcg(gpu):
