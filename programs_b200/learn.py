@@ -45,8 +45,6 @@ LAYOUT = "H32-NF4-NL3-spd-v2"
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, "weights", "gnn_pressure.npz")
-# trained for SOLV_OPT_MG_SMOOTHER 2 (the network's per-cell weights alone)
-DIAG_WEIGHTS = os.path.join(HERE, "weights", "gnn_pressure_diag.npz")
 
 
 def init_params(seed: int = 0) -> np.ndarray:
