@@ -219,17 +219,27 @@ def main(argv=None):
     ap.add_argument("--log-every", type=int, default=20)
     ap.add_argument("--device-assembly", action="store_true",
                     help="assembly, gradients and corrections on the GPU too")
+    ap.add_argument("--p-reduc", type=float, default=1e-10,
+                    help="pressure solve tolerance (the reference's loop uses 0.1)")
+    ap.add_argument("--p-iter", type=int, default=20000, help="(the reference: 20)")
+    ap.add_argument("--p-imat", type=int, default=1, help="plain pressure PCG: 0 Jacobi, 1 DIC")
+    ap.add_argument("--m-reduc", type=float, default=0.1)
+    ap.add_argument("--m-iter", type=int, default=5)
     a = ap.parse_args(argv)
     loop = run_device if a.device_assembly else run
-    u0, p0, h0, t0 = loop(a.size, a.outer, a.re, log_every=a.log_every)
-    out = {"size": a.size, "outer": a.outer, "plain": t0, "final_mass_plain": h0[-1]["mass"],
+    kw = dict(p_reduc=a.p_reduc, p_iter=a.p_iter, p_imat=a.p_imat, m_reduc=a.m_reduc,
+              m_iter=a.m_iter, log_every=a.log_every)
+    u0, p0, h0, t0 = loop(a.size, a.outer, a.re, **kw)
+    out = {"size": a.size, "outer": a.outer, "re": a.re, "p_reduc": a.p_reduc,
+           "p_imat": a.p_imat, "plain": t0, "final_mass_plain": h0[-1]["mass"],
            "p_iters_plain": int(np.sum([h["p_iters"] for h in h0]))}
     if a.learned:
         from .learn import DEFAULT_WEIGHTS, load_params
         w = load_params(a.weights or DEFAULT_WEIGHTS)
-        u1, p1, h1, t1 = loop(a.size, a.outer, a.re, learned=w, log_every=a.log_every)
+        u1, p1, h1, t1 = loop(a.size, a.outer, a.re, learned=w, **kw)
         out.update(learned=t1, p_iters_learned=int(np.sum([h["p_iters"] for h in h1])),
                    fallbacks=int(np.sum([h["fallbacks"] for h in h1])),
+                   final_mass_learned=h1[-1]["mass"],
                    rel_l2_u=rel_l2(u1[:, 0], u0[:, 0]), rel_l2_v=rel_l2(u1[:, 1], u0[:, 1]),
                    rel_l2_w=rel_l2(u1[:, 2], u0[:, 2]), rel_l2_p=rel_l2(p1, p0))
     print(json.dumps(out))
