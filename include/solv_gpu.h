@@ -203,6 +203,13 @@ int solv_gpu_fcg(solv_gpu_ctx *ctx, double reduc, int n_iter, double *phi,
 int solv_gpu_fcg_dev(solv_gpu_ctx *ctx, double reduc, int n_iter,
                      double *phi_dev, double *res0_dev, double *res0_n,
                      int not_r0, solv_gpu_stats *stats);
+/* The hierarchy's aggregation rule on a caller graph (host only, no GPU):
+ * `passes` passes of pairwise matching along the strongest coupling, then
+ * cells left alone join their strongest neighbour's aggregate.  Graph in
+ * CSR (ptr n+1, adj, positive strengths w); agg[i] = aggregate of cell i,
+ * *n_agg = their number.  No counterpart in the reference. */
+int solv_gpu_mg_aggregate(int n, const long long *ptr, const int *adj, const float *w,
+                          int passes, int *agg, int *n_agg);
 /* Aggregation of the hierarchy: for each cell of level - 1 (caller order
  * for level 1, i.e. the caller's cells), the index of its aggregate on
  * `level` (1..levels); n = that finer level's size, *n_coarse = the size of

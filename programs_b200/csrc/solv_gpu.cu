@@ -2052,6 +2052,27 @@ int solv_gpu_fcg_dev(solv_gpu_ctx* c, double reduc, int n_iter, double* phi, dou
   return solve_common(c, 2, 0, reduc, n_iter, 1, phi, res0, res0_n, not_r0, st);
 }
 
+int solv_gpu_mg_aggregate(int n, const long long* ptr, const int* adj, const float* w,
+                          int passes, int* agg, int* n_agg) {
+  if (n <= 0 || !ptr || !adj || !w || !agg || !n_agg || passes < 1 || passes > 8)
+    return SOLV_GPU_BAD_INPUT;
+  mg::Graph g;
+  g.n = n;
+  g.ptr.assign(ptr, ptr + n + 1);
+  if (g.ptr[0] != 0) return SOLV_GPU_BAD_INPUT;
+  for (int i = 0; i < n; ++i)
+    if (g.ptr[i + 1] < g.ptr[i]) return SOLV_GPU_BAD_INPUT;
+  const long long m = g.ptr[n];
+  g.adj.assign(adj, adj + m);
+  g.w.assign(w, w + m);
+  for (long long k = 0; k < m; ++k)
+    if (g.adj[k] < 0 || g.adj[k] >= n) return SOLV_GPU_BAD_INPUT;
+  std::vector<int> a;
+  *n_agg = mg::aggregate(g, passes, a);
+  std::copy(a.begin(), a.end(), agg);
+  return SOLV_GPU_OK;
+}
+
 int solv_gpu_mg_aggregates(solv_gpu_ctx* c, int level, int* agg, int n, int* n_coarse) {
   if (!c || !agg || !n_coarse) return set_err(c, SOLV_GPU_BAD_INPUT, "mg aggregates: null pointer");
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");

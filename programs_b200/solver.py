@@ -71,7 +71,7 @@ EXPORTS = [
     "solv_gpu_fcg", "solv_gpu_fcg_dev", "solv_gpu_gnn_n_params", "solv_gpu_gnn_set_params",
     "solv_gpu_gnn_get_params", "solv_gpu_gnn_forward_dev", "solv_gpu_gnn_grad_dev",
     "solv_gpu_gnn_get_grad", "solv_gpu_gnn_zero_grad", "solv_gpu_gnn_adam",
-    "solv_gpu_kernel_time", "solv_gpu_mg_aggregates",
+    "solv_gpu_kernel_time", "solv_gpu_mg_aggregates", "solv_gpu_mg_aggregate",
     "solv_gpu_create_", "solv_gpu_destroy_", "solv_gpu_matrix_set_", "solv_gpu_matrix_values_",
     "solv_gpu_res_", "solv_gpu_precond_", "solv_gpu_direct_", "solv_gpu_cg_", "solv_gpu_bicg_",
 ]
@@ -127,6 +127,8 @@ def lib():
     L.solv_gpu_kernel_time.argtypes = [vp, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_float)]
     L.solv_gpu_mg_aggregates.argtypes = [vp, ctypes.c_int, _i32p, ctypes.c_int, _i32p]
+    L.solv_gpu_mg_aggregate.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_longlong), _i32p,
+                                        ctypes.POINTER(ctypes.c_float), ctypes.c_int, _i32p, _i32p]
     for fn in (L.solv_gpu_cg_batch, L.solv_gpu_bicg_batch):
         fn.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, _f64p,
                        _f64p, _f64p, ctypes.c_int, _i32p, _f64p, ctypes.POINTER(Stats)]
@@ -431,6 +433,23 @@ class GpuSolver:
         ms = ctypes.c_float()
         self._check(self._lib.solv_gpu_spmv_dev(self._h, x_ptr, y_ptr, repeat, ctypes.byref(ms)))
         return ms.value
+
+
+def mg_aggregate(ptr, adj, w, passes: int = 3):
+    """The hierarchy's aggregation rule on a CSR graph (host only)."""
+    L = lib()
+    n = len(ptr) - 1
+    ptr = np.ascontiguousarray(ptr, np.int64)
+    adj = np.ascontiguousarray(adj, np.int32)
+    w = np.ascontiguousarray(w, np.float32)
+    agg = np.zeros(n, np.int32)
+    na = ctypes.c_int()
+    rc = L.solv_gpu_mg_aggregate(n, ptr.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                                 _p(adj, _i32p), w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                 passes, _p(agg, _i32p), ctypes.byref(na))
+    if rc:
+        raise SolverError(rc, "mg_aggregate: bad graph")
+    return agg, na.value
 
 
 def new_res0(n_cell: int, n_vc: int) -> np.ndarray:
