@@ -94,6 +94,40 @@ def simple_systems(size: int, n_mesh: int, per_mesh: int, seed: int = 0):
             yield m, P, b
 
 
+def device_systems(size: int, n_mesh: int, per_mesh: int, seed: int = 0, device: int = 0,
+                   stream=None):
+    """The systems of simple_systems (same draws, same values bit for bit),
+    assembled on the GPU (programs_b200.fv): yields (mesh, structure-only
+    FaceMatrix of the first system of each mesh or None, (p, n, pl) device
+    tensors, rhs)."""
+    import torch
+
+    from .fv import GpuFv
+    from .mesh import FaceMatrix
+    rng = np.random.default_rng(seed)
+    dev = torch.device("cuda", device)
+    for k in range(n_mesh):
+        jit = float(rng.uniform(0.0, 0.25))
+        m = Mesh.hex(size, jitter=jit, seed=seed * 1000 + k, permute=True)
+        m.renumber(Mesh.RCM)
+        m.cache_geometry()
+        fv = GpuFv(m, device)
+        if stream is not None:
+            fv._lib.fv_gpu_set_stream(fv._h, stream.cuda_stream)
+        ip, inb = m.faces()
+        shell = FaceMatrix(m.n_cell, ip, inb, np.zeros(ip.shape[0]), np.zeros(ip.shape[0]),
+                           np.ones(m.n_cell))
+        for j in range(per_mesh):
+            lid = float(np.exp(rng.uniform(np.log(0.1), np.log(2.0))))
+            dev_scale = float(rng.uniform(0.2, 1.0))
+            u = torch.from_numpy(cavity_field(m, lid * dev_scale)).to(dev)
+            _, _, pl_m, _, _ = fv.momentum_field(u, None, rho=1.0, mu=1e-3, u_lid=lid, urf=0.7)
+            pcn = fv.pressure_correction(pl_m, rho=1.0, pin=1)
+            b = poisson_rhs(m.n_cell, seed * 100000 + k * 1000 + j)
+            yield m, (shell if j == 0 else None), pcn, b
+        fv.close()
+
+
 def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=400):
     """[b, r_k1, r_k2, ...]: residuals b - A x_k of Jacobi-PCG after k
     iterations (the residuals the solver visits), as one (n, N) tensor."""
@@ -126,26 +160,30 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
     s.gnn_set_params(p)
     rng = np.random.default_rng(seed + 7)
     dev = torch.device("cuda", device)
+    # one stream for the library and for torch's element-wise work
+    stream = torch.cuda.Stream(device=dev)
+    s.set_stream(stream.cuda_stream)
     hist = []
     t0 = time.time()
     step = 0
-    for ep in range(epochs):
-        last_mesh = None
-        for m, P, b in simple_systems(size, n_mesh, per_mesh, seed=seed + ep):
-            if m is not last_mesh:
-                s.matrix_set(P)
-                last_mesh = m
-            else:
-                s.matrix_values(P.p, P.n, P.pl)
-            b_dev = torch.from_numpy(b).to(dev)
-            rs = _residual_samples(s, b_dev, samples, rng, torch)
-            val = s.gnn_grad_dev(b_dev.data_ptr(), rs.data_ptr(), rs.shape[0])
-            s.gnn_adam(lr, 1.0)
-            step += 1
-            hist.append(val)
-            if log_every and step % log_every == 0:
-                print(json.dumps({"step": step, "loss": float(np.mean(hist[-log_every:])),
-                                  "t": round(time.time() - t0, 1)}), flush=True)
+    with torch.cuda.stream(stream):
+        for ep in range(epochs):
+            for m, shell, (p_d, n_d, pl_d), b in device_systems(size, n_mesh, per_mesh,
+                                                                seed=seed + ep, device=device,
+                                                                stream=stream):
+                if shell is not None:
+                    s.matrix_set(shell)  # structure of a new mesh
+                s.matrix_values_dev(p_d.data_ptr(), n_d.data_ptr(), pl_d.data_ptr())
+                b_dev = torch.from_numpy(b).to(dev)
+                rs = _residual_samples(s, b_dev, samples, rng, torch)
+                val = s.gnn_grad_dev(b_dev.data_ptr(), rs.data_ptr(), rs.shape[0])
+                s.gnn_adam(lr, 1.0)
+                step += 1
+                hist.append(val)
+                if log_every and step % log_every == 0:
+                    print(json.dumps({"step": step, "loss": float(np.mean(hist[-log_every:])),
+                                      "t": round(time.time() - t0, 1)}), flush=True)
+    stream.synchronize()
     p = s.gnn_get_params()
     s.close()
     return p, hist
