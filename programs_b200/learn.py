@@ -1,13 +1,15 @@
 """Training and use of the learned preconditioner (the network in
 programs_b200/csrc/gnn.cuh, applied by solv_gpu_fcg).
 
-Training data are pressure-correction systems as the SIMPLE loop assembles
-them (spray-simulation/cfd_setup.f90:604-646: d = rho (V/a_P)_f area/l_pn,
-a_P the momentum diagonal of the current velocity field) on jittered hex
-meshes of a lid-driven cavity: jitter uniform in [0, 0.25], lid velocity in
-[0.1, 2].  Each mesh contributes several systems (different flow states);
-each system several residuals, taken from the Jacobi-PCG iterates the
-plain solver visits.  The losses need no reference solutions: with z the
+Training data are the pressure-correction systems the SIMPLE loop itself
+generates (spray-simulation/cfd_setup.f90:604-646: d = rho (V/a_P)_f
+area/l_pn, a_P the momentum diagonal of the current velocity field) on
+jittered hex meshes of a lid-driven cavity, jitter uniform in [0, 0.25],
+lid velocity in [0.1, 2]: the device-resident loop runs with the
+reference's own solver settings and every outer iteration contributes its
+matrix and mass-imbalance right-hand side (every other one a uniform random
+right-hand side instead, so that both kinds are seen); each system several
+residuals, taken from the Jacobi-PCG iterates the plain solver visits.  The losses need no reference solutions: with z the
 preconditioned residual, the energy J = 1/2 z'Az - z'r (loss 0, minimised
 by z = A^-1 r) or the scale-free -(z'r)^2/(z'Az) (the energy after the
 best step along z, which is what one CG step takes, free in the overall
@@ -15,10 +17,11 @@ scale of z as flexible CG is), for z = K r with the network's operator K
 alone (losses 0 and 1) or, as -log((z'r)^2/(z'Az)) so that every sample
 counts alike, for z = V(r), the V-cycle of the aggregation hierarchy with
 K as its finest-level smoother (loss 2, the default: the preconditioner
-solv_gpu_fcg applies), differentiated through the V-cycle.  Forward, backward and the Adam step run on the GPU in the
-library's own kernels; this module only orchestrates.
+solv_gpu_fcg applies), differentiated through the V-cycle.  Forward,
+backward and the Adam step run on the GPU in the library's own kernels;
+this module only orchestrates.
 
-  python -m programs_b200.learn --size 64 --systems 2000 --out weights.npz
+  python -m programs_b200.learn --size 64 --meshes 40 --per-mesh 50 --out weights.npz
 """
 from __future__ import annotations
 
@@ -128,6 +131,68 @@ def device_systems(size: int, n_mesh: int, per_mesh: int, seed: int = 0, device:
         fv.close()
 
 
+def loop_systems(size: int, n_mesh: int, per_mesh: int, seed: int = 0, device: int = 0,
+                 stream=None):
+    """Pressure-correction systems as the SIMPLE loop generates them: per
+    mesh (jitter uniform in [0, 0.25]) and lid velocity (log-uniform in
+    [0.1, 2], mu = 1e-3), per_mesh outer iterations of the device-resident
+    loop with the reference's own solver settings (momentum BiCGSTAB + DILU
+    to 0.1 in at most 5 iterations, pressure DIC-PCG to 0.1 in at most 20,
+    cfd_setup.f90:61,528,580,662).  Yields, at every outer iteration,
+    (structure-only FaceMatrix of a new mesh or None, (p, n, pl) device
+    tensors of the pressure-correction matrix, its right-hand side -- the
+    mass imbalance -- as a device tensor)."""
+    import torch
+
+    from .fv import GpuFv
+    from .mesh import FaceMatrix
+    rng = np.random.default_rng(seed)
+    dev = torch.device("cuda", device)
+    rho, mu = 1.0, 1e-3
+    for k in range(n_mesh):
+        jit = float(rng.uniform(0.0, 0.25))
+        lid = float(np.exp(rng.uniform(np.log(0.1), np.log(2.0))))
+        m = Mesh.hex(size, jitter=jit, seed=seed * 1000 + k, permute=True)
+        m.renumber(Mesh.RCM)
+        m.cache_geometry()
+        N = m.n_cell
+        fv = GpuFv(m, device)
+        sm, sp = GpuSolver(device), GpuSolver(device)
+        if stream is not None:
+            fv._lib.fv_gpu_set_stream(fv._h, stream.cuda_stream)
+            sm.set_stream(stream.cuda_stream)
+            sp.set_stream(stream.cuda_stream)
+        ip, inb = m.faces()
+        shell = FaceMatrix(N, ip, inb, np.zeros(ip.shape[0]), np.zeros(ip.shape[0]), np.ones(N))
+        sm.matrix_set(shell)
+        sp.matrix_set(shell)
+        _, vol_h = m.cell_geom()
+        vol = torch.from_numpy(vol_h).to(dev)
+        u = torch.zeros(N, 3, dtype=torch.float64, device=dev)
+        p = torch.zeros(N, dtype=torch.float64, device=dev)
+        F = None
+        for j in range(per_mesh):
+            gradp = fv.gradient(p)
+            Mp, Mn, Mpl, rhs, Fm = fv.momentum_field(u, flux=F, rho=rho, mu=mu, u_lid=lid, urf=0.7)
+            if F is None:
+                F = Fm
+            rhs -= gradp * vol[:, None]
+            sm.matrix_values_dev(Mp.data_ptr(), Mn.data_ptr(), Mpl.data_ptr())
+            res0 = rhs.t().contiguous()
+            sm.solv_bicg_dev(2, 0.1, 5, 3, u.data_ptr(), res0.data_ptr())
+            F = fv.face_flux(u, p, gradp, Mpl, rho)
+            Pp, Pn, Ppl = fv.pressure_correction(Mpl, rho=rho, pin=1)
+            b, _ = fv.mass_imbalance(F, pin=1)
+            yield (shell if j == 0 else None), (Pp, Pn, Ppl), b.clone()
+            sp.matrix_values_dev(Pp.data_ptr(), Pn.data_ptr(), Ppl.data_ptr())
+            pp = torch.zeros(N, dtype=torch.float64, device=dev)
+            sp.solv_cg_dev(1, 0.1, 20, 1, pp.data_ptr(), b.data_ptr(), not_r0=True)
+            fv.simple_correct(pp, fv.gradient(pp), Mpl, rho, 0.3, u, p, F)
+        sm.close()
+        sp.close()
+        fv.close()
+
+
 def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=400):
     """[b, r_k1, r_k2, ...]: residuals b - A x_k of Jacobi-PCG after k
     iterations (the residuals the solver visits), as one (n, N) tensor."""
@@ -148,9 +213,14 @@ def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=400):
 
 
 def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
-          init=None, log_every=50, device=0, loss=2, smoother=1):
+          init=None, log_every=50, device=0, loss=2, smoother=1, data="loop"):
     """smoother (loss 2): 1 trains the network's operator K as the V-cycle's
-    smoother, 2 its per-cell diagonal alone (learned Jacobi weights)."""
+    smoother, 2 its per-cell diagonal alone (learned Jacobi weights).
+    data: "loop" -- the systems the SIMPLE loop generates (loop_systems),
+    every other one with a uniform random right-hand side in place of the
+    mass imbalance, so that both kinds of right-hand side are seen;
+    "synthetic" -- cavity-like flow states with random right-hand sides
+    (device_systems)."""
     import torch
     from .solver import OPT_GNN_LOSS, OPT_MG_SMOOTHER
     s = GpuSolver(device)
@@ -168,13 +238,19 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
     step = 0
     with torch.cuda.stream(stream):
         for ep in range(epochs):
-            for m, shell, (p_d, n_d, pl_d), b in device_systems(size, n_mesh, per_mesh,
-                                                                seed=seed + ep, device=device,
-                                                                stream=stream):
+            if data == "loop":
+                gen = loop_systems(size, n_mesh, per_mesh, seed=seed + ep, device=device,
+                                   stream=stream)
+            else:
+                gen = ((shell, pcn, torch.from_numpy(b).to(dev)) for _, shell, pcn, b in
+                       device_systems(size, n_mesh, per_mesh, seed=seed + ep, device=device,
+                                      stream=stream))
+            for shell, (p_d, n_d, pl_d), b_dev in gen:
                 if shell is not None:
                     s.matrix_set(shell)  # structure of a new mesh
                 s.matrix_values_dev(p_d.data_ptr(), n_d.data_ptr(), pl_d.data_ptr())
-                b_dev = torch.from_numpy(b).to(dev)
+                if data == "loop" and step % 2 == 1:  # the other kind of right-hand side
+                    b_dev = torch.from_numpy(poisson_rhs(b_dev.shape[0], seed * 7919 + step)).to(dev)
                 rs = _residual_samples(s, b_dev, samples, rng, torch)
                 val = s.gnn_grad_dev(b_dev.data_ptr(), rs.data_ptr(), rs.shape[0])
                 s.gnn_adam(lr, 1.0)
@@ -203,13 +279,14 @@ def main(argv=None):
                     help="0 energy, 1 scale-free (network alone), 2 scale-free through the V-cycle")
     ap.add_argument("--smoother", type=int, default=1,
                     help="loss 2: 1 the operator K, 2 its diagonal (learned Jacobi weights)")
+    ap.add_argument("--data", default="loop", choices=["loop", "synthetic"])
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     a = ap.parse_args(argv)
     init = load_params(a.resume) if a.resume else None
     t = time.time()
     p, hist = train(a.size, a.meshes, a.per_mesh, a.samples, a.epochs, a.lr, a.seed, init,
-                    loss=a.loss, smoother=a.smoother)
-    meta = {"size": a.size, "loss": a.loss, "smoother": a.smoother, "systems": a.meshes * a.per_mesh * a.epochs,
+                    loss=a.loss, smoother=a.smoother, data=a.data)
+    meta = {"size": a.size, "loss": a.loss, "smoother": a.smoother, "data": a.data, "systems": a.meshes * a.per_mesh * a.epochs,
             "samples": a.samples,
             "lr": a.lr, "seed": a.seed, "first_loss": float(np.mean(hist[:20])),
             "last_loss": float(np.mean(hist[-20:])), "train_s": round(time.time() - t, 1)}
