@@ -1461,9 +1461,18 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
     CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
     if (na == 0) break;
-    // Nothing to recompute: the flexible formulas take beta from the last
-    // step's q (the replaced residual differs from the recursive one far
-    // below beta's own accuracy) and alpha from p.r of the next step.
+    // The next direction p = z + beta p takes z from the replaced residual,
+    // so beta = -(z.q)/(p.q) must too.  The fused Jacobi CG computed it in
+    // k_cg_update from the recursive residual: recompute it from the new
+    // one (near an ill-conditioned system's floor the two differ enough to
+    // stall the iteration).  FCG and the sweep-preconditioned CG take beta
+    // from the current z already; alpha always comes from p.r of the next
+    // step.
+    if (cur == 0 && imat <= 0) {
+      sg::k_cg_rz<float, V, true, true><<<G, B, 0, s>>>(sm, f.c, f.r, f.z, c->part.as<double>(),
+                                                        c->lanes.as<Lane>(), f.q);
+      c->launches++;
+    }
     CUDA_TRY(c, cudaGetLastError());
   }
   if (not_r0) {
