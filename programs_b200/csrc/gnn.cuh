@@ -657,7 +657,10 @@ __global__ void k_adam(int np, float* __restrict__ P, const float* __restrict__ 
                        float b2, float eps, float bc1, float bc2, float gscale) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= np) return;
-  const float g = G[t] * gscale;
+  // a non-finite gradient entry (a degenerate sample) is skipped: once in
+  // the moments it would turn the parameter into NaN for good
+  const float graw = G[t] * gscale;
+  const float g = isfinite(graw) ? graw : 0.0f;
   m[t] = b1 * m[t] + (1.0f - b1) * g;
   v[t] = b2 * v[t] + (1.0f - b2) * g * g;
   const float mh = m[t] / bc1, vh = v[t] / bc2;

@@ -631,7 +631,9 @@ __global__ void k_mg_loss_grad(int n, const float* __restrict__ az, const float*
                                const double* __restrict__ sums, float* __restrict__ g,
                                double* __restrict__ jsum) {
   const double zb = sums[0], zaz = sums[1];
-  const bool ok = zaz > 0.0 && zb != 0.0;
+  // a sample whose z is (numerically) orthogonal to b or not finite has no
+  // usable gradient (2/z.b explodes): it is skipped
+  const bool ok = zaz > 0.0 && isfinite(zaz) && isfinite(zb) && zb * zb > 1e-20 * zaz;
   const float ca = ok ? (float)(2.0 / zaz) : 0.0f, cb = ok ? (float)(2.0 / zb) : 0.0f;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     g[i] = ca * az[i] - cb * b[i];
