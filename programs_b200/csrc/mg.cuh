@@ -540,6 +540,41 @@ __global__ void k_mg_net(int n, sg::Rows<float> R, const float* __restrict__ gE,
   }
 }
 
+// ---- device: bounding the network smoother -----------------------------------------
+// v_i = a fixed pseudo-random value in [-1, 1) (power-iteration start)
+__global__ void k_mg_hashfill(int n, float* __restrict__ v) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    unsigned int h = (unsigned int)i * 2654435761u + 0x9e3779b9u;
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    v[i] = (float)(h & 0xFFFFFF) * (2.0f / 16777216.0f) - 1.0f;
+  }
+}
+
+// out += x.x (FP64, one atomic per block)
+__global__ void __launch_bounds__(256) k_mg_norm2(int n, const float* __restrict__ x,
+                                                  double* __restrict__ out) {
+  __shared__ double sh[8];
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    acc += (double)x[i] * x[i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+    atomicAdd(out, t);
+  }
+}
+
+// x *= c
+__global__ void k_mg_scale(int n, float c, float* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] *= c;
+}
+
 // dq = q^2: the network's per-cell scale as a Jacobi weight (smoother 2)
 __global__ void k_mg_square(int n, const float* __restrict__ q, float* __restrict__ dq) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)

@@ -151,6 +151,7 @@ struct solv_gpu_ctx {
   DevBuf mg_dq;                        // smoother 2: the network's per-cell weights q^2
   DevBuf g_zero;                       // smoother 2 training: face weights held at zero
   double mg_setup_s = 0.0;
+  double mg_smooth_scale = 1.0;        // factor the last solve applied to K (see mg_bound_smoother)
 };
 
 namespace {
@@ -745,6 +746,59 @@ int mg_vcycle(solv_gpu_ctx* c, const float* r, TZ* z, int mode, const float* q, 
 
 // The solve uses the hierarchy (built, and not switched off).
 bool mg_on(const solv_gpu_ctx* c) { return c->mg_max_levels > 0 && !c->mg.empty(); }
+
+// A smoother must damp: with lambda_max(w K A) >= 2 some error modes grow
+// under it and the V-cycle stops being a good preconditioner.  The network
+// has no such bound built in -- a right-hand side far from its training
+// data (a localised mass imbalance, say) can drive its per-cell scales up
+// -- so every solve estimates lambda_max(w K A) by power iteration on the
+// device and, above kSmoothMax, scales q = s D^-1/2 (the operator's only
+// per-cell factor, K scaling with q^2) so that the bound holds.  The
+// estimate is inflated by 5% (power iteration approaches lambda_max from
+// below).  Returns the factor applied to K (1 when none was needed).
+constexpr double kSmoothMax = 1.9;
+constexpr int kPowerIters = 8;
+
+int mg_bound_smoother(solv_gpu_ctx* c, double* applied) {
+  *applied = 1.0;
+  cudaStream_t s = c->stream;
+  const int N = c->N;
+  const int G = grid_for(c, N), B = c->block;
+  Rows<float> R0 = rows<float>(c);
+  float* v = c->mg_t0.as<float>();
+  float* y = c->mg_x0.as<float>();
+  double* acc = c->g_jsum.as<double>();
+  CUDA_TRY(c, c->g_jsum.ensure(3 * sizeof(double)));
+  acc = c->g_jsum.as<double>();
+  mg::k_mg_hashfill<<<G, B, 0, s>>>(N, v);
+  double prev = 0.0, lam = 0.0, h = 0.0;
+  for (int it = 0; it <= kPowerIters; ++it) {
+    CUDA_TRY(c, cudaMemsetAsync(acc, 0, sizeof(double), s));
+    mg::k_mg_norm2<<<std::min(G, 1184), 256, 0, s>>>(N, v, acc);
+    CUDA_TRY(c, cudaMemcpyAsync(&h, acc, sizeof(double), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(c, cudaStreamSynchronize(s));
+    const double nrm = std::sqrt(h);
+    if (!(nrm > 0.0) || !std::isfinite(nrm)) break;
+    if (it > 0) lam = nrm / prev;  // |w K A v| / |v| for the previous, unit v
+    if (it == kPowerIters) break;
+    mg::k_mg_scale<<<G, B, 0, s>>>(N, (float)(1.0 / nrm), v);
+    prev = 1.0;
+    sg::k_spmv<float, 1><<<G, B, 0, s>>>(N, R0, v, y);  // y = A v
+    mg::k_mg_net<false, float><<<G, B, 0, s>>>(N, R0, c->g_ge.as<float>(), c->g_q.as<float>(),
+                                                (float)c->mg_omega, y, nullptr, v, nullptr);
+    c->launches += 4;
+  }
+  CUDA_TRY(c, cudaGetLastError());
+  lam *= 1.05;
+  if (std::isfinite(lam) && lam > kSmoothMax) {
+    const double f = kSmoothMax / lam;
+    mg::k_mg_scale<<<G, B, 0, s>>>(N, (float)std::sqrt(f), c->g_q.as<float>());
+    c->launches++;
+    *applied = f;
+  }
+  CUDA_TRY(c, cudaGetLastError());
+  return SOLV_GPU_OK;
+}
 
 // Kernels in one V-cycle (launch statistics of graph replays).
 int mg_kernels(const solv_gpu_ctx* c) {
@@ -1379,6 +1433,11 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
       }
     }
     if (mg_on(c) && (rc = mg_values(c))) return rc;
+    if (mg_on(c) && c->mg_smoother == 1) {
+      double f = 1.0;
+      if ((rc = mg_bound_smoother(c, &f))) return rc;
+      c->mg_smooth_scale = f;
+    }
   } else if (imat <= 0) {
     sg::k_cg_rz<float, V, true><<<G, B, 0, s>>>(sm, f.c, f.r, f.z, c->part.as<double>(),
                                                 c->lanes.as<Lane>());
