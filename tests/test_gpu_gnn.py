@@ -423,7 +423,7 @@ def test_learned_smoother_stays_damping_on_simple_loop_systems(gpu):
     w K A has eigenvalues well above 2 (5.0 on this system); the per-solve
     power-iteration bound scales K back, so the V-cycle with the network
     smoother stays within a small factor of Jacobi smoothing (it needed 13x
-    the iterations unbounded) and the solution agrees with the oracle."""
+    the iterations unbounded) and the solution agrees with a direct solve."""
     A, b = _simple_loop_system()
     gpu.matrix_set(A)
     gpu.gnn_set_params(learn.load_params())
@@ -438,6 +438,7 @@ def test_learned_smoother_stays_damping_on_simple_loop_systems(gpu):
                 phi1 = phi
     finally:
         gpu.set_option(OPT_MG_SMOOTHER, 1)
-    ref = Oracle.from_matrix(A).solv_cg(0, 1e-12, 50000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
+    import scipy.sparse.linalg as spla
+    x = spla.spsolve(A.to_scipy().tocsc(), b)  # the classic-CG oracle stalls near 1e-9 here
     assert its[1] <= 2 * its[0] + 5, its
-    assert _rel(phi1, ref[0]) <= 1e-8
+    assert _rel(phi1[:, 0], x) <= 1e-8
