@@ -755,8 +755,12 @@ bool mg_on(const solv_gpu_ctx* c) { return c->mg_max_levels > 0 && !c->mg.empty(
 // device and, above kSmoothMax, scales q = s D^-1/2 (the operator's only
 // per-cell factor, K scaling with q^2) so that the bound holds.  The
 // estimate is inflated by 5% (power iteration approaches lambda_max from
-// below).  Returns the factor applied to K (1 when none was needed).
+// below).  Before that the per-cell scales are held at or above kScaleMin
+// (a quarter of the Jacobi weight): a network that drives some s_i towards
+// zero leaves those cells unsmoothed, which no bound on lambda_max sees.
+// Returns the factor applied to K (1 when none was needed).
 constexpr double kSmoothMax = 1.9;
+constexpr float kScaleMin = 0.5f;
 constexpr int kPowerIters = 8;
 
 int mg_bound_smoother(solv_gpu_ctx* c, double* applied) {
@@ -767,10 +771,11 @@ int mg_bound_smoother(solv_gpu_ctx* c, double* applied) {
   Rows<float> R0 = rows<float>(c);
   float* v = c->mg_t0.as<float>();
   float* y = c->mg_x0.as<float>();
-  double* acc = c->g_jsum.as<double>();
   CUDA_TRY(c, c->g_jsum.ensure(3 * sizeof(double)));
-  acc = c->g_jsum.as<double>();
+  double* acc = c->g_jsum.as<double>();
+  mg::k_mg_floor<<<G, B, 0, s>>>(N, kScaleMin, c->g_rsd.as<float>(), c->g_q.as<float>());
   mg::k_mg_hashfill<<<G, B, 0, s>>>(N, v);
+  c->launches += 2;
   double prev = 0.0, lam = 0.0, h = 0.0;
   for (int it = 0; it <= kPowerIters; ++it) {
     CUDA_TRY(c, cudaMemsetAsync(acc, 0, sizeof(double), s));
