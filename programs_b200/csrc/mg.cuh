@@ -570,10 +570,14 @@ __global__ void __launch_bounds__(256) k_mg_norm2(int n, const float* __restrict
 }
 
 // q_i = max(q_i, f rsd_i): the network's per-cell scale s = q / rsd held at
-// or above f, so no cell is left (almost) unsmoothed
+// or above f, so no cell is left (almost) unsmoothed.  A NaN stays NaN: a
+// broken network must reach flexible CG's hand-over to plain PCG, not be
+// quietly repaired here.
 __global__ void k_mg_floor(int n, float f, const float* __restrict__ rsd, float* __restrict__ q) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    q[i] = fmaxf(q[i], f * rsd[i]);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float lo = f * rsd[i];
+    if (q[i] < lo) q[i] = lo;
+  }
 }
 
 // x *= c
