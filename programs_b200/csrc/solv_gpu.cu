@@ -1585,6 +1585,7 @@ const char* solv_gpu_status_string(int s) {
     case SOLV_GPU_DEVICE_ERROR: return "CUDA error";
     case SOLV_GPU_NO_MATRIX: return "no matrix set";
     case SOLV_GPU_ZERO_RHS: return "zero initial residual (early return)";
+    case SOLV_GPU_TOO_LARGE: return "problem larger than the fixed scratch";
     default: return "unknown status";
   }
 }

@@ -44,6 +44,12 @@ def test_status_strings_and_no_device_path():
     L = lib()
     assert L.solv_gpu_status_string(0) == b"ok"
     assert L.solv_gpu_status_string(4) == b"bad input"
+    header = open(os.path.join(ROOT, "include", "solv_gpu.h")).read()
+    codes = [int(v) for v in re.findall(r"#define SOLV_GPU_[A-Z_]+ (\d+) +/\*", header)]
+    assert len(codes) >= 8
+    for code in codes:
+        assert L.solv_gpu_status_string(code) != b"unknown status", code
+    assert L.solv_gpu_status_string(99) == b"unknown status"
     if not torch.cuda.is_available():
         with pytest.raises(SolverError):
             GpuSolver(0)
