@@ -77,7 +77,13 @@ def test_res(gpu, case, V, not_r0):
     assert np.allclose(rn, rn_ref, rtol=NORM_TOL, atol=0)
 
 
-@pytest.mark.parametrize("imat", [0, 1, 2])
+# imat outside 0..2 follows the reference's branches: `if(imat>0)` with
+# `imat==1` / `imat==2` inside (solv_precond.f90:13-22, solv_direct.f90:11)
+# make imat <= 0 Jacobi and imat >= 3 the unmodified diagonal with both sweeps.
+IMATS = [-1, 0, 1, 2, 3]
+
+
+@pytest.mark.parametrize("imat", IMATS)
 def test_precond_bit_exact(gpu, case, imat):
     _, A, o = case
     c_ref, cr_ref = o.solv_precond(imat)
@@ -88,7 +94,7 @@ def test_precond_bit_exact(gpu, case, imat):
     assert np.array_equal(c, c_ref)
 
 
-@pytest.mark.parametrize("imat", [0, 1, 2])
+@pytest.mark.parametrize("imat", IMATS)
 def test_direct_bit_exact(gpu, case, imat):
     _, A, o = case
     c, cr = o.solv_precond(imat)

@@ -81,20 +81,25 @@ def test_cavity_fixture_matches_reader():
     assert (inb == 0).sum() == 150
 
 
-@pytest.mark.parametrize("imat", [0, 1, 2])
+@pytest.mark.parametrize("imat", [-1, 0, 1, 2, 3])
 def test_precond_is_the_incomplete_factorisation(imat):
-    """solv_direct applies M^-1 with M = (D+L) D^-1 (D+U), D = c_r."""
+    """solv_direct applies M^-1 with M = (D+L) D^-1 (D+U), D = c_r.  imat
+    outside 0..2 takes the reference's branches as written
+    (solv_precond.f90:13-22): <= 0 is Jacobi, >= 3 keeps D = pl (the
+    symmetric Gauss-Seidel factorisation) and still runs both sweeps."""
     m = Mesh.hex(5, seed=1)
     A, _ = m.momentum()
     o = Oracle.from_matrix(A)
     c, c_r = o.solv_precond(imat)
     S = A.to_scipy().tocsr()
-    if imat == 0:
+    if imat <= 0:
         M = sp.diags(A.pl)
         # Jacobi: x = b / (pl + small)
         b = uniform(2, A.n_cell)
-        assert np.allclose(o.solv_direct(0, c, c_r, b), b / (A.pl + 1e-20), rtol=1e-15)
+        assert np.allclose(o.solv_direct(imat, c, c_r, b), b / (A.pl + 1e-20), rtol=1e-15)
         return
+    if imat >= 3:
+        assert np.array_equal(c_r, A.pl)
     # the sweeps take L from ng%n and U from ng%p whatever imat is
     # (solv_direct.f90:19,33); imat only changes the diagonal D
     L = sp.tril(S, -1).tocsr()
