@@ -64,6 +64,17 @@ def _env_int(k, d):
         return d
 
 
+def max_over_ranks(x, dist=None, device=None):
+    """The largest of every rank's x: a job of replicas takes as long as its
+    slowest rank.  Every rank must call it, in the same order."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -325,11 +336,7 @@ def main():
         torch.cuda.synchronize()
         if clk:
             clk.__exit__()
-        ms = e0.elapsed_time(e1)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
         return ms / steps, st, launches, (clk.summary() if clk else None)
 
     def solution():
@@ -378,6 +385,7 @@ def main():
         dt = time.perf_counter() - t
         if k > 0:
             e2e.append(dt)
+    e2e_s = max_over_ranks(statistics.mean(e2e), dist, dev)
 
     # rooflines: kernels of the solve timed live on the solver's stream
     peak, peak_kind = _peaks()
@@ -420,7 +428,7 @@ def main():
             "learned_one_level": extra.get("one_level"),
             "speedup_vs_plain_fp64": ms_plain / ms_step,
             "first_call_s": first_s,
-            "e2e": {"value": statistics.mean(e2e) / world, "unit": "s/solve",
+            "e2e": {"value": e2e_s / world, "unit": "s/solve",
                     "h2d_bytes_per_step": 2 * N * 8, "d2h_bytes_per_step": 2 * N * 8 + 8},
             "roofline": {"bound": "hbm", "achieved": gbs[dominant], "peak": peak, "unit": "GB/s",
                          "frac": gbs[dominant] / peak, "traffic": traffic,
