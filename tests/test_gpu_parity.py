@@ -269,6 +269,84 @@ def test_bad_input_is_rejected(gpu):
         gpu.matrix_set(bad)
 
 
+def test_sizes_and_pointers_are_rejected_before_any_work(built):
+    """Empty systems, component counts outside 1..4 and null arrays return
+    BAD_INPUT from the host checks (a private context, so the shared one
+    keeps its matrix)."""
+    import ctypes
+    from programs_b200.solver import BAD_INPUT, NO_MATRIX, GpuSolver
+    s = GpuSolver(0)
+    try:
+        L, h = s._lib, s._h
+        f64 = ctypes.POINTER(ctypes.c_double)
+        i32 = ctypes.POINTER(ctypes.c_int)
+        ip = np.array([1], np.int32)
+        inb = np.array([2], np.int32)
+        one = np.ones(5)
+        P = lambda a, t: a.ctypes.data_as(t)
+        assert L.solv_gpu_cg(h, 0, 1e-10, 10, 1, P(one, f64), P(one, f64), P(one, f64), 0,
+                             None) == NO_MATRIX
+        assert L.solv_gpu_matrix_set(h, 0, 1, P(ip, i32), P(inb, i32), P(one, f64), P(one, f64),
+                                     P(one, f64)) == BAD_INPUT
+        assert L.solv_gpu_matrix_set(h, 2, -1, P(ip, i32), P(inb, i32), P(one, f64),
+                                     P(one, f64), P(one, f64)) == BAD_INPUT
+        assert L.solv_gpu_matrix_set(h, 2, 1, P(ip, i32), P(inb, i32), None, P(one, f64),
+                                     P(one, f64)) == BAD_INPUT
+        assert L.solv_gpu_matrix_set(h, 2, 1, P(ip, i32), P(inb, i32), P(one, f64), P(one, f64),
+                                     P(one, f64)) == OK
+        buf = np.zeros(2 * 5)
+        for n_vc in (0, 5):
+            assert L.solv_gpu_cg(h, 0, 1e-10, 10, n_vc, P(buf, f64), P(buf, f64), P(buf, f64),
+                                 0, None) == BAD_INPUT
+        assert L.solv_gpu_bicg(h, 0, 1e-10, 10, 1, None, P(buf, f64), P(buf, f64), 0,
+                               None) == BAD_INPUT
+    finally:
+        s.close()
+
+
+def _diagonal(N, F, seed):
+    """Every face a boundary face (in = 0, which every face loop of the
+    reference skips): the matrix is its diagonal and no row has a slot."""
+    from programs_b200.mesh import FaceMatrix
+    rng = np.random.default_rng(seed)
+    return FaceMatrix(N, rng.integers(1, N + 1, F).astype(np.int32), np.zeros(F, np.int32),
+                      rng.normal(size=F), rng.normal(size=F), rng.uniform(1.0, 3.0, N))
+
+
+@pytest.mark.parametrize("N,F", [(1, 1), (33, 5), (50, 20)])
+def test_matrix_without_interior_faces(gpu, N, F):
+    """One cell, a slice and one cell, and a partial slice: the product is
+    the diagonal, the factorisations leave it unchanged, and every solver
+    and precision finishes in the oracle's iteration (one)."""
+    from programs_b200.solver import OPT_PRECISION
+    A = _diagonal(N, F, N)
+    o = Oracle.from_matrix(A)
+    gpu.matrix_set(A)
+    x = uniform(4, N)
+    assert np.array_equal(gpu.spmv(x), o.spmv(x))
+    b = np.asfortranarray(uniform(3, N).reshape(N, 1))
+    for imat in (0, 1, 2):
+        c, cr = np.empty(N), np.empty(N)
+        gpu.solv_precond(imat, c, cr)
+        c_ref, cr_ref = o.solv_precond(imat)
+        assert np.array_equal(c, c_ref) and np.array_equal(cr, cr_ref)
+        for solver in ("cg", "bicg"):
+            ref = getattr(o, "solv_" + solver)(imat, 1e-10, 100, np.zeros((N, 1)), b)
+            for precision in (0, 1):
+                phi = np.zeros((N, 1))
+                res0 = b.copy(order="F")
+                gpu.set_option(OPT_PRECISION, precision)
+                try:
+                    st = getattr(gpu, "solv_" + solver)(imat, 1e-10, 100, phi, res0, np.zeros(1))
+                finally:
+                    gpu.set_option(OPT_PRECISION, 0)
+                assert st["status"] == OK, (imat, solver, precision)
+                assert _rel(phi, ref[0]) <= SOL_TOL, (imat, solver, precision)
+                assert np.array_equal(res0, ref[1])
+                if precision == 0:
+                    assert st["iters"][0] == int(ref[3][0])
+
+
 @pytest.mark.parametrize("fname,prefix,solvers", [("cavity_3d.npz", "", ("cg",)),
                                                   ("hex6.npz", "p_", ("cg", "bicg")),
                                                   ("hex6.npz", "m_", ("bicg",))])
