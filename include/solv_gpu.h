@@ -26,7 +26,10 @@
  *     on entry the right-hand side b, on exit the initial residual;
  *   - res0_n[ivc] returns the initial L1 norms (not the final ones);
  *   - the stopping rule is |r|_1 / (|r0|_1 + 1e-20) < reduc, per component.
- *   - imat: 0 Jacobi, 1 DIC, 2 DILU (solv_precond.f90:13-24).
+ *   - imat: 0 Jacobi, 1 DIC, 2 DILU (solv_precond.f90:13-24).  The solvers
+ *     reject other values; solv_gpu_precond / solv_gpu_direct take them as
+ *     the reference does (<= 0 Jacobi, >= 3 the unmodified diagonal with
+ *     both triangular sweeps).
  * Every pointer argument is a HOST pointer unless the name ends in _dev.
  * The reference has no error return; these return a status code.
  *
