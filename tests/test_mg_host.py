@@ -57,3 +57,24 @@ def test_one_pass_is_a_matching_and_bad_graphs_are_rejected():
     bad[0] = len(ptr) + 5
     with pytest.raises(SolverError):
         mg_aggregate(ptr, bad, w, 3)
+
+
+def test_isolated_cells_stay_alone_and_components_never_mix():
+    """A cell without neighbours (a row with its diagonal only) is its own
+    aggregate; two disconnected systems share no aggregate."""
+    import scipy.sparse as sp
+    from programs_b200.solver import mg_aggregate
+    A = Mesh.hex(6, jitter=0.2, seed=1).pressure(pin=0).to_scipy()
+    n1 = A.shape[0]
+    S = sp.block_diag([A, A, sp.identity(5)]).tocsr()
+    S.setdiag(0)
+    S.eliminate_zeros()
+    agg, na = mg_aggregate(S.indptr.astype(np.int64), S.indices.astype(np.int32),
+                           np.abs(S.data).astype(np.float32), 3)
+    size = np.bincount(agg, minlength=na)
+    assert np.all(size[agg[-5:]] == 1) and len(set(agg[-5:].tolist())) == 5
+    assert not set(agg[:n1].tolist()) & set(agg[n1:2 * n1].tolist())
+    assert size[np.unique(agg[:2 * n1])].min() >= 2
+    ptr = np.arange(8, dtype=np.int64) * 0
+    agg, na = mg_aggregate(ptr, np.zeros(0, np.int32), np.zeros(0, np.float32), 3)
+    assert na == 7 and np.array_equal(agg, np.arange(7))
