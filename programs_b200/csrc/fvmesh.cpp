@@ -219,22 +219,27 @@ fvm_mesh *fvm_mesh_read_neu(const char *path) {
     } else if (line.find("ELEMENTS/CELLS") != std::string::npos && ok_sizes) {
       m->n_cell = n_vol;
       m->cell_vert.resize((size_t)n_vol * 8);
+      std::vector<char> seen(n_vol, 0);
       for (int e = 0; e < n_vol; ++e) {
         int idx, ty, nv;
         in >> idx >> ty >> nv;
-        if (!in || ty != 4 || nv != 8 || idx < 1 || idx > n_vol) {
-          delete m;  // only brick elements are supported
+        if (!in || ty != 4 || nv != 8 || idx < 1 || idx > n_vol || seen[idx - 1]) {
+          delete m;  // only brick elements, each numbered once
           return nullptr;
         }
+        seen[idx - 1] = 1;
         for (int v = 0; v < 8; ++v) {
           int g;
           in >> g;
+          if (!in || g < 1 || g > n_vrt) { delete m; return nullptr; }
           m->cell_vert[(size_t)(idx - 1) * 8 + v] = g - 1;
         }
       }
     }
   }
   if (m->n_cell == 0 || m->vert.empty()) { delete m; return nullptr; }
+  for (int32_t g : m->cell_vert)
+    if (g < 0 || (size_t)g >= m->vert.size()) { delete m; return nullptr; }
   // hashed face matching: key = sorted vertex quadruple
   m->cell_nbr.assign((size_t)m->n_cell * 6, -1);
   struct Key {

@@ -112,3 +112,77 @@ def test_uniform_is_seeded():
     a = uniform(3, 1000)
     assert np.array_equal(a, uniform(3, 1000))
     assert a.min() >= -1 and a.max() < 1 and abs(a.mean()) < 0.1
+
+
+def _write_neu(path, nx, ny, nz, jitter=0.0, seed=0, cells=None, bad_vertex=False):
+    """A Gambit neutral file of an nx x ny x nz block of bricks (node order
+    x fastest, then y, then z, as Gambit numbers a brick), elements in a
+    shuffled order when `cells` gives one."""
+    rng = np.random.default_rng(seed)
+    node = lambda i, j, k: 1 + i + (nx + 1) * (j + (ny + 1) * k)
+    nn = (nx + 1) * (ny + 1) * (nz + 1)
+    xyz = np.stack(np.meshgrid(np.arange(nx + 1), np.arange(ny + 1), np.arange(nz + 1),
+                               indexing="ij"), -1).transpose(2, 1, 0, 3).reshape(-1, 3) * 1.0
+    xyz += rng.uniform(-jitter, jitter, xyz.shape)
+    bricks = []
+    for k in range(nz):
+        for j in range(ny):
+            for i in range(nx):
+                bricks.append([node(i + a, j + b, k + c) for c in (0, 1) for b in (0, 1)
+                               for a in (0, 1)])
+    order = list(range(len(bricks))) if cells is None else cells
+    if bad_vertex:
+        bricks[0][3] = nn + 7
+    with open(path, "w") as f:
+        f.write("        CONTROL INFO 2.4.6\n** GAMBIT NEUTRAL FILE\ntest block\n")
+        f.write("     NUMNP     NELEM     NGRPS    NBSETS     NDFCD     NDFVL\n")
+        f.write(f"{nn:10d}{len(bricks):10d}         1         0         3         3\n")
+        f.write("ENDOFSECTION\n   NODAL COORDINATES 2.4.6\n")
+        for q, (x, y, z) in enumerate(xyz):
+            f.write(f"{q + 1:10d}{x:20.11e}{y:20.11e}{z:20.11e}\n")
+        f.write("ENDOFSECTION\n      ELEMENTS/CELLS 2.4.6\n")
+        for e in order:
+            v = bricks[e]
+            f.write(f"{e + 1:8d} 4  8 " + " ".join(map(str, v[:7])) + "\n" + f"{v[7]:15d}\n")
+        f.write("ENDOFSECTION\n")
+    return bricks
+
+
+def test_gambit_reader_connectivity_matches_a_brute_force_search(tmp_path):
+    """The reader's hashed face matching against the quadratic search the
+    reference does (grd_conn.f90:77-93: every pair of cells, faces equal as
+    vertex sets), on a shuffled, jittered 4 x 3 x 2 block."""
+    nx, ny, nz = 4, 3, 2
+    p = str(tmp_path / "block.neu")
+    bricks = _write_neu(p, nx, ny, nz, jitter=0.1, seed=3,
+                        cells=list(np.random.default_rng(1).permutation(nx * ny * nz)))
+    m = Mesh.read_neu(p)
+    n_cell, n_face, n_bface, _ = m.sizes()
+    assert n_cell == nx * ny * nz
+    assert n_face - n_bface == (nx - 1) * ny * nz + nx * (ny - 1) * nz + nx * ny * (nz - 1)
+    assert n_bface == 2 * (ny * nz + nx * nz + nx * ny)
+    ip, inb = m.faces()
+    got = {(int(a), int(b)) for a, b in zip(ip, inb) if b > 0}
+    quads = [[0, 1, 5, 4], [1, 3, 7, 5], [3, 2, 6, 7], [2, 0, 4, 6], [1, 0, 2, 3], [4, 5, 7, 6]]
+    faces = [[frozenset(b[q] for q in f) for f in quads] for b in bricks]
+    want = set()
+    for a in range(len(bricks)):
+        for b in range(a + 1, len(bricks)):
+            if set(faces[a]) & set(faces[b]):
+                want.add((a + 1, b + 1))
+    assert got == want
+    assert np.all(inb[inb > 0] > ip[inb > 0]) and np.all(np.diff(ip) >= 0)
+    _, vol = m.cell_geom()
+    assert abs(vol.sum() - nx * ny * nz) < 0.5 and vol.min() > 0
+
+
+def test_gambit_reader_rejects_malformed_files(tmp_path):
+    p = str(tmp_path / "bad.neu")
+    _write_neu(p, 2, 2, 1, bad_vertex=True)
+    with pytest.raises(RuntimeError):
+        Mesh.read_neu(p)
+    _write_neu(p, 2, 2, 1, cells=[0, 1, 1, 3])  # element 2 twice, element 3 missing
+    with pytest.raises(RuntimeError):
+        Mesh.read_neu(p)
+    with pytest.raises(RuntimeError):
+        Mesh.read_neu(str(tmp_path / "missing.neu"))
