@@ -14,7 +14,8 @@ def _built(built):
 
 
 def _declared(header):
-    src = open(os.path.join(ROOT, "include", header)).read()
+    with open(os.path.join(ROOT, "include", header)) as f:
+        src = f.read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b((?:solv_gpu|fv_gpu)_\w+)\s*\(", src)))
 
@@ -44,7 +45,8 @@ def test_status_strings_and_no_device_path():
     L = lib()
     assert L.solv_gpu_status_string(0) == b"ok"
     assert L.solv_gpu_status_string(4) == b"bad input"
-    header = open(os.path.join(ROOT, "include", "solv_gpu.h")).read()
+    with open(os.path.join(ROOT, "include", "solv_gpu.h")) as f:
+        header = f.read()
     codes = [int(v) for v in re.findall(r"#define SOLV_GPU_[A-Z_]+ (\d+) +/\*", header)]
     assert len(codes) >= 8
     for code in codes:
