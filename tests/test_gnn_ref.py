@@ -171,3 +171,19 @@ def test_reference_vcycle_gradient_matches_finite_differences():
             assert abs(fd - g[k]) <= 1e-7 + 1e-4 * abs(g[k]), k
     finally:
         gnn_ref.ROUND = True
+
+
+def test_shipped_weights_load_and_record_their_training(tmp_path):
+    """The committed network: this build's layout, finite, not the untrained
+    Jacobi network, trained on 2,000 pressure systems of 64^3 meshes; a file
+    of another layout is refused rather than misread."""
+    import json
+    p = learn.load_params()
+    assert p.shape == (learn.N_PARAM,) and p.dtype == np.float32 and np.all(np.isfinite(p))
+    assert np.any(p[learn.P_WE:learn.P_WE + 32] != 0)    # face heads trained away from zero
+    meta = json.loads(str(np.load(learn.DEFAULT_WEIGHTS)["meta"]))
+    assert meta["size"] == 64 and meta["systems"] == 2000
+    bad = str(tmp_path / "bad.npz")
+    np.savez(bad, params=p[:-1], n_param=learn.N_PARAM - 1, layout=learn.LAYOUT, meta="{}")
+    with pytest.raises(ValueError):
+        learn.load_params(bad)
