@@ -47,6 +47,27 @@ struct Lane {
 enum : int { kLaneRunning = 0, kLaneConverged = 1, kLaneMaxIter = 2, kLaneNaN = 3,
              kLaneStall = 4 };
 
+// Flexible-CG beta = -(z.q)/(p.q) for the next direction p = z + beta p,
+// restarted (beta = 0) each time the lane has taken a multiple of n
+// iterations on its n-cell system.  CG ends within n steps in exact
+// arithmetic; past them the old direction only cancels the new one (on a
+// one-cell system z + beta p is exactly zero and the iteration stops
+// moving).  Systems with more cells than iterations never restart.
+__device__ __forceinline__ double flex_beta(const Lane& L, double zq, int n) {
+  return (L.pq > 0.0 && L.iter % n != 0) ? -zq / L.pq : 0.0;
+}
+
+// The step scalars of the FP32 inner iterations (mixed precision) divide
+// without the reference's absolute guard `+ small` (precision.f90:8): after
+// a reliable update the residual of a small or weakly driven system, and
+// with it every inner product, can lie far below 1e-20, where the guard
+// would shrink each step towards zero and the iteration would stall.  A
+// zero denominator gives a zero step.  The FP64 kernels keep the
+// reference's expressions unchanged.
+__device__ __forceinline__ double div0(double num, double den) {
+  return den != 0.0 ? num / den : 0.0;
+}
+
 template <typename T>
 struct Rows {
   const int* __restrict__ slice_ptr;    // element offset of each slice
@@ -564,7 +585,7 @@ __global__ void SG_BOUNDS(V) k_cg_rz(SegMap sm, const T* __restrict__ c, const T
       Lane& L = lanes[s * V + v];
       if (!L.active) continue;
       if (FLEX) {
-        L.beta = L.pq > 0.0 ? -tot[v] / L.pq : 0.0;
+        L.beta = flex_beta(L, tot[v], c1 - c0);
         continue;
       }
       double beta = 1.0 / L.s;   // :44
@@ -650,7 +671,8 @@ __global__ void SG_BOUNDS(V) k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict
       Lane& L = lanes[s * V + v];
       if (!L.active) continue;
       L.pq = tot[v];
-      L.alpha = L.s / (tot[v] + kSmall);  // :67-68
+      if constexpr (sizeof(T) == 4) L.alpha = div0(L.s, tot[v]);
+      else L.alpha = L.s / (tot[v] + kSmall);  // :67-68
     }
   }
 }
@@ -706,7 +728,7 @@ __global__ void SG_BOUNDS(V) k_cg_update(SegMap sm, const T* __restrict__ c, T* 
       else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);  // :82
       else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
       if (JAC && FLEX && L.active) {
-        L.beta = L.pq > 0.0 ? -tot[V + v] / L.pq : 0.0;
+        L.beta = flex_beta(L, tot[V + v], c1 - c0);
       } else if (JAC && L.active) {
         double beta = 1.0 / L.s;
         L.s_prev = L.s;
@@ -743,7 +765,8 @@ __global__ void SG_BOUNDS(V) k_bi_rho(SegMap sm, const T* __restrict__ r, const 
       Lane& L = lanes[s * V + v];
       if (!L.active) continue;
       L.rho = tot[v];
-      L.omeg = L.rho * L.gam / (L.alpha * L.beta0 + kSmall);
+      if constexpr (sizeof(T) == 4) L.omeg = div0(L.rho * L.gam, L.alpha * L.beta0);
+      else L.omeg = L.rho * L.gam / (L.alpha * L.beta0 + kSmall);
       L.beta0 = L.rho;
     }
   }
@@ -814,9 +837,11 @@ __global__ void SG_BOUNDS(V) k_bi_spmv(Rows<T> R, SegMap sm, const T* __restrict
       Lane& L = lanes[s * V + v];
       if (!L.active) continue;
       if (MODE == 0) {
-        L.gam = L.rho / (tot[v] + kSmall);
+        if constexpr (sizeof(T) == 4) L.gam = div0(L.rho, tot[v]);
+        else L.gam = L.rho / (tot[v] + kSmall);
       } else {
-        L.alpha = tot[v] / (tot[V + v] + kSmall);
+        if constexpr (sizeof(T) == 4) L.alpha = div0(tot[v], tot[V + v]);
+        else L.alpha = tot[v] / (tot[V + v] + kSmall);
       }
     }
   }
@@ -903,7 +928,8 @@ __global__ void SG_BOUNDS(V) k_bi_update(SegMap sm, T* __restrict__ phi, T* __re
       else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
       if (L.active) {
         L.rho = tot[V + v];
-        L.omeg = L.rho * L.gam / (L.alpha * L.beta0 + kSmall);
+        if constexpr (sizeof(T) == 4) L.omeg = div0(L.rho * L.gam, L.alpha * L.beta0);
+        else L.omeg = L.rho * L.gam / (L.alpha * L.beta0 + kSmall);
         L.beta0 = L.rho;
       }
     }
@@ -987,7 +1013,7 @@ __global__ void SG_BOUNDS(1) k_fcg_beta(SegMap sm, const T* __restrict__ z, cons
   double tot[1];
   if (seg_commit<1>(sm, b, s, part, acc, tot) && threadIdx.x == 0) {
     Lane& L = lanes[s];
-    L.beta = L.pq > 0.0 ? -tot[0] / L.pq : 0.0;
+    L.beta = flex_beta(L, tot[0], c1 - c0);
   }
 }
 

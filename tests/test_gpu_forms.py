@@ -76,6 +76,32 @@ def test_mixed_bicg_momentum_three_components(mixed, imat):
         assert _rel(phi[:, v], ref[0][:, v]) <= SOL_TOL
 
 
+@pytest.mark.parametrize("solver,imat", [("cg", 0), ("cg", 1), ("bicg", 0), ("bicg", 2)])
+def test_mixed_solve_of_a_weakly_driven_system(mixed, solver, imat):
+    """A right-hand side of size 1e-6 (a SIMPLE pressure correction near
+    convergence is driven about this weakly): the inner products of the
+    FP32 iteration fall far below the reference's absolute guard 1e-20 well
+    before the 1e-10 stopping rule, and the solve must still reach it, with
+    the solution 1e-6 times that of the unit right-hand side."""
+    m = Mesh.hex(12, seed=3)
+    m.renumber(Mesh.RCM)
+    A = m.pressure(pin=1) if solver == "cg" else m.momentum()[0]
+    mixed.matrix_set(A)
+    b1 = poisson_rhs(A.n_cell, 5) if solver == "cg" else uniform(5, A.n_cell)
+    S = A.to_scipy()
+    sols = []
+    for scale in (1.0, 1e-6):
+        b = np.asfortranarray((scale * b1).reshape(-1, 1))
+        phi = np.zeros((A.n_cell, 1))
+        res0 = b.copy(order="F")
+        rn = np.zeros(1)
+        st = getattr(mixed, "solv_" + solver)(imat, 1e-10, 5000, phi, res0, rn)
+        assert st["status"] == OK, scale
+        assert np.abs(b[:, 0] - S @ phi[:, 0]).sum() / rn[0] < 1e-10, scale
+        sols.append(phi[:, 0] / scale)
+    assert _rel(sols[1], sols[0]) <= MIX_BATCH_TOL
+
+
 def _batch_meshes(k, seed=0):
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.uniform(np.log(4), np.log(11), k)).astype(int)
