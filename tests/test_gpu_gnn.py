@@ -439,6 +439,6 @@ def test_learned_smoother_stays_damping_on_simple_loop_systems(gpu):
     finally:
         gpu.set_option(OPT_MG_SMOOTHER, 1)
     import scipy.sparse.linalg as spla
-    x = spla.spsolve(A.to_scipy().tocsc(), b)  # the classic-CG oracle stalls near 1e-9 here
+    x = spla.spsolve(A.to_scipy().tocsc(), b)  # the oracle's guarded step stalls near 1e-9 here
     assert its[1] <= 2 * its[0] + 5, its
     assert _rel(phi1[:, 0], x) <= 1e-8
