@@ -1528,8 +1528,8 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     // The next direction p = z + beta p takes z from the replaced residual,
     // so beta = -(z.q)/(p.q) must too.  The fused Jacobi CG computed it in
     // k_cg_update from the recursive residual: recompute it from the new
-    // one (near an ill-conditioned system's floor the two differ enough to
-    // stall the iteration).  FCG and the sweep-preconditioned CG take beta
+    // one, which is the residual the next step works on.  FCG and the
+    // sweep-preconditioned CG take beta
     // from the current z already; alpha always comes from p.r of the next
     // step.
     if (cur == 0 && imat <= 0) {
