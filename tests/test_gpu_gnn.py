@@ -442,3 +442,24 @@ def test_learned_smoother_stays_damping_on_simple_loop_systems(gpu):
     x = spla.spsolve(A.to_scipy().tocsc(), b)  # the oracle's guarded step stalls near 1e-9 here
     assert its[1] <= 2 * its[0] + 5, its
     assert _rel(phi1[:, 0], x) <= 1e-8
+
+
+def test_mixed_jacobi_cg_converges_on_simple_loop_systems(gpu):
+    """The same system and right-hand side with the mixed-precision Jacobi
+    CG (no network): the mass imbalance is small in absolute terms, and the
+    FP32 inner iteration, which divides without the reference's 1e-20 guard,
+    reaches 1e-12 where the oracle's guarded step stalls near 1e-9."""
+    import scipy.sparse.linalg as spla
+    A, b = _simple_loop_system()
+    gpu.matrix_set(A)
+    phi = np.zeros((A.n_cell, 1))
+    res0 = np.asfortranarray(b.reshape(-1, 1).copy())
+    rn = np.zeros(1)
+    gpu.set_option(OPT_PRECISION, 1)
+    try:
+        st = gpu.solv_cg(0, 1e-12, 20000, phi, res0, rn)
+    finally:
+        gpu.set_option(OPT_PRECISION, 0)
+    assert st["status"] == OK and st["iters"][0] < 2000, st["iters"][0]
+    x = spla.spsolve(A.to_scipy().tocsc(), b)
+    assert _rel(phi[:, 0], x) <= 1e-8
