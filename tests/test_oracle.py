@@ -182,3 +182,20 @@ def test_scipy_pin_for_each_preconditioner():
             phi, *_ = getattr(o, "solv_" + solver)(imat, 1e-10, 5000, np.zeros((A.n_cell, 1)),
                                                     b.reshape(-1, 1))
             assert _rel(phi[:, 0], x) <= 1e-8
+
+
+def test_reference_guard_floors_weakly_driven_systems():
+    """The reference's step alpha = s / (p.Ap + small), small = 1e-20
+    (solv_cg.f90:67-68, precision.f90:8), is not scale-free: on a SIMPLE
+    pressure correction driven by its mass imbalance (|b| <= 6e-4) the
+    Jacobi-PCG needs many times the iterations it needs for the same system
+    driven 1e4 times harder, whose solution is just 1e4 times larger."""
+    from test_gpu_gnn import _simple_loop_system
+    A, b = _simple_loop_system()
+    o = Oracle.from_matrix(A)
+    weak = o.solv_cg(0, 1e-10, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
+    strong = o.solv_cg(0, 1e-10, 20000, np.zeros((A.n_cell, 1)), 1e4 * b.reshape(-1, 1))
+    n_weak, n_strong = int(weak[3][0]), int(strong[3][0])
+    assert np.abs(b).max() < 1e-3
+    assert n_strong < 400 and n_weak > 10 * n_strong, (n_weak, n_strong)
+    assert _rel(weak[0] * 1e4, strong[0]) < 1e-6
