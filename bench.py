@@ -75,6 +75,20 @@ def max_over_ranks(x, dist=None, device=None):
     return float(t.item())
 
 
+def host_cpu():
+    """The host the CPU baseline ran on: model name and hardware threads."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "host_threads": os.cpu_count()}
+
+
 def _peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -229,7 +243,7 @@ def run_reference(args, rank):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": _config(args, A),
         "cpu_baseline": {"value": v, "unit": "s/solve", "cores": 1, "kind": "port",
-                         "sample": desc},
+                         "sample": desc, **host_cpu()},
         "e2e": {"value": v, "unit": "s/solve", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
@@ -407,7 +421,8 @@ def main():
         v, sample, dt = cpu_baseline(A, b, st_plain["iters"][0])
         cpu = {"value": v, "unit": "s/solve", "cores": 1, "kind": "port",
                "sample": f"{sample} oracle PCG iterations ({dt:.1f} s, single core) of this "
-                         f"system, scaled to the {st_plain['iters'][0]}-iteration plain solve"}
+                         f"system, scaled to the {st_plain['iters'][0]}-iteration plain solve",
+               **host_cpu()}
 
     if rank == 0:
         line = {

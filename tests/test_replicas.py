@@ -77,6 +77,7 @@ def test_reference_arm_under_torchrun_prints_once_from_rank_zero(built):
     assert d["e2e"] == {"value": d["value"], "unit": "s/solve", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] == 1
+    assert d["cpu_baseline"]["host_threads"] >= 1 and "cpu_model" in d["cpu_baseline"]
 
 
 @pytest.mark.parametrize("line,reasons", [
