@@ -653,6 +653,63 @@ void fvm_gradient(const fvm_mesh *m, int ncomp, const double *phi, double *grad)
     for (int k = 0; k < 3 * ncomp; ++k) grad[(size_t)c * 3 * ncomp + k] /= vol[c];
 }
 
+int fvm_gradient_sweeps(const fvm_mesh *m, int ncomp, const double *phi, const double *bval,
+                        int n_iter, int neu, double *grad) {
+  if (n_iter < 1 || neu < 0 || neu > 2 || (neu == 0 && !bval) || ncomp < 1) return -1;
+  const int N = m->n_cell;
+  const size_t F = m->f_ip.size(), G = (size_t)3 * ncomp * N;
+  std::vector<double> vol(N), v_r(N);
+  fvm_mesh_cell_geom(m, nullptr, vol.data());
+  for (int c = 0; c < N; ++c) v_r[c] = 1.0 / vol[c];  // cfd_grid.f90:546
+  // displacement of a cell centre to its auxiliary point on the face normal
+  auto aux = [](V3 xf, V3 nn, V3 xc) { return (xf - nn * dot(xf - xc, nn)) - xc; };
+  std::vector<double> g0(n_iter > 1 ? G : 0);
+  for (int iter = 1; iter <= n_iter; ++iter) {
+    std::fill(grad, grad + G, 0.0);
+    for (size_t f = 0; f < F; ++f) {
+      double s, l, w;
+      V3 nn, xf;
+      m->face_geom(f, s, nn, xf, l, w);
+      const int a = m->f_ip[f], b = m->f_in[f];
+      const V3 xa = m->xc[a];
+      for (int k = 0; k < ncomp; ++k) {
+        const double pa = phi[(size_t)a * ncomp + k];
+        const double *ga0 = iter > 1 ? &g0[((size_t)a * ncomp + k) * 3] : nullptr;
+        double pf;
+        if (b >= 0) {
+          const double pb = phi[(size_t)b * ncomp + k];
+          if (iter > 1) {
+            const double *gb0 = &g0[((size_t)b * ncomp + k) * 3];
+            const double pp = pa + dot({ga0[0], ga0[1], ga0[2]}, aux(xf, nn, xa));
+            const double pn = pb + dot({gb0[0], gb0[1], gb0[2]}, aux(xf, nn, m->xc[b]));
+            pf = w * pn + (1.0 - w) * pp;
+          } else {
+            pf = w * pb + (1.0 - w) * pa;
+          }
+        } else if (neu > 0) {
+          pf = pa;
+          if (iter > 1 && neu == 2) pf = pf + dot({ga0[0], ga0[1], ga0[2]}, xf - xa);
+        } else {
+          pf = bval[f * ncomp + k];
+        }
+        const double ps = pf * s;
+        double *ga = grad + ((size_t)a * ncomp + k) * 3;
+        ga[0] += ps * nn.x * v_r[a];
+        ga[1] += ps * nn.y * v_r[a];
+        ga[2] += ps * nn.z * v_r[a];
+        if (b >= 0) {
+          double *gb = grad + ((size_t)b * ncomp + k) * 3;
+          gb[0] -= ps * nn.x * v_r[b];
+          gb[1] -= ps * nn.y * v_r[b];
+          gb[2] -= ps * nn.z * v_r[b];
+        }
+      }
+    }
+    if (iter != n_iter) std::copy(grad, grad + G, g0.begin());
+  }
+  return 0;
+}
+
 void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
                    const double *ap, double rho, double *flux) {
   const size_t F = m->f_ip.size();

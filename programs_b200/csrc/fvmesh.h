@@ -112,6 +112,21 @@ void fvm_cavity_field(const fvm_mesh *m, double u_lid, double *u);
  * grad has 3*ncomp per cell. */
 void fvm_gradient(const fvm_mesh *m, int ncomp, const double *phi, double *grad);
 
+/* solv_grad in full (cfd_setup.f90:765-866, 3-d): n_iter Green-Gauss
+ * sweeps.  Sweep 1 takes interior face values phi_f = w phi_N + (1-w) phi_P;
+ * later sweeps first move phi_P and phi_N to their auxiliary points on the
+ * face normal through the face centre with the previous sweep's gradient,
+ * phi_P + g_P.dx_P (dx_P = x_P_aux - x_P, cfd_grid.f90:487-491, 512-516).
+ * Boundary faces: neu = 0 takes bval[f*ncomp + k] (values per face and
+ * component; only boundary entries are read), neu = 1 the cell value,
+ * neu = 2 the cell value plus,
+ * after sweep 1, g_P.(x_f - x_P).  Each face adds ((phi_f s) n) / V in the
+ * reference's face order, 1/V formed once per cell.  grad has 3*ncomp per
+ * cell.  Returns 0, or -1 for n_iter < 1, neu outside 0..2 or neu = 0
+ * without bval. */
+int fvm_gradient_sweeps(const fvm_mesh *m, int ncomp, const double *phi, const double *bval,
+                        int n_iter, int neu, double *grad);
+
 /* Face mass fluxes from the momentum-predicted velocity with Rhie-Chow
  * pressure smoothing (cfd_setup.f90:615-634): F = rho area (u_f . n)
  * - d ((p_N - p_P) - grad(p)_f . (x_N - x_P)), d = rho (V/a_P)_f area / l_pn;

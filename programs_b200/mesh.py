@@ -45,6 +45,9 @@ def _lib():
         lib.fvm_cavity_field.argtypes = [ctypes.c_void_p, ctypes.c_double, _f64p]
         lib.fvm_mesh_cache_geometry.argtypes = [ctypes.c_void_p]
         lib.fvm_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p]
+        lib.fvm_gradient_sweeps.restype = ctypes.c_int
+        lib.fvm_gradient_sweeps.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p,
+                                            ctypes.c_int, ctypes.c_int, _f64p]
         lib.fvm_face_flux.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, ctypes.c_double,
                                       _f64p]
         lib.fvm_mass_imbalance.restype = ctypes.c_double
@@ -241,6 +244,27 @@ def gradient(mesh: "Mesh", phi: np.ndarray) -> np.ndarray:
     k = 1 if phi.ndim == 1 else phi.shape[1]
     g = np.empty((mesh.n_cell, k, 3)) if k > 1 else np.empty((mesh.n_cell, 3))
     _lib().fvm_gradient(mesh._h, k, _p(phi, _f64p), _p(g, _f64p))
+    return g
+
+
+def gradient_sweeps(mesh: "Mesh", phi: np.ndarray, n_iter: int = 2, neu: int = 2,
+                    bval: np.ndarray | None = None) -> np.ndarray:
+    """solv_grad (cfd_setup.f90:765-866) with its sweeps and boundary modes:
+    n_iter Green-Gauss sweeps, later ones corrected with the previous
+    gradient; boundary faces neu = 0 Dirichlet from bval (one value per
+    face and component, boundary entries read), 1 the cell value, 2 the
+    cell value extrapolated to the face.  The reference's loop calls it
+    with n_iter = 2 (cfd_solve.f90:38), neu = 0 for velocity and 2 for
+    pressure (cfd_setup.f90:124, 689, 754)."""
+    phi = _c(phi)
+    k = 1 if phi.ndim == 1 else phi.shape[1]
+    g = np.empty((mesh.n_cell, k, 3)) if k > 1 else np.empty((mesh.n_cell, 3))
+    bv = None if bval is None else _c(np.broadcast_to(
+        np.asarray(bval, np.float64).reshape(mesh.n_face, -1), (mesh.n_face, k)))
+    rc = _lib().fvm_gradient_sweeps(mesh._h, k, _p(phi, _f64p), None if bv is None else
+                                    _p(bv, _f64p), int(n_iter), int(neu), _p(g, _f64p))
+    if rc != 0:
+        raise ValueError("gradient_sweeps: n_iter >= 1, neu in 0..2, bval needed for neu = 0")
     return g
 
 

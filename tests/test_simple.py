@@ -34,6 +34,57 @@ def test_gradient_of_constant_is_zero_and_linear_is_exact_inside(jitter, tol):
     assert np.abs(g[inner] - [3, -2, 0.5]).max() < tol
 
 
+def test_one_sweep_with_wall_values_is_the_single_sweep_gradient():
+    """solv_grad with n_iter = 1, neu = 1 is the one-sweep gradient above
+    (the 1/V factor per face instead of once per cell changes the rounding
+    only)."""
+    from programs_b200.mesh import gradient_sweeps
+    m = _mesh(8)
+    phi = np.random.default_rng(0).normal(size=(m.n_cell, 2))
+    g = gradient_sweeps(m, phi, 1, 1)
+    assert np.abs(g - gradient(m, phi)).max() < 1e-12 * np.abs(g).max()
+
+
+@pytest.mark.parametrize("jitter", [0.0, 0.2])
+def test_sweeps_known_answer_of_the_reference_self_check(jitter):
+    """The reference's built-in check (test_grad, cfd_setup.f90:871-921):
+    phi = x y with its exact values on the boundary faces (neu = 0), RMS
+    error of d/dx -> y and d/dy -> x for 1..6 sweeps.  Exact on a regular
+    mesh; on a skewed one the corrected sweeps cut the first sweep's error
+    several times and settle by the fourth."""
+    from programs_b200.mesh import gradient_sweeps
+    m = Mesh.hex(12, jitter=jitter, seed=1, permute=True)
+    xc, _ = m.cell_geom()
+    _, _, xf, _, _ = m.face_geom()
+    phi, bval = xc[:, 0] * xc[:, 1], xf[:, 0] * xf[:, 1]
+    exact = np.stack([xc[:, 1], xc[:, 0], np.zeros(m.n_cell)], 1)
+    err = [np.sqrt(((gradient_sweeps(m, phi, n, 0, bval) - exact) ** 2).mean(0)).max()
+           for n in range(1, 7)]
+    if jitter == 0.0:
+        assert max(err) < 1e-12
+    else:
+        assert err[1] < 0.3 * err[0] and abs(err[5] - err[3]) < 0.05 * err[3]
+    with pytest.raises(ValueError):
+        gradient_sweeps(m, phi, 2, 0)          # Dirichlet walls need their values
+    with pytest.raises(ValueError):
+        gradient_sweeps(m, phi, 0, 1)
+
+
+def test_extrapolated_walls_converge_to_a_linear_gradient():
+    """neu = 2 (the pressure gradient's walls, cfd_setup.f90:689, 754):
+    the wall value is the cell value moved to the face with the previous
+    sweep's gradient, so on a regular mesh each sweep halves the error of
+    a linear field; zero-gradient walls (neu = 1) keep it."""
+    from programs_b200.mesh import gradient_sweeps
+    m = Mesh.hex(10, jitter=0.0, seed=1, permute=True)
+    xc, _ = m.cell_geom()
+    a = np.array([0.7, -1.3, 0.4])
+    phi = xc @ a + 2.0
+    e = [np.abs(gradient_sweeps(m, phi, n, 2) - a).max() for n in (1, 2, 3, 30)]
+    assert abs(e[1] / e[0] - 0.5) < 1e-6 and abs(e[2] / e[1] - 0.5) < 1e-6 and e[3] < 1e-8
+    assert abs(np.abs(gradient_sweeps(m, phi, 4, 1) - a).max() - e[0]) < 1e-9
+
+
 def test_mass_imbalance_sums_to_zero_in_a_closed_box():
     m = _mesh()
     u = cavity_field(m, 1.0)
