@@ -187,3 +187,22 @@ def test_shipped_weights_load_and_record_their_training(tmp_path):
     np.savez(bad, params=p[:-1], n_param=learn.N_PARAM - 1, layout=learn.LAYOUT, meta="{}")
     with pytest.raises(ValueError):
         learn.load_params(bad)
+
+
+def test_training_systems_are_seeded_symmetric_pinned_pressure_corrections():
+    """The generator behind the shipped network's training data: per mesh
+    (jitter drawn in [0, 0.25]) several flow states; every system is the
+    symmetric pressure-correction matrix with cell 1 pinned, driven by a
+    uniform right-hand side with its mean removed and zero at the pinned
+    cell, and the same seed gives the same systems."""
+    def draw():
+        return [(P.p.copy(), P.n.copy(), P.pl.copy(), b.copy())
+                for _, P, b in learn.simple_systems(5, n_mesh=3, per_mesh=2, seed=4)]
+    first, again = draw(), draw()
+    assert len(first) == 6
+    for (p, n, pl, b), (p2, n2, pl2, b2) in zip(first, again):
+        assert np.array_equal(p, p2) and np.array_equal(pl, pl2) and np.array_equal(b, b2)
+        assert np.array_equal(p, n) and np.all(p <= 0)
+        assert np.all(pl > 0) and b[0] == 0.0 and np.all(np.abs(b) <= 2.0)
+    # different flow states on one mesh give different coefficients
+    assert not np.array_equal(first[0][2], first[1][2])
