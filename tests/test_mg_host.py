@@ -78,3 +78,19 @@ def test_isolated_cells_stay_alone_and_components_never_mix():
     ptr = np.arange(8, dtype=np.int64) * 0
     agg, na = mg_aggregate(ptr, np.zeros(0, np.int32), np.zeros(0, np.float32), 3)
     assert na == 7 and np.array_equal(agg, np.arange(7))
+
+
+def test_self_loops_change_nothing():
+    """A graph that keeps the matrix diagonal (every row its own neighbour)
+    aggregates exactly as the graph without it."""
+    from programs_b200.solver import mg_aggregate
+    A = Mesh.hex(5, jitter=0.2, seed=1).pressure(pin=0).to_scipy().tocsr()
+    S = A.copy()
+    S.data = np.abs(S.data)
+    T = A.copy()
+    T.setdiag(0)
+    T.eliminate_zeros()
+    T.data = np.abs(T.data)
+    got = [mg_aggregate(M.indptr.astype(np.int64), M.indices.astype(np.int32),
+                        M.data.astype(np.float32), 3) for M in (S, T)]
+    assert got[0][1] == got[1][1] and np.array_equal(got[0][0], got[1][0])
