@@ -1,5 +1,5 @@
 """CPU reference of the learned preconditioner (TEST INFRASTRUCTURE ONLY:
-the checker for programs_b200/csrc/gnn.cuh).
+the oracle that programs_b200/csrc/gnn.cuh is tested against).
 
 The reference code base has no learned preconditioner, so this restates
 the network and preconditioner as specified in gnn.cuh, in float64 on the

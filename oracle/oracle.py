@@ -1,8 +1,8 @@
 """ctypes wrapper of the CPU oracle (``oracle/liborc.so``).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()``
-and the CPU-baseline leg of ``bench.py`` as the checker -- never by the
-product path.  Function names and argument meanings follow the Fortran
+and the CPU-baseline leg of ``bench.py``, as the oracle results are
+compared with -- never by the product path.  Function names and argument meanings follow the Fortran
 subroutines they restate (spray-simulation/solv_*.f90).  Parity of the
 restatement is not pinned by the reference itself (no Fortran compiler, no
 golden vectors); it is cross-checked in tests/test_oracle.py.

@@ -1,7 +1,8 @@
 /*
  * solv_oracle.c -- line-faithful CPU restatement of the spray-simulation
- * linear-solver hot path (TEST INFRASTRUCTURE ONLY: the checker and the
- * single-core CPU baseline, never linked into the product library).
+ * linear-solver hot path (TEST INFRASTRUCTURE ONLY: the oracle the GPU
+ * path is tested against and the single-core CPU baseline, never linked
+ * into the product library).
  *
  * Each routine follows the Fortran loop order statement by statement so
  * that floating-point results match a gfortran build without -ffast-math:

@@ -1,7 +1,7 @@
 /*
  * solv_oracle.h -- CPU restatement of the spray-simulation linear solvers.
  *
- * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared
+ * TEST INFRASTRUCTURE ONLY.  This is the oracle the CUDA path is compared
  * against (and the timed single-core CPU baseline); no product code links it.
  *
  * Parity status: the reference solver is Fortran 90 and no Fortran compiler

@@ -72,7 +72,7 @@ def save_params(path: str, p: np.ndarray, meta: dict) -> None:
 def load_params(path: str = DEFAULT_WEIGHTS) -> np.ndarray:
     d = np.load(path)
     if int(d["n_param"]) != N_PARAM or str(d["layout"]) != LAYOUT:
-        raise ValueError(f"{path}: parameter layout does not match this build")
+        raise ValueError(f"{path}: parameter layout does not match this library's network")
     return np.asarray(d["params"], np.float32)
 
 

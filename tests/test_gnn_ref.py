@@ -174,7 +174,7 @@ def test_reference_vcycle_gradient_matches_finite_differences():
 
 
 def test_shipped_weights_load_and_record_their_training(tmp_path):
-    """The committed network: this build's layout, finite, not the untrained
+    """The committed network: the library's layout, finite, not the untrained
     Jacobi network, trained on 2,000 pressure systems of 64^3 meshes; a file
     of another layout is refused rather than misread."""
     import json
