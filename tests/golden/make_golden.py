@@ -32,6 +32,8 @@ from oracle.oracle import Oracle  # noqa: E402
 from programs_b200 import build  # noqa: E402
 from programs_b200.mesh import Mesh, poisson_rhs, uniform  # noqa: E402
 
+# where the reference checkout keeps the mesh it ships
+DEFAULT_NEU = "/root/reference/spray-simulation/cavity_3d.neu"
 REDUC = 1e-10
 N_ITER = 5000
 
@@ -70,7 +72,7 @@ def _matrix(A, prefix, out):
     out[prefix + "pl"] = A.pl
 
 
-def cavity(path: str) -> None:
+def cavity(path: str, outdir: str = HERE) -> None:
     m = Mesh.read_neu(path)
     A = m.pressure(pin=1)
     b = np.asfortranarray(poisson_rhs(A.n_cell, 7).reshape(-1, 1))
@@ -78,11 +80,11 @@ def cavity(path: str) -> None:
     _matrix(A, "", out)
     out["b"] = b
     _solves(A, b, "", out, solvers=("cg",))
-    np.savez_compressed(os.path.join(HERE, "cavity_3d.npz"), **out)
+    np.savez_compressed(os.path.join(outdir, "cavity_3d.npz"), **out)
     print("cavity_3d:", A.n_cell, "cells", A.n_face, "faces")
 
 
-def hex6() -> None:
+def hex6(outdir: str = HERE) -> None:
     m = Mesh.hex(6, jitter=0.15, seed=0, permute=True)
     P = m.pressure(pin=1)
     M, dt = m.momentum()
@@ -95,14 +97,14 @@ def hex6() -> None:
     out["m_b"] = bm
     _solves(P, bp, "p_", out, solvers=("cg", "bicg"))
     _solves(M, bm, "m_", out, solvers=("bicg",))
-    np.savez_compressed(os.path.join(HERE, "hex6.npz"), **out)
+    np.savez_compressed(os.path.join(outdir, "hex6.npz"), **out)
     print("hex6:", P.n_cell, "cells", P.n_face, "faces; momentum dt", dt)
 
 
 if __name__ == "__main__":
     build.build_all()
     hex6()
-    neu = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/spray-simulation/cavity_3d.neu"
+    neu = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_NEU
     if os.path.exists(neu):
         cavity(neu)
     else:

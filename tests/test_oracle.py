@@ -199,3 +199,26 @@ def test_reference_guard_floors_weakly_driven_systems():
     assert np.abs(b).max() < 1e-3
     assert n_strong < 400 and n_weak > 10 * n_strong, (n_weak, n_strong)
     assert _rel(weak[0] * 1e4, strong[0]) < 1e-6
+
+
+def test_fixtures_regenerate_bit_for_bit(tmp_path):
+    """tests/golden/make_golden.py rebuilds the committed fixtures exactly:
+    the mesh generator, the assembly, the seeded right-hand sides and the
+    oracle have not drifted from what the fixtures hold.  The cavity
+    fixture is rebuilt only where the reference's cavity_3d.neu is
+    available."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    mg.hex6(str(tmp_path))
+    names = ["hex6.npz"]
+    neu = os.environ.get("CAVITY_NEU", mg.DEFAULT_NEU)
+    if os.path.exists(neu):
+        mg.cavity(neu, str(tmp_path))
+        names.append("cavity_3d.npz")
+    for name in names:
+        new, old = np.load(str(tmp_path / name)), _load(name)
+        assert sorted(new.files) == sorted(old.files), name
+        for k in old.files:
+            assert np.array_equal(new[k], old[k]), (name, k)
