@@ -186,3 +186,19 @@ def test_gambit_reader_rejects_malformed_files(tmp_path):
         Mesh.read_neu(p)
     with pytest.raises(RuntimeError):
         Mesh.read_neu(str(tmp_path / "missing.neu"))
+
+
+def test_uneven_batch_generator():
+    """The uneven-mesh batch (log-uniform cell counts, seed 1): n systems of
+    n^3 cells, n the rounded cube root of each draw, all pinned pressure
+    systems; the same seed gives the same batch."""
+    from programs_b200.cases import batch_meshes
+    mats, rhs = batch_meshes(8, 27, 4000, seed=1)
+    sizes = [A.n_cell for A in mats]
+    assert len(mats) == len(rhs) == 8
+    roots = [round(s ** (1 / 3)) for s in sizes]
+    assert all(r ** 3 == s and 3 <= r <= 16 for r, s in zip(roots, sizes))
+    assert len(set(sizes)) >= 4
+    assert all(np.array_equal(A.p, A.n) and b.shape == (A.n_cell,) for A, b in zip(mats, rhs))
+    again, _ = batch_meshes(8, 27, 4000, seed=1)
+    assert [A.n_cell for A in again] == sizes and np.array_equal(again[3].p, mats[3].p)
