@@ -21,9 +21,11 @@ module solv_gpu_m
   logical, save :: have_structure = .false.
 
   interface
+    ! solv_gpu_create(solv_gpu_ctx **out, int device): out is the address
+    ! of the handle, passed by value
     integer(c_int) function c_create(pctx, device) bind(c, name='solv_gpu_create')
       import :: c_ptr, c_int
-      type(c_ptr) :: pctx
+      type(c_ptr), value :: pctx
       integer(c_int), value :: device
     end function
     integer(c_int) function c_destroy(h) bind(c, name='solv_gpu_destroy')
@@ -67,15 +69,13 @@ contains
 
   subroutine solv_gpu_init(device)
     integer, intent(in) :: device
-    type(c_ptr) :: p
     integer(c_int) :: rc
     integer(c_intptr_t), target :: h
     h = 0
     rc = c_create(c_loc(h), int(device, c_int))
-    if (rc /= 0) stop 'solv_gpu_init: no CUDA device'
+    if (rc /= 0 .or. h == 0) stop 'solv_gpu_init: no CUDA device'
     ctx = h
     have_structure = .false.
-    p = c_null_ptr
   end subroutine
 
   subroutine solv_gpu_final()
@@ -147,6 +147,8 @@ contains
     real(wp), dimension(:), intent(inout) :: res0_n
     real(c_double), allocatable :: buf(:,:)
     integer(c_int) :: rc, nr
+    if (size(res0, 1) /= size(pl) .or. size(res0, 2) /= size(res0_n)) &
+      stop 'solv_cg (gpu): res0 must be res0(n_cell, n_vc)'
     allocate(buf(size(res0_n), size(pl)))
     call solv_gpu_sync_values()
     call pack_phi(phi, size(pl), size(res0_n), buf)
@@ -167,6 +169,8 @@ contains
     real(wp), dimension(:), intent(inout) :: res0_n
     real(c_double), allocatable :: buf(:,:)
     integer(c_int) :: rc, nr
+    if (size(res0, 1) /= size(pl) .or. size(res0, 2) /= size(res0_n)) &
+      stop 'solv_bicg (gpu): res0 must be res0(n_cell, n_vc)'
     allocate(buf(size(res0_n), size(pl)))
     call solv_gpu_sync_values()
     call pack_phi(phi, size(pl), size(res0_n), buf)

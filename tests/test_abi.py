@@ -64,3 +64,53 @@ def test_fortran_interface_module_names_match():
     from programs_b200.solver import lib
     L = lib()
     assert bound and all(hasattr(L, n) for n in bound)
+
+
+def _c_params(header_src, name):
+    m = re.search(r"\b" + name + r"\s*\(([^;{]*)\)\s*;", header_src, flags=re.S)
+    assert m, name
+    body = m.group(1).strip()
+    return [] if body in ("", "void") else [p.strip() for p in body.split(",")]
+
+
+def _f_dummies(f90_src):
+    """bound C name -> [(dummy, attributes line)] for each interface body."""
+    out = {}
+    for m in re.finditer(r"function\s+\w+\s*\(([^)]*)\)\s*&?\s*bind\s*\(\s*c\s*,\s*name\s*=\s*'(\w+)'\s*\)"
+                         r"(.*?)end\s+function", f90_src, flags=re.S | re.I):
+        names = [a.strip() for a in m.group(1).replace("&", " ").split(",") if a.strip()]
+        decls = [l.strip() for l in m.group(3).splitlines() if "::" in l]
+        attrs = {}
+        for d in decls:
+            spec, vars_ = d.split("::", 1)
+            for v in vars_.split(","):
+                attrs[v.strip()] = spec.strip().lower()
+        out[m.group(2)] = [(n, attrs.get(n, "")) for n in names]
+    return out
+
+
+def test_fortran_interfaces_match_the_c_declarations():
+    """Arity and passing convention of every binding: C scalars by value;
+    a C data pointer is an array passed by reference, or an address
+    (c_ptr / c_intptr_t handle) passed by value; a pointer to a pointer is
+    an address passed by value, or a handle variable passed by reference."""
+    with open(os.path.join(ROOT, "include", "solv_gpu.h")) as f:
+        header = re.sub(r"/\*.*?\*/", "", f.read(), flags=re.S)
+    with open(os.path.join(ROOT, "programs_b200", "fortran", "solv_gpu_m.f90")) as f:
+        binds = _f_dummies(f.read())
+    assert binds
+    for cname, dummies in binds.items():
+        params = _c_params(header, cname)
+        assert len(params) == len(dummies), (cname, params, dummies)
+        for cp, (dn, spec) in zip(params, dummies):
+            stars = cp.count("*")
+            by_value = "value" in spec
+            address = "type(c_ptr)" in spec or "c_intptr_t" in spec
+            if stars == 0:
+                assert by_value and not address, (cname, cp, spec)
+            elif stars == 1:
+                assert (not by_value and "dimension" in spec) or (by_value and address), \
+                    (cname, cp, spec)
+            else:
+                assert (by_value and "type(c_ptr)" in spec) or \
+                    (not by_value and "c_intptr_t" in spec), (cname, cp, spec)
