@@ -114,3 +114,35 @@ def test_fortran_interfaces_match_the_c_declarations():
             else:
                 assert (by_value and "type(c_ptr)" in spec) or \
                     (not by_value and "c_intptr_t" in spec), (cname, cp, spec)
+
+
+def test_fortran_by_reference_shims_report_through_status():
+    """The gfortran-convention entry points (every argument by reference,
+    the handle an integer(8) holding the context address) return their
+    code in `status`: a null handle or a missing argument is BAD_INPUT,
+    and without a device create reports DEVICE_ERROR and a zero handle."""
+    import ctypes
+    import torch
+    from programs_b200.solver import lib
+    L = lib()
+    i64, i32, f64 = ctypes.c_int64, ctypes.c_int, ctypes.c_double
+    st = i32(-1)
+    h0 = i64(0)
+    one, zero = i32(1), i32(0)
+    red = f64(1e-10)
+    buf = (ctypes.c_double * 8)()
+    L.solv_gpu_cg_(ctypes.byref(h0), ctypes.byref(zero), ctypes.byref(red), ctypes.byref(one),
+                   ctypes.byref(one), buf, buf, buf, ctypes.byref(zero), ctypes.byref(st))
+    assert st.value == 4
+    st.value = -1
+    L.solv_gpu_bicg_(ctypes.byref(h0), None, ctypes.byref(red), ctypes.byref(one),
+                     ctypes.byref(one), buf, buf, buf, ctypes.byref(zero), ctypes.byref(st))
+    assert st.value == 4
+    st.value = -1
+    L.solv_gpu_destroy_(ctypes.byref(h0), ctypes.byref(st))
+    assert st.value == 4
+    if not torch.cuda.is_available():
+        h = i64(12345)
+        st.value = -1
+        L.solv_gpu_create_(ctypes.byref(h), ctypes.byref(zero), ctypes.byref(st))
+        assert st.value == 5 and h.value == 0
