@@ -146,3 +146,25 @@ def test_fortran_by_reference_shims_report_through_status():
         st.value = -1
         L.solv_gpu_create_(ctypes.byref(h), ctypes.byref(zero), ctypes.byref(st))
         assert st.value == 5 and h.value == 0
+
+
+def test_ctypes_stubs_match_the_header_arity():
+    """Every ctypes stub the Python layer declares (solver.py, fv.py,
+    mesh.py) takes as many arguments as the C declaration it binds."""
+    from programs_b200 import fv, mesh, solver
+    L = solver.lib()
+    fv._typed()
+    M = mesh._lib()
+    checked = 0
+    for lib_, header in ((L, "solv_gpu.h"), (L, "fv_gpu.h"),
+                         (M, os.path.join("..", "programs_b200", "csrc", "fvmesh.h"))):
+        with open(os.path.join(ROOT, "include", header)) as f:
+            src = re.sub(r"/\*.*?\*/", "", f.read(), flags=re.S)
+        for name in set(re.findall(r"\b((?:solv_gpu|fv_gpu|fvm)_\w+)\s*\(", src)):
+            fn = getattr(lib_, name, None)
+            types = getattr(fn, "argtypes", None) if fn is not None else None
+            if types is None:
+                continue
+            assert len(types) == len(_c_params(src, name)), name
+            checked += 1
+    assert checked >= 60, checked
