@@ -710,6 +710,37 @@ int fvm_gradient_sweeps(const fvm_mesh *m, int ncomp, const double *phi, const d
   return 0;
 }
 
+void fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, const double *grad,
+                           const double *flux, double mu, double c_bl, double *rhs) {
+  const size_t F = m->f_ip.size();
+  auto aux = [](V3 xf, V3 nn, V3 xc) { return (xf - nn * dot(xf - xc, nn)) - xc; };
+  for (size_t f = 0; f < F; ++f) {
+    const int a = m->f_ip[f], b = m->f_in[f];
+    if (b < 0) continue;
+    double s, l, w;
+    V3 nn, xf;
+    m->face_geom(f, s, nn, xf, l, w);
+    const V3 dxa = aux(xf, nn, m->xc[a]), dxb = aux(xf, nn, m->xc[b]);
+    const double c = flux[f], d = mu * s / l;
+    for (int k = 0; k < ncomp; ++k) {
+      const double pa = phi[(size_t)a * ncomp + k], pb = phi[(size_t)b * ncomp + k];
+      const double *ga = &grad[((size_t)a * ncomp + k) * 3];
+      const double *gb = &grad[((size_t)b * ncomp + k) * 3];
+      const double pa_aux = pa + dot({ga[0], ga[1], ga[2]}, dxa);
+      const double pb_aux = pb + dot({gb[0], gb[1], gb[2]}, dxb);
+      double cor = 0.0;
+      if (c != 0.0) {
+        const double pf = w * pb_aux + (1.0 - w) * pa_aux;
+        const double up = c > 0.0 ? pa : pb;
+        cor = c_bl * c * (up - pf);
+      }
+      cor = cor + d * ((pb_aux - pa_aux) - (pb - pa));
+      rhs[(size_t)a * ncomp + k] += cor;
+      rhs[(size_t)b * ncomp + k] -= cor;
+    }
+  }
+}
+
 void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
                    const double *ap, double rho, double *flux) {
   const size_t F = m->f_ip.size();

@@ -85,6 +85,66 @@ def test_extrapolated_walls_converge_to_a_linear_gradient():
     assert abs(np.abs(gradient_sweeps(m, phi, 4, 1) - a).max() - e[0]) < 1e-9
 
 
+def _cell_sums(m, per_face_p, per_face_n):
+    """Sum per-face owner and neighbour contributions into cells."""
+    ip, inb = m.faces()
+    out = np.zeros(m.n_cell)
+    np.add.at(out, ip - 1, per_face_p)
+    inner = inb > 0
+    np.add.at(out, inb[inner] - 1, per_face_n[inner])
+    return out
+
+
+def test_deferred_diffusion_correction_makes_a_linear_field_harmonic():
+    """On a skewed mesh the implicit two-point diffusion d (phi_N - phi_P)
+    misses the tangential part of the gradient; with the reference's
+    explicit correction d ((phi_N' - phi_P') - (phi_N - phi_P)) the face
+    flux is d (phi_N' - phi_P') = mu area grad.n for a linear field, so
+    every interior cell balances exactly (cfd_setup.f90:318-322)."""
+    from programs_b200.mesh import momentum_deferred
+    m = Mesh.hex(8, jitter=0.2, seed=4, permute=True)
+    xc, _ = m.cell_geom()
+    s, nrm, xf, l, w = m.face_geom()
+    ip, inb = m.faces()
+    a = np.array([0.7, -1.3, 0.4])
+    phi = xc @ a + 2.0
+    grad = np.tile(a, (m.n_cell, 1))
+    mu = 0.01
+    rhs = momentum_deferred(m, phi, grad, np.zeros(m.n_face), mu, c_bl=1.0)
+    inner = inb > 0
+    d = np.where(inner, mu * s / l, 0.0)
+    pb = np.where(inner, phi[np.maximum(inb, 1) - 1], 0.0)
+    pa = phi[ip - 1]
+    implicit = _cell_sums(m, d * (pa - pb), np.where(inner, d * (pb - pa), 0.0))
+    interior = np.bincount(ip - 1, weights=~inner, minlength=m.n_cell) == 0  # no wall face
+    scale = np.abs(implicit[interior]).max()
+    assert scale > 1e-4                                   # the skew is visible without it
+    assert np.abs(implicit[interior] - rhs[interior]).max() < 1e-10 * scale + 1e-15
+    assert abs(rhs.sum()) < 1e-12 * np.abs(rhs).sum()     # conservative
+
+
+def test_deferred_convection_term_is_central_minus_upwind():
+    """c_bl c (phi_up - phi_f): zero for a constant field; on a regular mesh
+    (auxiliary points at the cell centres, w = 1/2) exactly c (phi_up -
+    (phi_P + phi_N) / 2) per face, owner +, neighbour -."""
+    from programs_b200.mesh import momentum_deferred
+    m = Mesh.hex(6, jitter=0.0, seed=2, permute=True)
+    xc, _ = m.cell_geom()
+    ip, inb = m.faces()
+    c = np.random.default_rng(1).normal(size=m.n_face)
+    zero_grad = np.zeros((m.n_cell, 3))
+    assert np.abs(momentum_deferred(m, np.full(m.n_cell, 3.0), zero_grad, c, 0.0)).max() == 0.0
+    phi = xc[:, 0] - 2 * xc[:, 1]
+    grad = np.tile([1.0, -2.0, 0.0], (m.n_cell, 1))
+    got = momentum_deferred(m, phi, grad, c, 0.0, c_bl=0.5)
+    inner = inb > 0
+    pa = phi[ip - 1]
+    pb = np.where(inner, phi[np.maximum(inb, 1) - 1], 0.0)
+    cor = np.where(inner, 0.5 * c * (np.where(c > 0, pa, pb) - 0.5 * (pa + pb)), 0.0)
+    want = _cell_sums(m, cor, -cor)
+    assert np.abs(got - want).max() < 1e-13
+
+
 def test_mass_imbalance_sums_to_zero_in_a_closed_box():
     m = _mesh()
     u = cavity_field(m, 1.0)
