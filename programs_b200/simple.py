@@ -32,10 +32,13 @@ from .solver import GpuSolver, OPT_PRECISION
 
 def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15, seed=0,
         p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None, p_imat=1,
-        m_precision=0, device=0, log_every=0):
+        m_precision=0, device=0, log_every=0, make_solver=None):
     """Returns (u (N,3), p (N,), history, timings).  learned: weights array
     (FCG with the learned preconditioner for the pressure correction) or
-    None (plain FP64 PCG with imat p_imat)."""
+    None (plain FP64 PCG with imat p_imat).  make_solver(device) builds the
+    two solver contexts (default GpuSolver); anything with the same
+    matrix_set / matrix_values / solv_cg / solv_bicg / set_option / close
+    methods can stand in."""
     rho = 1.0
     mu = rho * u_lid * 1.0 / re
     m = Mesh.hex(size, jitter=jitter, seed=seed, permute=True)
@@ -46,8 +49,9 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
     u = np.zeros((N, 3))
     p = np.zeros(N)
     F = None
-    sm = GpuSolver(device)
-    sp = GpuSolver(device)
+    factory = make_solver or GpuSolver
+    sm = factory(device)
+    sp = factory(device)
     sm.set_option(OPT_PRECISION, m_precision)
     if learned is not None:
         sp.gnn_set_params(learned)
