@@ -213,14 +213,14 @@ def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=400):
 
 
 def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
-          init=None, log_every=50, device=0, loss=2, smoother=1, data="loop"):
+          init=None, log_every=50, device=0, loss=2, smoother=1, data="synthetic"):
     """smoother (loss 2): 1 trains the network's operator K as the V-cycle's
     smoother, 2 its per-cell diagonal alone (learned Jacobi weights).
-    data: "loop" -- the systems the SIMPLE loop generates (loop_systems),
-    every other one with a uniform random right-hand side in place of the
-    mass imbalance, so that both kinds of right-hand side are seen;
-    "synthetic" -- cavity-like flow states with random right-hand sides
-    (device_systems)."""
+    data: "synthetic" (the default, and what the shipped network was
+    trained on) -- cavity-like flow states with random right-hand sides
+    (device_systems); "loop" -- the systems the SIMPLE loop generates
+    (loop_systems), every other one with a uniform random right-hand side
+    in place of the mass imbalance, so that both kinds are seen."""
     import torch
     from .solver import OPT_GNN_LOSS, OPT_MG_SMOOTHER
     s = GpuSolver(device)
@@ -279,8 +279,12 @@ def main(argv=None):
                     help="0 energy, 1 scale-free (network alone), 2 scale-free through the V-cycle")
     ap.add_argument("--smoother", type=int, default=1,
                     help="loss 2: 1 the operator K, 2 its diagonal (learned Jacobi weights)")
-    ap.add_argument("--data", default="loop", choices=["loop", "synthetic"])
-    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--data", default="synthetic", choices=["synthetic", "loop"],
+                    help="synthetic: cavity-like flow states (the shipped network); "
+                         "loop: the SIMPLE loop's own systems")
+    ap.add_argument("--out", default="gnn_pressure_trained.npz",
+                    help="where to write the weights; the shipped network is "
+                         "programs_b200/weights/gnn_pressure.npz, replaced only when named")
     a = ap.parse_args(argv)
     init = load_params(a.resume) if a.resume else None
     t = time.time()
