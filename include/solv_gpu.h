@@ -61,8 +61,12 @@ extern "C" {
 #define SOLV_GPU_MAX_VC 4
 
 /* option keys for solv_gpu_set_option */
-#define SOLV_OPT_PRECISION 1    /* 0 = FP64 (default); 1 = FP32 inner
-                                   Krylov + FP64 iterative refinement      */
+#define SOLV_OPT_PRECISION 1    /* 0 = FP64 (default), the reference's
+                                   arithmetic; 1 = FP32 inner Krylov with
+                                   FP64 reliable updates (CG) or iterative
+                                   refinement (BiCGSTAB); its FP32 steps
+                                   divide without the absolute 1e-20 guard,
+                                   so weakly driven systems converge       */
 #define SOLV_OPT_INNER_REDUC 2  /* inner relative drop per refinement
                                    sweep (FP32 mode), default 1e-6         */
 #define SOLV_OPT_GRAPH_ITERS 3  /* Krylov iterations per CUDA-graph launch
