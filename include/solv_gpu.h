@@ -53,8 +53,9 @@ extern "C" {
 #define SOLV_GPU_BAD_INPUT 4    /* index out of range, sizes, null, ...    */
 #define SOLV_GPU_DEVICE_ERROR 5 /* CUDA error (message: solv_gpu_last_error) */
 #define SOLV_GPU_NO_MATRIX 7    /* no solv_gpu_matrix_set yet              */
-#define SOLV_GPU_ZERO_RHS 8     /* maxval(res0_n) < small: returned early
-                                   exactly as solv_cg.f90:21 does          */
+#define SOLV_GPU_ZERO_RHS 8     /* maxval(res0_n) < small: the solve ends
+                                   at once as solv_cg.f90:21 does; reported
+                                   in stats.status, the call returns OK    */
 #define SOLV_GPU_TOO_LARGE 9    /* beyond the fixed scratch of
                                    solv_gpu_res_noalloc (n_vc > 4)         */
 
