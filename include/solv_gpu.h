@@ -199,7 +199,9 @@ int solv_gpu_kernel_time(solv_gpu_ctx *ctx, int which, int repeat,
  * the coarse levels, dense inverse on the coarsest), and the V-cycle is the
  * preconditioner (SOLV_OPT_MG_*; the hierarchy is built on the host at the
  * first such solve after solv_gpu_matrix_set, from the coefficients then;
- * SOLV_OPT_MG_LEVELS 0 uses K alone).  If
+ * SOLV_OPT_MG_LEVELS 0 uses K alone).  Each solve bounds the smoother:
+ * per-cell scales are held at 0.5 or more and K is scaled so that eight
+ * power iterations find lambda_max(omega K A) <= 1.9.  If
  * the iteration loses positive curvature or produces NaN, plain Jacobi-PCG
  * takes over from the current iterate (stats.fallbacks); the FP64 residual
  * test |b - A x|_1 / |r0|_1 < reduc decides convergence either way.  Same
@@ -233,11 +235,15 @@ int solv_gpu_gnn_get_params(solv_gpu_ctx *ctx, float *params, int n);
  * path 0: inference kernels (BF16, tensor cores); 1: training kernels. */
 int solv_gpu_gnn_forward_dev(solv_gpu_ctx *ctx, const double *r0_dev,
                              const double *r_dev, double *z_dev, int path);
-/* Training: forward + backward of the energy J = 1/2 z'Âz - z'u, z = K u,
- * in the Jacobi-scaled space (minimised by K u = Â^-1 u) for the
- * preconditioner built from r0, averaged over n_samples residuals (each
- * n_cell long, consecutive, caller order, device); gradients add up in an
- * FP32 accumulator (zeroed first unless accumulate); loss = J / n_cell. */
+/* Training: forward + backward of the loss SOLV_OPT_GNN_LOSS selects, for
+ * the preconditioner built from r0, over n_samples residuals u (each
+ * n_cell long, consecutive, caller order, device): 0 the energy
+ * J = 1/2 z'Âz - z'u of z = K u in the Jacobi-scaled space (minimised by
+ * K u = Â^-1 u); 1 the scale-free J = -(z'u)^2 / (z'Âz), twice the energy
+ * after the best step along z; 2 J = -log((z'u)^2 / (z'Az)) with z the
+ * V-cycle applied to u (needs the hierarchy).  Gradients add up in an FP32
+ * accumulator (zeroed first unless accumulate); loss = sum J / (n_cell
+ * n_samples). */
 int solv_gpu_gnn_grad_dev(solv_gpu_ctx *ctx, const double *r0_dev,
                           const double *samples_dev, int n_samples,
                           double *loss, int accumulate);
@@ -248,9 +254,10 @@ int solv_gpu_gnn_adam(solv_gpu_ctx *ctx, float lr, float grad_scale);
 
 /* -- autotuner ------------------------------------------------------------ */
 /* No counterpart in the reference (it has no tunables).  Times candidate
- * launch shapes (threads per block 128/256/512, resident blocks per SM
- * 2/4/8/16 for the reduction kernels, Krylov iterations per CUDA graph
- * 8/32) on the current matrix with the given solver (0 CG, 1 BiCGSTAB),
+ * launch shapes (threads per block 128/256, resident blocks per SM 4/8/16
+ * for the reduction kernels, at most 2048 threads per SM, Krylov
+ * iterations per CUDA graph 8/32) on the current matrix with the given
+ * solver (0 CG, 1 BiCGSTAB),
  * preconditioner, component count and the context's precision, and leaves
  * the fastest set on the context. */
 typedef struct {
