@@ -710,9 +710,11 @@ int fvm_gradient_sweeps(const fvm_mesh *m, int ncomp, const double *phi, const d
   return 0;
 }
 
-void fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, const double *grad,
-                           const double *flux, double mu, double c_bl, double *rhs) {
+int fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, const double *grad,
+                          const double *flux, double mu, double c_bl, int scheme, double *rhs) {
+  if (scheme < 0 || scheme > 3) return -1;
   const size_t F = m->f_ip.size();
+  const double small = 1e-20;  // precision.f90:8
   auto aux = [](V3 xf, V3 nn, V3 xc) { return (xf - nn * dot(xf - xc, nn)) - xc; };
   for (size_t f = 0; f < F; ++f) {
     const int a = m->f_ip[f], b = m->f_in[f];
@@ -730,7 +732,22 @@ void fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, cons
       const double pb_aux = pb + dot({gb[0], gb[1], gb[2]}, dxb);
       double cor = 0.0;
       if (c != 0.0) {
-        const double pf = w * pb_aux + (1.0 - w) * pa_aux;
+        double pf;
+        if (scheme == 0) {
+          pf = w * pb_aux + (1.0 - w) * pa_aux;
+        } else {  // TVD (cfd_setup.f90:233-272)
+          const bool fwd = c > 0.0;
+          const double pc = fwd ? pa_aux : pb_aux, pd = fwd ? pb_aux : pa_aux;
+          const double *gc = fwd ? ga : gb;
+          const V3 xpa = m->xc[a] + dxa, xpb = m->xc[b] + dxb;
+          const V3 dx = fwd ? xpb - xpa : xpa - xpb;
+          const double pu = pd - 2.0 * dot({gc[0], gc[1], gc[2]}, dx);
+          double r = (pc - pu) / (pd - pc + small);
+          if (scheme == 1) r = std::max(0.0, std::min(1.0, r));
+          else if (scheme == 2) r = (r + std::fabs(r)) / (1.0 + std::fabs(r) + small);
+          else r = std::max({0.0, std::min(1.0, 2.0 * r), std::min(2.0, r)});
+          pf = pc + 0.5 * r * (pd - pc);
+        }
         const double up = c > 0.0 ? pa : pb;
         cor = c_bl * c * (up - pf);
       }
@@ -739,6 +756,7 @@ void fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, cons
       rhs[(size_t)b * ncomp + k] -= cor;
     }
   }
+  return 0;
 }
 
 void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,

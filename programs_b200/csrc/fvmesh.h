@@ -128,17 +128,21 @@ int fvm_gradient_sweeps(const fvm_mesh *m, int ncomp, const double *phi, const d
                         int n_iter, int neu, double *grad);
 
 /* The explicit (deferred-correction) right-hand-side terms of the
- * reference's momentum face loop, central scheme (cfd_setup.f90:185-200,
- * 226-230, 306-328, c_sch = 0): per interior face
+ * reference's momentum face loop (cfd_setup.f90:185-272, 306-328): per
+ * interior face
  *   cor = c_bl c (phi_up - phi_f) + d ((phi_N' - phi_P') - (phi_N - phi_P)),
- * phi_P' = phi_P + g_P.dx_P at the auxiliary points, phi_f = w phi_N' +
- * (1-w) phi_P', phi_up the upwind cell value of the face mass flux c
- * (flux[f], owner -> neighbour), d = mu area / l_pn; rhs_P += cor and
- * rhs_N -= cor for each of the ncomp components (grad: 3 per component
- * per cell).  rhs is accumulated into, not cleared; the implicit part is
- * the matrix of fvm_assemble_momentum_field. */
-void fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, const double *grad,
-                           const double *flux, double mu, double c_bl, double *rhs);
+ * phi_P' = phi_P + g_P.dx_P at the auxiliary points, phi_up the upwind
+ * cell value of the face mass flux c (flux[f], owner -> neighbour),
+ * d = mu area / l_pn; rhs_P += cor and rhs_N -= cor for each of the ncomp
+ * components (grad: 3 per component per cell).  The face value phi_f is
+ * by `scheme` (the reference's c_sch): 0 central, w phi_N' + (1-w) phi_P';
+ * 1 min-mod, 2 van Leer, 3 superbee: with C the upwind and D the downwind
+ * auxiliary value and U = D - 2 g_C.(x_D' - x_C'), r = (C - U) / (D - C +
+ * small), phi_f = C + psi(r) (D - C) / 2.  rhs is accumulated into, not
+ * cleared; the implicit part is the matrix of fvm_assemble_momentum_field.
+ * Returns 0, or -1 for a scheme outside 0..3. */
+int fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, const double *grad,
+                          const double *flux, double mu, double c_bl, int scheme, double *rhs);
 
 /* Face mass fluxes from the momentum-predicted velocity with Rhie-Chow
  * pressure smoothing (cfd_setup.f90:615-634): F = rho area (u_f . n)

@@ -45,8 +45,10 @@ def _lib():
         lib.fvm_cavity_field.argtypes = [ctypes.c_void_p, ctypes.c_double, _f64p]
         lib.fvm_mesh_cache_geometry.argtypes = [ctypes.c_void_p]
         lib.fvm_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p]
+        lib.fvm_momentum_deferred.restype = ctypes.c_int
         lib.fvm_momentum_deferred.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p, _f64p,
-                                              ctypes.c_double, ctypes.c_double, _f64p]
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                              _f64p]
         lib.fvm_gradient_sweeps.restype = ctypes.c_int
         lib.fvm_gradient_sweeps.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p,
                                             ctypes.c_int, ctypes.c_int, _f64p]
@@ -271,18 +273,22 @@ def gradient_sweeps(mesh: "Mesh", phi: np.ndarray, n_iter: int = 2, neu: int = 2
 
 
 def momentum_deferred(mesh: "Mesh", u: np.ndarray, grad: np.ndarray, flux: np.ndarray,
-                      mu: float, c_bl: float = 1.0) -> np.ndarray:
-    """The reference's explicit momentum terms (central-scheme deferred
-    correction blended by c_bl, non-orthogonal diffusion correction,
-    cfd_setup.f90:185-328) for a cell field u (n_cell,) or (n_cell, k),
-    its gradient (as gradient_sweeps returns it) and the face mass fluxes;
-    returns the right-hand-side increments, shaped like u."""
+                      mu: float, c_bl: float = 1.0, scheme: int = 0) -> np.ndarray:
+    """The reference's explicit momentum terms (deferred correction toward
+    the face values of `scheme` -- 0 central, 1 min-mod, 2 van Leer,
+    3 superbee -- blended by c_bl, and the non-orthogonal diffusion
+    correction, cfd_setup.f90:185-328) for a cell field u (n_cell,) or
+    (n_cell, k), its gradient (as gradient_sweeps returns it) and the face
+    mass fluxes; returns the right-hand-side increments, shaped like u."""
     u = _c(u)
     k = 1 if u.ndim == 1 else u.shape[1]
     g = _c(grad).reshape(mesh.n_cell, k, 3)
     out = np.zeros((mesh.n_cell, k))
-    _lib().fvm_momentum_deferred(mesh._h, k, _p(u, _f64p), _p(g, _f64p), _p(_c(flux), _f64p),
-                                 float(mu), float(c_bl), _p(out, _f64p))
+    rc = _lib().fvm_momentum_deferred(mesh._h, k, _p(u, _f64p), _p(g, _f64p),
+                                      _p(_c(flux), _f64p), float(mu), float(c_bl), int(scheme),
+                                      _p(out, _f64p))
+    if rc != 0:
+        raise ValueError("momentum_deferred: scheme is 0 (central) .. 3 (superbee)")
     return out[:, 0].copy() if u.ndim == 1 else out
 
 

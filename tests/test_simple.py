@@ -198,6 +198,28 @@ def test_host_loop_with_the_reference_solvers_reduces_the_mass_imbalance():
     assert mass[-1] < 1e-3 * mass[0], mass
 
 
+def test_tvd_schemes_are_central_on_linear_fields_and_upwind_without_gradient():
+    """c_sch 1..3 (min-mod, van Leer, superbee, cfd_setup.f90:253-272): on a
+    linear field with its exact gradient the ratio r is 1 and every limiter
+    gives psi(1) = 1, the central face value; with zero gradients the
+    reconstructed upstream value equals the downwind one, r = -1, psi = 0,
+    and the face value is the upwind one (no correction)."""
+    from programs_b200.mesh import momentum_deferred
+    m = Mesh.hex(6, jitter=0.0, seed=2, permute=True)
+    xc, _ = m.cell_geom()
+    c = np.random.default_rng(3).normal(size=m.n_face)
+    phi = 2 * xc[:, 0] + xc[:, 2]
+    grad = np.tile([2.0, 0.0, 1.0], (m.n_cell, 1))
+    central = momentum_deferred(m, phi, grad, c, 0.0, scheme=0)
+    assert np.abs(central).max() > 1e-3
+    for scheme in (1, 2, 3):
+        assert np.abs(momentum_deferred(m, phi, grad, c, 0.0, scheme=scheme) - central).max() < 1e-13
+        assert np.abs(momentum_deferred(m, phi, 0 * grad, c, 0.0, scheme=scheme)).max() < 1e-15
+    assert np.abs(momentum_deferred(m, phi, 0 * grad, c, 0.0, scheme=0)).max() > 1e-3
+    with pytest.raises(ValueError):
+        momentum_deferred(m, phi, grad, c, 0.0, scheme=4)
+
+
 def test_mass_imbalance_sums_to_zero_in_a_closed_box():
     m = _mesh()
     u = cavity_field(m, 1.0)
