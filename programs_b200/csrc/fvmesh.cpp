@@ -54,6 +54,10 @@ struct fvm_mesh {
   std::vector<V3> xc;              // cell centres
   int n_cell = 0;
   int n_bface = 0;
+  // face distance and interpolation weight: false = along the face normal
+  // between the auxiliary points (the linear weight), true = the
+  // reference's centre distance and 1 - |x_f - x_P| / l_pn
+  bool ref_weights = false;
   // optional cache of the face geometry (9 doubles per face) and volumes,
   // for repeated assembly on one mesh (fvm_mesh_cache_geometry)
   std::vector<double> geo, vol_cache;
@@ -120,7 +124,10 @@ struct fvm_mesh {
     xf = (v[0] + v[1] + v[2] + v[3]) * 0.25;
     V3 xp_aux = xf - nrm * dot(xf - xc[c], nrm);
     int nb = f_in[f];
-    if (nb >= 0) {
+    if (ref_weights) {  // cfd_grid.f90:520, 524, 534
+      l_pn = nb >= 0 ? mag(xc[nb] - xc[c]) : mag(xf - xc[c]);
+      w_fp = nb >= 0 ? 1.0 - mag(xf - xc[c]) / l_pn : 1.0;
+    } else if (nb >= 0) {
       V3 xn_aux = xf - nrm * dot(xf - xc[nb], nrm);
       l_pn = mag(xn_aux - xp_aux);
       w_fp = mag(xf - xp_aux) / l_pn;
@@ -306,6 +313,13 @@ void fvm_mesh_face_geom(const fvm_mesh *m, double *s, double *nrm, double *xf,
     if (l_pn) l_pn[f] = l;
     if (w_fp) w_fp[f] = w;
   }
+}
+
+void fvm_mesh_set_face_weights(fvm_mesh *m, int reference) {
+  const bool cached = !m->geo.empty();
+  m->ref_weights = reference != 0;
+  m->geo.clear();
+  if (cached) fvm_mesh_cache_geometry(m);
 }
 
 void fvm_mesh_cache_geometry(fvm_mesh *m) {

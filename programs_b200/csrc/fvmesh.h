@@ -50,6 +50,13 @@ void fvm_mesh_face_geom(const fvm_mesh *m, double *s, double *nrm, double *xf,
  * face / cell) so repeated assemblies on one mesh skip the geometry;
  * dropped by renumbering. */
 void fvm_mesh_cache_geometry(fvm_mesh *m);
+/* Which face distance l_pn and interpolation weight w_fp (on phi_N) the
+ * geometry reports, and with it every assembly: 0 (default) the distance
+ * between the two auxiliary points on the face normal and the linear
+ * weight |x_f - x_P,aux| / l_pn; 1 the reference's centre distance
+ * |x_N - x_P| and w_fp = 1 - |x_f - x_P| / l_pn (cfd_grid.f90:520, 524;
+ * boundary faces |x_f - x_P|, :534).  Both agree on regular meshes. */
+void fvm_mesh_set_face_weights(fvm_mesh *m, int reference);
 
 /* Cell centres (3 per cell) and volumes (either may be NULL). */
 void fvm_mesh_cell_geom(const fvm_mesh *m, double *xc, double *vol);

@@ -44,6 +44,7 @@ def _lib():
         lib.fvm_uniform.argtypes = [ctypes.c_uint64, ctypes.c_int64, _f64p]
         lib.fvm_cavity_field.argtypes = [ctypes.c_void_p, ctypes.c_double, _f64p]
         lib.fvm_mesh_cache_geometry.argtypes = [ctypes.c_void_p]
+        lib.fvm_mesh_set_face_weights.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.fvm_gradient.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p]
         lib.fvm_momentum_deferred.restype = ctypes.c_int
         lib.fvm_momentum_deferred.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, _f64p, _f64p,
@@ -176,6 +177,13 @@ class Mesh:
     def cache_geometry(self) -> None:
         """Keep face geometry and volumes for repeated assembly on this mesh."""
         self._lib.fvm_mesh_cache_geometry(self._h)
+
+    def set_face_weights(self, reference: bool) -> None:
+        """Face distance and interpolation weight of every assembly: False
+        (default) along the face normal between the auxiliary points, with
+        the linear weight; True the reference's centre distance and
+        w_fp = 1 - |x_f - x_P| / l_pn (cfd_grid.f90:520, 524)."""
+        self._lib.fvm_mesh_set_face_weights(self._h, 1 if reference else 0)
 
     def permute(self, perm: np.ndarray) -> None:
         """Apply a given permutation (new 1-based index of old cell i)."""

@@ -202,3 +202,36 @@ def test_uneven_batch_generator():
     assert all(np.array_equal(A.p, A.n) and b.shape == (A.n_cell,) for A, b in zip(mats, rhs))
     again, _ = batch_meshes(8, 27, 4000, seed=1)
     assert [A.n_cell for A in again] == sizes and np.array_equal(again[3].p, mats[3].p)
+
+
+def test_reference_face_weights_option():
+    """set_face_weights(True) reports the reference's l_pn = |x_N - x_P| and
+    w_fp = 1 - |x_f - x_P| / l_pn (cfd_grid.f90:520, 524; boundary faces
+    |x_f - x_P|, :534), cached or not; both definitions agree on a regular
+    mesh, and switching back restores the default exactly."""
+    m = Mesh.hex(6, jitter=0.2, seed=5, permute=True)
+    xc, _ = m.cell_geom()
+    ip, inb = m.faces()
+    base = m.face_geom()
+    m.cache_geometry()
+    m.set_face_weights(True)
+    s, nrm, xf, l, w = m.face_geom()
+    inner = inb > 0
+    P = xc[ip - 1]
+    N = xc[np.maximum(inb, 1) - 1]
+    lr = np.where(inner, np.linalg.norm(N - P, axis=1), np.linalg.norm(xf - P, axis=1))
+    assert np.allclose(l, lr, rtol=1e-14, atol=0)
+    assert np.allclose(w[inner], 1 - np.linalg.norm(xf - P, axis=1)[inner] / lr[inner],
+                       rtol=1e-14, atol=1e-15)
+    assert np.array_equal(s, base[0]) and np.array_equal(xf, base[2])
+    assert not np.allclose(l, base[3])                     # skew: the definitions differ
+    A = m.pressure(pin=1)
+    assert np.array_equal(A.p, A.n)
+    m.set_face_weights(False)
+    back = m.face_geom()
+    assert all(np.array_equal(x, y) for x, y in zip(back, base))
+    r = Mesh.hex(5, jitter=0.0, seed=1, permute=True)
+    g0 = r.face_geom()
+    r.set_face_weights(True)
+    g1 = r.face_geom()
+    assert np.allclose(g0[3], g1[3], rtol=1e-14) and np.allclose(g0[4], g1[4], rtol=1e-13)
