@@ -25,20 +25,26 @@ import time
 
 import numpy as np
 
-from .mesh import (Mesh, face_flux, gradient, mass_imbalance, momentum_field,
-                   pressure_correction, simple_correct)
+from .mesh import (Mesh, face_flux, gradient, gradient_sweeps, mass_imbalance,
+                   momentum_deferred, momentum_field, pressure_correction, simple_correct)
 from .solver import GpuSolver, OPT_PRECISION
 
 
 def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15, seed=0,
         p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None, p_imat=1,
-        m_precision=0, device=0, log_every=0, make_solver=None):
+        m_precision=0, device=0, log_every=0, make_solver=None, reference_terms=False):
     """Returns (u (N,3), p (N,), history, timings).  learned: weights array
     (FCG with the learned preconditioner for the pressure correction) or
     None (plain FP64 PCG with imat p_imat).  make_solver(device) builds the
     two solver contexts (default GpuSolver); anything with the same
     matrix_set / matrix_values / solv_cg / solv_bicg / set_option / close
-    methods can stand in."""
+    methods can stand in.  reference_terms adds what the reference's
+    assembly has beyond the implicit terms: gradients by n_grad = 2
+    corrected sweeps (cfd_solve.f90:38) with the velocity's wall values
+    (neu = 0, cfd_setup.f90:124) and extrapolated pressure walls (neu = 2,
+    :689, 754), and the explicit momentum terms (central deferred
+    correction, non-orthogonal diffusion correction, :185-328).  Host
+    assembly only: run_device has the implicit terms."""
     rho = 1.0
     mu = rho * u_lid * 1.0 / re
     m = Mesh.hex(size, jitter=jitter, seed=seed, permute=True)
@@ -49,6 +55,14 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
     u = np.zeros((N, 3))
     p = np.zeros(N)
     F = None
+    if reference_terms:
+        _, nrm, xf, _, _ = m.face_geom()
+        _, inb = m.faces()
+        wall_u = np.zeros((m.n_face, 3))  # no-slip walls, the y = 1 lid moving
+        wall_u[(inb == 0) & (nrm[:, 1] > 0.9) & (xf[:, 1] > 1.0 - 1e-9), 0] = u_lid
+        grad_p = lambda q: gradient_sweeps(m, q, 2, 2)
+    else:
+        grad_p = lambda q: gradient(m, q)
     factory = make_solver or GpuSolver
     sm = factory(device)
     sp = factory(device)
@@ -60,11 +74,13 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
     t0 = time.time()
     for k in range(n_outer):
         ta = time.time()
-        gradp = gradient(m, p)
+        gradp = grad_p(p)
         M, rhs, Fm = momentum_field(m, u, flux=F, rho=rho, mu=mu, u_lid=u_lid, urf=urf_u)
         if F is None:
             F = Fm
         rhs -= gradp * vol[:, None]
+        if reference_terms:
+            rhs += momentum_deferred(m, u, gradient_sweeps(m, u, 2, 0, wall_u), F, mu)
         t_asm += time.time() - ta
         ts = time.time()
         if k == 0:
@@ -96,7 +112,7 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
             stp = sp.solv_cg(p_imat, p_reduc, p_iter, pp, res0, rn_p, not_r0=True)
         t_solve_p += time.time() - ts
         ta = time.time()
-        gradpp = gradient(m, pp[:, 0])
+        gradpp = grad_p(pp[:, 0])
         simple_correct(m, pp[:, 0].copy(), gradpp, M.pl, rho, urf_p, u, p, F)
         t_asm += time.time() - ta
         rec = {"it": k, "mass": float(imb), "mom_res0": rn_m.tolist(), "p_iters": stp["iters"][0],
