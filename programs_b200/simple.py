@@ -32,7 +32,8 @@ from .solver import GpuSolver, OPT_PRECISION
 
 def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15, seed=0,
         p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None, p_imat=1,
-        m_precision=0, device=0, log_every=0, make_solver=None, reference_terms=False):
+        m_precision=0, device=0, log_every=0, make_solver=None, reference_terms=False,
+        reference_weights=False):
     """Returns (u (N,3), p (N,), history, timings).  learned: weights array
     (FCG with the learned preconditioner for the pressure correction) or
     None (plain FP64 PCG with imat p_imat).  make_solver(device) builds the
@@ -44,11 +45,15 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
     (neu = 0, cfd_setup.f90:124) and extrapolated pressure walls (neu = 2,
     :689, 754), and the explicit momentum terms (central deferred
     correction, non-orthogonal diffusion correction, :185-328).  Host
-    assembly only: run_device has the implicit terms."""
+    assembly only: run_device has the implicit terms.  reference_weights
+    takes the reference's face distance and interpolation weight
+    (Mesh.set_face_weights)."""
     rho = 1.0
     mu = rho * u_lid * 1.0 / re
     m = Mesh.hex(size, jitter=jitter, seed=seed, permute=True)
     m.renumber(Mesh.RCM)
+    if reference_weights:
+        m.set_face_weights(True)
     m.cache_geometry()
     N = m.n_cell
     _, vol = m.cell_geom()
@@ -129,7 +134,7 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
 
 def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15,
                seed=0, p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None,
-               p_imat=1, m_precision=0, device=0, log_every=0):
+               p_imat=1, m_precision=0, device=0, log_every=0, reference_weights=False):
     """The same outer loop with everything on the GPU: assembly, gradients,
     fluxes and corrections by the fv_gpu kernels (bit-for-bit the host
     functions), solves through the device-pointer entry points; only the
@@ -143,6 +148,8 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
     mu = rho * u_lid * 1.0 / re
     m = Mesh.hex(size, jitter=jitter, seed=seed, permute=True)
     m.renumber(Mesh.RCM)
+    if reference_weights:
+        m.set_face_weights(True)
     m.cache_geometry()
     N = m.n_cell
     ip, inb = m.faces()
@@ -245,10 +252,19 @@ def main(argv=None):
     ap.add_argument("--p-imat", type=int, default=1, help="plain pressure PCG: 0 Jacobi, 1 DIC")
     ap.add_argument("--m-reduc", type=float, default=0.1)
     ap.add_argument("--m-iter", type=int, default=5)
+    ap.add_argument("--reference-terms", action="store_true",
+                    help="host assembly with the reference's explicit momentum terms and "
+                         "corrected gradients")
+    ap.add_argument("--reference-weights", action="store_true",
+                    help="the reference's face distance and interpolation weight")
     a = ap.parse_args(argv)
+    if a.reference_terms and a.device_assembly:
+        ap.error("--reference-terms is host assembly only")
     loop = run_device if a.device_assembly else run
     kw = dict(p_reduc=a.p_reduc, p_iter=a.p_iter, p_imat=a.p_imat, m_reduc=a.m_reduc,
-              m_iter=a.m_iter, log_every=a.log_every)
+              m_iter=a.m_iter, log_every=a.log_every, reference_weights=a.reference_weights)
+    if a.reference_terms:
+        kw["reference_terms"] = True
     u0, p0, h0, t0 = loop(a.size, a.outer, a.re, **kw)
     out = {"size": a.size, "outer": a.outer, "re": a.re, "p_reduc": a.p_reduc,
            "p_imat": a.p_imat, "plain": t0, "final_mass_plain": h0[-1]["mass"],

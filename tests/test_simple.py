@@ -237,6 +237,10 @@ def test_host_loop_with_the_reference_explicit_terms():
     assert mass[-1] < 1e-2 * mass[0], mass
     rel = np.linalg.norm(u1 - u0) / np.linalg.norm(u0)
     assert 1e-4 < rel < 0.5, rel
+    u2, _, hist2, _ = simple.run(reference_terms=True, reference_weights=True, **kw)
+    mass2 = [h["mass"] for h in hist2]
+    assert np.all(np.isfinite(u2)) and mass2[-1] < 1e-2 * mass2[0], mass2
+    assert not np.array_equal(u2, u1)            # the weights differ on the skewed mesh
 
 
 def test_mass_imbalance_sums_to_zero_in_a_closed_box():
