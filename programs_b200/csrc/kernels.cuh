@@ -641,7 +641,8 @@ __global__ void SG_BOUNDS(V) k_cg_p(SegMap sm, const T* __restrict__ c, const T*
   }
 }
 
-// q = A p and p.q; alpha = s / (p.q + small)   (solv_cg.f90:56-68)
+// q = A p and p.q; alpha = s / (p.q + small)   (solv_cg.f90:56-68; the FP32
+// instantiation divides without the guard, div0)
 template <typename T, int V>
 __global__ void SG_BOUNDS(V) k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
                           double* __restrict__ part, Lane* __restrict__ lanes) {
@@ -740,7 +741,8 @@ __global__ void SG_BOUNDS(V) k_cg_update(SegMap sm, const T* __restrict__ c, T* 
 }
 
 // ===================== BiCGSTAB: solv_bicg.f90:27-118 ======================
-// rho = r.r0; omeg = rho*gam/(alpha*beta0+small); beta0 = rho  (:48-50)
+// rho = r.r0; omeg = rho*gam/(alpha*beta0+small); beta0 = rho  (:48-50;
+// FP32 without the guard, div0)
 template <typename T, int V>
 __global__ void SG_BOUNDS(V) k_bi_rho(SegMap sm, const T* __restrict__ r, const T* __restrict__ r0,
                          double* __restrict__ part, Lane* __restrict__ lanes) {
@@ -805,6 +807,7 @@ __global__ void SG_BOUNDS(V) k_bi_p(SegMap sm, const T* __restrict__ c, const T*
 
 // y = A z, and dots: MODE 0 -> y.r0 (gam = rho/(y.r0+small), :72-73)
 //                    MODE 1 -> y.r, y.y (alpha = (y.r)/(y.y+small), :98-100)
+// (FP32: the same quotients without the guard, div0)
 template <typename T, int V, int MODE>
 __global__ void SG_BOUNDS(V) k_bi_spmv(Rows<T> R, SegMap sm, const T* __restrict__ z, T* __restrict__ y,
                           const T* __restrict__ w, double* __restrict__ part,
