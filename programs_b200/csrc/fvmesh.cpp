@@ -206,40 +206,66 @@ fvm_mesh *fvm_mesh_read_neu(const char *path) {
   if (!in) return nullptr;
   auto *m = new fvm_mesh();
   std::string line;
-  int n_vrt = 0, n_vol = 0;
+  int n_vrt = 0, n_vol = 0, dim = 3;
   bool ok_sizes = false;
   while (std::getline(in, line)) {
     if (line.find("NUMNP") != std::string::npos) {
       std::getline(in, line);
       std::istringstream ss(line);
-      ss >> n_vrt >> n_vol;
+      int n_grp = 0, n_bset = 0, ndfcd = 3;
+      ss >> n_vrt >> n_vol >> n_grp >> n_bset >> ndfcd;
+      dim = ndfcd == 2 ? 2 : 3;
       ok_sizes = n_vrt > 0 && n_vol > 0;
     } else if (line.find("NODAL COORDINATES") != std::string::npos && ok_sizes) {
-      m->vert.resize(n_vrt);
+      // a 2-d mesh gets a second copy of its nodes one unit deep
+      m->vert.resize((size_t)n_vrt * (dim == 2 ? 2 : 1));
       for (int i = 0; i < n_vrt; ++i) {
         int idx;
-        double x, y, z;
-        in >> idx >> x >> y >> z;
+        double x, y, z = 0.0;
+        in >> idx >> x >> y;
+        if (dim == 3) in >> z;
         if (!in || idx < 1 || idx > n_vrt) { delete m; return nullptr; }
         m->vert[idx - 1] = {x, y, z};
+        if (dim == 2) m->vert[(size_t)n_vrt + idx - 1] = {x, y, 1.0};
       }
     } else if (line.find("ELEMENTS/CELLS") != std::string::npos && ok_sizes) {
       m->n_cell = n_vol;
       m->cell_vert.resize((size_t)n_vol * 8);
       std::vector<char> seen(n_vol, 0);
+      const int want_ty = dim == 2 ? 2 : 4, want_nv = dim == 2 ? 4 : 8;
       for (int e = 0; e < n_vol; ++e) {
         int idx, ty, nv;
         in >> idx >> ty >> nv;
-        if (!in || ty != 4 || nv != 8 || idx < 1 || idx > n_vol || seen[idx - 1]) {
-          delete m;  // only brick elements, each numbered once
+        if (!in || ty != want_ty || nv != want_nv || idx < 1 || idx > n_vol || seen[idx - 1]) {
+          delete m;  // bricks (3-d) or quadrilaterals (2-d), each numbered once
           return nullptr;
         }
         seen[idx - 1] = 1;
-        for (int v = 0; v < 8; ++v) {
-          int g;
-          in >> g;
-          if (!in || g < 1 || g > n_vrt) { delete m; return nullptr; }
-          m->cell_vert[(size_t)(idx - 1) * 8 + v] = g - 1;
+        int g[8];
+        for (int v = 0; v < nv; ++v) {
+          in >> g[v];
+          if (!in || g[v] < 1 || g[v] > n_vrt) { delete m; return nullptr; }
+          g[v] -= 1;
+        }
+        int32_t *cv = &m->cell_vert[(size_t)(idx - 1) * 8];
+        if (dim == 3) {
+          for (int v = 0; v < 8; ++v) cv[v] = g[v];
+        } else {
+          // the quadrilateral n1..n4 (in order around it) as the brick one
+          // unit deep in the brick's vertex order (x fastest): counter-
+          // clockwise seen from +z so that the brick's volume is positive
+          if (m->vert.size() < (size_t)2 * n_vrt) { delete m; return nullptr; }
+          double a2 = 0.0;
+          for (int v = 0; v < 4; ++v) {
+            const V3 p = m->vert[g[v]], q = m->vert[g[(v + 1) & 3]];
+            a2 += p.x * q.y - q.x * p.y;
+          }
+          if (a2 < 0.0) std::swap(g[1], g[3]);
+          const int lo[4] = {g[0], g[1], g[3], g[2]};
+          for (int v = 0; v < 4; ++v) {
+            cv[v] = lo[v];
+            cv[v + 4] = lo[v] + n_vrt;
+          }
         }
       }
     }

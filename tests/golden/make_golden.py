@@ -7,6 +7,9 @@
   solv_cg / solv_bicg outputs for imat = 0, 1, 2 together with a scipy
   sparse direct solution.  Reading the .neu needs the reference checkout,
   so this part only runs where it is present.
+* channel_2d.npz -- the same for the reference's 2-d mesh
+  (spray-simulation/channel_2d.neu, 1 554 quadrilaterals, read one unit
+  deep).
 * hex6.npz -- a 6x6x6 jittered, permuted hex mesh (seed 0): pressure and
   momentum matrices with the same set of outputs (3 right-hand sides for
   the momentum solve).
@@ -15,7 +18,7 @@ The tests re-run the oracle on the stored matrices and require the stored
 outputs bit for bit, check the solutions against the stored scipy solves,
 and run the GPU solvers against the same outputs.
 
-Usage: python tests/golden/make_golden.py [path/to/cavity_3d.neu]
+Usage: python tests/golden/make_golden.py [path/to/cavity_3d.neu [path/to/channel_2d.neu]]
 """
 from __future__ import annotations
 
@@ -32,8 +35,9 @@ from oracle.oracle import Oracle  # noqa: E402
 from programs_b200 import build  # noqa: E402
 from programs_b200.mesh import Mesh, poisson_rhs, uniform  # noqa: E402
 
-# where the reference checkout keeps the mesh it ships
+# where the reference checkout keeps the meshes it ships
 DEFAULT_NEU = "/root/reference/spray-simulation/cavity_3d.neu"
+DEFAULT_NEU_2D = "/root/reference/spray-simulation/channel_2d.neu"
 REDUC = 1e-10
 N_ITER = 5000
 
@@ -84,6 +88,19 @@ def cavity(path: str, outdir: str = HERE) -> None:
     print("cavity_3d:", A.n_cell, "cells", A.n_face, "faces")
 
 
+def channel(path: str, outdir: str = HERE) -> None:
+    """The reference's 2-d mesh (1 554 quadrilaterals, read one unit deep)."""
+    m = Mesh.read_neu(path)
+    A = m.pressure(pin=1)
+    b = np.asfortranarray(poisson_rhs(A.n_cell, 11).reshape(-1, 1))
+    out = {}
+    _matrix(A, "", out)
+    out["b"] = b
+    _solves(A, b, "", out, solvers=("cg",))
+    np.savez_compressed(os.path.join(outdir, "channel_2d.npz"), **out)
+    print("channel_2d:", A.n_cell, "cells", A.n_face, "faces")
+
+
 def hex6(outdir: str = HERE) -> None:
     m = Mesh.hex(6, jitter=0.15, seed=0, permute=True)
     P = m.pressure(pin=1)
@@ -109,3 +126,8 @@ if __name__ == "__main__":
         cavity(neu)
     else:
         print("cavity_3d.neu not found; cavity_3d.npz left as is")
+    neu2 = sys.argv[2] if len(sys.argv) > 2 else DEFAULT_NEU_2D
+    if os.path.exists(neu2):
+        channel(neu2)
+    else:
+        print("channel_2d.neu not found; channel_2d.npz left as is")

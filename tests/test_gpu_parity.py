@@ -348,10 +348,12 @@ def test_matrix_without_interior_faces(gpu, N, F):
 
 
 @pytest.mark.parametrize("fname,prefix,solvers", [("cavity_3d.npz", "", ("cg",)),
+                                                  ("channel_2d.npz", "", ("cg",)),
                                                   ("hex6.npz", "p_", ("cg", "bicg")),
                                                   ("hex6.npz", "m_", ("bicg",))])
 def test_golden_fixtures(gpu, fname, prefix, solvers):
-    """The committed fixtures (the reference's own cavity_3d mesh among them)."""
+    """The committed fixtures (the reference's own cavity_3d and channel_2d
+    meshes among them)."""
     import os
     from programs_b200.mesh import FaceMatrix
     d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", fname))

@@ -235,3 +235,59 @@ def test_reference_face_weights_option():
     r.set_face_weights(True)
     g1 = r.face_geom()
     assert np.allclose(g0[3], g1[3], rtol=1e-14) and np.allclose(g0[4], g1[4], rtol=1e-13)
+
+
+def _write_neu_2d(path, nx, ny, jitter=0.0, seed=0):
+    """A 2-d Gambit neutral file (NDFCD = 2) of an nx x ny block of
+    quadrilaterals, every other one listed clockwise."""
+    rng = np.random.default_rng(seed)
+    node = lambda i, j: 1 + i + (nx + 1) * j
+    xy = np.array([[i, j] for j in range(ny + 1) for i in range(nx + 1)], float)
+    inner = (xy[:, 0] > 0) & (xy[:, 0] < nx) & (xy[:, 1] > 0) & (xy[:, 1] < ny)
+    xy[inner] += rng.uniform(-jitter, jitter, (inner.sum(), 2))
+    quads = []
+    for j in range(ny):
+        for i in range(nx):
+            q = [node(i, j), node(i + 1, j), node(i + 1, j + 1), node(i, j + 1)]
+            quads.append(q if (i + j) % 2 == 0 else q[::-1])
+    with open(path, "w") as f:
+        f.write("        CONTROL INFO 2.3.16\n** GAMBIT NEUTRAL FILE\nquads\n")
+        f.write("     NUMNP     NELEM     NGRPS    NBSETS     NDFCD     NDFVL\n")
+        f.write(f"{len(xy):10d}{len(quads):10d}         1         0         2         2\n")
+        f.write("ENDOFSECTION\n   NODAL COORDINATES 2.3.16\n")
+        for q, (x, y) in enumerate(xy):
+            f.write(f"{q + 1:10d}{x:20.11e}{y:20.11e}\n")
+        f.write("ENDOFSECTION\n      ELEMENTS/CELLS 2.3.16\n")
+        for e, q in enumerate(quads):
+            f.write(f"{e + 1:8d}  2  4 " + " ".join(f"{v:7d}" for v in q) + "\n")
+        f.write("ENDOFSECTION\n")
+    return xy, quads
+
+
+def test_gambit_reader_extrudes_2d_quadrilaterals(tmp_path):
+    """A 2-d file (NDFCD = 2, quadrilaterals) becomes one layer of bricks
+    one unit deep -- the reference's 2-d convention, face area = edge
+    length, volume = area -- whichever way round each quad is listed; the
+    cells couple exactly where quads share an edge."""
+    nx, ny = 5, 4
+    p = str(tmp_path / "quads.neu")
+    xy, quads = _write_neu_2d(p, nx, ny, jitter=0.2, seed=2)
+    m = Mesh.read_neu(p)
+    n_cell, n_face, n_bface, _ = m.sizes()
+    assert n_cell == nx * ny
+    assert n_face - n_bface == (nx - 1) * ny + nx * (ny - 1)
+    assert n_bface == 2 * n_cell + 2 * (nx + ny)
+    xc, vol = m.cell_geom()
+    area = [0.5 * abs(sum(xy[q[k] - 1, 0] * xy[q[(k + 1) % 4] - 1, 1] -
+                          xy[q[(k + 1) % 4] - 1, 0] * xy[q[k] - 1, 1] for k in range(4)))
+            for q in quads]
+    assert vol.min() > 0 and np.allclose(vol, area, rtol=1e-12)
+    assert np.allclose(xc[:, 2], 0.5)
+    ip, inb = m.faces()
+    got = {(int(a), int(b)) for a, b in zip(ip, inb) if b > 0}
+    edges = [{frozenset((q[k], q[(k + 1) % 4])) for k in range(4)} for q in quads]
+    want = {(a + 1, b + 1) for a in range(len(quads)) for b in range(a + 1, len(quads))
+            if edges[a] & edges[b]}
+    assert got == want
+    A = m.pressure(pin=1)
+    assert np.array_equal(A.p, A.n) and np.all(A.pl > 0)

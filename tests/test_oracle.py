@@ -39,8 +39,8 @@ def _rel(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
 
 
-GOLDEN = [("cavity_3d.npz", "", ("cg",)), ("hex6.npz", "p_", ("cg", "bicg")),
-          ("hex6.npz", "m_", ("bicg",))]
+GOLDEN = [("cavity_3d.npz", "", ("cg",)), ("channel_2d.npz", "", ("cg",)),
+          ("hex6.npz", "p_", ("cg", "bicg")), ("hex6.npz", "m_", ("bicg",))]
 
 
 @pytest.mark.parametrize("fname,prefix,solvers", GOLDEN)
@@ -79,6 +79,19 @@ def test_cavity_fixture_matches_reader():
     assert np.all(inb[inb > 0] > ip[inb > 0])
     assert np.all(np.diff(ip) >= 0)
     assert (inb == 0).sum() == 150
+
+
+def test_channel_fixture_matches_reader():
+    """The reference's 2-d mesh (1 554 quadrilaterals) read one unit deep:
+    every quad edge is an interior face or a wall, and the front and back
+    of each cell are boundary faces (4 N = 2 interior + walls)."""
+    d = _load("channel_2d.npz")
+    ip, inb = d["ip"], d["inb"]
+    N = int(d["n_cell"])
+    n_int = int((inb > 0).sum())
+    walls = int((inb == 0).sum()) - 2 * N
+    assert N == 1554 and 4 * N == 2 * n_int + walls and walls > 0
+    assert np.all(inb[inb > 0] > ip[inb > 0]) and np.all(np.diff(ip) >= 0)
 
 
 @pytest.mark.parametrize("imat", [-1, 0, 1, 2, 3])
@@ -217,6 +230,9 @@ def test_fixtures_regenerate_bit_for_bit(tmp_path):
     if os.path.exists(neu):
         mg.cavity(neu, str(tmp_path))
         names.append("cavity_3d.npz")
+    if os.path.exists(mg.DEFAULT_NEU_2D):
+        mg.channel(mg.DEFAULT_NEU_2D, str(tmp_path))
+        names.append("channel_2d.npz")
     for name in names:
         new, old = np.load(str(tmp_path / name)), _load(name)
         assert sorted(new.files) == sorted(old.files), name
