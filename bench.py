@@ -187,19 +187,23 @@ def _traffic_from_profile(name):
     return None
 
 
-def cpu_baseline(A, b, iters_full, budget_s=15.0):
-    """Oracle plain PCG (single core: the reference is serial) on a bounded sample."""
+def cpu_baseline(A, b, iters_full, budget_s=15.0, repeats=3):
+    """Oracle plain PCG (single core: the reference is serial) on bounded
+    samples: the median over `repeats` runs of s iterations each, scaled to
+    the full solve.  Returns (s/solve, s, total seconds timed)."""
     from oracle.oracle import Oracle
     o = Oracle.from_matrix(A)
     rhs = b.reshape(-1, 1)
     t = time.perf_counter()
     o.solv_cg(0, 1e-10, 2, np.zeros((A.n_cell, 1)), rhs)
     per = (time.perf_counter() - t) / 2
-    s = max(2, min(200, int(budget_s / max(per, 1e-6))))
-    t = time.perf_counter()
-    o.solv_cg(0, 1e-10, s, np.zeros((A.n_cell, 1)), rhs)
-    dt = time.perf_counter() - t
-    return dt / s * iters_full, s, dt
+    s = max(2, min(200, int(budget_s / repeats / max(per, 1e-6))))
+    runs = []
+    for _ in range(repeats):
+        t = time.perf_counter()
+        o.solv_cg(0, 1e-10, s, np.zeros((A.n_cell, 1)), rhs)
+        runs.append(time.perf_counter() - t)
+    return statistics.median(runs) / s * iters_full, s, sum(runs)
 
 
 def _config(args, A):
@@ -420,8 +424,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         v, sample, dt = cpu_baseline(A, b, st_plain["iters"][0])
         cpu = {"value": v, "unit": "s/solve", "cores": 1, "kind": "port",
-               "sample": f"{sample} oracle PCG iterations ({dt:.1f} s, single core) of this "
-                         f"system, scaled to the {st_plain['iters'][0]}-iteration plain solve",
+               "sample": f"median of 3 runs of {sample} oracle PCG iterations ({dt:.1f} s in "
+                         f"all, single core) of this system, scaled to the "
+                         f"{st_plain['iters'][0]}-iteration plain solve",
                **host_cpu()}
 
     if rank == 0:

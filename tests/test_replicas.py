@@ -92,3 +92,15 @@ def test_clock_sampler_reads_nvidia_smi_lines(line, reasons):
     s = c.summary()
     assert s["samples"] == 2 and s["reasons"] == reasons
     assert s["sm_mhz"] == float(line.split(",")[1]) and s["sm_max_mhz"] == 1965.0
+
+
+def test_cpu_baseline_is_a_median_of_bounded_samples(built):
+    """bench.cpu_baseline: the oracle's plain PCG timed as the median of
+    three bounded runs, scaled to the full solve's iteration count."""
+    import bench
+    from programs_b200.mesh import Mesh, poisson_rhs
+    A = Mesh.hex(10, jitter=0.15, seed=0, permute=True).pressure(pin=1)
+    b = poisson_rhs(A.n_cell, 1)
+    v, s, total = bench.cpu_baseline(A, b, 1000, budget_s=0.3)
+    assert v > 0 and 2 <= s <= 200 and total > 0
+    assert v < 1000 * total          # per-iteration time times 1000, not more
