@@ -101,6 +101,16 @@ extern "C" {
                                    Jacobi), 0 = damped Jacobi (no network) */
 #define SOLV_OPT_MG_OMEGA 12    /* smoother damping (default 0.8)          */
 #define SOLV_OPT_MG_ALPHA 13    /* coarse-correction scale (default 2)     */
+#define SOLV_OPT_FCG_STALL_ITERS 14 /* learned preconditioner: iterations
+                                   without the residual falling below
+                                   SOLV_OPT_FCG_STALL_DROP times its value
+                                   at the start of the window after which
+                                   Jacobi-PCG takes over (default 100)     */
+#define SOLV_OPT_FCG_STALL_DROP 15 /* the drop a window must reach
+                                   (default 0.5)                           */
+#define SOLV_OPT_MG_SCALE_MIN 16 /* floor on the network's per-cell scales
+                                   (default 0.5; 0 leaves them as the
+                                   network makes them)                     */
 
 typedef struct solv_gpu_ctx solv_gpu_ctx;
 
@@ -202,8 +212,10 @@ int solv_gpu_kernel_time(solv_gpu_ctx *ctx, int which, int repeat,
  * SOLV_OPT_MG_LEVELS 0 uses K alone).  Each solve bounds the smoother:
  * per-cell scales are held at 0.5 or more and K is scaled so that eight
  * power iterations find lambda_max(omega K A) <= 1.9.  If
- * the iteration loses positive curvature or produces NaN, plain Jacobi-PCG
- * takes over from the current iterate (stats.fallbacks); the FP64 residual
+ * the iteration loses positive curvature or produces NaN, or its residual
+ * stalls (SOLV_OPT_FCG_STALL_*, or the FP64 residual fails to improve by
+ * 10% over three reliable updates), plain Jacobi-PCG takes over from the
+ * current iterate (stats.fallbacks); the FP64 residual
  * test |b - A x|_1 / |r0|_1 < reduc decides convergence either way.  Same
  * argument meaning as solv_gpu_cg with imat ignored, n_vc = 1, one system;
  * the matrix must be symmetric (the pressure system). */
@@ -317,10 +329,13 @@ int solv_gpu_bicg_batch_dev(solv_gpu_ctx *ctx, int imat, double reduc,
  * before any stream capture.  Calls overlapping on the GPU share that
  * scratch and race.  The scratch's counters are cleared by every call;
  * nothing the caller passes must start at zero (res0_n is overwritten).
- * Limits: n_vc <= 4 (SOLV_GPU_TOO_LARGE beyond).
- * Face contributions are added with atomics, so r agrees with solv_res to
- * rounding, not bit for bit.  Returns SOLV_GPU_BAD_INPUT if a face index is
- * out of range. */
+ * Limits: n_vc <= 4 (SOLV_GPU_TOO_LARGE beyond; n_vc < 1 is
+ * SOLV_GPU_BAD_INPUT).  Face contributions are added with atomics, so r
+ * agrees with solv_res to rounding, not bit for bit.  Face indices are
+ * checked on the GPU before res0 is written: if one is out of range the
+ * call returns SOLV_GPU_BAD_INPUT and res0, res0_n are left unchanged.  A
+ * launch error still pending from the caller's earlier work is cleared at
+ * entry and not reported as this call's. */
 int solv_gpu_res_noalloc(int n_cell, int n_face, const int *ip_dev,
                          const int *in_dev, const double *p_dev,
                          const double *n_dev, const double *pl_dev, int n_vc,

@@ -38,13 +38,22 @@ def make_system(size, system="pressure", seed=0, renumber="rcm"):
     return A, b
 
 
-def batch_meshes(n_sys, lo, hi, seed=1):
-    """n_sys pressure systems with log-uniform cell counts in [lo, hi]."""
+def batch_sizes(n_sys, lo, hi, seed=1):
+    """Edge lengths of the n_sys hex meshes with log-uniform cell counts in
+    [lo, hi] (seeded)."""
     rng = np.random.default_rng(seed)
     cells = np.exp(rng.uniform(np.log(lo), np.log(hi), n_sys))
+    return [max(2, int(round(nc ** (1.0 / 3.0)))) for nc in cells]
+
+
+def batch_meshes(n_sys, lo, hi, seed=1, pick=None):
+    """n_sys pressure systems with log-uniform cell counts in [lo, hi]; with
+    `pick`, only the systems of those indices (the same systems the full
+    batch holds at those places)."""
     mats, rhs = [], []
-    for k, nc in enumerate(cells):
-        n = max(2, int(round(nc ** (1.0 / 3.0))))
+    for k, n in enumerate(batch_sizes(n_sys, lo, hi, seed)):
+        if pick is not None and k not in pick:
+            continue
         m = Mesh.hex(n, jitter=0.15, seed=1000 + k, permute=True)
         m.renumber(Mesh.RCM)
         A = m.pressure(pin=1)

@@ -429,90 +429,247 @@ __global__ void SG_BOUNDS(V) k_mp_accum(SegMap sm, const int* __restrict__ mask,
   }
 }
 
-// ---- preconditioner: solv_precond.f90:10-29, one wavefront level -----------
-// c_i = pl_i - sum_{j<i} (n*n) c_j   (DIC)   or  - (p*c_j)*n  (DILU);
-// c_r = c; c = 1/(c + small).  face p/n looked up through slot_src.
-__global__ void k_precond_level(int i0, int i1, const int* __restrict__ cells, int imat,
-                                Rows<double> R, const int* __restrict__ slot_src,
-                                const double* __restrict__ fp, const double* __restrict__ fn,
-                                double* __restrict__ c, double* __restrict__ c_r) {
-  const int t = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= i1) return;
-  const int i = cells ? cells[t] : t;
-  RowIt<double> it(R, i);
-  double d = R.diag[i];
-  if (imat > 0) {
-    for (int k = 0; k < it.w; ++k) {
-      const int e = it.base + k * kWarp;
-      const int j = R.col[e];
-      if (j >= 0 && j < i) {
-        const int f = slot_src[e] >> 1;
-        const double cj = __ldcg(&c[j]);
+// ---- sync-free triangular recurrences ---------------------------------------
+// solv_precond (the DIC/DILU factorisation) and solv_direct (the two
+// triangular sweeps) are recurrences over the cells: in the internal order
+// every lower neighbour of a cell has a lower index (and every upper one a
+// higher index), so a cell can be computed as soon as the values of its
+// lower (forward) or upper (backward) neighbours exist.  One cooperative
+// launch does a whole recurrence: warp w of W owns the 32-cell slices
+// w, w + W, w + 2W, ... (backward: counted from the top) and takes them in
+// that order; the output array starts out filled with a signalling-NaN
+// pattern ("pending"), which arithmetic never produces (it returns quiet
+// NaNs), and a cell reads a neighbour's value with a relaxed load until it
+// is no longer pending.  All warps are resident at once (cooperative
+// launch), so the lowest unfinished slice always has its owner running and
+// its inputs done: the recurrence cannot deadlock.  Each cell still adds its
+// neighbour terms one by one in slot (face) order, with the reference's
+// operations, so the results are bit for bit those of the sequential loops.
+// Every wait is bounded (kSweepPolls polls): a wait that runs out sets
+// SweepCtl::err, every warp then stops waiting, and the host reports the
+// error and refills the pending state before the next sweep.
+struct SweepCtl {
+  int err;      // a wait ran out (sticky until the host clears it)
+  int pad[3];
+};
+constexpr int kSweepPolls = 1 << 20;
+constexpr int kSweepThreads = 256;
+
+template <typename T> struct Pending;
+template <> struct Pending<double> {
+  using U = unsigned long long;
+  static constexpr U bits = 0x7ff5a5a5a5a5a5a5ull;  // signalling NaN
+  static __device__ __forceinline__ double value() { return __longlong_as_double((long long)bits); }
+  static __device__ __forceinline__ double from(U u) { return __longlong_as_double((long long)u); }
+};
+template <> struct Pending<float> {
+  using U = unsigned int;
+  static constexpr U bits = 0x7fa5a5a5u;  // signalling NaN
+  static __device__ __forceinline__ float value() { return __int_as_float((int)bits); }
+  static __device__ __forceinline__ float from(U u) { return __int_as_float((int)u); }
+};
+
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned int ld_relaxed(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(__double_as_longlong(v))
+               : "memory");
+}
+__device__ __forceinline__ void st_relaxed(float* p, float v) {
+  asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(__float_as_int(v)) : "memory");
+}
+__device__ __forceinline__ int ld_err(const SweepCtl* ctl) {
+  return (int)ld_relaxed(reinterpret_cast<const unsigned int*>(&ctl->err));
+}
+
+// v = *p once it is no longer pending
+template <typename T>
+__device__ __forceinline__ bool take(const T* p, T& v) {
+  using P = Pending<T>;
+  const typename P::U u = ld_relaxed(reinterpret_cast<const typename P::U*>(p));
+  v = P::from(u);
+  return u != P::bits;
+}
+
+// x[0 .. n) = pending
+template <typename T>
+__global__ void k_fill_pending(long long n, T* __restrict__ x) {
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+       e += (long long)gridDim.x * blockDim.x)
+    x[e] = Pending<T>::value();
+}
+
+// Warp-level driver of one recurrence.  `step(i, k)` advances cell i (this
+// lane's) from slot k as far as its inputs allow and returns the next slot
+// (w when the cell is done and stored).  Slices are taken in the order that
+// makes every dependency point to an earlier (or the same) slice.
+template <bool UP, typename Step>
+__device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ slice_w,
+                                             SweepCtl* ctl, Step&& step) {
+  const int lane = threadIdx.x & 31;
+  const int ns = (n + 31) >> 5;
+  const int W = gridDim.x * (blockDim.x >> 5);
+  const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (int r = gw; r < ns; r += W) {
+    const int s = UP ? ns - 1 - r : r;
+    const int i = s * 32 + lane;
+    const int w = __ldg(&slice_w[s]);
+    int k = i < n ? 0 : w;
+    k = step(i, k, true);
+    for (int poll = 0;; ++poll) {
+      __syncwarp();
+      if (__all_sync(0xffffffffu, k >= w)) break;
+      if (poll >= kSweepPolls || ((poll & 63) == 63 && ld_err(ctl))) {
+        if (lane == 0) atomicExch(&ctl->err, 1);
+        break;
+      }
+      __nanosleep(20);
+      if (k < w) k = step(i, k, false);
+    }
+  }
+}
+
+// solv_precond.f90:10-29: d_i = pl_i - sum_{j<i} n^2 c_j (DIC, imat 1) or
+// - (p c_j) n (DILU, imat 2) in face order; c_r = d; c = 1/(d + small).
+// imat <= 0 is Jacobi (no recurrence; k_precond_jacobi), imat >= 3 keeps
+// d = pl (the reference's fall-through).  c must start out pending.
+__global__ void __launch_bounds__(kSweepThreads) k_precond_sf(
+    int n, int imat, Rows<double> R, const int* __restrict__ slot_src,
+    const double* __restrict__ fp, const double* __restrict__ fn, double* c,
+    double* __restrict__ c_r, SweepCtl* ctl) {
+  const int lane = threadIdx.x & 31;
+  double d = 0.0;
+  int base = 0;
+  sweep_slices<false>(n, R.slice_w, ctl, [&](int i, int k, bool first) -> int {
+    const int w = __ldg(&R.slice_w[i >> 5]);
+    if (first) {
+      if (i >= n) return w;
+      base = __ldg(&R.slice_ptr[i >> 5]) + lane;
+      d = R.diag[i];
+    }
+    if (imat == 1 || imat == 2) {
+      for (; k < w; ++k) {
+        const int e = base + k * kWarp;
+        const int j = __ldg(&R.col[e]);
+        if (!(j >= 0 && j < i)) continue;
+        double cj;
+        if (!take(&c[j], cj)) return k;
+        const int f = __ldg(&slot_src[e]) >> 1;
         if (imat == 1) {
           const double nf = fn[f];
           d = sub(d, mul(mul(nf, nf), cj));
-        } else if (imat == 2) {
+        } else {
           d = sub(d, mul(mul(fp[f], cj), fn[f]));
         }
       }
     }
-  }
-  c_r[i] = d;
-  c[i] = 1.0 / add(d, kSmall);
+    c_r[i] = d;
+    st_relaxed(&c[i], 1.0 / add(d, kSmall));
+    return w;
+  });
 }
 
-// ---- sweeps: solv_direct.f90:11-38, one wavefront level --------------------
-// forward: x_i = (b_i - sum_{j<i} n x_j) * c_i
-template <typename T, int V>
-__global__ void k_fwd_level(int i0, int i1, const int* __restrict__ cells, Rows<T> R,
-                            const T* __restrict__ c, const T* __restrict__ bvec,
-                            T* __restrict__ x, const int* __restrict__ n_active) {
-  const int t = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= i1 || (n_active && *n_active == 0)) return;
-  const int i = cells ? cells[t] : t;
-  RowIt<T> it(R, i);
-  T acc[V];
-#pragma unroll
-  for (int v = 0; v < V; ++v) acc[v] = bvec[(size_t)i * V + v];
-  for (int k = 0; k < it.w; ++k) {
-    const int e = it.base + k * kWarp;
-    const int j = __ldg(&R.col[e]);
-    if (j >= 0 && j < i) {
-      const T a = R.sval[e];
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, __ldcg(&x[(size_t)j * V + v])));
-    }
+// Jacobi diagonal (solv_precond.f90:13 with imat <= 0): c_r = pl, c = 1/(pl+small)
+__global__ void k_precond_jacobi(int n, const double* __restrict__ diag, double* __restrict__ c,
+                                 double* __restrict__ c_r) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double d = diag[i];
+    c_r[i] = d;
+    c[i] = 1.0 / add(d, kSmall);
   }
-  const T ci = c[i];
-#pragma unroll
-  for (int v = 0; v < V; ++v) x[(size_t)i * V + v] = mul(acc[v], ci);
 }
-// backward, with the x = x*c_r scaling of :26 fused in:
-// x_i = (x_i c_r_i - sum_{j>i} p x_j) * c_i
+
+// solv_direct.f90:12-24 forward sweep, x_i = (b_i - sum_{j<i} n x_j) c_i, into
+// t (which starts out pending); the backward sweep's output x is reset to
+// pending on the way.
 template <typename T, int V>
-__global__ void k_bwd_level(int i0, int i1, const int* __restrict__ cells, Rows<T> R,
-                            const T* __restrict__ c, const T* __restrict__ c_r,
-                            T* __restrict__ x, const int* __restrict__ n_active) {
-  const int t = i0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= i1 || (n_active && *n_active == 0)) return;
-  const int i = cells ? cells[t] : t;
-  RowIt<T> it(R, i);
-  const T cr = c_r[i];
+__global__ void __launch_bounds__(kSweepThreads, 4) k_fwd_sf(
+    int n, Rows<T> R, const T* __restrict__ c, const T* __restrict__ bvec, T* t, T* x,
+    SweepCtl* ctl, const int* __restrict__ n_active) {
+  if (n_active && *n_active == 0) return;
+  const int lane = threadIdx.x & 31;
   T acc[V];
+  int base = 0;
+  sweep_slices<false>(n, R.slice_w, ctl, [&](int i, int k, bool first) -> int {
+    const int w = __ldg(&R.slice_w[i >> 5]);
+    if (first) {
+      if (i >= n) return w;
+      base = __ldg(&R.slice_ptr[i >> 5]) + lane;
 #pragma unroll
-  for (int v = 0; v < V; ++v) acc[v] = mul(x[(size_t)i * V + v], cr);
-  for (int k = 0; k < it.w; ++k) {
-    const int e = it.base + k * kWarp;
-    const int j = __ldg(&R.col[e]);
-    if (j > i) {
+      for (int v = 0; v < V; ++v) acc[v] = bvec[(size_t)i * V + v];
+    }
+    for (; k < w; ++k) {
+      const int e = base + k * kWarp;
+      const int j = __ldg(&R.col[e]);
+      if (!(j >= 0 && j < i)) continue;
+      T xv[V];
+      bool ok = true;
+#pragma unroll
+      for (int v = 0; v < V; ++v) ok &= take(&t[(size_t)j * V + v], xv[v]);
+      if (!ok) return k;
       const T a = R.sval[e];
 #pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, __ldcg(&x[(size_t)j * V + v])));
+      for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, xv[v]));
     }
-  }
-  const T ci = c[i];
+    const T ci = c[i];
 #pragma unroll
-  for (int v = 0; v < V; ++v) x[(size_t)i * V + v] = mul(acc[v], ci);
+    for (int v = 0; v < V; ++v) {
+      st_relaxed(&t[(size_t)i * V + v], mul(acc[v], ci));
+      x[(size_t)i * V + v] = Pending<T>::value();
+    }
+    return w;
+  });
+}
+
+// solv_direct.f90:26-38 backward sweep with the x = x c_r scaling of :26:
+// x_i = (t_i c_r_i - sum_{j>i} p x_j) c_i; x starts out pending, and each
+// t_i is reset to pending once read, ready for the next forward sweep.
+template <typename T, int V>
+__global__ void __launch_bounds__(kSweepThreads, 4) k_bwd_sf(
+    int n, Rows<T> R, const T* __restrict__ c, const T* __restrict__ c_r, T* t, T* x,
+    SweepCtl* ctl, const int* __restrict__ n_active) {
+  if (n_active && *n_active == 0) return;
+  const int lane = threadIdx.x & 31;
+  T acc[V];
+  int base = 0;
+  sweep_slices<true>(n, R.slice_w, ctl, [&](int i, int k, bool first) -> int {
+    const int w = __ldg(&R.slice_w[i >> 5]);
+    if (first) {
+      if (i >= n) return w;
+      base = __ldg(&R.slice_ptr[i >> 5]) + lane;
+      const T cr = c_r[i];
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] = mul(t[(size_t)i * V + v], cr);
+    }
+    for (; k < w; ++k) {
+      const int e = base + k * kWarp;
+      const int j = __ldg(&R.col[e]);
+      if (!(j > i)) continue;
+      T xv[V];
+      bool ok = true;
+#pragma unroll
+      for (int v = 0; v < V; ++v) ok &= take(&x[(size_t)j * V + v], xv[v]);
+      if (!ok) return k;
+      const T a = R.sval[e];
+#pragma unroll
+      for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, xv[v]));
+    }
+    const T ci = c[i];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+      st_relaxed(&x[(size_t)i * V + v], mul(acc[v], ci));
+      t[(size_t)i * V + v] = Pending<T>::value();
+    }
+    return w;
+  });
 }
 // Jacobi: x = b*c (solv_direct.f90:41)
 template <typename T, int V>

@@ -18,7 +18,8 @@
 // make that first call before any stream capture.  All calls on a device
 // share the one array: the ticket and counter are cleared at the start of
 // every call, and calls that overlap on the GPU (different streams, no
-// ordering between them) race on it.
+// ordering between them) race on it.  Face indices are checked on the GPU
+// before res0 is touched; a bad one leaves res0 and res0_n as they were.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,9 +46,25 @@ static __device__ __align__(256) NaScratch g_na_scratch;
 std::mutex g_na_mutex;
 NaScratch* g_na_ptr[kNaMaxDevices] = {nullptr};
 
+// Face indices checked before anything is written: a face whose ip or in
+// lies outside 1..n (in = 0 marks a boundary face) counts in S->bad, and
+// the kernels below leave res0 and res0_n alone when the count is not zero.
+__global__ void k_na_check(int n, int nf, const int* __restrict__ ip, const int* __restrict__ in,
+                           NaScratch* __restrict__ S) {
+  int bad = 0;
+  for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf;
+       f += (long long)gridDim.x * blockDim.x) {
+    const int a = ip[f], b = in[f];
+    bad += (a < 1 || a > n || b < 0 || b > n);
+  }
+  if (bad) atomicAdd(&S->bad, bad);
+}
+
 // r_i -= pl_i phi_i (column-major r, cell-major phi)
 __global__ void k_na_cells(int n, int nv, const double* __restrict__ pl,
-                           const double* __restrict__ phi, double* __restrict__ r) {
+                           const double* __restrict__ phi, double* __restrict__ r,
+                           const NaScratch* __restrict__ S) {
+  if (S->bad) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     for (int v = 0; v < nv; ++v)
@@ -58,15 +75,12 @@ __global__ void k_na_cells(int n, int nv, const double* __restrict__ pl,
 __global__ void k_na_faces(int n, int nf, int nv, const int* __restrict__ ip,
                            const int* __restrict__ in, const double* __restrict__ p,
                            const double* __restrict__ nn, const double* __restrict__ phi,
-                           double* __restrict__ r, NaScratch* __restrict__ S) {
+                           double* __restrict__ r, const NaScratch* __restrict__ S) {
+  if (S->bad) return;
   for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf;
        f += (long long)gridDim.x * blockDim.x) {
     if (in[f] == 0) continue;  // boundary face
     const int a = ip[f] - 1, b = in[f] - 1;
-    if (a < 0 || a >= n || b < 0 || b >= n) {
-      atomicAdd(&S->bad, 1);
-      continue;
-    }
     for (int v = 0; v < nv; ++v) {
       atomicAdd(&r[(size_t)v * n + a], -p[f] * phi[(size_t)b * nv + v]);
       atomicAdd(&r[(size_t)v * n + b], -nn[f] * phi[(size_t)a * nv + v]);
@@ -81,6 +95,7 @@ k_na_l1(int n, int nv, const double* __restrict__ r, double* __restrict__ out,
         NaScratch* __restrict__ S) {
   __shared__ double sh[kNaMaxVc][kNaThreads / 32];
   __shared__ bool last;
+  if (S->bad) return;
   double acc[kNaMaxVc] = {0.0, 0.0, 0.0, 0.0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -135,19 +150,24 @@ extern "C" int solv_gpu_res_noalloc(int n_cell, int n_face, const int* ip, const
                                     const double* p, const double* n, const double* pl,
                                     int n_vc, const double* phi, double* res0,
                                     double* res0_n, int not_r0, void* stream) {
-  if (n_cell <= 0 || n_face < 0 || !ip || !in || !p || !n || !pl || !phi || !res0 || !res0_n)
+  if (n_cell <= 0 || n_face < 0 || n_vc < 1 || !ip || !in || !p || !n || !pl || !phi || !res0 ||
+      !res0_n)
     return SOLV_GPU_BAD_INPUT;
-  if (n_vc < 1 || n_vc > kNaMaxVc) return SOLV_GPU_TOO_LARGE;  // scratch holds 4 components
+  if (n_vc > kNaMaxVc) return SOLV_GPU_TOO_LARGE;  // the scratch holds 4 components
   NaScratch* S = nullptr;
   int rc = na_scratch(&S);
   if (rc) return rc;
+  // a launch error left over from the caller's earlier work is not this
+  // call's: clear it so that only these launches are checked below
+  (void)cudaGetLastError();
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(&S->ticket, 0, sizeof(unsigned int) + sizeof(int), st) != cudaSuccess)
     return SOLV_GPU_DEVICE_ERROR;
   const int gc = (int)std::min<long long>(((long long)n_cell + kNaThreads - 1) / kNaThreads, 4096);
   const int gf = (int)std::min<long long>(((long long)n_face + kNaThreads - 1) / kNaThreads, 4096);
+  if (!not_r0 && n_face > 0) k_na_check<<<gf, kNaThreads, 0, st>>>(n_cell, n_face, ip, in, S);
   if (!not_r0) {
-    k_na_cells<<<gc, kNaThreads, 0, st>>>(n_cell, n_vc, pl, phi, res0);
+    k_na_cells<<<gc, kNaThreads, 0, st>>>(n_cell, n_vc, pl, phi, res0, S);
     if (n_face > 0)
       k_na_faces<<<gf, kNaThreads, 0, st>>>(n_cell, n_face, n_vc, ip, in, p, n, phi, res0, S);
   }

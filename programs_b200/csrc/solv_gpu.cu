@@ -100,9 +100,7 @@ struct solv_gpu_ctx {
   int N = 0, F = 0;
   bool orient_std = true;
   int n_seg = 1;             // independent systems (block-diagonal batch)
-  std::vector<int> lvl_ptr;  // level l = lvl_cells[lvl_ptr[l] .. lvl_ptr[l+1])
-  bool lvl_contig = true;    // single system: level l is the internal range itself
-  DevBuf lvl_cells;          // internal cell ids by (level, system, caller index)
+  std::vector<int> lvl_ptr;  // cells per wavefront level (counts, for the statistics)
   std::vector<int> seg_c0_caller, seg_c1_caller;  // system ranges in internal order
   long long n_slots = 0;
   int n_slice = 0;
@@ -120,6 +118,12 @@ struct solv_gpu_ctx {
   DevBuf w_phi, w_r0, w_r, w_p, w_q, w_v, w_z, w_c, w_cr, w_in, w_out;
   DevBuf wf_r, wf_p, wf_q, wf_v, wf_z, wf_phi, wf_c, wf_cr, wf_r0;  // FP32
   DevBuf w_x, w_b;  // solv_gpu_direct / spmv staging
+  // triangular sweeps (kernels.cuh, sync-free recurrences): the forward
+  // sweep's output t, all "pending" between sweeps; the wait-timeout flag
+  DevBuf w_t, wf_t;
+  bool t_ready = false, tf_ready = false;  // t / tf hold only the pending pattern
+  DevBuf sweep_ctl;
+  std::map<const void*, int> coop_blocks;  // resident blocks per SM, per sweep kernel
 
   // captured iteration graphs, keyed by (solver, imat, V, fp32)
   std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;
@@ -152,6 +156,12 @@ struct solv_gpu_ctx {
   DevBuf g_zero;                       // smoother 2 training: face weights held at zero
   double mg_setup_s = 0.0;
   double mg_smooth_scale = 1.0;        // factor the last solve applied to K (see mg_bound_smoother)
+  float mg_scale_min = 0.5f;           // floor on the network's per-cell scales
+  // the learned preconditioner hands over to Jacobi-PCG when its residual
+  // stalls: fcg_stall_iters iterations without falling below fcg_stall_drop
+  // times the value at the start of the window
+  int fcg_stall_iters = 100;
+  double fcg_stall_drop = 0.5;
 };
 
 namespace {
@@ -336,18 +346,11 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
       seg_c1[k] = cnt[(size_t)(k + 1) * nl];
     }
   }
-  // level lists (only needed when a level spans several systems)
+  // cells per level (the sweep depth reported in the statistics)
   std::vector<int> lcnt(nl + 1, 0);
   for (int i = 0; i < N; ++i) lcnt[lev[i] + 1]++;
   for (int l = 0; l < nl; ++l) lcnt[l + 1] += lcnt[l];
   c->lvl_ptr.assign(lcnt.begin(), lcnt.end());
-  c->lvl_contig = nsys == 1;
-  std::vector<int> lcells;
-  if (!c->lvl_contig) {
-    lcells.resize(N);
-    std::vector<int> pos(lcnt.begin(), lcnt.end() - 1);
-    for (int k = 0; k < N; ++k) lcells[pos[lev[old_of_new[k]]]++] = k;  // (level, system, index)
-  }
   // sliced ELL, 32 cells per slice
   const int ns = (N + 31) / 32;
   std::vector<int> sp(ns + 1, 0);
@@ -384,6 +387,7 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
   c->N = N;
   c->F = F;
   c->n_seg = nsys;
+  c->t_ready = c->tf_ready = false;
   c->orient_std = orient;
   c->n_slots = total;
   c->n_slice = ns;
@@ -407,10 +411,6 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
   CUDA_TRY(c, cudaMemcpyAsync(c->slice_w.p, sw.data(), ns, cudaMemcpyHostToDevice, st));
   CUDA_TRY(c, cudaMemcpyAsync(c->col.p, hcol.data(), total * sizeof(int), cudaMemcpyHostToDevice, st));
   CUDA_TRY(c, cudaMemcpyAsync(c->slot_src.p, hsrc.data(), total * sizeof(int), cudaMemcpyHostToDevice, st));
-  if (!c->lvl_contig) {
-    CUDA_TRY(c, c->lvl_cells.ensure(N * sizeof(int)));
-    CUDA_TRY(c, cudaMemcpyAsync(c->lvl_cells.p, lcells.data(), N * sizeof(int), cudaMemcpyHostToDevice, st));
-  }
   CUDA_TRY(c, cudaStreamSynchronize(st));  // host vectors die here
   c->seg_c0_caller.assign(seg_c0.begin(), seg_c0.end());
   c->seg_c1_caller.assign(seg_c1.begin(), seg_c1.end());
@@ -755,12 +755,12 @@ bool mg_on(const solv_gpu_ctx* c) { return c->mg_max_levels > 0 && !c->mg.empty(
 // device and, above kSmoothMax, scales q = s D^-1/2 (the operator's only
 // per-cell factor, K scaling with q^2) so that the bound holds.  The
 // estimate is inflated by 5% (power iteration approaches lambda_max from
-// below).  Before that the per-cell scales are held at or above kScaleMin
-// (a quarter of the Jacobi weight): a network that drives some s_i towards
-// zero leaves those cells unsmoothed, which no bound on lambda_max sees.
+// below).  Before that the per-cell scales are held at or above
+// mg_scale_min (default 0.5, a quarter of the Jacobi weight): a network that
+// drives some s_i towards zero leaves those cells unsmoothed, which no bound
+// on lambda_max sees.
 // Returns the factor applied to K (1 when none was needed).
 constexpr double kSmoothMax = 1.9;
-constexpr float kScaleMin = 0.5f;
 constexpr int kPowerIters = 8;
 
 int mg_bound_smoother(solv_gpu_ctx* c, double* applied) {
@@ -773,7 +773,7 @@ int mg_bound_smoother(solv_gpu_ctx* c, double* applied) {
   float* y = c->mg_x0.as<float>();
   CUDA_TRY(c, c->g_jsum.ensure(3 * sizeof(double)));
   double* acc = c->g_jsum.as<double>();
-  mg::k_mg_floor<<<G, B, 0, s>>>(N, kScaleMin, c->g_rsd.as<float>(), c->g_q.as<float>());
+  mg::k_mg_floor<<<G, B, 0, s>>>(N, c->mg_scale_min, c->g_rsd.as<float>(), c->g_q.as<float>());
   mg::k_mg_hashfill<<<G, B, 0, s>>>(N, v);
   c->launches += 2;
   double prev = 0.0, lam = 0.0, h = 0.0;
@@ -832,55 +832,95 @@ int run_res(solv_gpu_ctx* c, int V, const double* phi, double* r, int not_r0) {
   return SOLV_GPU_OK;
 }
 
-// solv_precond: c, c_r in internal order (FP64)
-void launch_precond(solv_gpu_ctx* c, int imat, double* cc, double* cr) {
-  if (imat <= 0) {
-    sg::k_precond_level<<<(c->N + c->block - 1) / c->block, c->block, 0, c->stream>>>(
-        0, c->N, nullptr, 0, rows<double>(c), c->slot_src.as<int>(), c->fp.as<double>(),
-        c->fn.as<double>(), cc, cr);
-    c->launches++;
-    return;
+// Cooperative launch of a sync-free recurrence (kernels.cuh): every block
+// resident at once, at most one warp per 32-cell slice.
+template <typename... KArgs, typename... Args>
+int coop_launch(solv_gpu_ctx* c, void (*kern)(KArgs...), Args... args) {
+  auto it = c->coop_blocks.find((const void*)kern);
+  int per_sm = 0;
+  if (it != c->coop_blocks.end()) {
+    per_sm = it->second;
+  } else {
+    CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sg::kSweepThreads, 0));
+    if (per_sm < 1) return set_err(c, SOLV_GPU_DEVICE_ERROR, "sweep kernel cannot be resident");
+    c->coop_blocks[(const void*)kern] = per_sm;
   }
-  const int nl = (int)c->lvl_ptr.size() - 1;
-  const int* cells = c->lvl_contig ? nullptr : c->lvl_cells.as<int>();
-  for (int l = 0; l < nl; ++l) {
-    int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
-    sg::k_precond_level<<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
-        i0, i1, cells, imat, rows<double>(c), c->slot_src.as<int>(), c->fp.as<double>(),
-        c->fn.as<double>(), cc, cr);
-    c->launches++;
-  }
+  const long long warps = ((long long)c->N + 31) / 32;
+  const long long want = (warps + sg::kSweepThreads / 32 - 1) / (sg::kSweepThreads / 32);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)std::max(1LL, std::min<long long>(want, (long long)per_sm * c->n_sm)));
+  cfg.blockDim = dim3(sg::kSweepThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CUDA_TRY(c, cudaLaunchKernelEx(&cfg, kern, args...));
+  c->launches++;
+  return SOLV_GPU_OK;
 }
 
-// x = M^-1 b  (solv_direct), internal order, V components
+sg::SweepCtl* sweep_ctl(solv_gpu_ctx* c) { return c->sweep_ctl.as<sg::SweepCtl>(); }
+
+// A wait of a sweep ran out (SweepCtl::err): report it, clear the flag, and
+// have the pending state of the sweep buffers rebuilt before the next use.
+int sweep_check(solv_gpu_ctx* c) {
+  sg::SweepCtl h{};
+  CUDA_TRY(c, cudaMemcpyAsync(&h, c->sweep_ctl.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  if (!h.err) return SOLV_GPU_OK;
+  CUDA_TRY(c, cudaMemsetAsync(c->sweep_ctl.p, 0, sizeof(sg::SweepCtl), c->stream));
+  c->t_ready = c->tf_ready = false;
+  return set_err(c, SOLV_GPU_DEVICE_ERROR, "triangular sweep: a wait for a neighbour ran out");
+}
+
+// solv_precond: c, c_r in internal order (FP64).  DIC / DILU is one
+// sync-free recurrence over the cells (c starts out pending).
+int launch_precond(solv_gpu_ctx* c, int imat, double* cc, double* cr) {
+  if (imat <= 0) {
+    sg::k_precond_jacobi<<<grid_for(c, c->N), c->block, 0, c->stream>>>(c->N, c->diag.as<double>(),
+                                                                         cc, cr);
+    c->launches++;
+    CUDA_TRY(c, cudaGetLastError());
+    return SOLV_GPU_OK;
+  }
+  sg::k_fill_pending<double><<<grid_for(c, c->N), c->block, 0, c->stream>>>(c->N, cc);
+  c->launches++;
+  return coop_launch(c, sg::k_precond_sf, c->N, imat, rows<double>(c), (const int*)c->slot_src.as<int>(),
+                     (const double*)c->fp.as<double>(), (const double*)c->fn.as<double>(), cc, cr,
+                     sweep_ctl(c));
+}
+
+// x = M^-1 b  (solv_direct), internal order, V components: the forward
+// sweep into the workspace t, the backward sweep from t into x (both
+// sync-free recurrences, one cooperative launch each).
+template <typename T>
+T* sweep_t(solv_gpu_ctx* c) {
+  if constexpr (std::is_same<T, double>::value) return c->w_t.as<double>();
+  else return c->wf_t.as<float>();
+}
+
 template <typename T, int V>
-void launch_direct(solv_gpu_ctx* c, int imat, const T* cc, const T* cr, T* x, const T* b,
-                   const int* n_active) {
+int launch_direct(solv_gpu_ctx* c, int imat, const T* cc, const T* cr, T* x, const T* b,
+                  const int* n_active) {
   if (imat <= 0) {
     sg::k_jacobi<T, V><<<grid_for(c, c->N), c->block, 0, c->stream>>>(c->N, cc, b, x);
     c->launches++;
-    return;
+    return SOLV_GPU_OK;
   }
-  const int nl = (int)c->lvl_ptr.size() - 1;
-  const int* cells = c->lvl_contig ? nullptr : c->lvl_cells.as<int>();
   Rows<T> R = rows<T>(c);
-  for (int l = 0; l < nl; ++l) {
-    int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
-    sg::k_fwd_level<T, V><<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
-        i0, i1, cells, R, cc, b, x, n_active);
-  }
-  for (int l = nl - 1; l >= 0; --l) {
-    int i0 = c->lvl_ptr[l], i1 = c->lvl_ptr[l + 1];
-    sg::k_bwd_level<T, V><<<(i1 - i0 + c->block - 1) / c->block, c->block, 0, c->stream>>>(
-        i0, i1, cells, R, cc, cr, x, n_active);
-  }
-  c->launches += 2 * nl;
+  T* t = sweep_t<T>(c);
+  int rc = coop_launch(c, sg::k_fwd_sf<T, V>, c->N, R, cc, b, t, x, sweep_ctl(c), n_active);
+  if (rc) return rc;
+  return coop_launch(c, sg::k_bwd_sf<T, V>, c->N, R, cc, cr, t, x, sweep_ctl(c), n_active);
 }
 
 // Workspace for V components in precision T.
 template <typename T>
 struct WS {
-  T *phi, *r, *r0, *p, *q, *v, *z, *c, *cr;
+  T *phi, *r, *r0, *p, *q, *v, *z, *c, *cr, *t;
 };
 
 template <typename T>
@@ -903,6 +943,26 @@ int ensure_ws(solv_gpu_ctx* c, int V, WS<T>& w) {
   w.phi = b[0]->as<T>(); w.r = b[1]->as<T>(); w.r0 = b[2]->as<T>(); w.p = b[3]->as<T>();
   w.q = b[4]->as<T>(); w.v = b[5]->as<T>(); w.z = b[6]->as<T>(); w.c = b[7]->as<T>();
   w.cr = b[8]->as<T>();
+  // the sweeps' t: all pending before every forward sweep
+  DevBuf& tb = f ? c->wf_t : c->w_t;
+  bool& ready = f ? c->tf_ready : c->t_ready;
+  void* old = tb.p;
+  CUDA_TRY(c, tb.ensure(nv));
+  if (old != tb.p) {
+    drop_graphs(c);
+    ready = false;
+  }
+  if (!c->sweep_ctl.p) {
+    CUDA_TRY(c, c->sweep_ctl.ensure(sizeof(sg::SweepCtl)));
+    CUDA_TRY(c, cudaMemsetAsync(c->sweep_ctl.p, 0, sizeof(sg::SweepCtl), c->stream));
+  }
+  if (!ready) {
+    sg::k_fill_pending<T><<<grid_for(c, (long long)c->N * V), c->block, 0, c->stream>>>(
+        (long long)c->N * V, tb.as<T>());
+    CUDA_TRY(c, cudaGetLastError());
+    ready = true;
+  }
+  w.t = tb.as<T>();
   return SOLV_GPU_OK;
 }
 
@@ -912,7 +972,7 @@ int ensure_ws(solv_gpu_ctx* c, int V, WS<T>& w) {
 // orthogonality the classic formulas rely on, and on a 256^3 pressure system
 // the classic ones needed several times the FP64 iteration count.
 template <typename T, int V>
-void cg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
+int cg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
   constexpr bool FLEX = std::is_same<T, float>::value;
   SegMap sm = segmap(c);
   double* part = c->part.as<double>();
@@ -920,7 +980,7 @@ void cg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
   const int G = c->seg.total_blk, B = c->block;
   cudaStream_t st = c->stream;
   if (imat > 0) {
-    launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active);
+    if (int rc = launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active)) return rc;
     sg::k_cg_rz<T, V, false, FLEX><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, part, lanes, w.q);
     sg::k_cg_p<T, V, false, FLEX><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes, part);
     sg::k_cg_spmv<T, V><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, part, lanes);
@@ -934,12 +994,13 @@ void cg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
                                                        lanes);
     c->launches += 3;
   }
+  return SOLV_GPU_OK;
 }
 
 // One BiCGSTAB iteration (solv_bicg.f90:42-118); rho/omeg of its head were
 // produced by the previous k_bi_update (or k_bi_rho before the first).
 template <typename T, int V>
-void bicg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
+int bicg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
   SegMap sm = segmap(c);
   double* part = c->part.as<double>();
   Lane* lanes = c->lanes.as<Lane>();
@@ -948,20 +1009,21 @@ void bicg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
   // w.q holds u, w.v holds v
   if (imat > 0) {
     sg::k_bi_p<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.p, w.q, w.z, lanes);
-    launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.p, sm.n_active);
+    if (int rc = launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.p, sm.n_active)) return rc;
   } else {
     sg::k_bi_p<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.r, w.p, w.q, w.z, lanes);
   }
   sg::k_bi_spmv<T, V, 0><<<G, B, 0, st>>>(rows<T>(c), sm, w.z, w.q, w.r0, part, lanes);
   if (imat > 0) {
     sg::k_bi_half<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.z, w.q, lanes);
-    launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active);
+    if (int rc = launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active)) return rc;
   } else {
     sg::k_bi_half<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.z, w.q, lanes);
   }
   sg::k_bi_spmv<T, V, 1><<<G, B, 0, st>>>(rows<T>(c), sm, w.z, w.v, w.r, part, lanes);
   sg::k_bi_update<T, V><<<G, B, 0, st>>>(sm, w.phi, w.r, w.z, w.v, w.r0, part, lanes);
   c->launches += 5;
+  return SOLV_GPU_OK;
 }
 
 // One flexible-CG iteration with the learned preconditioner (one system):
@@ -998,10 +1060,11 @@ void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
 template <typename T, int V>
 int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& graph_launches) {
   const int K = c->graph_iters;
-  auto body = [&]() {
-    if (solver == 0) cg_iteration<T, V>(c, imat, w);
-    else if (solver == 1) bicg_iteration<T, V>(c, imat, w);
-    else if constexpr (V == 1) fcg_iteration<T>(c, w);
+  auto body = [&]() -> int {
+    if (solver == 0) return cg_iteration<T, V>(c, imat, w);
+    if (solver == 1) return bicg_iteration<T, V>(c, imat, w);
+    if constexpr (V == 1) fcg_iteration<T>(c, w);
+    return SOLV_GPU_OK;
   };
   cudaGraphExec_t exec = nullptr;
   if (K > 0) {
@@ -1013,9 +1076,14 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
       cudaGraph_t g;
       CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       int l0 = c->launches;
-      for (int k = 0; k < K; ++k) body();
+      int rc = SOLV_GPU_OK;
+      for (int k = 0; k < K && !rc; ++k) rc = body();
       cudaError_t e = cudaStreamEndCapture(c->stream, &g);
       c->launches = l0;
+      if (rc) {
+        if (e == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+      }
       CUDA_TRY(c, e);
       e = cudaGraphInstantiate(&exec, g, 0);
       cudaGraphDestroy(g);
@@ -1029,8 +1097,7 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     // kernels per iteration (for the launch count statistics)
     int l0 = c->launches;
     // count by dry accounting: replicate the arithmetic of body()
-    int nl = (int)c->lvl_ptr.size() - 1;
-    int sweep = imat > 0 ? 2 * nl : 1;
+    int sweep = imat > 0 ? 2 : 1;  // forward + backward recurrence, or Jacobi
     if (solver == 0) per_launch_kernels = imat > 0 ? sweep + 4 : 3;
     else if (solver == 1) per_launch_kernels = imat > 0 ? 2 * sweep + 5 : 5;
     else per_launch_kernels = 4 + (mg_on(c) ? mg_kernels(c) : 1);
@@ -1043,7 +1110,7 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
       c->launches += K * per_launch_kernels;
       done += K;
     } else {
-      body();
+      if (int rc = body()) return rc;
       done += 1;
     }
     CUDA_TRY(c, cudaGetLastError());
@@ -1088,7 +1155,7 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
     if (out_ratio) std::fill(out_ratio, out_ratio + nl, 0.0);
     return SOLV_GPU_OK;
   }
-  launch_precond(c, imat, w.c, w.cr);  // solv_precond
+  if ((rc = launch_precond(c, imat, w.c, w.cr))) return rc;  // solv_precond
   CUDA_TRY(c, cudaMemcpyAsync(w.r, w.r0, (size_t)N * V * sizeof(double), cudaMemcpyDeviceToDevice, s));
   CUDA_TRY(c, cudaMemsetAsync(w.p, 0, (size_t)N * V * sizeof(double), s));
   CUDA_TRY(c, cudaMemsetAsync(w.q, 0, (size_t)N * V * sizeof(double), s));
@@ -1196,7 +1263,7 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
     return SOLV_GPU_OK;
   }
   // preconditioner in FP64 (solv_precond), rounded to FP32 for the sweeps
-  launch_precond(c, imat, w.c, w.cr);
+  if ((rc = launch_precond(c, imat, w.c, w.cr))) return rc;
   sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.c, f.c);
   sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.cr, f.cr);
   c->launches += 2;
@@ -1389,7 +1456,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     if (out_ratio) std::fill(out_ratio, out_ratio + nl, 0.0);
     return SOLV_GPU_OK;
   }
-  launch_precond(c, imat, w.c, w.cr);
+  if ((rc = launch_precond(c, imat, w.c, w.cr))) return rc;
   sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.c, f.c);
   sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.cr, f.cr);
   sg::k_mp_start<V><<<grid_for(c, NV), c->block, 0, s>>>(NV, w.r0, f.r, f.r0, f.phi);
@@ -1451,8 +1518,23 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
   CUDA_TRY(c, cudaGetLastError());
   const double delta = c->reliable_delta;
   int updates = 0, gl_total = 0, launched = 0;
-  int cur = solver;  // the learned preconditioner hands over to Jacobi-PCG once it stalls
+  // The learned preconditioner hands over to Jacobi-PCG, from the current
+  // iterate, when it loses positive curvature or produces NaN (the lane
+  // reports kLaneStall), when its residual stalls -- fcg_stall_iters
+  // iterations without the residual falling below fcg_stall_drop times its
+  // value at the start of that window -- or when the FP64 residual stops
+  // improving across reliable updates.
+  int cur = solver;
   c->fallbacks = 0;
+  std::vector<int> win_iter(nl, 0);
+  std::vector<double> win_l1(l1_last);
+  bool fell_back = false;
+  auto hand_over = [&]() {
+    if (cur != 2) return;
+    cur = 0;
+    fell_back = true;
+    c->fallbacks++;
+  };
   const int K = std::max(1, c->graph_iters);
   while (na > 0) {
     int gl = 0;
@@ -1462,15 +1544,20 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->lanes.p, nl * sizeof(Lane), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(c, cudaStreamSynchronize(s));
     bool need = false;
-    bool fell_back = false;
+    fell_back = false;
     std::vector<char> trig(nl, 0);
     for (int l = 0; l < nl; ++l) {
       if (final_[l]) continue;
       if (!hl[l].active || hl[l].l1 < delta * l1_last[l]) need = trig[l] = 1;
-      if (cur == 2 && hl[l].status == sg::kLaneStall) {
-        cur = 0;  // no positive curvature from the network: plain PCG from here
-        fell_back = true;
-        c->fallbacks++;
+      if (cur != 2) continue;
+      if (hl[l].status == sg::kLaneStall) {
+        hand_over();  // no positive curvature from the network
+      } else if (hl[l].l1 <= c->fcg_stall_drop * win_l1[l]) {
+        win_iter[l] = hl[l].iter;  // progress: a new window starts here
+        win_l1[l] = hl[l].l1;
+      } else if (hl[l].iter - win_iter[l] >= c->fcg_stall_iters) {
+        hand_over();  // the residual stalled
+        need = trig[l] = 1;
       }
     }
     if (fell_back) {  // restart the search direction (it may hold NaN)
@@ -1511,16 +1598,26 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
         status_v[l] = sg::kLaneMaxIter;
       } else if (trig[l]) {
         // this lane asked for the update but its FP64 residual did not
-        // improve on the last one it asked for: FP32 floor
+        // improve on the last one it asked for: FP32 floor, or, for the
+        // learned preconditioner, a stall that Jacobi-PCG takes over
         stalls[l] = l1[l] > 0.9 * l1_last[l] ? stalls[l] + 1 : 0;
-        if (stalls[l] >= 3) {
+        if (stalls[l] >= 3 && cur == 2) {
+          hand_over();
+          stalls[l] = 0;
+        } else if (stalls[l] >= 3) {
           final_[l] = 1;
           status_v[l] = sg::kLaneMaxIter;
         }
       }
       if (final_[l]) L.active = 0;
       if (trig[l]) l1_last[l] = l1[l];  // lanes along for the ride keep their window
+      win_iter[l] = L.iter;  // the stall window restarts from the FP64 residual
+      win_l1[l] = l1[l];
       na += L.active;
+    }
+    if (fell_back) {
+      CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
+      CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
     }
     CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
     CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
@@ -1711,6 +1808,18 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
         drop_graphs(c);
       }
       return SOLV_GPU_OK;
+    case SOLV_OPT_FCG_STALL_ITERS:
+      if (value < 1 || value > 1e7) return set_err(c, SOLV_GPU_BAD_INPUT, "stall window in 1..1e7");
+      c->fcg_stall_iters = (int)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_FCG_STALL_DROP:
+      if (!(value > 0 && value < 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "stall drop in (0,1)");
+      c->fcg_stall_drop = value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_MG_SCALE_MIN:
+      if (!(value >= 0 && value <= 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "scale floor in [0,1]");
+      c->mg_scale_min = (float)value;
+      return SOLV_GPU_OK;
     case SOLV_OPT_INNER_MAX_ITER:
       if (value < 1 || value > 1e7) return set_err(c, SOLV_GPU_BAD_INPUT, "inner max iter in 1..1e7");
       c->inner_max_iter = (int)value;
@@ -1800,7 +1909,13 @@ int solv_gpu_precond(solv_gpu_ctx* c, int imat, double* cc, double* cr) {
   CUDA_TRY(c, c->w_out.ensure(bytes));
   cudaStream_t s = c->stream;
   const int* o2n = c->old_of_new.as<int>();
-  launch_precond(c, imat, c->w_x.as<double>(), c->w_b.as<double>());
+  {
+    WS<double> w;  // the sweep state, allocated with the workspace
+    int rc = ensure_ws<double>(c, 1, w);
+    if (rc || (rc = launch_precond(c, imat, c->w_x.as<double>(), c->w_b.as<double>())) ||
+        (rc = sweep_check(c)))
+      return rc;
+  }
   sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, c->w_x.as<double>(), c->w_out.as<double>());
   CUDA_TRY(c, cudaMemcpyAsync(cc, c->w_out.p, bytes, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(c, cudaStreamSynchronize(s));
@@ -1831,7 +1946,9 @@ int solv_gpu_direct(solv_gpu_ctx* c, int imat, const double* cc, const double* c
     return SOLV_GPU_OK;
   };
   if ((rc = up(cc, w.c)) || (rc = up(cr, w.cr)) || (rc = up(b, w.r))) return rc;
-  launch_direct<double, 1>(c, imat, w.c, w.cr, w.z, w.r, nullptr);
+  if ((rc = launch_direct<double, 1>(c, imat, w.c, w.cr, w.z, w.r, nullptr)) ||
+      (rc = sweep_check(c)))
+    return rc;
   sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, w.z, c->w_in.as<double>());
   CUDA_TRY(c, cudaMemcpyAsync(x, c->w_in.p, bytes, cudaMemcpyDeviceToHost, s));
   CUDA_TRY(c, cudaStreamSynchronize(s));
@@ -1973,6 +2090,10 @@ static int solve_common(solv_gpu_ctx* c, int solver, int imat, double reduc, int
   CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
   int rc = solve_dispatch(c, solver, imat, reduc, n_iter, n_vc, phi_dev, res0_dev, res0_n, not_r0,
                           st, out_iters, out_ratio);
+  if (imat > 0 && c->sweep_ctl.p && (rc == SOLV_GPU_OK || rc == SOLV_GPU_MAXITER || rc == SOLV_GPU_NAN)) {
+    const int rs = sweep_check(c);
+    if (rs) rc = rs;
+  }
   CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
   CUDA_TRY(c, cudaEventSynchronize(c->ev1));
   if (st) {

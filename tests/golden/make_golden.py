@@ -19,6 +19,10 @@ outputs bit for bit, check the solutions against the stored scipy solves,
 and run the GPU solvers against the same outputs.
 
 Usage: python tests/golden/make_golden.py [path/to/cavity_3d.neu [path/to/channel_2d.neu]]
+
+Without arguments the two .neu files are looked up in the directory named
+by the environment variable SPRAY_SIMULATION_DIR (the reference's
+spray-simulation/ checkout); with neither, only hex6.npz is rebuilt.
 """
 from __future__ import annotations
 
@@ -35,9 +39,13 @@ from oracle.oracle import Oracle  # noqa: E402
 from programs_b200 import build  # noqa: E402
 from programs_b200.mesh import Mesh, poisson_rhs, uniform  # noqa: E402
 
-# where the reference checkout keeps the meshes it ships
-DEFAULT_NEU = "/root/reference/spray-simulation/cavity_3d.neu"
-DEFAULT_NEU_2D = "/root/reference/spray-simulation/channel_2d.neu"
+
+def reference_mesh(name: str) -> str | None:
+    """Path of a mesh the reference ships (spray-simulation/<name>), from
+    the directory in SPRAY_SIMULATION_DIR; None when that is not set."""
+    d = os.environ.get("SPRAY_SIMULATION_DIR")
+    return os.path.join(d, name) if d else None
+
 REDUC = 1e-10
 N_ITER = 5000
 
@@ -121,13 +129,13 @@ def hex6(outdir: str = HERE) -> None:
 if __name__ == "__main__":
     build.build_all()
     hex6()
-    neu = sys.argv[1] if len(sys.argv) > 1 else DEFAULT_NEU
-    if os.path.exists(neu):
+    neu = sys.argv[1] if len(sys.argv) > 1 else reference_mesh("cavity_3d.neu")
+    if neu and os.path.exists(neu):
         cavity(neu)
     else:
         print("cavity_3d.neu not found; cavity_3d.npz left as is")
-    neu2 = sys.argv[2] if len(sys.argv) > 2 else DEFAULT_NEU_2D
-    if os.path.exists(neu2):
+    neu2 = sys.argv[2] if len(sys.argv) > 2 else reference_mesh("channel_2d.neu")
+    if neu2 and os.path.exists(neu2):
         channel(neu2)
     else:
         print("channel_2d.neu not found; channel_2d.npz left as is")

@@ -1,0 +1,186 @@
+"""GPU parity against the CPU oracle on the benchmark configurations at
+their configured sizes, through the C-ABI.
+
+* C1 exactly: the 32^3 pressure-correction Poisson system (jitter +-15%,
+  cells permuted with seed 0, coefficients area/l_pn, cell 1 pinned,
+  zero-mean uniform right-hand side), FP64 Jacobi PCG and DIC PCG to a
+  1e-10 L1-relative residual, in the permuted order as given and after the
+  framework's RCM renumbering: the returned initial residual bit for bit,
+  res0_n to 1e-12, iteration counts within 2, solutions within 1e-8.
+* C2 at 128^3: the upwind momentum system (Taylor-Green flux, Pe up to 50,
+  CFL 5), BiCGSTAB with DILU in FP64 (iterations within 2, solution within
+  1e-8) and with FP32 inner iterations inside FP64 refinement (the true FP64
+  residual below 1e-10 and the solution within 1e-8 of the oracle's).
+* A slice of C3: four systems of the 64-mesh batch (8k to 500k cells,
+  seed 1), among them its largest, solved as one batch in FP64 and with
+  FP32 inner iterations; each system against its own oracle solve.
+* C4 at 256^3, when the full-size oracle fixture is present
+  (tests/golden/oracle_pcg_256.json, made by make_oracle_full.py): the
+  plain FP64 PCG against the oracle's own iteration count and its solution
+  at 4096 seeded cells, and the learned + mixed solve against the same.
+
+The oracle solves run in threads (the ctypes calls release the GIL).
+"""
+import json
+import os
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+from programs_b200.cases import batch_meshes, batch_sizes, make_system
+from programs_b200.mesh import Mesh, poisson_rhs
+from programs_b200.solver import OK, OPT_PRECISION
+
+pytestmark = pytest.mark.gpu
+
+SOL_TOL = 1e-8     # converged solutions, relative 2-norm
+NORM_TOL = 1e-12   # L1 norms through a tree reduction
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
+
+
+def _true_ratio(A, b, x):
+    return float(np.abs(b - A.to_scipy() @ x).sum() / np.abs(b).sum())
+
+
+# ---- C1: 32^3 pressure, plain FP64 PCG ------------------------------------------
+@pytest.fixture(scope="module", params=["as_given", "rcm"])
+def c1(request):
+    m = Mesh.hex(32, jitter=0.15, seed=0, permute=True)
+    if request.param == "rcm":
+        m.renumber(Mesh.RCM)
+    A = m.pressure(pin=1)
+    b = poisson_rhs(A.n_cell, 1)
+    assert A.n_cell == 32768 and int((A.inb > 0).sum()) == 95232
+    return A, b, Oracle.from_matrix(A)
+
+
+@pytest.mark.parametrize("imat", [0, 1])
+def test_c1_pressure_32_plain_pcg(gpu, c1, imat):
+    A, b, o = c1
+    ref = o.solv_cg(imat, 1e-10, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
+    gpu.matrix_set(A)
+    phi = np.zeros((A.n_cell, 1))
+    res0 = np.asfortranarray(b.reshape(-1, 1).copy())
+    rn = np.zeros(1)
+    st = gpu.solv_cg(imat, 1e-10, 20000, phi, res0, rn)
+    assert st["status"] == OK
+    assert np.array_equal(res0, ref[1])
+    assert abs(rn[0] - ref[2][0]) <= NORM_TOL * ref[2][0]
+    assert abs(st["iters"][0] - int(ref[3][0])) <= 2, (st["iters"][0], ref[3][0])
+    assert _rel(phi, ref[0]) <= SOL_TOL
+    assert _true_ratio(A, b, phi[:, 0]) < 1e-10
+
+
+# ---- C2: 128^3 momentum, BiCGSTAB + DILU ----------------------------------------
+@pytest.fixture(scope="module")
+def c2():
+    A, b = make_system(128, "momentum")
+    assert A.n_cell == 128 ** 3
+    ref = Oracle.from_matrix(A).solv_bicg(2, 1e-10, 1000, np.zeros((A.n_cell, 1)),
+                                          b.reshape(-1, 1))
+    return A, b, ref
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_c2_momentum_128_bicgstab_dilu(gpu, c2, precision):
+    A, b, ref = c2
+    gpu.matrix_set(A)
+    gpu.set_option(OPT_PRECISION, precision)
+    try:
+        phi = np.zeros((A.n_cell, 1))
+        res0 = np.asfortranarray(b.reshape(-1, 1).copy())
+        rn = np.zeros(1)
+        st = gpu.solv_bicg(2, 1e-10, 1000, phi, res0, rn)
+    finally:
+        gpu.set_option(OPT_PRECISION, 0)
+    assert st["status"] == OK
+    assert abs(rn[0] - ref[2][0]) <= NORM_TOL * ref[2][0]
+    assert _rel(phi, ref[0]) <= SOL_TOL
+    assert _true_ratio(A, b, phi[:, 0]) < 1e-10
+    if precision == 0:
+        assert np.array_equal(res0, ref[1])
+        assert abs(st["iters"][0] - int(ref[3][0])) <= 2, (st["iters"][0], ref[3][0])
+
+
+# ---- C3: a slice of the 64-mesh uneven batch ------------------------------------
+C3_N, C3_LO, C3_HI = 64, 8000, 500000
+
+
+@pytest.fixture(scope="module")
+def c3():
+    sizes = batch_sizes(C3_N, C3_LO, C3_HI, seed=1)
+    order = np.argsort(sizes)
+    pick = sorted({int(order[0]), int(order[len(order) // 3]), int(order[2 * len(order) // 3]),
+                   int(order[-1])})
+    mats, rhs = batch_meshes(C3_N, C3_LO, C3_HI, seed=1, pick=set(pick))
+    assert max(A.n_cell for A in mats) > 400000
+    with ThreadPoolExecutor(len(mats)) as ex:
+        refs = list(ex.map(lambda ab: Oracle.from_matrix(ab[0]).solv_cg(
+            0, 1e-10, 20000, np.zeros((ab[0].n_cell, 1)), ab[1].reshape(-1, 1)),
+            zip(mats, rhs)))
+    return mats, rhs, refs
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_c3_uneven_batch_slice(gpu, c3, precision):
+    mats, rhs, refs = c3
+    cell_ptr = gpu.matrix_set_batch(mats)
+    b = np.concatenate(rhs)
+    gpu.set_option(OPT_PRECISION, precision)
+    try:
+        phi = np.zeros((cell_ptr[-1], 1))
+        res0 = np.asfortranarray(b.reshape(-1, 1).copy())
+        st = gpu.solv_cg_batch(0, 1e-10, 20000, phi, res0)
+    finally:
+        gpu.set_option(OPT_PRECISION, 0)
+    assert st["status"] == OK
+    for k, (A, ref) in enumerate(zip(mats, refs)):
+        sl = slice(cell_ptr[k], cell_ptr[k + 1])
+        assert np.isclose(st["res0_n"][k, 0], ref[2][0], rtol=NORM_TOL)
+        assert _true_ratio(A, rhs[k], phi[sl, 0]) < 1e-10
+        if precision == 0:
+            assert _rel(phi[sl], ref[0]) <= SOL_TOL
+            assert abs(int(st["iters_all"][k, 0]) - int(ref[3][0])) <= 2
+        else:
+            # two different iterations stopped at 1e-10: within cond(A) x 1e-10
+            assert _rel(phi[sl], ref[0]) <= 1e-7
+
+
+# ---- C4: 256^3 pressure against the full-size oracle solve ----------------------
+ORACLE_256 = os.path.join(GOLD, "oracle_pcg_256.json")
+
+
+@pytest.mark.skipif(not os.path.exists(ORACLE_256), reason="full-size oracle fixture absent")
+def test_c4_pressure_256_against_full_oracle_solve(gpu):
+    import bench
+    from programs_b200 import learn
+    with open(ORACLE_256) as f:
+        ref = json.load(f)
+    A, b = bench.build_system(256, seed=0)
+    assert A.n_cell == ref["n_cell"]
+    idx = np.asarray(ref["sample_idx"])
+    xs = np.asarray(ref["sample_x"])
+    gpu.matrix_set(A)
+    phi = np.zeros((A.n_cell, 1))
+    rn = np.zeros(1)
+    st = gpu.solv_cg(0, 1e-10, 100000, phi, np.asfortranarray(b.reshape(-1, 1).copy()), rn)
+    assert st["status"] == OK
+    assert abs(rn[0] - ref["res0_n"]) <= NORM_TOL * ref["res0_n"]
+    assert abs(st["iters"][0] - ref["iterations"]) <= 2, (st["iters"][0], ref["iterations"])
+    assert _rel(phi[idx, 0], xs) <= SOL_TOL
+    assert abs(np.linalg.norm(phi) - ref["x_l2"]) <= SOL_TOL * ref["x_l2"]
+    # the learned + mixed solve to the same stopping rule: its own FP64
+    # residual, and its distance to the oracle's solution (both carry about
+    # cond(A) x 1e-10 of error of their own)
+    gpu.gnn_set_params(learn.load_params())
+    phi_l = np.zeros((A.n_cell, 1))
+    st = gpu.solv_fcg(1e-10, 100000, phi_l, np.asfortranarray(b.reshape(-1, 1).copy()), rn)
+    assert st["status"] == OK and st["fallbacks"] == 0
+    assert _true_ratio(A, b, phi_l[:, 0]) < 1e-10
+    assert _rel(phi_l[idx, 0], xs) <= 5e-8

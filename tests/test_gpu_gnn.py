@@ -7,7 +7,8 @@
   the CPU reference;
 * flexible CG: the untrained network (= the Jacobi step) reproduces PCG;
   any network converges to the FP64 oracle's solution (the FP64 residual
-  decides); a broken network hands over to plain PCG;
+  decides); a broken network (NaN) and a network whose residual stalls
+  hand over to plain PCG;
 * training lowers the loss and the FCG iteration count (the gain test);
 * multigrid: with the network's operator as the finest-level smoother of the
   aggregation V-cycle, the untrained network equals Jacobi smoothing, the
@@ -24,7 +25,8 @@ from oracle import gnn_ref
 from oracle.oracle import Oracle
 from programs_b200 import learn
 from programs_b200.mesh import Mesh, cavity_field, momentum_field, pressure_correction, uniform
-from programs_b200.solver import (OK, OPT_MG_LEVELS, OPT_MG_SMOOTHER, OPT_PRECISION)
+from programs_b200.solver import (OK, OPT_FCG_STALL_DROP, OPT_FCG_STALL_ITERS, OPT_MG_LEVELS,
+                                  OPT_MG_SCALE_MIN, OPT_MG_SMOOTHER, OPT_PRECISION)
 
 pytestmark = pytest.mark.gpu
 
@@ -324,6 +326,55 @@ def test_multigrid_broken_network_falls_back_to_pcg(gpu):
     phi, st, rn = _solve_fcg(gpu, A, b)
     x_ref, _ = _ref_iters(A, b)
     assert st["status"] == OK and st["fallbacks"] >= 1
+    assert _rel(phi, x_ref) <= AGREE_1E10
+
+
+def test_starved_smoother_stalls_and_hands_over_to_pcg(gpu):
+    """A network whose per-cell scales are all near zero (b_a = -30, s about
+    4e-7) leaves the finest level unsmoothed: the V-cycle is then only the
+    coarse correction, which keeps positive curvature but cannot reduce the
+    error outside the coarse space, so flexible CG stalls.  With the scale
+    floor switched off the stall detector must hand over to Jacobi-PCG from
+    the current iterate, which converges to the oracle's solution; with the
+    default floor (0.5) the same network is held back to a working smoother
+    and needs no hand-over."""
+    A = _system(16, seed=9)
+    gpu.matrix_set(A)
+    p = learn.init_params(0)
+    p[learn.P_BA] = -30.0
+    gpu.gnn_set_params(p)
+    b = _rhs(A, 13)
+    x_ref, _ = _ref_iters(A, b)
+    gpu.set_option(OPT_MG_SCALE_MIN, 0.0)
+    try:
+        phi, st, rn = _solve_fcg(gpu, A, b)
+    finally:
+        gpu.set_option(OPT_MG_SCALE_MIN, 0.5)
+    assert st["status"] == OK and st["fallbacks"] == 1, st
+    assert np.abs(b - A.to_scipy() @ phi[:, 0]).sum() / rn[0] < 1e-10
+    assert _rel(phi, x_ref) <= AGREE_1E10
+    phi, st, rn = _solve_fcg(gpu, A, b)
+    assert st["status"] == OK and st["fallbacks"] == 0, st
+    assert _rel(phi, x_ref) <= AGREE_1E10
+
+
+def test_stall_window_hands_over_once(gpu):
+    """The stall window itself: demanding a 1e6 drop within every window of
+    one iteration makes the first check hand the solve over to Jacobi-PCG,
+    exactly once, and the solve still ends at the oracle's solution."""
+    A = _system(12, seed=10)
+    gpu.matrix_set(A)
+    gpu.gnn_set_params(learn.init_params(0))
+    b = _rhs(A, 14)
+    x_ref, _ = _ref_iters(A, b)
+    gpu.set_option(OPT_FCG_STALL_ITERS, 1)
+    gpu.set_option(OPT_FCG_STALL_DROP, 1e-6)
+    try:
+        phi, st, rn = _solve_fcg(gpu, A, b)
+    finally:
+        gpu.set_option(OPT_FCG_STALL_ITERS, 100)
+        gpu.set_option(OPT_FCG_STALL_DROP, 0.5)
+    assert st["status"] == OK and st["fallbacks"] == 1, st
     assert _rel(phi, x_ref) <= AGREE_1E10
 
 

@@ -217,21 +217,22 @@ def test_reference_guard_floors_weakly_driven_systems():
 def test_fixtures_regenerate_bit_for_bit(tmp_path):
     """tests/golden/make_golden.py rebuilds the committed fixtures exactly:
     the mesh generator, the assembly, the seeded right-hand sides and the
-    oracle have not drifted from what the fixtures hold.  The cavity
-    fixture is rebuilt only where the reference's cavity_3d.neu is
-    available."""
+    oracle have not drifted from what the fixtures hold.  The fixtures of
+    the reference's own meshes are rebuilt only where SPRAY_SIMULATION_DIR
+    names the reference's spray-simulation/ directory."""
     import importlib.util
     spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
     mg = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mg)
     mg.hex6(str(tmp_path))
     names = ["hex6.npz"]
-    neu = os.environ.get("CAVITY_NEU", mg.DEFAULT_NEU)
-    if os.path.exists(neu):
+    neu = mg.reference_mesh("cavity_3d.neu")
+    if neu and os.path.exists(neu):
         mg.cavity(neu, str(tmp_path))
         names.append("cavity_3d.npz")
-    if os.path.exists(mg.DEFAULT_NEU_2D):
-        mg.channel(mg.DEFAULT_NEU_2D, str(tmp_path))
+    neu2 = mg.reference_mesh("channel_2d.neu")
+    if neu2 and os.path.exists(neu2):
+        mg.channel(neu2, str(tmp_path))
         names.append("channel_2d.npz")
     for name in names:
         new, old = np.load(str(tmp_path / name)), _load(name)

@@ -87,10 +87,19 @@ def test_noalloc_rejects_what_it_cannot_hold():
     inb_bad[np.argmax(A.inb > 0)] = N + 7  # one face points past the last cell
     inb = torch.from_numpy(inb_bad).to(dev)
     p, n, pl = (torch.from_numpy(x).to(dev) for x in (A.p, A.n, A.pl))
-    phi = torch.zeros(N * 5, dtype=torch.float64, device=dev)
-    r = torch.zeros(N * 5, dtype=torch.float64, device=dev)
-    rn = torch.zeros(5, dtype=torch.float64, device=dev)
+    phi = torch.ones(N * 5, dtype=torch.float64, device=dev)
+    r = torch.full((N * 5,), 2.0, dtype=torch.float64, device=dev)
+    rn = torch.full((5,), 3.0, dtype=torch.float64, device=dev)
     fn = _noalloc()
     args = (ip.data_ptr(), inb.data_ptr(), p.data_ptr(), n.data_ptr(), pl.data_ptr())
     assert fn(N, F, *args, 5, phi.data_ptr(), r.data_ptr(), rn.data_ptr(), 0, None) == 9  # n_vc > 4
+    assert fn(N, F, *args, 0, phi.data_ptr(), r.data_ptr(), rn.data_ptr(), 0, None) == 4  # n_vc < 1
+    assert fn(N, F, *args, -1, phi.data_ptr(), r.data_ptr(), rn.data_ptr(), 0, None) == 4
     assert fn(N, F, *args, 1, phi.data_ptr(), r.data_ptr(), rn.data_ptr(), 0, None) == 4  # bad index
+    # the bad index is found before anything is written
+    assert bool((r == 2.0).all()) and bool((rn == 3.0).all())
+    # and the scratch is left usable: a valid call right after succeeds
+    inb_ok = torch.from_numpy(A.inb.astype(np.int32)).to(dev)
+    args_ok = (ip.data_ptr(), inb_ok.data_ptr(), p.data_ptr(), n.data_ptr(), pl.data_ptr())
+    assert fn(N, F, *args_ok, 1, phi.data_ptr(), r.data_ptr(), rn.data_ptr(), 0, None) == 0
+    assert float(rn[0]) >= 0.0 and float(rn[0]) != 3.0
