@@ -191,7 +191,11 @@ int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
  * path: which 0 = FP64 matrix product, 1 = FP32 matrix product, 2 = the
  * learned preconditioner's one-level application (FP32), 3 = one V-cycle
  * of the multigrid preconditioner (FP32, all its kernels, with the current
- * SOLV_OPT_MG_* settings).  No counterpart in the reference; used for
+ * SOLV_OPT_MG_* settings), 4 = the V-cycle's level-0 residual t = b - A x
+ * (FP32), 5 = the network operator's smoothing step (FP32), 6 = the
+ * flexible-CG product q = A p with p.q and p.r (FP32), 7 = the FP64 CG
+ * product q = A p with p.q, 8 = one DILU application M^-1 r (forward and
+ * backward recurrence, FP64).  No counterpart in the reference; used for
  * roofline reporting. */
 int solv_gpu_kernel_time(solv_gpu_ctx *ctx, int which, int repeat,
                          float *ms_per_launch);

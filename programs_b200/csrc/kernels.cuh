@@ -196,12 +196,17 @@ struct RowIt {
 // FP64).  For the smooth vectors late Krylov iterations produce, x_j - x_i
 // is exact and small, so the product keeps its relative accuracy instead of
 // losing log10(cond) digits to cancellation; same bytes moved.
-// FP32 rows are walked kRowChunk slots at a time: the column indices, the
-// coefficients and the gathered x of a chunk are all loaded before any of
-// them is used, so a warp keeps several independent gathers in flight; the
-// sums still run slot by slot.  (FP64 keeps the plain walk: chunks would
-// spill under the reduction kernels' 32-register cap.)
+// Rows are walked a chunk of slots at a time (4 in FP32, 2 in FP64, where
+// wider chunks would spill under the reduction kernels' 32-register cap):
+// the column indices, the coefficients and the gathered x of a chunk are
+// all loaded before any of them is used, so a warp keeps several
+// independent gathers in flight; the sums still run slot by slot in face
+// order, so the FP64 product stays bit for bit the reference's.
+#ifndef SG_ROW_CHUNK64
+#define SG_ROW_CHUNK64 2
+#endif
 constexpr int kRowChunk = 4;
+constexpr int kRowChunk64 = SG_ROW_CHUNK64;
 
 template <typename T, int V>
 __device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
@@ -242,14 +247,30 @@ __device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
   } else {
 #pragma unroll
     for (int v = 0; v < V; ++v) y[v] = mul(d, x[(size_t)i * V + v]);
-    for (int k = 0; k < it.w; ++k) {
-      const int e = it.base + k * kWarp;
-      const int j = __ldg(&R.col[e]);
-      if (j >= 0) {
-        const T a = R.val[e];
+    constexpr int C = V == 1 ? kRowChunk64 : 1;
+    for (int k0 = 0; k0 < it.w; k0 += C) {
+      int j[C];
+      T a[C], xv[C][V];
 #pragma unroll
-        for (int v = 0; v < V; ++v) y[v] = add(y[v], mul(a, x[(size_t)j * V + v]));
+      for (int u = 0; u < C; ++u) {
+        j[u] = -1;
+        a[u] = T(0);
+        if (k0 + u < it.w) {
+          const int e = it.base + (k0 + u) * kWarp;
+          j[u] = __ldg(&R.col[e]);
+          a[u] = R.val[e];
+        }
       }
+#pragma unroll
+      for (int u = 0; u < C; ++u)
+#pragma unroll
+        for (int v = 0; v < V; ++v) xv[u][v] = j[u] >= 0 ? x[(size_t)j[u] * V + v] : T(0);
+#pragma unroll
+      for (int u = 0; u < C; ++u)
+        if (j[u] >= 0) {
+#pragma unroll
+          for (int v = 0; v < V; ++v) y[v] = add(y[v], mul(a[u], xv[u][v]));
+        }
     }
   }
 }

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -1668,6 +1669,87 @@ int solve_dispatch(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_it
                    double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
                    solv_gpu_stats* st, int* out_iters, double* out_ratio);
 
+// Device time per launch of the kernels that dominate the solves, each
+// launched `repeat` times back to back on workspace vectors (CUDA events on
+// the context's stream):
+//   4 k_mg_resid       level-0 residual t = b - A x of the V-cycle (FP32)
+//   5 k_mg_net<false>  the network's smoothing step x = w K b (FP32)
+//   6 k_fcg_spmv       flexible-CG product q = A p with p.q and p.r (FP32)
+//   7 k_cg_spmv        FP64 CG product q = A p with p.q (the plain PCG's)
+//   8 one DILU application z = M^-1 r, forward + backward recurrence (FP64)
+int kernel_time_solve(solv_gpu_ctx* c, int which, int repeat, float* ms_per_launch) {
+  const int N = c->N;
+  cudaStream_t s = c->stream;
+  int rc;
+  if (c->n_seg != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "kernel_time: one system only");
+  std::function<int()> launch;
+  WS<double> w;
+  WS<float> f;
+  if ((rc = ensure_ws<double>(c, 1, w)) || (rc = ensure_ws<float>(c, 1, f)) ||
+      (rc = ensure_f32_matrix(c)))
+    return rc;
+  sg::k_mp_start<1><<<grid_for(c, N), c->block, 0, s>>>(N, c->diag.as<double>(), f.r, f.p, f.q);
+  sg::k_mp_start<1><<<grid_for(c, N), c->block, 0, s>>>(N, c->diag.as<double>(), f.z, f.v, f.phi);
+  CUDA_TRY(c, cudaMemcpyAsync(w.p, c->diag.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(w.r, c->diag.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  SegMap sm = segmap(c);
+  {
+    Lane L{};
+    L.active = 1;
+    L.n_iter = 1 << 30;
+    L.reduc = 0.0;
+    L.res0_n = 1.0;
+    L.s = 1.0;
+    L.gs = 1.0;
+    const int one = 1;
+    CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, &L, sizeof(Lane), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+  }
+  const int G = c->seg.total_blk, B = c->block;
+  double* part = c->part.as<double>();
+  Lane* lanes = c->lanes.as<Lane>();
+  if (which == 4) {
+    launch = [&]() {
+      mg::k_mg_resid<<<grid_for(c, N), B, 0, s>>>(N, rows<float>(c), f.r, f.p, f.q, nullptr);
+      return SOLV_GPU_OK;
+    };
+  } else if (which == 5) {
+    if ((rc = gnn_prepare(c))) return rc;
+    gnn_build<float>(c, f.r);
+    launch = [&]() {
+      mg::k_mg_net<false, float><<<grid_for(c, N), B, 0, s>>>(
+          N, rows<float>(c), c->g_ge.as<float>(), c->g_q.as<float>(), (float)c->mg_omega, f.r,
+          nullptr, f.q, nullptr);
+      return SOLV_GPU_OK;
+    };
+  } else if (which == 6) {
+    launch = [&]() {
+      sg::k_fcg_spmv<float><<<G, B, 0, s>>>(rows<float>(c), sm, f.p, f.q, f.r, part, lanes);
+      return SOLV_GPU_OK;
+    };
+  } else if (which == 7) {
+    launch = [&]() {
+      sg::k_cg_spmv<double, 1><<<G, B, 0, s>>>(rows<double>(c), sm, w.p, w.q, part, lanes);
+      return SOLV_GPU_OK;
+    };
+  } else {
+    if ((rc = launch_precond(c, 2, w.c, w.cr))) return rc;
+    launch = [&]() { return launch_direct<double, 1>(c, 2, w.c, w.cr, w.z, w.r, nullptr); };
+  }
+  if ((rc = launch())) return rc;
+  CUDA_TRY(c, cudaEventRecord(c->ev0, s));
+  for (int k = 0; k < repeat; ++k)
+    if ((rc = launch())) return rc;
+  CUDA_TRY(c, cudaEventRecord(c->ev1, s));
+  CUDA_TRY(c, cudaEventSynchronize(c->ev1));
+  CUDA_TRY(c, cudaGetLastError());
+  if (which == 8 && (rc = sweep_check(c))) return rc;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  *ms_per_launch = ms / repeat;
+  return SOLV_GPU_OK;
+}
+
 }  // namespace
 
 // =============================== C-ABI ========================================
@@ -1993,12 +2075,13 @@ int solv_gpu_spmv_dev(solv_gpu_ctx* c, const double* x_dev, double* y_dev, int r
 int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_launch) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
-  if (which < 0 || which > 3 || repeat < 1 || !ms_per_launch)
+  if (which < 0 || which > 8 || repeat < 1 || !ms_per_launch)
     return set_err(c, SOLV_GPU_BAD_INPUT, "kernel_time: bad arguments");
   CUDA_TRY(c, cudaSetDevice(c->dev));
   const int N = c->N;
   cudaStream_t s = c->stream;
   int rc;
+  if (which >= 4) return kernel_time_solve(c, which, repeat, ms_per_launch);
   if (which == 0) {
     WS<double> w;
     if ((rc = ensure_ws<double>(c, 1, w))) return rc;

@@ -425,7 +425,10 @@ class GpuSolver:
         return d
 
     def kernel_time(self, which: int, repeat: int = 20) -> float:
-        """ms per launch: 0 FP64 SpMV, 1 FP32 SpMV, 2 learned-preconditioner apply."""
+        """ms per launch (solv_gpu_kernel_time): 0 FP64 SpMV, 1 FP32 SpMV, 2 the
+        network operator, 3 one V-cycle, 4 level-0 residual of the V-cycle,
+        5 the network's smoothing step, 6 flexible-CG product, 7 FP64 CG
+        product, 8 one DILU application (both recurrences)."""
         ms = ctypes.c_float()
         self._check(self._lib.solv_gpu_kernel_time(self._h, which, repeat, ctypes.byref(ms)))
         return ms.value

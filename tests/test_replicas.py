@@ -12,6 +12,7 @@ import socket
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
@@ -78,6 +79,14 @@ def test_reference_arm_under_torchrun_prints_once_from_rank_zero(built):
                         "d2h_bytes_per_step": 0}
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] == 1
     assert d["cpu_baseline"]["host_threads"] >= 1 and "cpu_model" in d["cpu_baseline"]
+    # the value is an extrapolation and says so; the step time is what was measured
+    assert d["cpu_baseline"]["sample"].startswith("EXTRAPOLATED")
+    assert d["oracle_iterations"] > 0 and "full oracle solve" in d["oracle_iterations_source"]
+    assert d["ms_per_step"] < 1e3 * d["value"]
+    chk = d["extrapolation_check"]
+    assert set(chk) == {"32^3", "64^3"}
+    for v in chk.values():
+        assert v["iterations"] > 0 and 0.3 < v["extrapolated_over_full"] < 3.0
 
 
 @pytest.mark.parametrize("line,reasons", [
@@ -94,13 +103,35 @@ def test_clock_sampler_reads_nvidia_smi_lines(line, reasons):
     assert s["sm_mhz"] == float(line.split(",")[1]) and s["sm_max_mhz"] == 1965.0
 
 
-def test_cpu_baseline_is_a_median_of_bounded_samples(built):
-    """bench.cpu_baseline: the oracle's plain PCG timed as the median of
-    three bounded runs, scaled to the full solve's iteration count."""
+def test_cpu_oracle_sample_is_bounded(built):
+    """bench.cpu_oracle_sample: the oracle's plain PCG timed per iteration
+    over bounded samples (the CPU baseline extrapolates from these)."""
     import bench
     from programs_b200.mesh import Mesh, poisson_rhs
     A = Mesh.hex(10, jitter=0.15, seed=0, permute=True).pressure(pin=1)
     b = poisson_rhs(A.n_cell, 1)
-    v, s, total = bench.cpu_baseline(A, b, 1000, budget_s=0.3)
-    assert v > 0 and 2 <= s <= 200 and total > 0
-    assert v < 1000 * total          # per-iteration time times 1000, not more
+    per, s = bench.cpu_oracle_sample(A, b, 0.3, repeats=3)
+    assert len(per) == 3 and all(p > 0 for p in per) and 2 <= s <= 400
+
+
+def test_oracle_iteration_counts_are_the_oracles_own(built):
+    """The CPU baseline extrapolates with the oracle's own iteration count:
+    recorded from a full 256^3 oracle solve, computed in full for small
+    systems -- never the GPU solver's count."""
+    import bench
+    from oracle.oracle import Oracle
+    full = bench.oracle_full_solve(256)
+    assert full is not None and full["iterations"] > 1000
+    A, b = bench.build_system(10)
+    it, src = bench.oracle_iterations(A, b, 10)
+    ref = Oracle.from_matrix(A).solv_cg(0, 1e-10, 100000, np.zeros((A.n_cell, 1)),
+                                        b.reshape(-1, 1))
+    assert it == int(ref[3][0]) and src == "full oracle solve, this run"
+
+
+def test_extrapolation_check_compares_full_solves(built):
+    import bench
+    chk = bench.extrapolation_check(sizes=(8, 12), sample=5)
+    assert set(chk) == {"8^3", "12^3"}
+    for v in chk.values():
+        assert v["full_solve_s"] > 0 and v["extrapolated_s"] > 0 and v["iterations"] > 0
