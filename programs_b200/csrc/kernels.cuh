@@ -528,10 +528,14 @@ __global__ void k_fill_pending(long long n, T* __restrict__ x) {
     x[e] = Pending<T>::value();
 }
 
-// Warp-level driver of one recurrence.  `step(i, k)` advances cell i (this
-// lane's) from slot k as far as its inputs allow and returns the next slot
-// (w when the cell is done and stored).  Slices are taken in the order that
-// makes every dependency point to an earlier (or the same) slice.
+// Warp-level driver of one recurrence.  `step(i, k, first)` advances cell i
+// (this lane's) from slot k as far as its inputs allow and returns the next
+// slot (w when the cell is done and stored).  Slices are taken in the order
+// that makes every dependency point to an earlier (or the same) slice.  A
+// warp whose lanes wait spins for kSweepSpin polls, then sleeps briefly
+// between polls.
+constexpr int kSweepSpin = 64;
+
 template <bool UP, typename Step>
 __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ slice_w,
                                              SweepCtl* ctl, Step&& step) {
@@ -543,8 +547,7 @@ __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ 
     const int s = UP ? ns - 1 - r : r;
     const int i = s * 32 + lane;
     const int w = __ldg(&slice_w[s]);
-    int k = i < n ? 0 : w;
-    k = step(i, k, true);
+    int k = step(i, i < n ? 0 : w, true);
     for (int poll = 0;; ++poll) {
       __syncwarp();
       if (__all_sync(0xffffffffu, k >= w)) break;
@@ -552,10 +555,44 @@ __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ 
         if (lane == 0) atomicExch(&ctl->err, 1);
         break;
       }
-      __nanosleep(20);
+      if (poll >= kSweepSpin) __nanosleep(64);
       if (k < w) k = step(i, k, false);
     }
   }
+}
+
+// One advance of a recurrence row: from slot k, the slots of the dependency
+// side (`dep(j)`) are taken in chunks of C -- all their values loaded at
+// once (one round trip to L2 per chunk), then added in slot order up to the
+// first one still pending.  `use(e, xv)` folds a ready value in.  Returns
+// the slot to resume from (w when the row is complete).
+template <int C, int V, typename T, typename Dep, typename Use>
+__device__ __forceinline__ int advance(const Rows<T>& R, int base, int w, int k, const T* vals,
+                                       Dep&& dep, Use&& use) {
+  while (k < w) {
+    int j[C];
+    T xv[C][V];
+    bool rdy[C];
+#pragma unroll
+    for (int u = 0; u < C; ++u) {
+      j[u] = k + u < w ? __ldg(&R.col[base + (k + u) * kWarp]) : -1;
+      rdy[u] = true;
+      if (j[u] >= 0 && dep(j[u])) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) rdy[u] &= take(&vals[(size_t)j[u] * V + v], xv[u][v]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < C; ++u) {
+      if (k >= w) return w;
+      if (j[u] >= 0 && dep(j[u])) {
+        if (!rdy[u]) return k;
+        use(base + k * kWarp, xv[u]);
+      }
+      ++k;
+    }
+  }
+  return k;
 }
 
 // solv_precond.f90:10-29: d_i = pl_i - sum_{j<i} n^2 c_j (DIC, imat 1) or
@@ -577,20 +614,17 @@ __global__ void __launch_bounds__(kSweepThreads) k_precond_sf(
       d = R.diag[i];
     }
     if (imat == 1 || imat == 2) {
-      for (; k < w; ++k) {
-        const int e = base + k * kWarp;
-        const int j = __ldg(&R.col[e]);
-        if (!(j >= 0 && j < i)) continue;
-        double cj;
-        if (!take(&c[j], cj)) return k;
-        const int f = __ldg(&slot_src[e]) >> 1;
-        if (imat == 1) {
-          const double nf = fn[f];
-          d = sub(d, mul(mul(nf, nf), cj));
-        } else {
-          d = sub(d, mul(mul(fp[f], cj), fn[f]));
-        }
-      }
+      k = advance<4, 1>(R, base, w, k, c, [&](int j) { return j < i; },
+                        [&](int e, const double (&cj)[1]) {
+                          const int f = __ldg(&slot_src[e]) >> 1;
+                          if (imat == 1) {
+                            const double nf = fn[f];
+                            d = sub(d, mul(mul(nf, nf), cj[0]));
+                          } else {
+                            d = sub(d, mul(mul(fp[f], cj[0]), fn[f]));
+                          }
+                        });
+      if (k < w) return k;
     }
     c_r[i] = d;
     st_relaxed(&c[i], 1.0 / add(d, kSmall));
@@ -607,6 +641,8 @@ __global__ void k_precond_jacobi(int n, const double* __restrict__ diag, double*
     c[i] = 1.0 / add(d, kSmall);
   }
 }
+
+template <int V> struct SweepChunk { static constexpr int value = V == 1 ? 4 : 2; };
 
 // solv_direct.f90:12-24 forward sweep, x_i = (b_i - sum_{j<i} n x_j) c_i, into
 // t (which starts out pending); the backward sweep's output x is reset to
@@ -627,19 +663,14 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_fwd_sf(
 #pragma unroll
       for (int v = 0; v < V; ++v) acc[v] = bvec[(size_t)i * V + v];
     }
-    for (; k < w; ++k) {
-      const int e = base + k * kWarp;
-      const int j = __ldg(&R.col[e]);
-      if (!(j >= 0 && j < i)) continue;
-      T xv[V];
-      bool ok = true;
+    k = advance<SweepChunk<V>::value, V>(R, base, w, k, t, [&](int j) { return j < i; },
+                                         [&](int e, const T (&xv)[V]) {
+                                           const T a = R.sval[e];
 #pragma unroll
-      for (int v = 0; v < V; ++v) ok &= take(&t[(size_t)j * V + v], xv[v]);
-      if (!ok) return k;
-      const T a = R.sval[e];
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, xv[v]));
-    }
+                                           for (int v = 0; v < V; ++v)
+                                             acc[v] = sub(acc[v], mul(a, xv[v]));
+                                         });
+    if (k < w) return k;
     const T ci = c[i];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
@@ -670,19 +701,14 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_bwd_sf(
 #pragma unroll
       for (int v = 0; v < V; ++v) acc[v] = mul(t[(size_t)i * V + v], cr);
     }
-    for (; k < w; ++k) {
-      const int e = base + k * kWarp;
-      const int j = __ldg(&R.col[e]);
-      if (!(j > i)) continue;
-      T xv[V];
-      bool ok = true;
+    k = advance<SweepChunk<V>::value, V>(R, base, w, k, x, [&](int j) { return j > i; },
+                                         [&](int e, const T (&xv)[V]) {
+                                           const T a = R.sval[e];
 #pragma unroll
-      for (int v = 0; v < V; ++v) ok &= take(&x[(size_t)j * V + v], xv[v]);
-      if (!ok) return k;
-      const T a = R.sval[e];
-#pragma unroll
-      for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, xv[v]));
-    }
+                                           for (int v = 0; v < V; ++v)
+                                             acc[v] = sub(acc[v], mul(a, xv[v]));
+                                         });
+    if (k < w) return k;
     const T ci = c[i];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
@@ -692,6 +718,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_bwd_sf(
     return w;
   });
 }
+
 // Jacobi: x = b*c (solv_direct.f90:41)
 template <typename T, int V>
 __global__ void k_jacobi(int n, const T* __restrict__ c, const T* __restrict__ bvec,
