@@ -32,8 +32,8 @@ structure itself: `first_call_s` reports that first solve.
 The other configurations are timed after the headline and reported as
 extra keys (`configs`): the 32^3 plain PCG of the reference's own scale,
 BiCGSTAB + DILU on the 128^3 momentum system in FP64 and with FP32 inner
-iterations, and the batched solves (u, v, w on one 96^3 mesh; 64 uneven
-meshes of 8k-500k cells).
+iterations (in RCM order and in the multicolour order), and the batched
+solves (u, v, w on one 96^3 mesh; 64 uneven meshes of 8k-500k cells).
 
 The reference arm (--impl reference) and `cpu_baseline` time the CPU
 oracle -- the line-faithful C restatement of the Fortran solver, single
@@ -366,13 +366,16 @@ def time_configs(s, torch, dev):
     s.matrix_set(A)
     b = poisson_rhs(A.n_cell, 1).reshape(-1, 1)
     out["pressure_32_plain_pcg"] = timed_solve("cg", 0, 1, b)
-    # C2: 128^3 momentum, BiCGSTAB + DILU, FP64 and FP32 inner
-    A, b = make_system(128, "momentum")
-    s.matrix_set(A)
-    c2 = {"levels": s.levels}
-    for name, prec in (("fp64", 0), ("fp32_inner", 1)):
-        c2[name] = timed_solve("bicg", 2, 1, b.reshape(-1, 1), precision=prec)
-    out["momentum_128_bicgstab_dilu"] = c2
+    # C2: 128^3 momentum, BiCGSTAB + DILU, FP64 and FP32 inner, in RCM order
+    # (the recurrences 382 levels deep) and in the multicolour order (2
+    # levels; a different factorisation, so other iteration counts)
+    for order in ("rcm", "color"):
+        A, b = make_system(128, "momentum", renumber=order)
+        s.matrix_set(A)
+        c2 = {"sweep_levels": s.levels}
+        for name, prec in (("fp64", 0), ("fp32_inner", 1)):
+            c2[name] = timed_solve("bicg", 2, 1, b.reshape(-1, 1), precision=prec)
+        out[f"momentum_128_bicgstab_dilu_{order}"] = c2
     # C3a: u, v, w on one 96^3 mesh (shared matrix), BiCGSTAB + DILU, FP32 inner
     A, b = make_system(96, "momentum")
     s.matrix_set(A)

@@ -29,6 +29,8 @@ def make_system(size, system="pressure", seed=0, renumber="rcm"):
         m.renumber(Mesh.RCM)
     elif renumber == "sfc":
         m.renumber(Mesh.SFC)
+    elif renumber == "color":
+        m.renumber(Mesh.COLOR)
     if system == "pressure":
         A = m.pressure(pin=1)
         b = poisson_rhs(A.n_cell, seed + 1)
@@ -77,7 +79,7 @@ def main(argv=None):
     ap.add_argument("--n-vc", type=int, default=1)
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--graph-iters", type=int, default=16)
-    ap.add_argument("--renumber", default="rcm", choices=["rcm", "sfc", "none"])
+    ap.add_argument("--renumber", default="rcm", choices=["rcm", "sfc", "color", "none"])
     ap.add_argument("--n-sys", type=int, default=64)
     ap.add_argument("--min", type=int, default=8000)
     ap.add_argument("--max", type=int, default=500000)

@@ -400,6 +400,39 @@ int fvm_mesh_renumber(fvm_mesh *m, int method, int *perm) {
   const int N = m->n_cell;
   std::vector<int32_t> order;  // order[new] = old
   order.reserve(N);
+  if (method == 4) {
+    // Multicolour: reverse Cuthill-McKee first (locality), then a greedy
+    // colouring in that order (smallest colour no coloured neighbour has),
+    // then cells colour by colour, each colour in RCM order.  The lower
+    // triangle then couples only earlier colours, so the DIC / DILU
+    // recurrences are as deep as the number of colours (2 for a hex mesh:
+    // its face graph is bipartite and RCM visits it level by level).
+    std::vector<int> rcm(N);
+    if (fvm_mesh_renumber(m, 1, rcm.data()) != 0) return -1;
+    std::vector<int> colour(N, -1);
+    int nc = 0;
+    for (int c = 0; c < N; ++c) {
+      unsigned used = 0;
+      for (int k = 0; k < 6; ++k) {
+        const int nb = m->cell_nbr[(size_t)c * 6 + k];
+        if (nb >= 0 && colour[nb] >= 0 && colour[nb] < 32) used |= 1u << colour[nb];
+      }
+      int col = 0;
+      while (col < 32 && (used >> col & 1u)) ++col;
+      colour[c] = col;
+      nc = std::max(nc, col + 1);
+    }
+    order.resize(N);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return colour[a] < colour[b]; });
+    std::vector<int32_t> second(N);
+    for (int i = 0; i < N; ++i) second[order[i]] = i + 1;
+    if (fvm_mesh_renumber(m, 3, second.data()) != 0) return -1;
+    if (perm)
+      for (int c = 0; c < N; ++c) perm[c] = second[rcm[c] - 1];
+    return 0;
+  }
   if (method == 1) {
     // Reverse Cuthill-McKee: BFS from a pseudo-peripheral cell (repeated
     // BFS to the farthest, least-connected cell), neighbours by degree.

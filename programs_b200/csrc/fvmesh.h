@@ -63,7 +63,9 @@ void fvm_mesh_cell_geom(const fvm_mesh *m, double *xc, double *vol);
 
 /* Renumber cells.  method 1 = reverse Cuthill-McKee, 2 = Morton
  * space-filling curve of the cell centres, 3 = a given permutation in
- * perm (new 1-based index of old cell i).  The face list is re-emitted
+ * perm (new 1-based index of old cell i), 4 = multicolour (a greedy
+ * colouring in RCM order, cells colour by colour, RCM order inside a
+ * colour: the DIC / DILU recurrences become as deep as the colour count).  The face list is re-emitted
  * under the new numbering.  On return perm (if not NULL and method != 3)
  * holds the permutation applied.  Returns 0, or -1 on bad input. */
 int fvm_mesh_renumber(fvm_mesh *m, int method, int *perm);

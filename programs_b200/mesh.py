@@ -101,6 +101,7 @@ class FaceMatrix:
 class Mesh:
     RCM = 1
     SFC = 2
+    COLOR = 4  # multicolour: colour by colour, RCM order inside a colour
 
     def __init__(self, handle: int):
         if not handle:
@@ -167,7 +168,8 @@ class Mesh:
         return xc, vol
 
     def renumber(self, method: int) -> np.ndarray:
-        """Renumber cells in place (RCM or SFC); returns new index of old cell (1-based)."""
+        """Renumber cells in place (RCM, SFC or COLOR); returns new index of old
+        cell (1-based)."""
         perm = np.empty(self.n_cell, np.int32)
         rc = self._lib.fvm_mesh_renumber(self._h, method, _p(perm, _i32p))
         if rc != 0:

@@ -46,6 +46,8 @@ CASES = {
     "p12_sfc": lambda: _pressure(12, seed=3, renumber=Mesh.SFC),
     "m10_perm": lambda: _momentum(10),
     "m12_rcm": lambda: _momentum(12, seed=2, renumber=Mesh.RCM),
+    "p12_color": lambda: _pressure(12, seed=4, renumber=Mesh.COLOR),
+    "m12_color": lambda: _momentum(12, seed=5, renumber=Mesh.COLOR),
 }
 
 

@@ -42,7 +42,7 @@ def test_geometry_closes():
     assert np.abs(acc).max() < 1e-14
 
 
-@pytest.mark.parametrize("method", [Mesh.RCM, Mesh.SFC])
+@pytest.mark.parametrize("method", [Mesh.RCM, Mesh.SFC, Mesh.COLOR])
 @pytest.mark.parametrize("jitter", [0.0, 0.15])
 def test_renumber_is_a_similarity(method, jitter):
     """A renumbered mesh gives the permuted matrix.  The face list is re-emitted
@@ -72,6 +72,37 @@ def test_rcm_reduces_bandwidth():
     ip, inb = m.faces()
     bw1 = np.abs(inb[inb > 0] - ip[inb > 0]).max()
     assert bw1 < bw0 / 4
+
+
+def _sweep_depth(A):
+    """Wavefront levels of the lower-triangular recurrence (DIC / DILU)."""
+    N = A.n_cell
+    nb = [[] for _ in range(N)]
+    for a, b in zip(A.ip, A.inb):
+        if b > 0:
+            nb[a - 1].append(b - 1)
+            nb[b - 1].append(a - 1)
+    lev = np.zeros(N, int)
+    for i in range(N):
+        lev[i] = max([lev[j] + 1 for j in nb[i] if j < i], default=0)
+    return int(lev.max()) + 1
+
+
+@pytest.mark.parametrize("shape", [(9, 9, 9), (12, 7, 1)])
+def test_multicolour_ordering_makes_the_recurrences_two_deep(shape):
+    """A hex mesh's face graph is bipartite: the multicolour ordering puts
+    the cells in two colours, so every lower neighbour of a cell lies in
+    the other, earlier colour and the DIC / DILU recurrences are two levels
+    deep (against about nx + ny + nz in RCM order)."""
+    m = Mesh.hex(*shape, jitter=0.15, seed=6, permute=True)
+    m.renumber(Mesh.RCM)
+    depth_rcm = _sweep_depth(m.pressure(pin=1))
+    m = Mesh.hex(*shape, jitter=0.15, seed=6, permute=True)
+    m.renumber(Mesh.COLOR)
+    A = m.pressure(pin=1)
+    assert _sweep_depth(A) == 2 and depth_rcm > 2 * min(s for s in shape if s > 1)
+    ip, inb = m.faces()
+    assert np.all(inb[inb > 0] > ip[inb > 0])
 
 
 def test_given_permutation():
