@@ -388,16 +388,16 @@ def test_golden_fixtures(gpu, fname, prefix, solvers):
                 assert abs(st["iters"][v] - int(d[k + "iters"][v])) <= max(2, tol * int(d[k + "iters"][v]))
 
 
-def _two_components(gpu, A, b, imat, solver, it_tol=0.0):
+def _two_components(gpu, A, b, imat, solver, it_tol=0.0, reduc=1e-10):
     """n_vc = 2 (the reference's 2-d momentum, u and v) through the C-ABI
     against the oracle, both components in one call."""
     o = Oracle.from_matrix(A)
-    ref = getattr(o, "solv_" + solver)(imat, 1e-10, 5000, np.zeros((A.n_cell, 2)), b)
+    ref = getattr(o, "solv_" + solver)(imat, reduc, 5000, np.zeros((A.n_cell, 2)), b)
     gpu.matrix_set(A)
     phi = np.zeros((A.n_cell, 2))
     res0 = np.asfortranarray(b.copy())
     rn = np.zeros(2)
-    st = getattr(gpu, "solv_" + solver)(imat, 1e-10, 5000, phi, res0, rn)
+    st = getattr(gpu, "solv_" + solver)(imat, reduc, 5000, phi, res0, rn)
     assert st["status"] == OK and len(st["iters"]) == 2
     assert np.array_equal(res0, ref[1])
     for v in range(2):
@@ -418,8 +418,10 @@ def test_two_components_on_the_reference_channel_2d(gpu, imat):
     A = FaceMatrix(int(d["n_cell"]), d["ip"], d["inb"], d["p"], d["n"], d["pl"])
     b = np.asfortranarray(np.stack([d["b"][:, 0], uniform(31, A.n_cell)], axis=1))
     # BiCGSTAB on this symmetric pressure system converges erratically (as in
-    # test_golden_fixtures): iteration counts within 15%
-    _two_components(gpu, A, b, imat, "bicg", it_tol=0.15)
+    # test_golden_fixtures): iteration counts within 15%, and the tree-ordered
+    # reductions take the GPU along a slightly different path, so both solves
+    # run to 1e-12, where the paths' end points agree within the 1e-8 bar
+    _two_components(gpu, A, b, imat, "bicg", it_tol=0.15, reduc=1e-12)
 
 
 @pytest.mark.parametrize("imat", [0, 2])
