@@ -196,14 +196,16 @@ struct RowIt {
 // FP64).  For the smooth vectors late Krylov iterations produce, x_j - x_i
 // is exact and small, so the product keeps its relative accuracy instead of
 // losing log10(cond) digits to cancellation; same bytes moved.
-// Rows are walked a chunk of slots at a time (4 in FP32, 2 in FP64, where
-// wider chunks would spill under the reduction kernels' 32-register cap):
-// the column indices, the coefficients and the gathered x of a chunk are
-// all loaded before any of them is used, so a warp keeps several
-// independent gathers in flight; the sums still run slot by slot in face
-// order, so the FP64 product stays bit for bit the reference's.
+// Rows are walked a chunk of slots at a time: the column indices, the
+// coefficients and the gathered x of a chunk are all loaded before any of
+// them is used, so a warp keeps several independent gathers in flight; the
+// sums still run slot by slot in face order, so the FP64 product stays bit
+// for bit the reference's.  FP32 takes 4 slots at a time (0.52 -> 0.69 of
+// copy bandwidth); FP64 one: two slots spilled under the reduction
+// kernels' 32-register cap and made the FP64 products slower at 256^3
+// (0.30 -> 0.38 ms for y = A x, 0.289 -> 0.306 ms for the CG product).
 #ifndef SG_ROW_CHUNK64
-#define SG_ROW_CHUNK64 2
+#define SG_ROW_CHUNK64 1
 #endif
 constexpr int kRowChunk = 4;
 constexpr int kRowChunk64 = SG_ROW_CHUNK64;

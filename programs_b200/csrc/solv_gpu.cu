@@ -270,6 +270,14 @@ int grid_for(solv_gpu_ctx* c, long long n) {
   return (int)std::max(1LL, std::min(g, cap));
 }
 
+// Grid of the grid-stride matrix products: one full wave (2048 threads per
+// SM), so no block is left for a second, nearly empty wave.
+int grid_resident(solv_gpu_ctx* c, long long n) {
+  long long g = (n + c->block - 1) / c->block;
+  long long cap = (long long)c->n_sm * std::max(1, 2048 / c->block);
+  return (int)std::max(1LL, std::min(g, cap));
+}
+
 // ---- matrix structure --------------------------------------------------------
 int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in, int nsys,
                      const int* cell_ptr) {
@@ -720,26 +728,26 @@ int mg_vcycle(solv_gpu_ctx* c, const float* r, TZ* z, int mode, const float* q, 
   MgLevel& L1 = *c->mg[0];
   int k = 0;
   if (net) {
-    mg::k_mg_net<false, float><<<grid_for(c, N), B, 0, s>>>(N, R0, ge, q, w, r, nullptr, x0, na);
-    mg::k_mg_resid<<<grid_for(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
+    mg::k_mg_net<false, float><<<grid_resident(c, N), B, 0, s>>>(N, R0, ge, q, w, r, nullptr, x0, na);
+    mg::k_mg_resid<<<grid_resident(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
     k += 2;
   } else {
-    mg::k_mg_pre<<<grid_for(c, N), B, 0, s>>>(N, R0, d0, w, r, x0, t0, na);
+    mg::k_mg_pre<<<grid_resident(c, N), B, 0, s>>>(N, R0, d0, w, r, x0, t0, na);
     k += 1;
   }
   mg::k_mg_restrict<<<grid_for(c, L1.n), B, 0, s>>>(L1.n, L1.agg_ptr.as<int>(),
                                                     L1.agg_cells.as<int>(), t0, L1.b.as<float>(),
                                                     na);
   k += 1 + mg_coarse_cycle(c, na);
-  mg::k_mg_prolong<<<grid_for(c, N), B, 0, s>>>(N, L1.agg_of.as<int>(), a, L1.y.as<float>(), x0,
+  mg::k_mg_prolong<<<grid_resident(c, N), B, 0, s>>>(N, L1.agg_of.as<int>(), a, L1.y.as<float>(), x0,
                                                 na);
   k += 1;
   if (net) {
-    mg::k_mg_resid<<<grid_for(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
-    mg::k_mg_net<true, TZ><<<grid_for(c, N), B, 0, s>>>(N, R0, ge, q, w, t0, x0, z, na);
+    mg::k_mg_resid<<<grid_resident(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
+    mg::k_mg_net<true, TZ><<<grid_resident(c, N), B, 0, s>>>(N, R0, ge, q, w, t0, x0, z, na);
     k += 2;
   } else {
-    mg::k_mg_post<TZ><<<grid_for(c, N), B, 0, s>>>(N, R0, d0, w, r, x0, z, na);
+    mg::k_mg_post<TZ><<<grid_resident(c, N), B, 0, s>>>(N, R0, d0, w, r, x0, z, na);
     k += 1;
   }
   return k;
@@ -1710,14 +1718,14 @@ int kernel_time_solve(solv_gpu_ctx* c, int which, int repeat, float* ms_per_laun
   Lane* lanes = c->lanes.as<Lane>();
   if (which == 4) {
     launch = [&]() {
-      mg::k_mg_resid<<<grid_for(c, N), B, 0, s>>>(N, rows<float>(c), f.r, f.p, f.q, nullptr);
+      mg::k_mg_resid<<<grid_resident(c, N), B, 0, s>>>(N, rows<float>(c), f.r, f.p, f.q, nullptr);
       return SOLV_GPU_OK;
     };
   } else if (which == 5) {
     if ((rc = gnn_prepare(c))) return rc;
     gnn_build<float>(c, f.r);
     launch = [&]() {
-      mg::k_mg_net<false, float><<<grid_for(c, N), B, 0, s>>>(
+      mg::k_mg_net<false, float><<<grid_resident(c, N), B, 0, s>>>(
           N, rows<float>(c), c->g_ge.as<float>(), c->g_q.as<float>(), (float)c->mg_omega, f.r,
           nullptr, f.q, nullptr);
       return SOLV_GPU_OK;
@@ -2053,8 +2061,8 @@ int solv_gpu_spmv_dev(solv_gpu_ctx* c, const double* x_dev, double* y_dev, int r
   if (repeat < 1) repeat = 1;
   CUDA_TRY(c, cudaEventRecord(c->ev0, s));
   for (int k = 0; k < repeat; ++k)
-    sg::k_spmv<double, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<double>(c), c->w_x.as<double>(),
-                                                           c->w_b.as<double>());
+    sg::k_spmv<double, 1><<<grid_resident(c, N), c->block, 0, s>>>(N, rows<double>(c), c->w_x.as<double>(),
+                                                                c->w_b.as<double>());
   CUDA_TRY(c, cudaEventRecord(c->ev1, s));
   sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, c->w_b.as<double>(), y_dev);
   CUDA_TRY(c, cudaStreamSynchronize(s));
@@ -2086,10 +2094,10 @@ int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_l
     WS<double> w;
     if ((rc = ensure_ws<double>(c, 1, w))) return rc;
     CUDA_TRY(c, cudaMemsetAsync(w.p, 0, N * sizeof(double), s));
-    sg::k_spmv<double, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
+    sg::k_spmv<double, 1><<<grid_resident(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
     CUDA_TRY(c, cudaEventRecord(c->ev0, s));
     for (int k = 0; k < repeat; ++k)
-      sg::k_spmv<double, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
+      sg::k_spmv<double, 1><<<grid_resident(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
     CUDA_TRY(c, cudaEventRecord(c->ev1, s));
   } else {
     WS<float> f;
@@ -2115,7 +2123,7 @@ int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_l
     }
     auto launch = [&]() {
       if (which == 1)
-        sg::k_spmv<float, 1><<<grid_for(c, N), c->block, 0, s>>>(N, rows<float>(c), f.p, f.q);
+        sg::k_spmv<float, 1><<<grid_resident(c, N), c->block, 0, s>>>(N, rows<float>(c), f.p, f.q);
       else if (which == 2)
         gnn::k_gnn_apply<float><<<grid_for(c, N), c->block, 0, s>>>(
             N, rows<float>(c), c->g_ge.as<float>(), c->g_q.as<float>(), f.p, f.q, nullptr);

@@ -407,21 +407,22 @@ def _two_components(gpu, A, b, imat, solver, it_tol=0.0, reduc=1e-10):
             (v, st["iters"][v], ref[3][v])
 
 
-@pytest.mark.parametrize("imat", [0, 2])
-def test_two_components_on_the_reference_channel_2d(gpu, imat):
+@pytest.mark.parametrize("solver,imat", [("cg", 0), ("cg", 1), ("bicg", 2)])
+def test_two_components_on_the_reference_channel_2d(gpu, solver, imat):
     """The reference's own 2-d mesh (channel_2d.neu, read one unit deep):
-    two right-hand sides solved together by BiCGSTAB, as the reference's 2-d
-    momentum solve does (solv_bicg.f90:27 loops ivc = 1, n_vc = 2)."""
+    two right-hand sides solved together, as the reference's 2-d momentum
+    solve does (solv_bicg.f90:27 and solv_cg.f90:26 loop ivc = 1, n_vc = 2).
+    On this symmetric pressure system the pairings are the reference's own
+    CG ones and DILU BiCGSTAB (Jacobi BiCGSTAB, which the reference never
+    uses, wanders on it)."""
     import os
     from programs_b200.mesh import FaceMatrix
     d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "channel_2d.npz"))
     A = FaceMatrix(int(d["n_cell"]), d["ip"], d["inb"], d["p"], d["n"], d["pl"])
     b = np.asfortranarray(np.stack([d["b"][:, 0], uniform(31, A.n_cell)], axis=1))
     # BiCGSTAB on this symmetric pressure system converges erratically (as in
-    # test_golden_fixtures): iteration counts within 15%, and the tree-ordered
-    # reductions take the GPU along a slightly different path, so both solves
-    # run to 1e-12, where the paths' end points agree within the 1e-8 bar
-    _two_components(gpu, A, b, imat, "bicg", it_tol=0.15, reduc=1e-12)
+    # test_golden_fixtures): its iteration counts within 15%
+    _two_components(gpu, A, b, imat, solver, it_tol=0.15 if solver == "bicg" else 0.0)
 
 
 @pytest.mark.parametrize("imat", [0, 2])
