@@ -421,8 +421,12 @@ def test_two_components_on_the_reference_channel_2d(gpu, solver, imat):
     A = FaceMatrix(int(d["n_cell"]), d["ip"], d["inb"], d["p"], d["n"], d["pl"])
     b = np.asfortranarray(np.stack([d["b"][:, 0], uniform(31, A.n_cell)], axis=1))
     # BiCGSTAB on this symmetric pressure system converges erratically (as in
-    # test_golden_fixtures): its iteration counts within 15%
-    _two_components(gpu, A, b, imat, solver, it_tol=0.15 if solver == "bicg" else 0.0)
+    # test_golden_fixtures): its iteration counts within 15%, and the
+    # tree-ordered reductions take it along a slightly different path whose
+    # end point at 1e-10 lies 1.06e-8 from the oracle's; both run to 1e-12
+    bicg = solver == "bicg"
+    _two_components(gpu, A, b, imat, solver, it_tol=0.15 if bicg else 0.0,
+                    reduc=1e-12 if bicg else 1e-10)
 
 
 @pytest.mark.parametrize("imat", [0, 2])
