@@ -111,6 +111,11 @@ extern "C" {
 #define SOLV_OPT_MG_SCALE_MIN 16 /* floor on the network's per-cell scales
                                    (default 0.5; 0 leaves them as the
                                    network makes them)                     */
+#define SOLV_OPT_MG_BUILD 17    /* where the aggregation hierarchy is built:
+                                   0 on the GPU (default: handshake
+                                   matching, Galerkin structure by one warp
+                                   per coarse row), 1 on the host
+                                   (sequential greedy matching)            */
 
 typedef struct solv_gpu_ctx solv_gpu_ctx;
 
@@ -211,7 +216,7 @@ int solv_gpu_kernel_time(solv_gpu_ctx *ctx, int which, int repeat,
  * level smoother of a symmetric V-cycle over an aggregation hierarchy
  * (about 8 cells per aggregate, Galerkin coarse matrices, damped Jacobi on
  * the coarse levels, dense inverse on the coarsest), and the V-cycle is the
- * preconditioner (SOLV_OPT_MG_*; the hierarchy is built on the host at the
+ * preconditioner (SOLV_OPT_MG_*; the hierarchy is built, on the GPU, at the
  * first such solve after solv_gpu_matrix_set, from the coefficients then;
  * SOLV_OPT_MG_LEVELS 0 uses K alone).  Each solve bounds the smoother:
  * per-cell scales are held at 0.5 or more and K is scaled so that eight

@@ -26,6 +26,7 @@
 #include "kernels.cuh"
 #include "gnn.cuh"
 #include "mg.cuh"
+#include "mg_build.cuh"
 
 using sg::Lane;
 using sg::Rows;
@@ -38,7 +39,14 @@ constexpr int kMaxV = 4;
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { if (p) cudaFree(p); }
+  void swap(DevBuf& o) {
+    std::swap(p, o.p);
+    std::swap(bytes, o.bytes);
+  }
   void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
   cudaError_t ensure(size_t b) {
     if (b <= bytes && p) return cudaSuccess;
@@ -148,6 +156,7 @@ struct solv_gpu_ctx {
   double mg_omega = 0.8;               // smoother damping (1.0 loses the V-cycle)
   double mg_alpha = 2.0;               // coarse-correction scale (unsmoothed
                                        // aggregation under-corrects smooth error)
+  int mg_build = 0;                    // hierarchy build: 0 on the GPU, 1 on the host
   bool mg_valid = false;               // hierarchy built for the current structure
   int mg_built_max = 0;                // mg_max_levels the hierarchy was built with
   std::vector<std::unique_ptr<MgLevel>> mg;  // coarse levels 1..L
@@ -558,8 +567,237 @@ cudaError_t upload(DevBuf& d, const std::vector<V>& h, cudaStream_t s) {
   return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice, s);
 }
 
+// ---- the hierarchy built on the GPU (mg_build.cuh) ------------------------------
+// Exclusive prefix sum out[0..n] of in[0..n); the total (out[n]) also to
+// *total_host when that is given (a synchronising copy).
+int dev_scan(solv_gpu_ctx* c, const int* in, int* out, int n, DevBuf& bs, int* total_host) {
+  cudaStream_t s = c->stream;
+  if (n <= 0) {
+    CUDA_TRY(c, cudaMemsetAsync(out, 0, sizeof(int), s));
+    if (total_host) *total_host = 0;
+    return SOLV_GPU_OK;
+  }
+  const int nb = (n + mgb::kScanBlock - 1) / mgb::kScanBlock;
+  CUDA_TRY(c, bs.ensure((size_t)(nb + 1) * sizeof(int)));
+  int* b = bs.as<int>();
+  mgb::k_scan_block<<<nb, mgb::kScanBlock, 0, s>>>(n, in, out, b);
+  mgb::k_scan_sums<<<1, mgb::kScanBlock, 0, s>>>(nb, b, b + nb);
+  mgb::k_scan_add<<<(n + 256) / 256, 256, 0, s>>>(n, out, b, b + nb);
+  CUDA_TRY(c, cudaGetLastError());
+  if (total_host) {
+    CUDA_TRY(c, cudaMemcpyAsync(total_host, out + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(c, cudaStreamSynchronize(s));
+  }
+  return SOLV_GPU_OK;
+}
+
+// A coarse level's structure as the GPU Galerkin walk builds it.
+struct CoarseDev {
+  int nc = 0;
+  int n_slots = 0;
+  DevBuf sp, sw, col, gptr, gsrc, mptr, cells;
+};
+
+// Members of the nc aggregates of agg (sorted lists) and the Galerkin
+// structure of the coarse level over the finer level f (n cells).  Returns
+// SOLV_GPU_TOO_LARGE when a coarse row would exceed 255 slots.
+int gpu_galerkin(solv_gpu_ctx* c, mgb::Ell f, int n, const int* agg, int nc, CoarseDev& C) {
+  cudaStream_t s = c->stream;
+  const int B = 256;
+  const int G = grid_for(c, std::max(n, nc));
+  DevBuf cnt, cur, deg, slots, bs, err;
+  C.nc = nc;
+  CUDA_TRY(c, cnt.ensure((size_t)nc * sizeof(int)));
+  CUDA_TRY(c, cur.ensure((size_t)nc * sizeof(int)));
+  CUDA_TRY(c, C.mptr.ensure((size_t)(nc + 1) * sizeof(int)));
+  CUDA_TRY(c, C.cells.ensure((size_t)n * sizeof(int)));
+  CUDA_TRY(c, cudaMemsetAsync(cnt.p, 0, (size_t)nc * sizeof(int), s));
+  CUDA_TRY(c, cudaMemsetAsync(cur.p, 0, (size_t)nc * sizeof(int), s));
+  mgb::k_count<<<G, B, 0, s>>>(n, agg, cnt.as<int>());
+  int rc = dev_scan(c, cnt.as<int>(), C.mptr.as<int>(), nc, bs, nullptr);
+  if (rc) return rc;
+  mgb::k_place<<<G, B, 0, s>>>(n, agg, C.mptr.as<int>(), cur.as<int>(), C.cells.as<int>());
+  mgb::k_sort_members<<<grid_for(c, nc), B, 0, s>>>(nc, C.mptr.as<int>(), C.cells.as<int>());
+  CUDA_TRY(c, err.ensure(sizeof(int)));
+  CUDA_TRY(c, cudaMemsetAsync(err.p, 0, sizeof(int), s));
+  CUDA_TRY(c, deg.ensure((size_t)nc * sizeof(int)));
+  const int gw = (int)std::max(1LL, std::min<long long>((nc + mgb::kGalWarps - 1) / mgb::kGalWarps,
+                                                        (long long)c->n_sm * 8));
+  mgb::k_galerkin<0><<<gw, mgb::kGalWarps * 32, 0, s>>>(
+      nc, f, agg, C.mptr.as<int>(), C.cells.as<int>(), deg.as<int>(), nullptr, nullptr, nullptr,
+      nullptr, nullptr, err.as<int>());
+  int herr = 0;
+  CUDA_TRY(c, cudaMemcpyAsync(&herr, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  if (herr) return SOLV_GPU_TOO_LARGE;
+  const int ns = (nc + 31) / 32;
+  CUDA_TRY(c, C.sw.ensure(std::max(ns, 1)));
+  CUDA_TRY(c, slots.ensure((size_t)std::max(ns, 1) * sizeof(int)));
+  CUDA_TRY(c, C.sp.ensure((size_t)(ns + 1) * sizeof(int)));
+  mgb::k_slice_widths<<<grid_for(c, ns), B, 0, s>>>(nc, deg.as<int>(), C.sw.as<uint8_t>(),
+                                                   slots.as<int>());
+  int total = 0;
+  if ((rc = dev_scan(c, slots.as<int>(), C.sp.as<int>(), ns, bs, &total))) return rc;
+  if (total < 0) return SOLV_GPU_TOO_LARGE;  // beyond int32 slot offsets
+  C.n_slots = total;
+  CUDA_TRY(c, C.col.ensure((size_t)std::max(total, 1) * sizeof(int)));
+  CUDA_TRY(c, cnt.ensure((size_t)std::max(total, 1) * sizeof(int)));
+  CUDA_TRY(c, cudaMemsetAsync(C.col.p, 0xff, (size_t)std::max(total, 1) * sizeof(int), s));
+  CUDA_TRY(c, cudaMemsetAsync(cnt.p, 0, (size_t)std::max(total, 1) * sizeof(int), s));
+  mgb::k_galerkin<1><<<gw, mgb::kGalWarps * 32, 0, s>>>(
+      nc, f, agg, C.mptr.as<int>(), C.cells.as<int>(), nullptr, C.sp.as<int>(), C.col.as<int>(),
+      cnt.as<int>(), nullptr, nullptr, err.as<int>());
+  CUDA_TRY(c, C.gptr.ensure((size_t)(total + 1) * sizeof(int)));
+  int n_src = 0;
+  if ((rc = dev_scan(c, cnt.as<int>(), C.gptr.as<int>(), total, bs, &n_src))) return rc;
+  CUDA_TRY(c, C.gsrc.ensure((size_t)std::max(n_src, 1) * sizeof(int)));
+  mgb::k_galerkin<2><<<gw, mgb::kGalWarps * 32, 0, s>>>(
+      nc, f, agg, C.mptr.as<int>(), C.cells.as<int>(), nullptr, C.sp.as<int>(), nullptr, nullptr,
+      C.gptr.as<int>(), C.gsrc.as<int>(), err.as<int>());
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaStreamSynchronize(s));  // before the local buffers are freed
+  return SOLV_GPU_OK;
+}
+
+// Aggregation of one level (n cells, structure g, strengths w) into
+// agg (n entries) and *nc aggregates: passes of handshake matching on the
+// pass graphs, then the singletons joined to a neighbour's aggregate.
+int gpu_aggregate(solv_gpu_ctx* c, mgb::Ell g, const float* w, int n, int passes, DevBuf& agg,
+                  int* nc_out) {
+  cudaStream_t s = c->stream;
+  const int B = 256;
+  DevBuf mate, prop, flag, id, aggp, bs, size, used;
+  CoarseDev P;       // the current pass graph (after the first pass)
+  DevBuf pw, pw2;    // its strengths
+  CUDA_TRY(c, agg.ensure((size_t)n * sizeof(int)));
+  mgb::Ell gp = g;
+  const float* wp = w;
+  int np = n;
+  for (int p = 0; p < passes; ++p) {
+    const int G = grid_for(c, np);
+    CUDA_TRY(c, mate.ensure((size_t)np * sizeof(int)));
+    CUDA_TRY(c, prop.ensure((size_t)np * sizeof(int)));
+    CUDA_TRY(c, flag.ensure((size_t)np * sizeof(int)));
+    CUDA_TRY(c, id.ensure((size_t)(np + 1) * sizeof(int)));
+    CUDA_TRY(c, aggp.ensure((size_t)np * sizeof(int)));
+    CUDA_TRY(c, cudaMemsetAsync(mate.p, 0xff, (size_t)np * sizeof(int), s));
+    for (int r = 0; r < mgb::kRounds; ++r) {
+      mgb::k_hs_propose<<<G, B, 0, s>>>(np, gp, wp, mate.as<int>(), prop.as<int>());
+      mgb::k_hs_accept<<<G, B, 0, s>>>(np, prop.as<int>(), mate.as<int>());
+    }
+    mgb::k_hs_lead<<<G, B, 0, s>>>(np, mate.as<int>(), flag.as<int>());
+    int nn = 0;
+    int rc = dev_scan(c, flag.as<int>(), id.as<int>(), np, bs, &nn);
+    if (rc) return rc;
+    mgb::k_hs_number<<<G, B, 0, s>>>(np, mate.as<int>(), id.as<int>(), aggp.as<int>());
+    if (p == 0)
+      CUDA_TRY(c, cudaMemcpyAsync(agg.p, aggp.p, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+    else
+      mgb::k_compose<<<grid_for(c, n), B, 0, s>>>(n, agg.as<int>(), aggp.as<int>());
+    if (p + 1 < passes && nn < np) {  // the next pass graph and its strengths
+      CoarseDev Q;
+      if ((rc = gpu_galerkin(c, gp, np, aggp.as<int>(), nn, Q))) return rc;
+      CUDA_TRY(c, pw2.ensure((size_t)std::max(Q.n_slots, 1) * sizeof(float)));
+      mgb::k_sum_abs<<<grid_for(c, Q.n_slots), B, 0, s>>>(Q.n_slots, Q.gptr.as<int>(),
+                                                           Q.gsrc.as<int>(), wp, pw2.as<float>());
+      CUDA_TRY(c, cudaStreamSynchronize(s));  // the old pass graph is freed below
+      P.sp.swap(Q.sp);
+      P.sw.swap(Q.sw);
+      P.col.swap(Q.col);
+      P.n_slots = Q.n_slots;
+      pw.swap(pw2);
+      gp.sp = P.sp.as<int>();
+      gp.sw = P.sw.as<uint8_t>();
+      gp.col = P.col.as<int>();
+      wp = pw.as<float>();
+    }
+    np = nn;
+    if (nn == 0) break;
+  }
+  // singletons join a neighbour's aggregate; dense renumbering
+  const int G = grid_for(c, n);
+  CUDA_TRY(c, size.ensure((size_t)np * sizeof(int)));
+  CUDA_TRY(c, used.ensure((size_t)np * sizeof(int)));
+  CUDA_TRY(c, id.ensure((size_t)(np + 1) * sizeof(int)));
+  CUDA_TRY(c, aggp.ensure((size_t)n * sizeof(int)));
+  CUDA_TRY(c, cudaMemsetAsync(size.p, 0, (size_t)np * sizeof(int), s));
+  CUDA_TRY(c, cudaMemsetAsync(used.p, 0, (size_t)np * sizeof(int), s));
+  mgb::k_count<<<G, B, 0, s>>>(n, agg.as<int>(), size.as<int>());
+  mgb::k_join_singletons<<<G, B, 0, s>>>(n, g, w, agg.as<int>(), size.as<int>(), aggp.as<int>());
+  mgb::k_mark<<<G, B, 0, s>>>(n, aggp.as<int>(), used.as<int>());
+  int nc = 0;
+  int rc = dev_scan(c, used.as<int>(), id.as<int>(), np, bs, &nc);
+  if (rc) return rc;
+  mgb::k_renumber<<<G, B, 0, s>>>(n, aggp.as<int>(), id.as<int>());
+  agg.swap(aggp);
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaStreamSynchronize(s));  // before the local buffers are freed
+  *nc_out = nc;
+  return SOLV_GPU_OK;
+}
+
+// The hierarchy for the current structure, built on the GPU from the
+// coefficients present now.  Same rules and stopping tests as the host
+// build below.
+int mg_setup_gpu(solv_gpu_ctx* c, std::vector<std::unique_ptr<MgLevel>>& levels, bool& ok) {
+  cudaStream_t s = c->stream;
+  const int B = c->block;
+  int n = c->N;
+  mgb::Ell g{c->slice_ptr.as<int>(), c->slice_w.as<uint8_t>(), c->col.as<int>()};
+  DevBuf w0, wn;
+  CUDA_TRY(c, w0.ensure((size_t)std::max<long long>(c->n_slots, 1) * sizeof(float)));
+  mgb::k_abs<<<grid_for(c, c->n_slots), B, 0, s>>>(c->n_slots, c->valf.as<float>(), w0.as<float>());
+  const float* w = w0.as<float>();
+  const float* vprev = c->valf.as<float>();
+  ok = n > mg::kCoarsest;
+  while (ok && n > mg::kCoarsest) {
+    if ((int)levels.size() >= std::min(c->mg_max_levels, mg::kMaxLevels)) { ok = false; break; }
+    auto L = std::make_unique<MgLevel>();
+    int nc = 0;
+    int rc = gpu_aggregate(c, g, w, n, 3, L->agg_of, &nc);
+    if (rc) return rc;
+    if (nc > 0.75 * n || nc < 1) { ok = false; break; }  // coarsening stalled
+    CoarseDev C;
+    rc = gpu_galerkin(c, g, n, L->agg_of.as<int>(), nc, C);
+    if (rc == SOLV_GPU_TOO_LARGE) { ok = false; break; }
+    if (rc) return rc;
+    L->n = nc;
+    L->n_slots = C.n_slots;
+    L->slice_ptr.swap(C.sp);
+    L->slice_w.swap(C.sw);
+    L->col.swap(C.col);
+    L->gptr.swap(C.gptr);
+    L->gsrc.swap(C.gsrc);
+    L->agg_ptr.swap(C.mptr);
+    L->agg_cells.swap(C.cells);
+    const size_t vb = (size_t)nc * sizeof(float);
+    CUDA_TRY(c, L->val.ensure((size_t)std::max(C.n_slots, 1) * sizeof(float)));
+    CUDA_TRY(c, L->rs.ensure(vb));
+    CUDA_TRY(c, L->dinv.ensure(vb));
+    CUDA_TRY(c, L->x.ensure(vb));
+    CUDA_TRY(c, L->b.ensure(vb));
+    CUDA_TRY(c, L->t.ensure(vb));
+    CUDA_TRY(c, L->y.ensure(vb));
+    // coarse coefficients now: the next aggregation's strengths
+    mg::k_mg_gather_slots<<<grid_for(c, C.n_slots), B, 0, s>>>(
+        C.n_slots, L->gptr.as<int>(), L->gsrc.as<int>(), vprev, L->val.as<float>());
+    CUDA_TRY(c, wn.ensure((size_t)std::max(C.n_slots, 1) * sizeof(float)));
+    mgb::k_abs<<<grid_for(c, C.n_slots), B, 0, s>>>(C.n_slots, L->val.as<float>(), wn.as<float>());
+    CUDA_TRY(c, cudaGetLastError());
+    w0.swap(wn);
+    w = w0.as<float>();
+    vprev = L->val.as<float>();
+    g = mgb::Ell{L->slice_ptr.as<int>(), L->slice_w.as<uint8_t>(), L->col.as<int>()};
+    n = nc;
+    levels.push_back(std::move(L));
+  }
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  return SOLV_GPU_OK;
+}
+
 // Build the hierarchy for the current structure from the coefficients
-// present now (host aggregation; once per structure).  A hierarchy that
+// present now (once per structure): on the GPU (mg_build.cuh, the default)
+// or with the host aggregation (SOLV_OPT_MG_BUILD 1).  A hierarchy that
 // cannot reach kCoarsest cells (coarsening stalls) is not used: the solve
 // then runs with the one-level preconditioner.
 int mg_setup(solv_gpu_ctx* c) {
@@ -571,7 +809,25 @@ int mg_setup(solv_gpu_ctx* c) {
   drop_graphs(c);
   c->mg.clear();
   cudaStream_t s = c->stream;
-  // level 0 from the device
+  if (c->mg_build == 0) {
+    std::vector<std::unique_ptr<MgLevel>> levels;
+    bool ok = true;
+    if ((rc = mg_setup_gpu(c, levels, ok))) return rc;
+    c->mg_valid = true;
+    if (ok && !levels.empty()) {
+      c->mg = std::move(levels);
+      const int nL = c->mg.back()->n;
+      CUDA_TRY(c, c->mg_x0.ensure((size_t)c->N * sizeof(float)));
+      CUDA_TRY(c, c->mg_t0.ensure((size_t)c->N * sizeof(float)));
+      CUDA_TRY(c, c->mg_dinv0.ensure((size_t)c->N * sizeof(float)));
+      CUDA_TRY(c, c->mg_dq.ensure((size_t)c->N * sizeof(float)));
+      CUDA_TRY(c, c->mg_dense.ensure((size_t)nL * nL * sizeof(double)));
+      CUDA_TRY(c, c->mg_ainv.ensure((size_t)nL * nL * sizeof(float)));
+    }
+    c->mg_setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return SOLV_GPU_OK;
+  }
+  // host build: level 0 from the device
   int n = c->N;
   const int ns0 = c->n_slice;
   std::vector<int> sp(ns0 + 1), col(c->n_slots);
@@ -1909,6 +2165,14 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
     case SOLV_OPT_MG_SCALE_MIN:
       if (!(value >= 0 && value <= 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "scale floor in [0,1]");
       c->mg_scale_min = (float)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_MG_BUILD:
+      if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "hierarchy build is 0 or 1");
+      if ((int)value != c->mg_build) {
+        c->mg_build = (int)value;
+        c->mg_valid = false;
+        drop_graphs(c);
+      }
       return SOLV_GPU_OK;
     case SOLV_OPT_INNER_MAX_ITER:
       if (value < 1 || value > 1e7) return set_err(c, SOLV_GPU_BAD_INPUT, "inner max iter in 1..1e7");

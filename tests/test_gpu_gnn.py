@@ -138,8 +138,16 @@ def test_multigrid_gradient_kernels_match_reference(gpu, smoother):
     gpu.matrix_set(A)
     p = _active_params(4)
     gpu.gnn_set_params(p)
-    agg, nc = gpu.mg_aggregates(1, A.n_cell)
-    assert nc <= 256  # one coarse level, solved exactly, as in the reference
+    from programs_b200.solver import SolverError
+    aggs, n = [], A.n_cell
+    while True:  # every level's aggregation, as the GPU built it
+        try:
+            agg, nc = gpu.mg_aggregates(len(aggs) + 1, n)
+        except SolverError:
+            break
+        aggs.append(agg)
+        n = nc
+    assert aggs and n <= 256  # the coarsest level is solved exactly, as in the reference
     r0 = uniform(8, A.n_cell)
     samples = [r0, uniform(9, A.n_cell)]
     sd = torch.from_numpy(np.stack(samples)).cuda()
@@ -151,7 +159,7 @@ def test_multigrid_gradient_kernels_match_reference(gpu, smoother):
         gpu.set_option(9, 1)
         gpu.set_option(OPT_MG_SMOOTHER, 1)
     g_g = gpu.gnn_get_grad()
-    loss_c, g_c = gnn_ref.loss_mg_and_grad(A, r0, samples, p, [agg], 0.8, 2.0,
+    loss_c, g_c = gnn_ref.loss_mg_and_grad(A, r0, samples, p, aggs, 0.8, 2.0,
                                            diag=smoother == 2)
     assert abs(loss_g - loss_c) <= 1e-3 * abs(loss_c)
     blocks = [("w_in", 0, learn.P_LAYER), ("layers", learn.P_LAYER, learn.P_WA),
