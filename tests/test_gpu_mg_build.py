@@ -2,13 +2,13 @@
 
 * every level's aggregation covers all aggregates 0..nc-1, each aggregate is
   connected in the finer level's face graph (pairs of neighbours, joined
-  singletons), and every level coarsens by at least a factor of 3;
+  singletons), and every level coarsens at least twofold;
 * the build is deterministic: a second build of the same structure gives the
   same aggregations;
 * the V-cycle over it preconditions as well as the host build's (sequential
   greedy matching): iteration counts of the Jacobi-smoothed multigrid FCG
   within 25% of each other, both converging to the oracle's solution.
-(every level coarsens at least twofold; three passes of pairing aim at 8)
+(three passes of pairing aim at eightfold)
 """
 import numpy as np
 import pytest
