@@ -65,6 +65,26 @@ int fv_gpu_gradient(fv_gpu *fv, int ncomp, const double *phi, double *grad);
 /* Face mass fluxes with Rhie-Chow pressure smoothing (cfd_setup.f90:615-634). */
 int fv_gpu_face_flux(fv_gpu *fv, const double *u, const double *p, const double *gradp,
                      const double *ap, double rho, double *flux);
+/* The same with the pressures taken at the face's auxiliary points,
+ * p_P + grad(p)_P . dx_P, as the reference's pressure-correction face loop
+ * does (cfd_setup.f90:611-620); bit-for-bit fvm_face_flux_aux. */
+int fv_gpu_face_flux_aux(fv_gpu *fv, const double *u, const double *p, const double *gradp,
+                         const double *ap, double rho, double *flux);
+/* solv_grad in full (cfd_setup.f90:765-866): n_iter Green-Gauss sweeps,
+ * the later ones with the face values moved to the auxiliary points by the
+ * previous sweep's gradient; walls by neu (0 the values bval[f*ncomp + k],
+ * 1 the cell value, 2 the cell value extrapolated with the previous
+ * gradient); bit-for-bit fvm_gradient_sweeps. */
+int fv_gpu_gradient_sweeps(fv_gpu *fv, int ncomp, const double *phi, const double *bval,
+                           int n_iter, int neu, double *grad);
+/* The explicit momentum terms (cfd_setup.f90:185-272, 306-328), added to
+ * rhs: deferred correction toward the face value of `scheme` (0 central,
+ * 1 min-mod, 2 van Leer, 3 superbee) on the auxiliary-point values,
+ * blended by c_bl, and the non-orthogonal diffusion correction;
+ * bit-for-bit fvm_momentum_deferred. */
+int fv_gpu_momentum_deferred(fv_gpu *fv, int ncomp, const double *phi, const double *grad,
+                             const double *flux, double mu, double c_bl, int scheme,
+                             double *rhs);
 /* Mass imbalance b_i = -(net outflow of cell i), b = 0 at cell `pin`;
  * *total (host) = sum |b| (a deterministic tree sum). */
 int fv_gpu_mass_imbalance(fv_gpu *fv, const double *flux, int pin, double *b, double *total);

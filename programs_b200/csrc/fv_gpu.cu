@@ -33,10 +33,33 @@ __device__ __forceinline__ double lerp(double w, double an, double ap) {
 struct Geo {
   int n_cell, n_face;
   const int *ip, *in;          // 0-based, in = -1 on boundary faces
-  const double *s, *nrm, *xfy, *l, *w;
+  const double *s, *nrm, *xf, *l, *w;
   const double *xc, *vol;
   const int *cf_ptr, *cf;      // faces of each cell, ascending
 };
+
+// std::min / std::max as the host evaluates them (ties and NaN included)
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+
+// displacement from a cell centre xc to its auxiliary point on the face:
+// (x_f - n ((x_f - x_c).n)) - x_c, the host's V3 operations in order
+struct Dx {
+  double x, y, z;
+};
+__device__ __forceinline__ double dot3(double ax, double ay, double az, double bx, double by,
+                                       double bz) {
+  return da(da(dm(ax, bx), dm(ay, by)), dm(az, bz));
+}
+__device__ __forceinline__ Dx aux_dx(const Geo& g, int f, int c) {
+  const double* xf = g.xf + 3 * f;
+  const double* nn = g.nrm + 3 * f;
+  const double* xc = g.xc + 3 * c;
+  const double t = dot3(ds(xf[0], xc[0]), ds(xf[1], xc[1]), ds(xf[2], xc[2]), nn[0], nn[1], nn[2]);
+  return {ds(ds(xf[0], dm(nn[0], t)), xc[0]), ds(ds(xf[1], dm(nn[1], t)), xc[1]),
+          ds(ds(xf[2], dm(nn[2], t)), xc[2])};
+}
+
 
 constexpr int kBlock = 256;
 constexpr int kRedBlocks = 1024;
@@ -96,7 +119,7 @@ __global__ void k_fv_mom_cells(Geo g, const double* __restrict__ u, const double
         const double d = -p[f];
         s = da(s, d);
         // the moving lid: the y = 1 wall (outward normal +y)
-        if (g.nrm[3 * f + 1] > 0.9 && g.xfy[f] > 1.0 - 1e-9) rx = da(rx, dm(d, u_lid));
+        if (g.nrm[3 * f + 1] > 0.9 && g.xf[3 * f + 1] > 1.0 - 1e-9) rx = da(rx, dm(d, u_lid));
       } else if (g.ip[f] == c) {
         s = ds(s, p[f]);
       } else {
@@ -172,10 +195,162 @@ __global__ void k_fv_gradient(Geo g, int nc, const double* __restrict__ phi,
   }
 }
 
+// ---- solv_grad in full: corrected Green-Gauss sweeps ---------------------------------
+// One sweep of fvm_gradient_sweeps (cfd_setup.f90:765-866): the face value
+// of each face (previous sweep's gradient g0 at the auxiliary points after
+// the first sweep; walls by neu), its term ((phi_f s) n) / V added by each
+// of the face's cells in ascending face order, 1/V (vr) formed once per
+// cell.  bval[f*nc + k] are the wall values for neu = 0.
+__device__ __forceinline__ double sweep_face_value(const Geo& g, int f, int nc, int k,
+                                                   const double* __restrict__ phi,
+                                                   const double* __restrict__ bval, int neu,
+                                                   const double* __restrict__ g0) {
+  const int a = g.ip[f], b = g.in[f];
+  const double pa = phi[(size_t)a * nc + k];
+  const double* ga0 = g0 ? g0 + ((size_t)a * nc + k) * 3 : nullptr;
+  if (b >= 0) {
+    const double pb = phi[(size_t)b * nc + k];
+    if (g0) {
+      const double* gb0 = g0 + ((size_t)b * nc + k) * 3;
+      const Dx xa = aux_dx(g, f, a), xb = aux_dx(g, f, b);
+      const double pp = da(pa, dot3(ga0[0], ga0[1], ga0[2], xa.x, xa.y, xa.z));
+      const double pn = da(pb, dot3(gb0[0], gb0[1], gb0[2], xb.x, xb.y, xb.z));
+      return lerp(g.w[f], pn, pp);
+    }
+    return lerp(g.w[f], pb, pa);
+  }
+  if (neu > 0) {
+    double pf = pa;
+    if (g0 && neu == 2) {
+      const double* xf = g.xf + 3 * f;
+      const double* xc = g.xc + 3 * a;
+      pf = da(pf, dot3(ga0[0], ga0[1], ga0[2], ds(xf[0], xc[0]), ds(xf[1], xc[1]),
+                       ds(xf[2], xc[2])));
+    }
+    return pf;
+  }
+  return bval[(size_t)f * nc + k];
+}
+
+__global__ void k_fv_grad_sweep(Geo g, int nc, const double* __restrict__ phi,
+                                const double* __restrict__ bval, int neu,
+                                const double* __restrict__ vr, const double* __restrict__ g0,
+                                double* __restrict__ grad) {
+  const long long tot = (long long)g.n_cell * nc;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / nc), k = (int)(t % nc);
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+    const double v = vr[c];
+    for (int q = g.cf_ptr[c]; q < g.cf_ptr[c + 1]; ++q) {
+      const int f = g.cf[q];
+      const double ps = dm(sweep_face_value(g, f, nc, k, phi, bval, neu, g0), g.s[f]);
+      const double* nn = g.nrm + 3 * f;
+      const double tx = dm(dm(ps, nn[0]), v), ty = dm(dm(ps, nn[1]), v),
+                   tz = dm(dm(ps, nn[2]), v);
+      if (g.ip[f] == c) {
+        gx = da(gx, tx); gy = da(gy, ty); gz = da(gz, tz);
+      } else {
+        gx = ds(gx, tx); gy = ds(gy, ty); gz = ds(gz, tz);
+      }
+    }
+    double* o = grad + ((size_t)c * nc + k) * 3;
+    o[0] = gx;
+    o[1] = gy;
+    o[2] = gz;
+  }
+}
+
+__global__ void k_fv_recip(int n, const double* __restrict__ vol, double* __restrict__ vr) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x)
+    vr[c] = dd(1.0, vol[c]);  // cfd_grid.f90:546
+}
+
+// ---- explicit momentum terms: fvm_momentum_deferred ------------------------------------
+// Per interior face and component (cfd_setup.f90:185-272, 306-328):
+// cor = c_bl c (phi_up - phi_f) + d ((phi_N' - phi_P') - (phi_N - phi_P)),
+// the face value by `scheme` (0 central, 1 min-mod, 2 van Leer, 3 superbee
+// on the auxiliary-point values); then each cell adds +cor (owner) or
+// -cor (neighbour) of its faces in ascending face order.
+__global__ void k_fv_deferred_faces(Geo g, int nc, const double* __restrict__ phi,
+                                    const double* __restrict__ grad,
+                                    const double* __restrict__ flux, double mu, double c_bl,
+                                    int scheme, double* __restrict__ cor) {
+  const long long tot = (long long)g.n_face * nc;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(t / nc), k = (int)(t % nc);
+    const int a = g.ip[f], b = g.in[f];
+    if (b < 0) {
+      cor[t] = 0.0;
+      continue;
+    }
+    const double w = g.w[f];
+    const Dx xa = aux_dx(g, f, a), xb = aux_dx(g, f, b);
+    const double c = flux[f], d = dd(dm(mu, g.s[f]), g.l[f]);
+    const double pa = phi[(size_t)a * nc + k], pb = phi[(size_t)b * nc + k];
+    const double* ga = grad + ((size_t)a * nc + k) * 3;
+    const double* gb = grad + ((size_t)b * nc + k) * 3;
+    const double pa_aux = da(pa, dot3(ga[0], ga[1], ga[2], xa.x, xa.y, xa.z));
+    const double pb_aux = da(pb, dot3(gb[0], gb[1], gb[2], xb.x, xb.y, xb.z));
+    double r_cor = 0.0;
+    if (c != 0.0) {
+      double pf;
+      if (scheme == 0) {
+        pf = lerp(w, pb_aux, pa_aux);
+      } else {
+        const bool fwd = c > 0.0;
+        const double pc = fwd ? pa_aux : pb_aux, pd = fwd ? pb_aux : pa_aux;
+        const double* gc = fwd ? ga : gb;
+        const double* xcA = g.xc + 3 * a;
+        const double* xcB = g.xc + 3 * b;
+        const double xpa[3] = {da(xcA[0], xa.x), da(xcA[1], xa.y), da(xcA[2], xa.z)};
+        const double xpb[3] = {da(xcB[0], xb.x), da(xcB[1], xb.y), da(xcB[2], xb.z)};
+        double dx[3];
+        for (int q = 0; q < 3; ++q) dx[q] = fwd ? ds(xpb[q], xpa[q]) : ds(xpa[q], xpb[q]);
+        const double pu = ds(pd, dm(2.0, dot3(gc[0], gc[1], gc[2], dx[0], dx[1], dx[2])));
+        double r = dd(ds(pc, pu), da(ds(pd, pc), 1e-20));
+        if (scheme == 1) {
+          r = smax(0.0, smin(1.0, r));
+        } else if (scheme == 2) {
+          r = dd(da(r, fabs(r)), da(da(1.0, fabs(r)), 1e-20));
+        } else {  // std::max({0, min(1, 2r), min(2, r)}): the first largest
+          double m = 0.0;
+          const double c1 = smin(1.0, dm(2.0, r)), c2 = smin(2.0, r);
+          if (m < c1) m = c1;
+          if (m < c2) m = c2;
+          r = m;
+        }
+        pf = da(pc, dm(dm(0.5, r), ds(pd, pc)));
+      }
+      const double up = c > 0.0 ? pa : pb;
+      r_cor = dm(dm(c_bl, c), ds(up, pf));
+    }
+    cor[t] = da(r_cor, dm(d, ds(ds(pb_aux, pa_aux), ds(pb, pa))));
+  }
+}
+
+__global__ void k_fv_deferred_cells(Geo g, int nc, const double* __restrict__ cor,
+                                    double* __restrict__ rhs) {
+  const long long tot = (long long)g.n_cell * nc;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(t / nc), k = (int)(t % nc);
+    double acc = rhs[t];
+    for (int q = g.cf_ptr[c]; q < g.cf_ptr[c + 1]; ++q) {
+      const int f = g.cf[q];
+      if (g.in[f] < 0) continue;
+      const double x = cor[(size_t)f * nc + k];
+      acc = g.ip[f] == c ? da(acc, x) : ds(acc, x);
+    }
+    rhs[t] = acc;
+  }
+}
+
 // ---- Rhie-Chow face fluxes ------------------------------------------------------------
 __global__ void k_fv_face_flux(Geo g, const double* __restrict__ u, const double* __restrict__ pr,
                                const double* __restrict__ gp, const double* __restrict__ ap,
-                               double rho, double* __restrict__ flux) {
+                               double rho, int aux, double* __restrict__ flux) {
   for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < g.n_face; f += gridDim.x * blockDim.x) {
     const int a = g.ip[f], b = g.in[f];
     if (b < 0) {
@@ -191,7 +366,13 @@ __global__ void k_fv_face_flux(Geo g, const double* __restrict__ u, const double
                  gz = lerp(w, gp[3 * b + 2], gp[3 * a + 2]);
     const double dx = ds(g.xc[3 * b], g.xc[3 * a]), dy = ds(g.xc[3 * b + 1], g.xc[3 * a + 1]),
                  dz = ds(g.xc[3 * b + 2], g.xc[3 * a + 2]);
-    const double dp = ds(ds(pr[b], pr[a]), da(da(dm(gx, dx), dm(gy, dy)), dm(gz, dz)));
+    double pa = pr[a], pb = pr[b];
+    if (aux) {  // cfd_setup.f90:611-614
+      const Dx xa = aux_dx(g, f, a), xb = aux_dx(g, f, b);
+      pa = da(pa, dot3(gp[3 * a], gp[3 * a + 1], gp[3 * a + 2], xa.x, xa.y, xa.z));
+      pb = da(pb, dot3(gp[3 * b], gp[3 * b + 1], gp[3 * b + 2], xb.x, xb.y, xb.z));
+    }
+    const double dp = ds(ds(pb, pa), da(da(dm(gx, dx), dm(gy, dy)), dm(gz, dz)));
     const double un = da(da(dm(ufx, nn[0]), dm(ufy, nn[1])), dm(ufz, nn[2]));
     flux[f] = ds(dm(dm(rho, g.s[f]), un), dm(d, dp));
   }
@@ -270,7 +451,8 @@ struct fv_gpu {
   int dev = 0;
   cudaStream_t stream = nullptr;
   Geo g{};
-  DBuf ip, in, s, nrm, xfy, l, w, xc, vol, cf_ptr, cf, dface, part, total;
+  DBuf ip, in, s, nrm, xf, l, w, xc, vol, vr, cf_ptr, cf, dface, part, total, tmp;
+  size_t tmp_bytes = 0;
 };
 
 namespace {
@@ -280,6 +462,18 @@ cudaError_t up(DBuf& b, const T* h, size_t count) {
   cudaError_t e = cudaMalloc(&b.p, std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess || count == 0) return e;
   return cudaMemcpy(b.p, h, count * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+// The context's scratch of at least `bytes` (grown in order on its stream).
+double* scratch(fv_gpu* fv, size_t bytes) {
+  if (fv->tmp_bytes >= bytes && fv->tmp.p) return fv->tmp.as<double>();
+  if (cudaStreamSynchronize(fv->stream) != cudaSuccess) return nullptr;
+  if (fv->tmp.p) cudaFree(fv->tmp.p);
+  fv->tmp.p = nullptr;
+  fv->tmp_bytes = 0;
+  if (cudaMalloc(&fv->tmp.p, bytes) != cudaSuccess) return nullptr;
+  fv->tmp_bytes = bytes;
+  return fv->tmp.as<double>();
 }
 
 int enter(fv_gpu* fv) {
@@ -319,8 +513,6 @@ int fv_gpu_create(fv_gpu** out, int device, int n_cell, int n_face, const int* i
     cf[pos[a[f]]++] = f;
     if (b[f] >= 0) cf[pos[b[f]]++] = f;
   }
-  std::vector<double> xfy(n_face);
-  for (int f = 0; f < n_face; ++f) xfy[f] = xf[3 * f + 1];
   if (cudaSetDevice(device) != cudaSuccess) return SOLV_GPU_DEVICE_ERROR;
   fv_gpu* fv = new fv_gpu;
   fv->dev = device;
@@ -331,7 +523,7 @@ int fv_gpu_create(fv_gpu** out, int device, int n_cell, int n_face, const int* i
   chk(up(fv->in, b.data(), F));
   chk(up(fv->s, area, F));
   chk(up(fv->nrm, nrm, 3 * F));
-  chk(up(fv->xfy, xfy.data(), F));
+  chk(up(fv->xf, xf, 3 * F));
   chk(up(fv->l, l_pn, F));
   chk(up(fv->w, w_fp, F));
   chk(up(fv->xc, xc, 3 * N));
@@ -341,6 +533,12 @@ int fv_gpu_create(fv_gpu** out, int device, int n_cell, int n_face, const int* i
   chk(cudaMalloc(&fv->dface.p, std::max<size_t>(F, 1) * sizeof(double)));
   chk(cudaMalloc(&fv->part.p, kRedBlocks * sizeof(double)));
   chk(cudaMalloc(&fv->total.p, sizeof(double)));
+  chk(cudaMalloc(&fv->vr.p, std::max<size_t>(N, 1) * sizeof(double)));
+  if (e == cudaSuccess) {
+    k_fv_recip<<<grid(n_cell), kBlock>>>(n_cell, fv->vol.as<double>(), fv->vr.as<double>());
+    chk(cudaGetLastError());
+    chk(cudaDeviceSynchronize());
+  }
   if (e != cudaSuccess) {
     delete fv;
     return SOLV_GPU_DEVICE_ERROR;
@@ -352,7 +550,7 @@ int fv_gpu_create(fv_gpu** out, int device, int n_cell, int n_face, const int* i
   g.in = fv->in.as<int>();
   g.s = fv->s.as<double>();
   g.nrm = fv->nrm.as<double>();
-  g.xfy = fv->xfy.as<double>();
+  g.xf = fv->xf.as<double>();
   g.l = fv->l.as<double>();
   g.w = fv->w.as<double>();
   g.xc = fv->xc.as<double>();
@@ -417,7 +615,55 @@ int fv_gpu_face_flux(fv_gpu* fv, const double* u, const double* p, const double*
   if (rc) return rc;
   if (!u || !p || !gradp || !ap || !flux) return SOLV_GPU_BAD_INPUT;
   const Geo& g = fv->g;
-  k_fv_face_flux<<<grid(g.n_face), kBlock, 0, fv->stream>>>(g, u, p, gradp, ap, rho, flux);
+  k_fv_face_flux<<<grid(g.n_face), kBlock, 0, fv->stream>>>(g, u, p, gradp, ap, rho, 0, flux);
+  return done();
+}
+
+int fv_gpu_face_flux_aux(fv_gpu* fv, const double* u, const double* p, const double* gradp,
+                         const double* ap, double rho, double* flux) {
+  int rc = enter(fv);
+  if (rc) return rc;
+  if (!u || !p || !gradp || !ap || !flux) return SOLV_GPU_BAD_INPUT;
+  const Geo& g = fv->g;
+  k_fv_face_flux<<<grid(g.n_face), kBlock, 0, fv->stream>>>(g, u, p, gradp, ap, rho, 1, flux);
+  return done();
+}
+
+int fv_gpu_gradient_sweeps(fv_gpu* fv, int ncomp, const double* phi, const double* bval,
+                           int n_iter, int neu, double* grad) {
+  int rc = enter(fv);
+  if (rc) return rc;
+  if (ncomp < 1 || ncomp > 16 || !phi || !grad || n_iter < 1 || n_iter > 64 || neu < 0 ||
+      neu > 2 || (neu == 0 && !bval))
+    return SOLV_GPU_BAD_INPUT;
+  const Geo& g = fv->g;
+  const size_t G = (size_t)3 * ncomp * g.n_cell;
+  double* t = scratch(fv, n_iter > 1 ? 2 * G * sizeof(double) : sizeof(double));
+  if (!t) return SOLV_GPU_DEVICE_ERROR;
+  const double* g0 = nullptr;
+  for (int it = 1; it <= n_iter; ++it) {
+    double* out = it == n_iter ? grad : t + ((it & 1) ? 0 : G);
+    k_fv_grad_sweep<<<grid((long long)g.n_cell * ncomp), kBlock, 0, fv->stream>>>(
+        g, ncomp, phi, bval, neu, fv->vr.as<double>(), g0, out);
+    g0 = out;
+  }
+  return done();
+}
+
+int fv_gpu_momentum_deferred(fv_gpu* fv, int ncomp, const double* phi, const double* grad,
+                             const double* flux, double mu, double c_bl, int scheme,
+                             double* rhs) {
+  int rc = enter(fv);
+  if (rc) return rc;
+  if (ncomp < 1 || ncomp > 16 || !phi || !grad || !flux || !rhs || scheme < 0 || scheme > 3)
+    return SOLV_GPU_BAD_INPUT;
+  const Geo& g = fv->g;
+  double* cor = scratch(fv, std::max<size_t>((size_t)g.n_face * ncomp, 1) * sizeof(double));
+  if (!cor) return SOLV_GPU_DEVICE_ERROR;
+  k_fv_deferred_faces<<<grid((long long)g.n_face * ncomp), kBlock, 0, fv->stream>>>(
+      g, ncomp, phi, grad, flux, mu, c_bl, scheme, cor);
+  k_fv_deferred_cells<<<grid((long long)g.n_cell * ncomp), kBlock, 0, fv->stream>>>(g, ncomp, cor,
+                                                                                    rhs);
   return done();
 }
 

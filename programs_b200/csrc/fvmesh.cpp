@@ -832,9 +832,11 @@ int fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, const
   return 0;
 }
 
-void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
-                   const double *ap, double rho, double *flux) {
+namespace {
+void face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
+               const double *ap, double rho, int aux_points, double *flux) {
   const size_t F = m->f_ip.size();
+  auto aux = [](V3 xf, V3 nn, V3 xc) { return (xf - nn * dot(xf - xc, nn)) - xc; };
   std::vector<double> vol(m->n_cell);
   fvm_mesh_cell_geom(m, nullptr, vol.data());
   for (size_t f = 0; f < F; ++f) {
@@ -853,9 +855,25 @@ void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const do
     const double d = rho * p_r * s * v / l;
     V3 gf{w * gradp[3 * b] + (1 - w) * gradp[3 * a], w * gradp[3 * b + 1] + (1 - w) * gradp[3 * a + 1],
           w * gradp[3 * b + 2] + (1 - w) * gradp[3 * a + 2]};
-    const double dp = (p[b] - p[a]) - dot(gf, m->xc[b] - m->xc[a]);
+    double pa = p[a], pb = p[b];
+    if (aux_points) {  // cfd_setup.f90:611-614: p at the auxiliary points
+      pa = pa + dot({gradp[3 * a], gradp[3 * a + 1], gradp[3 * a + 2]}, aux(x, nn, m->xc[a]));
+      pb = pb + dot({gradp[3 * b], gradp[3 * b + 1], gradp[3 * b + 2]}, aux(x, nn, m->xc[b]));
+    }
+    const double dp = (pb - pa) - dot(gf, m->xc[b] - m->xc[a]);
     flux[f] = rho * s * dot(uf, nn) - d * dp;
   }
+}
+}  // namespace
+
+void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
+                   const double *ap, double rho, double *flux) {
+  face_flux(m, u, p, gradp, ap, rho, 0, flux);
+}
+
+void fvm_face_flux_aux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
+                       const double *ap, double rho, double *flux) {
+  face_flux(m, u, p, gradp, ap, rho, 1, flux);
 }
 
 double fvm_mass_imbalance(const fvm_mesh *m, const double *flux, int pin, double *b) {

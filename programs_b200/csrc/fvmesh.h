@@ -159,6 +159,12 @@ int fvm_momentum_deferred(const fvm_mesh *m, int ncomp, const double *phi, const
  * zero on walls. */
 void fvm_face_flux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
                    const double *ap, double rho, double *flux);
+/* The same fluxes with the pressures taken at the auxiliary points of the
+ * face, p_P + grad(p)_P . dx_P, as the reference's pressure-correction face
+ * loop does (cfd_setup.f90:611-620):
+ * dp = (p_N' - p_P') - grad(p)_f . (x_N - x_P). */
+void fvm_face_flux_aux(const fvm_mesh *m, const double *u, const double *p, const double *gradp,
+                       const double *ap, double rho, double *flux);
 
 /* Mass imbalance right-hand side b_i = -sum of outflow of cell i; cell
  * `pin` (1-based) gets 0.  Returns sum |b|. */

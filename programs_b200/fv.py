@@ -29,6 +29,9 @@ def _typed():
     L.fv_gpu_pressure_correction.argtypes = [_vp, _vp, _d, _i, _vp, _vp, _vp]
     L.fv_gpu_gradient.argtypes = [_vp, _i, _vp, _vp]
     L.fv_gpu_face_flux.argtypes = [_vp, _vp, _vp, _vp, _vp, _d, _vp]
+    L.fv_gpu_face_flux_aux.argtypes = [_vp, _vp, _vp, _vp, _vp, _d, _vp]
+    L.fv_gpu_gradient_sweeps.argtypes = [_vp, _i, _vp, _vp, _i, _i, _vp]
+    L.fv_gpu_momentum_deferred.argtypes = [_vp, _i, _vp, _vp, _vp, _d, _d, _i, _vp]
     L.fv_gpu_mass_imbalance.argtypes = [_vp, _vp, _i, _vp, ctypes.POINTER(_d)]
     L.fv_gpu_simple_correct.argtypes = [_vp, _vp, _vp, _vp, _d, _d, _vp, _vp, _vp]
     L._fv_typed = True
@@ -98,11 +101,29 @@ class GpuFv:
         self._check(self._lib.fv_gpu_gradient(self._h, k, _ptr(phi), _ptr(g)))
         return g
 
-    def face_flux(self, u, p, gradp, ap, rho=1.0):
+    def face_flux(self, u, p, gradp, ap, rho=1.0, aux=False):
+        """Rhie-Chow face fluxes; aux takes the pressures at the auxiliary
+        points (cfd_setup.f90:611-620)."""
         f = self._new(self.n_face)
-        self._check(self._lib.fv_gpu_face_flux(self._h, _ptr(u), _ptr(p), _ptr(gradp), _ptr(ap),
-                                               rho, _ptr(f)))
+        fn = self._lib.fv_gpu_face_flux_aux if aux else self._lib.fv_gpu_face_flux
+        self._check(fn(self._h, _ptr(u), _ptr(p), _ptr(gradp), _ptr(ap), rho, _ptr(f)))
         return f
+
+    def gradient_sweeps(self, phi, n_iter=2, neu=2, bval=None):
+        """solv_grad in full: n_iter corrected sweeps, walls by neu (bval:
+        (n_face, ncomp) wall values for neu = 0)."""
+        k = 1 if phi.dim() == 1 else phi.shape[1]
+        g = self._new(self.n_cell, k, 3) if k > 1 else self._new(self.n_cell, 3)
+        self._check(self._lib.fv_gpu_gradient_sweeps(self._h, k, _ptr(phi), _ptr(bval), n_iter,
+                                                     neu, _ptr(g)))
+        return g
+
+    def momentum_deferred(self, u, grad, flux, mu, rhs, c_bl=1.0, scheme=0):
+        """Adds the explicit momentum terms to rhs (in place)."""
+        k = 1 if u.dim() == 1 else u.shape[1]
+        self._check(self._lib.fv_gpu_momentum_deferred(self._h, k, _ptr(u), _ptr(grad), _ptr(flux),
+                                                       mu, c_bl, scheme, _ptr(rhs)))
+        return rhs
 
     def mass_imbalance(self, flux, pin=1):
         b = self._new(self.n_cell)

@@ -55,6 +55,8 @@ def _lib():
                                             ctypes.c_int, ctypes.c_int, _f64p]
         lib.fvm_face_flux.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, ctypes.c_double,
                                       _f64p]
+        lib.fvm_face_flux_aux.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, _f64p, ctypes.c_double,
+                                      _f64p]
         lib.fvm_mass_imbalance.restype = ctypes.c_double
         lib.fvm_mass_imbalance.argtypes = [ctypes.c_void_p, _f64p, ctypes.c_int, _f64p]
         lib.fvm_simple_correct.argtypes = [ctypes.c_void_p, _f64p, _f64p, _f64p, ctypes.c_double,
@@ -302,11 +304,13 @@ def momentum_deferred(mesh: "Mesh", u: np.ndarray, grad: np.ndarray, flux: np.nd
     return out[:, 0].copy() if u.ndim == 1 else out
 
 
-def face_flux(mesh: "Mesh", u, p, gradp, ap, rho=1.0) -> np.ndarray:
+def face_flux(mesh: "Mesh", u, p, gradp, ap, rho=1.0, aux=False) -> np.ndarray:
+    """Rhie-Chow face fluxes; aux takes the pressures at the face's
+    auxiliary points, as the reference does (cfd_setup.f90:611-620)."""
     f = np.empty(mesh.n_face)
     u, p, gradp, ap = _c(u), _c(p), _c(gradp), _c(ap)
-    _lib().fvm_face_flux(mesh._h, _p(u, _f64p), _p(p, _f64p), _p(gradp, _f64p), _p(ap, _f64p),
-                         rho, _p(f, _f64p))
+    fn = _lib().fvm_face_flux_aux if aux else _lib().fvm_face_flux
+    fn(mesh._h, _p(u, _f64p), _p(p, _f64p), _p(gradp, _f64p), _p(ap, _f64p), rho, _p(f, _f64p))
     return f
 
 

@@ -44,9 +44,10 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
     corrected sweeps (cfd_solve.f90:38) with the velocity's wall values
     (neu = 0, cfd_setup.f90:124) and extrapolated pressure walls (neu = 2,
     :689, 754), and the explicit momentum terms (central deferred
-    correction, non-orthogonal diffusion correction, :185-328).  Host
-    assembly only: run_device has the implicit terms.  reference_weights
-    takes the reference's face distance and interpolation weight
+    correction, non-orthogonal diffusion correction, :185-328) and the
+    pressures at the auxiliary points in the face fluxes (:611-620).
+    run_device does the same on the GPU.  reference_weights takes the
+    reference's face distance and interpolation weight
     (Mesh.set_face_weights)."""
     rho = 1.0
     mu = rho * u_lid * 1.0 / re
@@ -99,7 +100,7 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
         u = phi
         t_solve_m += time.time() - ts
         ta = time.time()
-        F = face_flux(m, u, p, gradp, M.pl, rho)
+        F = face_flux(m, u, p, gradp, M.pl, rho, aux=reference_terms)
         P = pressure_correction(m, M.pl, rho=rho, pin=1)
         b, imb = mass_imbalance(m, F, pin=1)
         t_asm += time.time() - ta
@@ -134,12 +135,15 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
 
 def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15,
                seed=0, p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None,
-               p_imat=1, m_precision=0, device=0, log_every=0, reference_weights=False):
-    """The same outer loop with everything on the GPU: assembly, gradients,
-    fluxes and corrections by the fv_gpu kernels (bit-for-bit the host
-    functions), solves through the device-pointer entry points; only the
-    mass-imbalance norm comes back per iteration.  Same arguments and
-    returns as run(); timings are wall clock with the stream synchronised."""
+               p_imat=1, m_precision=0, device=0, log_every=0, reference_weights=False,
+               reference_terms=False, renumber="rcm"):
+    """The same outer loop with everything on the GPU: assembly, gradients
+    (the corrected sweeps too), the explicit momentum terms, fluxes and
+    corrections by the fv_gpu kernels (bit-for-bit the host functions),
+    solves through the device-pointer entry points; only the mass-imbalance
+    norm comes back per iteration.  Same arguments and returns as run();
+    renumber "color" takes the multicolour cell order (two-level DIC / DILU
+    recurrences); timings are wall clock with the stream synchronised."""
     import torch
 
     from .fv import GpuFv
@@ -147,13 +151,18 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
     rho = 1.0
     mu = rho * u_lid * 1.0 / re
     m = Mesh.hex(size, jitter=jitter, seed=seed, permute=True)
-    m.renumber(Mesh.RCM)
+    m.renumber(Mesh.COLOR if renumber == "color" else Mesh.RCM)
     if reference_weights:
         m.set_face_weights(True)
     m.cache_geometry()
     N = m.n_cell
     ip, inb = m.faces()
     _, vol_h = m.cell_geom()
+    wall_u = None
+    if reference_terms:  # no-slip walls, the y = 1 lid moving (velocity wall values)
+        _, nrm, xf, _, _ = m.face_geom()
+        wall_h = np.zeros((m.n_face, 3))
+        wall_h[(inb == 0) & (nrm[:, 1] > 0.9) & (xf[:, 1] > 1.0 - 1e-9), 0] = u_lid
     dev = torch.device("cuda", device)
     stream = torch.cuda.Stream(device=dev)
     fv = GpuFv(m, device)
@@ -177,20 +186,30 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
         stream.synchronize()
         return time.time() - t
 
+    if reference_terms:
+        grad_p = lambda q: fv.gradient_sweeps(q, 2, 2)
+    else:
+        grad_p = fv.gradient
     with torch.cuda.stream(stream):
         vol = torch.from_numpy(vol_h).to(dev)
+        if reference_terms:
+            wall_u = torch.from_numpy(wall_h).to(dev)
         u = torch.zeros(N, 3, dtype=torch.float64, device=dev)
         p = torch.zeros(N, dtype=torch.float64, device=dev)
         F = None
         t0 = time.time()
         for k in range(n_outer):
             ta = time.time()
-            gradp = fv.gradient(p)
+            gradp = grad_p(p)
             Mp, Mn, Mpl, rhs, Fm = fv.momentum_field(u, flux=F, rho=rho, mu=mu, u_lid=u_lid,
                                                      urf=urf_u)
             if F is None:
                 F = Fm
             rhs -= gradp * vol[:, None]
+            if reference_terms:  # summed apart, then added, as the host loop does
+                dcor = torch.zeros_like(rhs)
+                fv.momentum_deferred(u, fv.gradient_sweeps(u, 2, 0, wall_u), F, mu, dcor)
+                rhs += dcor
             t_asm += sync_time(ta)
             ts = time.time()
             sm.matrix_values_dev(Mp.data_ptr(), Mn.data_ptr(), Mpl.data_ptr())
@@ -198,7 +217,7 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
             rn_m, stm = sm.solv_bicg_dev(2, m_reduc, m_iter, 3, u.data_ptr(), res0.data_ptr())
             t_solve_m += sync_time(ts)
             ta = time.time()
-            F = fv.face_flux(u, p, gradp, Mpl, rho)
+            F = fv.face_flux(u, p, gradp, Mpl, rho, aux=reference_terms)
             Pp, Pn, Ppl = fv.pressure_correction(Mpl, rho=rho, pin=1)
             b, imb = fv.mass_imbalance(F, pin=1)
             t_asm += sync_time(ta)
@@ -213,7 +232,7 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
                                            b.data_ptr(), not_r0=True)
             t_solve_p += sync_time(ts)
             ta = time.time()
-            gradpp = fv.gradient(pp)
+            gradpp = grad_p(pp)
             fv.simple_correct(pp, gradpp, Mpl, rho, urf_p, u, p, F)
             t_asm += sync_time(ta)
             rec = {"it": k, "mass": float(imb), "mom_res0": list(map(float, rn_m)),
@@ -253,18 +272,20 @@ def main(argv=None):
     ap.add_argument("--m-reduc", type=float, default=0.1)
     ap.add_argument("--m-iter", type=int, default=5)
     ap.add_argument("--reference-terms", action="store_true",
-                    help="host assembly with the reference's explicit momentum terms and "
-                         "corrected gradients")
+                    help="the reference's explicit momentum terms, corrected gradients and "
+                         "auxiliary-point face pressures")
+    ap.add_argument("--renumber", default="rcm", choices=["rcm", "color"],
+                    help="cell order of the device loop's mesh")
     ap.add_argument("--reference-weights", action="store_true",
                     help="the reference's face distance and interpolation weight")
     a = ap.parse_args(argv)
-    if a.reference_terms and a.device_assembly:
-        ap.error("--reference-terms is host assembly only")
     loop = run_device if a.device_assembly else run
     kw = dict(p_reduc=a.p_reduc, p_iter=a.p_iter, p_imat=a.p_imat, m_reduc=a.m_reduc,
               m_iter=a.m_iter, log_every=a.log_every, reference_weights=a.reference_weights)
     if a.reference_terms:
         kw["reference_terms"] = True
+    if a.device_assembly:
+        kw["renumber"] = a.renumber
     u0, p0, h0, t0 = loop(a.size, a.outer, a.re, **kw)
     out = {"size": a.size, "outer": a.outer, "re": a.re, "p_reduc": a.p_reduc,
            "p_imat": a.p_imat, "plain": t0, "final_mass_plain": h0[-1]["mass"],

@@ -291,11 +291,14 @@ def test_simple_loop_converges_and_learned_path_agrees(gpu):
 def test_device_resident_loop_reproduces_the_host_assembly_loop(gpu):
     """Assembly, gradients, fluxes and corrections on the GPU (fv_gpu) are
     bit-for-bit the host functions and the solves see identical inputs, so
-    the whole outer loop reproduces the host-assembly loop exactly."""
+    the whole outer loop reproduces the host-assembly loop exactly -- with
+    the implicit terms alone and with the reference's explicit momentum
+    terms, corrected gradient sweeps and auxiliary-point face pressures."""
     from programs_b200 import simple
-    u0, p0, h0, _ = simple.run(size=10, n_outer=6, re=200.0)
-    u1, p1, h1, _ = simple.run_device(size=10, n_outer=6, re=200.0)
-    assert np.array_equal(u1, u0) and np.array_equal(p1, p0)
-    assert [h["p_iters"] for h in h1] == [h["p_iters"] for h in h0]
-    for a, b in zip(h0, h1):
-        assert abs(a["mass"] - b["mass"]) <= 1e-12 * a["mass"]
+    for ref in (False, True):  # implicit terms only; with the reference's explicit terms
+        u0, p0, h0, _ = simple.run(size=10, n_outer=6, re=200.0, reference_terms=ref)
+        u1, p1, h1, _ = simple.run_device(size=10, n_outer=6, re=200.0, reference_terms=ref)
+        assert np.array_equal(u1, u0) and np.array_equal(p1, p0), ref
+        assert [h["p_iters"] for h in h1] == [h["p_iters"] for h in h0]
+        for a, b in zip(h0, h1):
+            assert abs(a["mass"] - b["mass"]) <= 1e-12 * a["mass"]
