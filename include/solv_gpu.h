@@ -105,9 +105,10 @@ extern "C" {
                                    without the residual falling below
                                    SOLV_OPT_FCG_STALL_DROP times its value
                                    at the start of the window after which
-                                   Jacobi-PCG takes over (default 100)     */
+                                   Jacobi-PCG takes over (default 200)     */
 #define SOLV_OPT_FCG_STALL_DROP 15 /* the drop a window must reach
-                                   (default 0.5)                           */
+                                   (default 0.9: a stall is no progress,
+                                   not slow progress)                      */
 #define SOLV_OPT_MG_SCALE_MIN 16 /* floor on the network's per-cell scales
                                    (default 0.5; 0 leaves them as the
                                    network makes them)                     */
