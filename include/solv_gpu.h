@@ -105,7 +105,7 @@ extern "C" {
                                    without the residual falling below
                                    SOLV_OPT_FCG_STALL_DROP times its value
                                    at the start of the window after which
-                                   Jacobi-PCG takes over (default 200)     */
+                                   Jacobi-PCG takes over (default 1000)    */
 #define SOLV_OPT_FCG_STALL_DROP 15 /* the drop a window must reach
                                    (default 0.9: a stall is no progress,
                                    not slow progress)                      */

@@ -170,7 +170,7 @@ struct solv_gpu_ctx {
   // the learned preconditioner hands over to Jacobi-PCG when its residual
   // stalls: fcg_stall_iters iterations without falling below fcg_stall_drop
   // times the value at the start of the window
-  int fcg_stall_iters = 200;
+  int fcg_stall_iters = 1000;
   double fcg_stall_drop = 0.9;
 };
 

@@ -380,7 +380,7 @@ def test_stall_window_hands_over_once(gpu):
     try:
         phi, st, rn = _solve_fcg(gpu, A, b)
     finally:
-        gpu.set_option(OPT_FCG_STALL_ITERS, 200)
+        gpu.set_option(OPT_FCG_STALL_ITERS, 1000)
         gpu.set_option(OPT_FCG_STALL_DROP, 0.9)
     assert st["status"] == OK and st["fallbacks"] == 1, st
     assert _rel(phi, x_ref) <= AGREE_1E10
