@@ -276,6 +276,9 @@ def main(argv=None):
                          "auxiliary-point face pressures")
     ap.add_argument("--renumber", default="rcm", choices=["rcm", "color"],
                     help="cell order of the device loop's mesh")
+    ap.add_argument("--learned-m-precision", type=int, default=1,
+                    help="momentum solves of the learned run: 1 FP32 inner iterations with "
+                         "FP64 refinement, 0 FP64")
     ap.add_argument("--reference-weights", action="store_true",
                     help="the reference's face distance and interpolation weight")
     a = ap.parse_args(argv)
@@ -288,14 +291,18 @@ def main(argv=None):
         kw["renumber"] = a.renumber
     u0, p0, h0, t0 = loop(a.size, a.outer, a.re, **kw)
     out = {"size": a.size, "outer": a.outer, "re": a.re, "p_reduc": a.p_reduc,
-           "p_imat": a.p_imat, "plain": t0, "final_mass_plain": h0[-1]["mass"],
+           "p_imat": a.p_imat, "reference_terms": a.reference_terms,
+           "renumber": a.renumber if a.device_assembly else "rcm",
+           "plain": t0, "final_mass_plain": h0[-1]["mass"], "first_mass": h0[0]["mass"],
            "p_iters_plain": int(np.sum([h["p_iters"] for h in h0]))}
     if a.learned:
         from .learn import DEFAULT_WEIGHTS, load_params
         w = load_params(a.weights or DEFAULT_WEIGHTS)
-        u1, p1, h1, t1 = loop(a.size, a.outer, a.re, learned=w, **kw)
+        u1, p1, h1, t1 = loop(a.size, a.outer, a.re, learned=w,
+                              m_precision=a.learned_m_precision, **kw)
         out.update(learned=t1, p_iters_learned=int(np.sum([h["p_iters"] for h in h1])),
                    fallbacks=int(np.sum([h["fallbacks"] for h in h1])),
+                   m_precision_learned=a.learned_m_precision,
                    final_mass_learned=h1[-1]["mass"],
                    rel_l2_u=rel_l2(u1[:, 0], u0[:, 0]), rel_l2_v=rel_l2(u1[:, 1], u0[:, 1]),
                    rel_l2_w=rel_l2(u1[:, 2], u0[:, 2]), rel_l2_p=rel_l2(p1, p0))
