@@ -456,9 +456,9 @@ def main():
         s.set_option(OPT_MG_SMOOTHER, m["smoother"])
 
     tune = None
-    if not args.no_tune:
-        configure("mixed" if args.method != "plain" else "plain")
-        tune = s.autotune("cg", 0, 1)
+    if not args.no_tune:  # the measured method's own launch shapes and vector width
+        configure(args.method)
+        tune = s.autotune(METHODS[args.method]["solver"], 0, 1)
     torch.cuda.synchronize()
 
     def solve(method, reduc=1e-10):

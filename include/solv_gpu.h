@@ -112,6 +112,10 @@ extern "C" {
 #define SOLV_OPT_MG_SCALE_MIN 16 /* floor on the network's per-cell scales
                                    (default 0.5; 0 leaves them as the
                                    network makes them)                     */
+#define SOLV_OPT_VECTOR_WIDTH 18 /* FP32 matrix products (mixed-precision
+                                   Krylov, flexible CG, V-cycle): matrix
+                                   slots each thread loads before it sums
+                                   them, 2, 4 (default) or 8              */
 #define SOLV_OPT_MG_BUILD 17    /* where the aggregation hierarchy is built:
                                    0 on the GPU (default: handshake
                                    matching, Galerkin structure by one warp
@@ -278,13 +282,20 @@ int solv_gpu_gnn_adam(solv_gpu_ctx *ctx, float lr, float grad_scale);
 /* No counterpart in the reference (it has no tunables).  Times candidate
  * launch shapes (threads per block 128/256, resident blocks per SM 4/8/16
  * for the reduction kernels, at most 2048 threads per SM, Krylov
- * iterations per CUDA graph 8/32) on the current matrix with the given
- * solver (0 CG, 1 BiCGSTAB),
- * preconditioner, component count and the context's precision, and leaves
- * the fastest set on the context. */
+ * iterations per CUDA graph 8/32 and, where the iteration runs in FP32 --
+ * precision 1, or the learned solve -- the products' vector width 2/4/8)
+ * on the current matrix (one system or a batch) with the given solver
+ * (0 CG, 1 BiCGSTAB, 2 the learned flexible CG of solv_gpu_fcg: one
+ * system, n_vc = 1, parameters set), preconditioner, component count and
+ * the context's precision, and leaves the fastest set on the context.
+ * ms_per_iter_before is the per-iteration time of the settings in effect
+ * before the call, measured the same way; those settings stay eligible, so
+ * ms_per_iter <= ms_per_iter_before. */
 typedef struct {
   int block, grid_per_sm, graph_iters, candidates;
   double ms_per_iter;
+  int vector_width;
+  double ms_per_iter_before;
 } solv_gpu_tune;
 int solv_gpu_autotune(solv_gpu_ctx *ctx, int solver, int imat, int n_vc,
                       solv_gpu_tune *out);

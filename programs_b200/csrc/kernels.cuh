@@ -210,7 +210,7 @@ struct RowIt {
 constexpr int kRowChunk = 4;
 constexpr int kRowChunk64 = SG_ROW_CHUNK64;
 
-template <typename T, int V>
+template <typename T, int V, int CH = kRowChunk>
 __device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
                                           const T* __restrict__ x, T (&y)[V]) {
   RowIt<T> it(R, i);
@@ -222,11 +222,11 @@ __device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
       xi[v] = x[(size_t)i * V + v];
       y[v] = d * xi[v];
     }
-    for (int k0 = 0; k0 < it.w; k0 += kRowChunk) {
-      int j[kRowChunk];
-      T a[kRowChunk], xv[kRowChunk][V];
+    for (int k0 = 0; k0 < it.w; k0 += CH) {
+      int j[CH];
+      T a[CH], xv[CH][V];
 #pragma unroll
-      for (int u = 0; u < kRowChunk; ++u) {
+      for (int u = 0; u < CH; ++u) {
         j[u] = -1;
         a[u] = T(0);
         if (k0 + u < it.w) {
@@ -236,11 +236,11 @@ __device__ __forceinline__ void row_apply(const Rows<T>& R, int i,
         }
       }
 #pragma unroll
-      for (int u = 0; u < kRowChunk; ++u)
+      for (int u = 0; u < CH; ++u)
 #pragma unroll
         for (int v = 0; v < V; ++v) xv[u][v] = j[u] >= 0 ? x[(size_t)j[u] * V + v] : xi[v];
 #pragma unroll
-      for (int u = 0; u < kRowChunk; ++u)
+      for (int u = 0; u < CH; ++u)
         if (j[u] >= 0) {
 #pragma unroll
           for (int v = 0; v < V; ++v) y[v] = fmaf(a[u], xv[u][v] - xi[v], y[v]);
@@ -850,7 +850,7 @@ __global__ void SG_BOUNDS(V) k_cg_p(SegMap sm, const T* __restrict__ c, const T*
 
 // q = A p and p.q; alpha = s / (p.q + small)   (solv_cg.f90:56-68; the FP32
 // instantiation divides without the guard, div0)
-template <typename T, int V>
+template <typename T, int V, int CH = kRowChunk>
 __global__ void SG_BOUNDS(V) k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
                           double* __restrict__ part, Lane* __restrict__ lanes) {
   const int b = blockIdx.x, s = sm.blk_seg[b];
@@ -865,7 +865,7 @@ __global__ void SG_BOUNDS(V) k_cg_spmv(Rows<T> R, SegMap sm, const T* __restrict
   for (int v = 0; v < V; ++v) acc[v] = 0.0;
   for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
     T y[V];
-    row_apply<T, V>(R, i, p, y);
+    row_apply<T, V, CH>(R, i, p, y);
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       q[(size_t)i * V + v] = y[v];
@@ -1015,7 +1015,7 @@ __global__ void SG_BOUNDS(V) k_bi_p(SegMap sm, const T* __restrict__ c, const T*
 // y = A z, and dots: MODE 0 -> y.r0 (gam = rho/(y.r0+small), :72-73)
 //                    MODE 1 -> y.r, y.y (alpha = (y.r)/(y.y+small), :98-100)
 // (FP32: the same quotients without the guard, div0)
-template <typename T, int V, int MODE>
+template <typename T, int V, int MODE, int CH = kRowChunk>
 __global__ void SG_BOUNDS(V) k_bi_spmv(Rows<T> R, SegMap sm, const T* __restrict__ z, T* __restrict__ y,
                           const T* __restrict__ w, double* __restrict__ part,
                           Lane* __restrict__ lanes) {
@@ -1032,7 +1032,7 @@ __global__ void SG_BOUNDS(V) k_bi_spmv(Rows<T> R, SegMap sm, const T* __restrict
   for (int k = 0; k < NR; ++k) acc[k] = 0.0;
   for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
     T t[V];
-    row_apply<T, V>(R, i, z, t);
+    row_apply<T, V, CH>(R, i, z, t);
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       y[(size_t)i * V + v] = t[v];
@@ -1227,7 +1227,7 @@ __global__ void SG_BOUNDS(1) k_fcg_beta(SegMap sm, const T* __restrict__ z, cons
   }
 }
 
-template <typename T>
+template <typename T, int CH = kRowChunk>
 __global__ void SG_BOUNDS(1) k_fcg_spmv(Rows<T> R, SegMap sm, const T* __restrict__ p, T* __restrict__ q,
                            const T* __restrict__ r, double* __restrict__ part,
                            Lane* __restrict__ lanes) {
@@ -1238,7 +1238,7 @@ __global__ void SG_BOUNDS(1) k_fcg_spmv(Rows<T> R, SegMap sm, const T* __restric
   double acc[2] = {0.0, 0.0};
   for (int i = c0 + sm.blk_rank[b] * blockDim.x + threadIdx.x; i < c1; i += stride) {
     T y[1];
-    row_apply<T, 1>(R, i, p, y);
+    row_apply<T, 1, CH>(R, i, p, y);
     q[i] = y[0];
     acc[0] += prod(p[i], y[0]);
     acc[1] += prod(p[i], r[i]);

@@ -443,6 +443,7 @@ k_mg_invert(int n, double* __restrict__ A, float* __restrict__ Ainv) {
 // ---- device: the V-cycle ---------------------------------------------------------
 // x = w D^-1 b and t = b - A x (pre-smoothing from zero, then its residual;
 // x_j at the neighbours is recomputed from b_j).
+template <int CH = sg::kRowChunk>
 __global__ void k_mg_pre(int n, sg::Rows<float> R, const float* __restrict__ dinv, float w,
                          const float* __restrict__ b, float* __restrict__ x,
                          float* __restrict__ t, const int* __restrict__ n_active) {
@@ -452,11 +453,11 @@ __global__ void k_mg_pre(int n, sg::Rows<float> R, const float* __restrict__ din
     const float bi = b[i];
     const float xi = w * dinv[i] * bi;
     float y = R.diag[i] * xi;
-    for (int k0 = 0; k0 < it.w; k0 += sg::kRowChunk) {
-      int j[sg::kRowChunk];
-      float a[sg::kRowChunk], xj[sg::kRowChunk];
+    for (int k0 = 0; k0 < it.w; k0 += CH) {
+      int j[CH];
+      float a[CH], xj[CH];
 #pragma unroll
-      for (int u = 0; u < sg::kRowChunk; ++u) {
+      for (int u = 0; u < CH; ++u) {
         j[u] = -1;
         a[u] = 0.0f;
         if (k0 + u < it.w) {
@@ -466,9 +467,9 @@ __global__ void k_mg_pre(int n, sg::Rows<float> R, const float* __restrict__ din
         }
       }
 #pragma unroll
-      for (int u = 0; u < sg::kRowChunk; ++u) xj[u] = j[u] >= 0 ? w * dinv[j[u]] * b[j[u]] : xi;
+      for (int u = 0; u < CH; ++u) xj[u] = j[u] >= 0 ? w * dinv[j[u]] * b[j[u]] : xi;
 #pragma unroll
-      for (int u = 0; u < sg::kRowChunk; ++u)
+      for (int u = 0; u < CH; ++u)
         if (j[u] >= 0) y = fmaf(a[u], xj[u] - xi, y);
     }
     x[i] = xi;
@@ -477,26 +478,27 @@ __global__ void k_mg_pre(int n, sg::Rows<float> R, const float* __restrict__ din
 }
 
 // t = b - A x
+template <int CH = sg::kRowChunk>
 __global__ void k_mg_resid(int n, sg::Rows<float> R, const float* __restrict__ b,
                            const float* __restrict__ x, float* __restrict__ t,
                            const int* __restrict__ n_active) {
   if (n_active && *n_active == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float y[1];
-    sg::row_apply<float, 1>(R, i, x, y);
+    sg::row_apply<float, 1, CH>(R, i, x, y);
     t[i] = b[i] - y[0];
   }
 }
 
 // y = x + w D^-1 (b - A x)  (post-smoothing; y and x are different arrays)
-template <typename TO>
+template <typename TO, int CH = sg::kRowChunk>
 __global__ void k_mg_post(int n, sg::Rows<float> R, const float* __restrict__ dinv, float w,
                           const float* __restrict__ b, const float* __restrict__ x,
                           TO* __restrict__ y, const int* __restrict__ n_active) {
   if (n_active && *n_active == 0) return;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float ax[1];
-    sg::row_apply<float, 1>(R, i, x, ax);
+    sg::row_apply<float, 1, CH>(R, i, x, ax);
     y[i] = (TO)(x[i] + w * dinv[i] * (b[i] - ax[0]));
   }
 }

@@ -20,6 +20,7 @@
 #include <memory>
 #include <string>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/solv_gpu.h"
@@ -170,6 +171,7 @@ struct solv_gpu_ctx {
   // the learned preconditioner hands over to Jacobi-PCG when its residual
   // stalls: fcg_stall_iters iterations without falling below fcg_stall_drop
   // times the value at the start of the window
+  int row_chunk = sg::kRowChunk;       // FP32 products: matrix slots a thread loads per step
   int fcg_stall_iters = 1000;
   double fcg_stall_drop = 0.9;
 };
@@ -285,6 +287,17 @@ int grid_resident(solv_gpu_ctx* c, long long n) {
   long long g = (n + c->block - 1) / c->block;
   long long cap = (long long)c->n_sm * std::max(1, 2048 / c->block);
   return (int)std::max(1LL, std::min(g, cap));
+}
+
+// Run f with the FP32 products' gather width (slots loaded per step) as a
+// compile-time constant: f(std::integral_constant<int, CH>()).
+template <typename F>
+void with_chunk(int ch, F&& f) {
+  switch (ch) {
+    case 2: f(std::integral_constant<int, 2>()); break;
+    case 8: f(std::integral_constant<int, 8>()); break;
+    default: f(std::integral_constant<int, 4>()); break;
+  }
 }
 
 // ---- matrix structure --------------------------------------------------------
@@ -938,9 +951,11 @@ int mg_coarse_cycle(solv_gpu_ctx* c, const int* na) {
   for (int l = 0; l + 1 < L; ++l) {
     MgLevel& F = *c->mg[l];
     MgLevel& C = *c->mg[l + 1];
-    mg::k_mg_pre<<<grid_for(c, F.n), B, 0, s>>>(F.n, F.rows(), F.dinv.as<float>(), w,
-                                                F.b.as<float>(), F.x.as<float>(),
-                                                F.t.as<float>(), na);
+    with_chunk(c->row_chunk, [&](auto ch) {
+      mg::k_mg_pre<decltype(ch)::value><<<grid_for(c, F.n), B, 0, s>>>(
+          F.n, F.rows(), F.dinv.as<float>(), w, F.b.as<float>(), F.x.as<float>(), F.t.as<float>(),
+          na);
+    });
     mg::k_mg_restrict<<<grid_for(c, C.n), B, 0, s>>>(C.n, C.agg_ptr.as<int>(),
                                                      C.agg_cells.as<int>(), F.t.as<float>(),
                                                      C.b.as<float>(), na);
@@ -957,9 +972,11 @@ int mg_coarse_cycle(solv_gpu_ctx* c, const int* na) {
     MgLevel& C = *c->mg[l + 1];
     mg::k_mg_prolong<<<grid_for(c, F.n), B, 0, s>>>(F.n, C.agg_of.as<int>(), a, C.y.as<float>(),
                                                     F.x.as<float>(), na);
-    mg::k_mg_post<float><<<grid_for(c, F.n), B, 0, s>>>(F.n, F.rows(), F.dinv.as<float>(), w,
-                                                        F.b.as<float>(), F.x.as<float>(),
-                                                        F.y.as<float>(), na);
+    with_chunk(c->row_chunk, [&](auto ch) {
+      mg::k_mg_post<float, decltype(ch)::value><<<grid_for(c, F.n), B, 0, s>>>(
+          F.n, F.rows(), F.dinv.as<float>(), w, F.b.as<float>(), F.x.as<float>(), F.y.as<float>(),
+          na);
+    });
     k += 2;
   }
   return k;
@@ -983,12 +1000,18 @@ int mg_vcycle(solv_gpu_ctx* c, const float* r, TZ* z, int mode, const float* q, 
   const float* d0 = mode == 2 ? c->mg_dq.as<float>() : c->mg_dinv0.as<float>();
   MgLevel& L1 = *c->mg[0];
   int k = 0;
+  const int ch = c->row_chunk;
   if (net) {
     mg::k_mg_net<false, float><<<grid_resident(c, N), B, 0, s>>>(N, R0, ge, q, w, r, nullptr, x0, na);
-    mg::k_mg_resid<<<grid_resident(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
+    with_chunk(ch, [&](auto cc) {
+      mg::k_mg_resid<decltype(cc)::value><<<grid_resident(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
+    });
     k += 2;
   } else {
-    mg::k_mg_pre<<<grid_resident(c, N), B, 0, s>>>(N, R0, d0, w, r, x0, t0, na);
+    with_chunk(ch, [&](auto cc) {
+      mg::k_mg_pre<decltype(cc)::value><<<grid_resident(c, N), B, 0, s>>>(N, R0, d0, w, r, x0,
+                                                                          t0, na);
+    });
     k += 1;
   }
   mg::k_mg_restrict<<<grid_for(c, L1.n), B, 0, s>>>(L1.n, L1.agg_ptr.as<int>(),
@@ -999,11 +1022,16 @@ int mg_vcycle(solv_gpu_ctx* c, const float* r, TZ* z, int mode, const float* q, 
                                                 na);
   k += 1;
   if (net) {
-    mg::k_mg_resid<<<grid_resident(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
+    with_chunk(ch, [&](auto cc) {
+      mg::k_mg_resid<decltype(cc)::value><<<grid_resident(c, N), B, 0, s>>>(N, R0, r, x0, t0, na);
+    });
     mg::k_mg_net<true, TZ><<<grid_resident(c, N), B, 0, s>>>(N, R0, ge, q, w, t0, x0, z, na);
     k += 2;
   } else {
-    mg::k_mg_post<TZ><<<grid_resident(c, N), B, 0, s>>>(N, R0, d0, w, r, x0, z, na);
+    with_chunk(ch, [&](auto cc) {
+      mg::k_mg_post<TZ, decltype(cc)::value><<<grid_resident(c, N), B, 0, s>>>(N, R0, d0, w, r,
+                                                                               x0, z, na);
+    });
     k += 1;
   }
   return k;
@@ -1231,6 +1259,36 @@ int ensure_ws(solv_gpu_ctx* c, int V, WS<T>& w) {
   return SOLV_GPU_OK;
 }
 
+// q = A p with p.q (the CG product); FP32 products with the context's
+// gather width.
+template <typename T, int V>
+void cg_spmv(solv_gpu_ctx* c, const SegMap& sm, WS<T>& w, double* part, Lane* lanes) {
+  const int G = c->seg.total_blk, B = c->block;
+  if constexpr (std::is_same<T, float>::value) {
+    with_chunk(c->row_chunk, [&](auto ch) {
+      sg::k_cg_spmv<T, V, decltype(ch)::value><<<G, B, 0, c->stream>>>(rows<T>(c), sm, w.p, w.q,
+                                                                      part, lanes);
+    });
+  } else {
+    sg::k_cg_spmv<T, V><<<G, B, 0, c->stream>>>(rows<T>(c), sm, w.p, w.q, part, lanes);
+  }
+}
+
+// y = A z with its dots (BiCGSTAB, MODE as k_bi_spmv)
+template <typename T, int V, int MODE>
+void bi_spmv(solv_gpu_ctx* c, const SegMap& sm, const T* z, T* y, const T* wv, double* part,
+             Lane* lanes) {
+  const int G = c->seg.total_blk, B = c->block;
+  if constexpr (std::is_same<T, float>::value) {
+    with_chunk(c->row_chunk, [&](auto ch) {
+      sg::k_bi_spmv<T, V, MODE, decltype(ch)::value><<<G, B, 0, c->stream>>>(rows<T>(c), sm, z, y,
+                                                                            wv, part, lanes);
+    });
+  } else {
+    sg::k_bi_spmv<T, V, MODE><<<G, B, 0, c->stream>>>(rows<T>(c), sm, z, y, wv, part, lanes);
+  }
+}
+
 // One CG iteration (solv_cg.f90:37-84) on workspace w.  The FP32 inner
 // iteration of the mixed-precision solve takes the flexible-CG step and
 // direction formulas (FLEX in kernels.cuh): FP32 products lose the
@@ -1248,13 +1306,13 @@ int cg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
     if (int rc = launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active)) return rc;
     sg::k_cg_rz<T, V, false, FLEX><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, part, lanes, w.q);
     sg::k_cg_p<T, V, false, FLEX><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes, part);
-    sg::k_cg_spmv<T, V><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, part, lanes);
+    cg_spmv<T, V>(c, sm, w, part, lanes);
     sg::k_cg_update<T, V, false, FLEX><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.p, w.q, part,
                                                         lanes);
     c->launches += 4;
   } else {
     sg::k_cg_p<T, V, true, FLEX><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes, part);
-    sg::k_cg_spmv<T, V><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, part, lanes);
+    cg_spmv<T, V>(c, sm, w, part, lanes);
     sg::k_cg_update<T, V, true, FLEX><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.p, w.q, part,
                                                        lanes);
     c->launches += 3;
@@ -1278,14 +1336,14 @@ int bicg_iteration(solv_gpu_ctx* c, int imat, WS<T>& w) {
   } else {
     sg::k_bi_p<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.r, w.p, w.q, w.z, lanes);
   }
-  sg::k_bi_spmv<T, V, 0><<<G, B, 0, st>>>(rows<T>(c), sm, w.z, w.q, w.r0, part, lanes);
+  bi_spmv<T, V, 0>(c, sm, w.z, w.q, w.r0, part, lanes);
   if (imat > 0) {
     sg::k_bi_half<T, V, false><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.z, w.q, lanes);
     if (int rc = launch_direct<T, V>(c, imat, w.c, w.cr, w.z, w.r, sm.n_active)) return rc;
   } else {
     sg::k_bi_half<T, V, true><<<G, B, 0, st>>>(sm, w.c, w.phi, w.r, w.z, w.q, lanes);
   }
-  sg::k_bi_spmv<T, V, 1><<<G, B, 0, st>>>(rows<T>(c), sm, w.z, w.v, w.r, part, lanes);
+  bi_spmv<T, V, 1>(c, sm, w.z, w.v, w.r, part, lanes);
   sg::k_bi_update<T, V><<<G, B, 0, st>>>(sm, w.phi, w.r, w.z, w.v, w.r0, part, lanes);
   c->launches += 5;
   return SOLV_GPU_OK;
@@ -1315,7 +1373,10 @@ void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
   c->launches += nk - 1;
   sg::k_fcg_beta<T><<<G, B, 0, st>>>(sm, w.z, w.q, part, lanes);            // beta
   sg::k_cg_p<T, 1, false><<<G, B, 0, st>>>(sm, w.c, w.r, w.z, w.p, lanes);   // p = z + beta p
-  sg::k_fcg_spmv<T><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, w.r, part, lanes);
+  with_chunk(c->row_chunk, [&](auto ch) {
+    sg::k_fcg_spmv<T, decltype(ch)::value><<<G, B, 0, st>>>(rows<T>(c), sm, w.p, w.q, w.r, part,
+                                                            lanes);
+  });
   sg::k_fcg_update<T><<<G, B, 0, st>>>(sm, w.phi, w.r, w.p, w.q, part, lanes);
   c->launches += 5;
 }
@@ -1974,7 +2035,10 @@ int kernel_time_solve(solv_gpu_ctx* c, int which, int repeat, float* ms_per_laun
   Lane* lanes = c->lanes.as<Lane>();
   if (which == 4) {
     launch = [&]() {
-      mg::k_mg_resid<<<grid_resident(c, N), B, 0, s>>>(N, rows<float>(c), f.r, f.p, f.q, nullptr);
+      with_chunk(c->row_chunk, [&](auto cc) {
+        mg::k_mg_resid<decltype(cc)::value><<<grid_resident(c, N), B, 0, s>>>(N, rows<float>(c), f.r,
+                                                                             f.p, f.q, nullptr);
+      });
       return SOLV_GPU_OK;
     };
   } else if (which == 5) {
@@ -1988,7 +2052,10 @@ int kernel_time_solve(solv_gpu_ctx* c, int which, int repeat, float* ms_per_laun
     };
   } else if (which == 6) {
     launch = [&]() {
-      sg::k_fcg_spmv<float><<<G, B, 0, s>>>(rows<float>(c), sm, f.p, f.q, f.r, part, lanes);
+      with_chunk(c->row_chunk, [&](auto cc) {
+        sg::k_fcg_spmv<float, decltype(cc)::value><<<G, B, 0, s>>>(rows<float>(c), sm, f.p, f.q,
+                                                                   f.r, part, lanes);
+      });
       return SOLV_GPU_OK;
     };
   } else if (which == 7) {
@@ -2165,6 +2232,14 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
     case SOLV_OPT_MG_SCALE_MIN:
       if (!(value >= 0 && value <= 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "scale floor in [0,1]");
       c->mg_scale_min = (float)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_VECTOR_WIDTH:
+      if (value != 2 && value != 4 && value != 8)
+        return set_err(c, SOLV_GPU_BAD_INPUT, "vector width is 2, 4 or 8");
+      if ((int)value != c->row_chunk) {
+        c->row_chunk = (int)value;
+        drop_graphs(c);
+      }
       return SOLV_GPU_OK;
     case SOLV_OPT_MG_BUILD:
       if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "hierarchy build is 0 or 1");
@@ -2502,16 +2577,23 @@ int solv_gpu_bicg_dev(solv_gpu_ctx* c, int imat, double reduc, int n_iter, int n
 
 // ---- autotuner -----------------------------------------------------------------
 // Chooses threads per block, resident blocks per SM of the reduction
-// kernels and Krylov iterations per CUDA graph for the current matrix,
-// solver, preconditioner, component count and precision.  Each candidate is
-// timed on the device by differencing a short and a long capped solve of a
-// seeded right-hand side (so setup and layout conversion cancel out); the
-// fastest per-iteration time wins and is left set on the context.
+// kernels, Krylov iterations per CUDA graph and, where the iteration runs in
+// FP32 (precision 1, or the learned FCG), the products' vector width (matrix
+// slots a thread loads per step) for the current matrix (one system or a
+// batch), solver, preconditioner, component count and precision.  Each
+// candidate is timed on the device by differencing a short and a long
+// capped solve of a seeded right-hand side (so setup and layout conversion
+// cancel out); the fastest per-iteration time wins and is left set on the
+// context.  The configuration in effect before tuning is timed the same
+// way, first, stays eligible, and is reported beside the winner.
 int solv_gpu_autotune(solv_gpu_ctx* c, int solver, int imat, int n_vc, solv_gpu_tune* out) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");
-  if (n_vc < 1 || n_vc > kMaxV || imat < 0 || imat > 2 || solver < 0 || solver > 1)
+  if (n_vc < 1 || n_vc > kMaxV || imat < 0 || imat > 2 || solver < 0 || solver > 2)
     return set_err(c, SOLV_GPU_BAD_INPUT, "autotune: bad solver / imat / n_vc");
+  if (solver == 2 && (n_vc != 1 || c->n_seg != 1 || !c->g_has_params))
+    return set_err(c, SOLV_GPU_BAD_INPUT,
+                   "autotune: the learned solve needs one system, n_vc = 1 and network parameters");
   CUDA_TRY(c, cudaSetDevice(c->dev));
   const int N = c->N, V = n_vc, nl = c->n_seg * V;
   const size_t nv = (size_t)N * V;
@@ -2543,44 +2625,59 @@ int solv_gpu_autotune(solv_gpu_ctx* c, int solver, int imat, int n_vc, solv_gpu_
     ms = (float)st.solve_ms;
     return SOLV_GPU_OK;
   };
+  const int k_short = 4, k_long = 36;
+  // per-iteration time of the context's current settings
+  auto measure = [&](double& per) -> int {
+    int rc = build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
+    if (rc) return rc;
+    float t0 = 0, t1 = 0, w = 0;
+    if ((rc = run(k_short, w))) return rc;  // warm: graph capture, workspace
+    if ((rc = run(k_short, t0)) || (rc = run(k_long, t1))) return rc;
+    per = (t1 - t0) / (double)(k_long - k_short);
+    return SOLV_GPU_OK;
+  };
+  const bool fp32 = c->precision == 1 || solver == 2;
   const int blocks[] = {128, 256};
   const int gps[] = {4, 8, 16};
   const int graphs[] = {8, 32};
-  const int k_short = 4, k_long = 36;
+  std::vector<int> widths = fp32 ? std::vector<int>{2, 4, 8} : std::vector<int>{c->row_chunk};
   const int precision = c->precision;
   // the tuner measures capped iterations: keep FP32 sweeps as long as the cap
   const int inner_keep = c->inner_max_iter;
-  double best = 1e300;
-  int bb = c->block, bg = c->grid_per_sm, bk = c->graph_iters;
+  double per_default = 0.0;
+  drop_graphs(c);
+  int rc = measure(per_default);
+  if (rc) return rc;
+  // the settings before the call stay eligible: tuning never makes it slower
+  double best = per_default > 0 ? per_default : 1e300;
+  int bb = c->block, bg = c->grid_per_sm, bk = c->graph_iters, bw = c->row_chunk;
   int tried = 0;
-  for (int gi : graphs) {
-    c->graph_iters = gi;
-    drop_graphs(c);
-    for (int bl : blocks)
-      for (int g : gps) {
-        if (g * bl > 2048) continue;  // the reduction grid stays resident
-        c->block = bl;
-        c->grid_per_sm = g;
-        int rc = build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
-        if (rc) return rc;
-        float t0 = 0, t1 = 0, w = 0;
-        if ((rc = run(k_short, w))) return rc;  // warm: graph capture, workspace
-        if ((rc = run(k_short, t0)) || (rc = run(k_long, t1))) return rc;
-        double per = (t1 - t0) / (double)(k_long - k_short);
-        ++tried;
-        if (per > 0 && per < best) {
-          best = per;
-          bb = bl; bg = g; bk = gi;
+  for (int gi : graphs)
+    for (int vw : widths)
+      for (int bl : blocks)
+        for (int g : gps) {
+          if (g * bl > 2048) continue;  // the reduction grid stays resident
+          c->graph_iters = gi;
+          c->row_chunk = vw;
+          c->block = bl;
+          c->grid_per_sm = g;
+          drop_graphs(c);
+          double per = 0.0;
+          if ((rc = measure(per))) return rc;
+          ++tried;
+          if (per > 0 && per < best) {
+            best = per;
+            bb = bl; bg = g; bk = gi; bw = vw;
+          }
         }
-      }
-  }
   c->precision = precision;
   c->inner_max_iter = inner_keep;
   c->block = bb;
   c->grid_per_sm = bg;
   c->graph_iters = bk;
+  c->row_chunk = bw;
   drop_graphs(c);
-  int rc = build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
+  rc = build_segments(c, c->seg_c0_caller, c->seg_c1_caller);
   if (rc) return rc;
   if (out) {
     out->block = bb;
@@ -2588,6 +2685,8 @@ int solv_gpu_autotune(solv_gpu_ctx* c, int solver, int imat, int n_vc, solv_gpu_
     out->graph_iters = bk;
     out->ms_per_iter = best;
     out->candidates = tried;
+    out->vector_width = bw;
+    out->ms_per_iter_before = per_default;
   }
   return SOLV_GPU_OK;
 }

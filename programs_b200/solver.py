@@ -32,6 +32,7 @@ OPT_PRECISION, OPT_INNER_REDUC, OPT_GRAPH_ITERS, OPT_BLOCK, OPT_GRID_PER_SM, OPT
 OPT_INNER_MAX_ITER, OPT_RELIABLE_DELTA, OPT_GNN_LOSS = 7, 8, 9
 OPT_MG_LEVELS, OPT_MG_SMOOTHER, OPT_MG_OMEGA, OPT_MG_ALPHA = 10, 11, 12, 13
 OPT_FCG_STALL_ITERS, OPT_FCG_STALL_DROP, OPT_MG_SCALE_MIN, OPT_MG_BUILD = 14, 15, 16, 17
+OPT_VECTOR_WIDTH = 18
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -57,7 +58,8 @@ class Stats(ctypes.Structure):
 class Tune(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int), ("grid_per_sm", ctypes.c_int),
                 ("graph_iters", ctypes.c_int), ("candidates", ctypes.c_int),
-                ("ms_per_iter", ctypes.c_double)]
+                ("ms_per_iter", ctypes.c_double), ("vector_width", ctypes.c_int),
+                ("ms_per_iter_before", ctypes.c_double)]
 
 
 # Exported symbols of include/solv_gpu.h (the tests check them all).
@@ -352,12 +354,15 @@ class GpuSolver:
         self._check(self._lib.solv_gpu_gnn_adam(self._h, lr, grad_scale))
 
     def autotune(self, solver: str = "cg", imat: int = 0, n_vc: int = 1) -> dict:
-        """Pick launch shapes for this matrix (left set on the context)."""
+        """Pick launch shapes (and, for FP32 iterations, the products' vector
+        width) for this matrix and solver ("cg", "bicg" or "fcg", the learned
+        solve); the choice is left set on the context."""
         t = Tune()
-        self._check(self._lib.solv_gpu_autotune(self._h, 0 if solver == "cg" else 1, imat, n_vc,
-                                                ctypes.byref(t)))
+        code = {"cg": 0, "bicg": 1, "fcg": 2}[solver]
+        self._check(self._lib.solv_gpu_autotune(self._h, code, imat, n_vc, ctypes.byref(t)))
         return {"block": t.block, "grid_per_sm": t.grid_per_sm, "graph_iters": t.graph_iters,
-                "candidates": t.candidates, "ms_per_iter": t.ms_per_iter}
+                "vector_width": t.vector_width, "candidates": t.candidates,
+                "ms_per_iter": t.ms_per_iter, "ms_per_iter_before": t.ms_per_iter_before}
 
     # -- batches of independent systems ----------------------------------------
     def matrix_set_batch(self, mats) -> np.ndarray:
