@@ -112,6 +112,12 @@ extern "C" {
 #define SOLV_OPT_MG_SCALE_MIN 16 /* floor on the network's per-cell scales
                                    (default 0.5; 0 leaves them as the
                                    network makes them)                     */
+#define SOLV_OPT_PERSISTENT 19  /* FP64 Jacobi PCG (imat 0, n_vc 1, one
+                                   system or a batch): 1 runs the whole
+                                   Krylov loop as one launch, a cluster of
+                                   8 thread blocks per system with the step
+                                   kernels fused (no host polls, no graph);
+                                   0 (default) the graph of step kernels   */
 #define SOLV_OPT_VECTOR_WIDTH 18 /* FP32 matrix products (mixed-precision
                                    Krylov, flexible CG, V-cycle): matrix
                                    slots each thread loads before it sums

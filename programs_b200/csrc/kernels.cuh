@@ -15,6 +15,7 @@
 // CPU restatement; reductions use a fixed tree and are run-to-run
 // deterministic.
 #pragma once
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -1282,6 +1283,144 @@ __global__ void SG_BOUNDS(1) k_fcg_update(SegMap sm, T* __restrict__ phi, T* __r
     if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);
     else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);
     else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
+  }
+}
+
+// ============ persistent fused Jacobi PCG: one thread-block cluster per system ============
+// The whole Krylov loop of solv_cg.f90:37-84 with imat = 0 in one launch:
+// each cluster of kPcgCluster CTAs owns one system (segment) and iterates it
+// to its stopping test, fusing the Jacobi step into the direction update,
+// the product with p.q, and the solution / residual update with |r|_1 and
+// r.z.  Per iteration three cluster barriers (after p; after the p.q
+// partials; after the update's partials); each CTA reduces its cells in a
+// fixed tree, puts its partials in shared memory, and every CTA sums the
+// cluster's partials in rank order over distributed shared memory -- so all
+// CTAs hold the same scalars and take the same branch, and the sums are
+// deterministic.  Per-cell arithmetic is the graph path's (k_cg_p,
+// k_cg_spmv, k_cg_update with JAC), so a solve differs from it only in the
+// reduction trees.  The loop is bounded by the lane's n_iter.
+constexpr int kPcgCluster = 8;
+constexpr int kPcgThreads = 1024;
+
+__device__ __forceinline__ double cluster_block_sum(double v, double* red) {
+  // fixed-order block sum; result in every thread
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  v = warp_sum(v);
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (w == 0) {
+    t = l < (int)(blockDim.x >> 5) ? red[l] : 0.0;
+    t = warp_sum(t);
+    if (l == 0) red[32] = t;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
+    Rows<double> R, const int* __restrict__ seg_c0, const int* __restrict__ seg_c1,
+    const double* __restrict__ c, double* __restrict__ phi, double* __restrict__ r,
+    double* __restrict__ p, double* __restrict__ q, Lane* __restrict__ lanes,
+    int* __restrict__ n_active) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  __shared__ double red[33];
+  __shared__ double part[2][2];  // this CTA's partials: [product][update]
+  const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
+  const int sys = blockIdx.x / cs;
+  const int c0 = seg_c0[sys], c1 = seg_c1[sys];
+  const int stride = cs * blockDim.x;
+  const int first = c0 + rank * blockDim.x + threadIdx.x;
+  Lane L = lanes[sys];
+  if (!L.active) return;  // uniform over the cluster
+  auto cluster_total = [&](int slot, int k) {
+    double t = 0.0;
+    for (int q2 = 0; q2 < cs; ++q2) t += *cl.map_shared_rank(&part[slot][k], q2);
+    return t;
+  };
+  // s = r.(c r), beta = (1/s_old) s (k_cg_rz with JAC)
+  {
+    double a = 0.0;
+    for (int i = first; i < c1; i += stride) {
+      const double ri = r[i];
+      a += prod(ri, mul(ri, c[i]));
+    }
+    a = cluster_block_sum(a, red);
+    if (threadIdx.x == 0) part[1][0] = a;
+    cl.sync();
+    const double s_new = cluster_total(1, 0);
+    const double beta = 1.0 / L.s;
+    L.s_prev = L.s;
+    L.s = s_new;
+    L.beta = beta * L.s;
+  }
+  int status = kLaneRunning;
+  while (true) {
+    // (a partial slot is rewritten only two barriers after its last read)
+    // p = z + beta p, z = c r (k_cg_p with JAC)
+    for (int i = first; i < c1; i += stride) {
+      const double zi = mul(r[i], c[i]);
+      p[i] = add(zi, mul(L.beta, p[i]));
+    }
+    cl.sync();  // p complete in the cluster
+    // q = A p, p.q (k_cg_spmv); neighbours' p read past L1
+    double a = 0.0;
+    for (int i = first; i < c1; i += stride) {
+      RowIt<double> it(R, i);
+      const double pi = __ldcg(&p[i]);
+      double y = mul(R.diag[i], pi);
+      for (int k = 0; k < it.w; ++k) {
+        const int e = it.base + k * kWarp;
+        const int j = __ldg(&R.col[e]);
+        if (j >= 0) y = add(y, mul(R.val[e], __ldcg(&p[j])));
+      }
+      q[i] = y;
+      a += prod(pi, y);
+    }
+    a = cluster_block_sum(a, red);
+    if (threadIdx.x == 0) part[0][0] = a;
+    cl.sync();
+    const double pq = cluster_total(0, 0);
+    L.pq = pq;
+    L.alpha = L.s / (pq + kSmall);  // solv_cg.f90:67-68
+    // phi += alpha p; r -= alpha q; |r|_1; r.(c r) (k_cg_update with JAC)
+    double l1 = 0.0, rz = 0.0;
+    for (int i = first; i < c1; i += stride) {
+      phi[i] = add(phi[i], mul(L.alpha, p[i]));
+      const double rn = sub(r[i], mul(L.alpha, q[i]));
+      r[i] = rn;
+      l1 += fabs(rn);
+      rz += prod(rn, mul(rn, c[i]));
+    }
+    l1 = cluster_block_sum(l1, red);
+    rz = cluster_block_sum(rz, red);
+    if (threadIdx.x == 0) {
+      part[1][0] = l1;
+      part[1][1] = rz;
+    }
+    cl.sync();
+    const double t1 = cluster_total(1, 0), t2 = cluster_total(1, 1);
+    L.iter += 1;
+    L.l1 = t1;
+    const double ratio = t1 / (L.res0_n + kSmall);  // solv_cg.f90:81
+    L.ratio = ratio;
+    if (!(ratio == ratio) || isinf(ratio)) status = kLaneNaN;
+    else if (ratio < L.reduc) status = kLaneConverged;  // :82
+    else if (L.iter >= L.n_iter) status = kLaneMaxIter;
+    if (status != kLaneRunning) break;
+    const double beta = 1.0 / L.s;
+    L.s_prev = L.s;
+    L.s = t2;
+    L.beta = beta * L.s;
+  }
+  cl.sync();  // no CTA leaves while others may still read its partials
+  if (rank == 0 && threadIdx.x == 0) {
+    L.active = 0;
+    L.status = status;
+    lanes[sys] = L;
+    atomicSub(n_active, 1);
   }
 }
 

@@ -172,6 +172,7 @@ struct solv_gpu_ctx {
   // stalls: fcg_stall_iters iterations without falling below fcg_stall_drop
   // times the value at the start of the window
   int row_chunk = sg::kRowChunk;       // FP32 products: matrix slots a thread loads per step
+  int persistent = 0;                  // FP64 Jacobi PCG as one cluster-persistent launch
   int fcg_stall_iters = 1000;
   double fcg_stall_drop = 0.9;
 };
@@ -1495,8 +1496,9 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   sg::k_lane_init<<<(nl + 255) / 256, 256, 0, s>>>(c->lanes.as<Lane>(), nl, n_iter, reduc,
                                                    c->n_active.as<int>());
   SegMap sm = segmap(c);
+  const bool fused = c->persistent && solver == 0 && imat <= 0 && V == 1;
   if (solver == 0) {
-    if (imat <= 0) {
+    if (imat <= 0 && !fused) {
       sg::k_cg_rz<double, V, true><<<c->seg.total_blk, c->block, 0, s>>>(
           sm, w.c, w.r, w.z, c->part.as<double>(), c->lanes.as<Lane>());
       c->launches++;
@@ -1509,8 +1511,27 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   c->launches += 2;
   CUDA_TRY(c, cudaGetLastError());
   int gl = 0;
-  rc = iterate<double, V>(c, solver, imat, n_iter, w, gl);
-  if (rc) return rc;
+  if (fused) {  // the whole loop in one launch: one cluster per system
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(c->n_seg * sg::kPcgCluster));
+    cfg.blockDim = dim3(sg::kPcgThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = sg::kPcgCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(c, cudaLaunchKernelEx(&cfg, sg::k_pcg_cluster, rows<double>(c), sm.seg_c0, sm.seg_c1,
+                                   (const double*)w.c, w.phi, w.r, w.p, w.q, c->lanes.as<Lane>(),
+                                   c->n_active.as<int>()));
+    c->launches++;
+  } else {
+    rc = iterate<double, V>(c, solver, imat, n_iter, w, gl);
+    if (rc) return rc;
+  }
   sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, V, o2n, w.phi, phi_dev);
   c->launches++;
   CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->lanes.p, nl * sizeof(Lane), cudaMemcpyDeviceToHost, s));
@@ -2232,6 +2253,10 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
     case SOLV_OPT_MG_SCALE_MIN:
       if (!(value >= 0 && value <= 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "scale floor in [0,1]");
       c->mg_scale_min = (float)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_PERSISTENT:
+      if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "persistent is 0 or 1");
+      c->persistent = (int)value;
       return SOLV_GPU_OK;
     case SOLV_OPT_VECTOR_WIDTH:
       if (value != 2 && value != 4 && value != 8)
