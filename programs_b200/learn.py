@@ -212,8 +212,22 @@ def _residual_samples(s: GpuSolver, b_dev, n_samples, rng, torch, max_k=400):
     return out
 
 
+def validation_loss(s: GpuSolver, systems, torch) -> float:
+    """Mean loss of the current parameters over fixed held-out systems
+    [(shell, (p, n, pl), b)], each with its right-hand side as the one
+    sample: the same systems before and after training, so the two numbers
+    compare (the running training loss mixes systems of different kinds)."""
+    vals = []
+    for shell, (p_d, n_d, pl_d), b_dev in systems:
+        s.matrix_set(shell)
+        s.matrix_values_dev(p_d.data_ptr(), n_d.data_ptr(), pl_d.data_ptr())
+        vals.append(s.gnn_grad_dev(b_dev.data_ptr(), b_dev.data_ptr(), 1))
+    s.gnn_zero_grad()
+    return float(np.mean(vals))
+
+
 def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
-          init=None, log_every=50, device=0, loss=2, smoother=1, data="synthetic"):
+          init=None, log_every=50, device=0, loss=2, smoother=1, data="synthetic", n_val=6):
     """smoother (loss 2): 1 trains the network's operator K as the V-cycle's
     smoother, 2 its per-cell diagonal alone (learned Jacobi weights).
     data: "synthetic" (the default, and what the shipped network was
@@ -237,6 +251,18 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
     t0 = time.time()
     step = 0
     with torch.cuda.stream(stream):
+        # held-out systems of the same kind (another seed), each kept whole
+        val_sys = []
+        if data == "loop":
+            vgen = loop_systems(size, n_val, 1, seed=seed + 1000, device=device, stream=stream)
+            for shell, (p_d, n_d, pl_d), b in vgen:
+                val_sys.append((shell, (p_d.clone(), n_d.clone(), pl_d.clone()), b.clone()))
+        else:
+            for _, shell, (p_d, n_d, pl_d), b in device_systems(size, n_val, 1, seed=seed + 1000,
+                                                                  device=device, stream=stream):
+                val_sys.append((shell, (p_d.clone(), n_d.clone(), pl_d.clone()),
+                                torch.from_numpy(b).to(dev)))
+        val_before = validation_loss(s, val_sys, torch)
         for ep in range(epochs):
             if data == "loop":
                 gen = loop_systems(size, n_mesh, per_mesh, seed=seed + ep, device=device,
@@ -259,10 +285,12 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
                 if log_every and step % log_every == 0:
                     print(json.dumps({"step": step, "loss": float(np.mean(hist[-log_every:])),
                                       "t": round(time.time() - t0, 1)}), flush=True)
+        val_after = validation_loss(s, val_sys, torch)
     stream.synchronize()
     p = s.gnn_get_params()
     s.close()
-    return p, hist
+    return p, hist, {"val_loss_before": val_before, "val_loss_after": val_after,
+                     "val_systems": len(val_sys)}
 
 
 def main(argv=None):
@@ -288,12 +316,13 @@ def main(argv=None):
     a = ap.parse_args(argv)
     init = load_params(a.resume) if a.resume else None
     t = time.time()
-    p, hist = train(a.size, a.meshes, a.per_mesh, a.samples, a.epochs, a.lr, a.seed, init,
-                    loss=a.loss, smoother=a.smoother, data=a.data)
-    meta = {"size": a.size, "loss": a.loss, "smoother": a.smoother, "data": a.data, "systems": a.meshes * a.per_mesh * a.epochs,
-            "samples": a.samples,
+    p, hist, val = train(a.size, a.meshes, a.per_mesh, a.samples, a.epochs, a.lr, a.seed, init,
+                         loss=a.loss, smoother=a.smoother, data=a.data)
+    meta = {"size": a.size, "loss": a.loss, "smoother": a.smoother, "data": a.data,
+            "systems": a.meshes * a.per_mesh * a.epochs, "samples": a.samples,
             "lr": a.lr, "seed": a.seed, "first_loss": float(np.mean(hist[:20])),
-            "last_loss": float(np.mean(hist[-20:])), "train_s": round(time.time() - t, 1)}
+            "last_loss": float(np.mean(hist[-20:])), **val,
+            "train_s": round(time.time() - t, 1)}
     save_params(a.out, p, meta)
     print(json.dumps(meta))
 

@@ -228,9 +228,10 @@ def test_training_gains_over_the_untrained_network(one_level):
     systems (comparable losses from step to step), not the SIMPLE loop's,
     whose losses vary too much between systems for a short run's mean."""
     p0 = learn.init_params(0)
-    p, hist = learn.train(size=12, n_mesh=4, per_mesh=12, samples=4, epochs=3, lr=3e-3, seed=0,
-                          init=p0, log_every=0, loss=1, data="synthetic")
+    p, hist, val = learn.train(size=12, n_mesh=4, per_mesh=12, samples=4, epochs=3, lr=3e-3,
+                               seed=0, init=p0, log_every=0, loss=1, data="synthetic")
     assert np.mean(hist[-10:]) < np.mean(hist[:10])
+    assert val["val_loss_after"] < val["val_loss_before"], val  # held-out systems
     A = _system(14, seed=11, lid=0.7, jitter=0.12)
     gpu.matrix_set(A)
     b = _rhs(A, 8)
@@ -433,9 +434,10 @@ def test_multigrid_training_gains_over_jacobi_smoothing(gpu):
     fewer FCG iterations than the same V-cycle with Jacobi smoothing (the
     untrained network)."""
     p0 = learn.init_params(0)
-    p, hist = learn.train(size=24, n_mesh=3, per_mesh=16, samples=4, epochs=2, lr=3e-3, seed=0,
-                          init=p0, log_every=0, loss=2, data="synthetic")
+    p, hist, val = learn.train(size=24, n_mesh=3, per_mesh=16, samples=4, epochs=2, lr=3e-3,
+                               seed=0, init=p0, log_every=0, loss=2, data="synthetic")
     assert np.mean(hist[-8:]) < np.mean(hist[:8])
+    assert val["val_loss_after"] < val["val_loss_before"], val  # held-out systems
     A = _system(32, seed=12, lid=0.8, jitter=0.15)
     gpu.matrix_set(A)
     b = _rhs(A, 15)
