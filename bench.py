@@ -376,11 +376,23 @@ def time_configs(s, torch, dev):
         for name, prec in (("fp64", 0), ("fp32_inner", 1)):
             c2[name] = timed_solve("bicg", 2, 1, b.reshape(-1, 1), precision=prec)
         out[f"momentum_128_bicgstab_dilu_{order}"] = c2
-    # C3a: u, v, w on one 96^3 mesh (shared matrix), BiCGSTAB + DILU, FP32 inner
-    A, b = make_system(96, "momentum")
+    # C3a: u, v, w on one 96^3 mesh (shared matrix), BiCGSTAB + DILU, FP32
+    # inner, in both cell orders
+    for order in ("rcm", "color"):
+        A, b = make_system(96, "momentum", renumber=order)
+        s.matrix_set(A)
+        B = np.stack([b, uniform(11, A.n_cell), uniform(12, A.n_cell)], axis=1)
+        out[f"momentum_96_uvw_bicgstab_dilu_fp32_inner_{order}"] = timed_solve(
+            "bicg", 2, 3, B, precision=1)
+    # C1 again with the cluster-persistent fused PCG (the whole loop in one launch)
+    from programs_b200.solver import OPT_PERSISTENT
+    m = Mesh.hex(32, jitter=0.15, seed=0, permute=True)
+    A = m.pressure(pin=1)
     s.matrix_set(A)
-    B = np.stack([b, uniform(11, A.n_cell), uniform(12, A.n_cell)], axis=1)
-    out["momentum_96_uvw_bicgstab_dilu_fp32_inner"] = timed_solve("bicg", 2, 3, B, precision=1)
+    s.set_option(OPT_PERSISTENT, 1)
+    out["pressure_32_plain_pcg_persistent"] = timed_solve("cg", 0, 1,
+                                                          poisson_rhs(A.n_cell, 1).reshape(-1, 1))
+    s.set_option(OPT_PERSISTENT, 0)
     # C3b: 64 uneven pressure meshes (8k-500k cells, seed 1) in one batch, FP32 inner
     mats, rhs = batch_meshes(64, 8000, 500000, seed=1)
     cp = s.matrix_set_batch(mats)
