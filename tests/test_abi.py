@@ -34,7 +34,7 @@ def test_every_fv_symbol_is_exported():
     from programs_b200.solver import lib
     L = lib()
     names = _declared("fv_gpu.h")
-    assert len(names) == 9
+    assert len(names) == 12
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
 

@@ -302,3 +302,40 @@ def test_device_resident_loop_reproduces_the_host_assembly_loop(gpu):
         assert [h["p_iters"] for h in h1] == [h["p_iters"] for h in h0]
         for a, b in zip(h0, h1):
             assert abs(a["mass"] - b["mass"]) <= 1e-12 * a["mass"]
+
+
+def test_face_flux_at_the_auxiliary_points():
+    """The reference's pressure-correction face loop takes the pressures at
+    the auxiliary points (cfd_setup.f90:611-620).  On a mesh without jitter
+    the auxiliary points are the cell centres (to rounding) and the two
+    fluxes agree; on a skewed mesh, for a linear pressure with its exact
+    gradient and no velocity, the plain form's smoothing term vanishes and
+    the auxiliary form keeps -d g.(x_N' - x_P') (d > 0), as the reference's
+    formula does."""
+    from programs_b200.mesh import face_flux, momentum_field
+    g = np.array([0.3, -0.2, 0.5])
+    for jitter in (0.0, 0.2):
+        m = Mesh.hex(7, jitter=jitter, seed=4, permute=True)
+        m.renumber(Mesh.RCM)
+        A, _, _ = momentum_field(m, cavity_field(m, 1.0))
+        xc, _ = m.cell_geom()
+        p = xc @ g
+        gp = np.tile(g, (m.n_cell, 1))
+        u0 = np.zeros((m.n_cell, 3))
+        f0 = face_flux(m, u0, p, gp, A.pl)
+        f1 = face_flux(m, u0, p, gp, A.pl, aux=True)
+        assert np.abs(f0).max() < 1e-14
+        if jitter == 0.0:
+            assert np.abs(f1).max() < 1e-14
+            continue
+        ip, inb = m.faces()
+        _, nrm, xf, _, _ = m.face_geom()
+        inner = np.nonzero(inb > 0)[0]
+        a, b = ip[inner] - 1, inb[inner] - 1
+        def aux(c):
+            t = np.einsum("ij,ij->i", xf[inner] - xc[c], nrm[inner])
+            return (xf[inner] - nrm[inner] * t[:, None]) - xc[c]
+        dp_aux = (aux(b) - aux(a)) @ g
+        big = np.abs(dp_aux) > 1e-10
+        assert big.sum() > inner.size // 2
+        assert np.all(f1[inner][big] / dp_aux[big] < 0)  # -d dp_aux with d > 0
