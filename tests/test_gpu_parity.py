@@ -432,3 +432,29 @@ def test_two_components_on_a_one_cell_deep_momentum_system(gpu, imat):
     A, _ = m.momentum()
     b = np.asfortranarray(np.stack([uniform(41, A.n_cell), uniform(42, A.n_cell)], axis=1))
     _two_components(gpu, A, b, imat, "bicg")
+
+
+@pytest.mark.parametrize("solver,imat", [("cg", 1), ("bicg", 2)])
+def test_four_components(gpu, solver, imat):
+    """n_vc = 4, the largest component count the library takes: four
+    right-hand sides in one call against the oracle, component by component
+    (CG with DIC on the pressure system, BiCGSTAB with DILU on momentum)."""
+    m = Mesh.hex(14, jitter=0.15, seed=7, permute=True)
+    m.renumber(Mesh.RCM)
+    A = m.pressure(pin=1) if solver == "cg" else m.momentum()[0]
+    cols = ([poisson_rhs(A.n_cell, 60 + v) for v in range(4)] if solver == "cg"
+            else [uniform(60 + v, A.n_cell) for v in range(4)])
+    b = np.asfortranarray(np.stack(cols, axis=1))
+    ref = getattr(Oracle.from_matrix(A), "solv_" + solver)(imat, 1e-10, 5000,
+                                                           np.zeros((A.n_cell, 4)), b)
+    gpu.matrix_set(A)
+    phi = np.zeros((A.n_cell, 4))
+    res0 = np.asfortranarray(b.copy())
+    rn = np.zeros(4)
+    st = getattr(gpu, "solv_" + solver)(imat, 1e-10, 5000, phi, res0, rn)
+    assert st["status"] == OK and len(st["iters"]) == 4
+    assert np.array_equal(res0, ref[1])
+    for v in range(4):
+        assert _rel(phi[:, v], ref[0][:, v]) <= SOL_TOL, v
+        assert abs(rn[v] - ref[2][v]) <= NORM_TOL * ref[2][v]
+        assert abs(st["iters"][v] - int(ref[3][v])) <= 2, (v, st["iters"][v], ref[3][v])
