@@ -350,6 +350,10 @@ class GpuSolver:
                                                      ctypes.byref(nc)))
         return agg, nc.value
 
+    def gnn_zero_grad(self) -> None:
+        """Clear the accumulated gradient."""
+        self._check(self._lib.solv_gpu_gnn_zero_grad(self._h))
+
     def gnn_adam(self, lr: float, grad_scale: float = 1.0) -> None:
         self._check(self._lib.solv_gpu_gnn_adam(self._h, lr, grad_scale))
 
