@@ -6,9 +6,12 @@
 //   1. three passes of pairwise matching.  Each pass is a handshake: every
 //      cell still free proposes to its most strongly coupled free neighbour
 //      (ties: the lower index), and two cells that propose to each other
-//      pair up; kRounds such rounds, then the cells left over stay alone.
-//      Pairs are numbered by their lower member (a prefix sum over the
-//      cells), which keeps the locality of the level's numbering.  Passes 2
+//      pair up; kRounds such rounds, then a cell left over joins the pair of
+//      its most strongly coupled matched neighbour (on dense coarse graphs
+//      proposals often form cycles and leave many cells unmatched; joined,
+//      they still coarsen).  Aggregates are numbered by their lower pair
+//      member (a prefix sum over the cells), which keeps the locality of
+//      the level's numbering.  Passes 2
 //      and 3 match the pass graphs: the aggregates so far, coupled by the
 //      summed strengths of the couplings between them;
 //   2. a cell left alone by all passes joins the aggregate of its most
@@ -156,20 +159,37 @@ __global__ void k_hs_accept(int n, const int* __restrict__ prop, int* __restrict
   }
 }
 
-// flag[i] = 1 where i is its pair's lower member (or alone)
-__global__ void k_hs_lead(int n, const int* __restrict__ mate, int* __restrict__ flag) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    flag[i] = (mate[i] < 0 || i < mate[i]) ? 1 : 0;
-}
-
-// agg[i] = number of the pair's lower member; then the composed map of the
-// level's cells (comp[x] = agg[comp[x]], or agg itself on the first pass)
-__global__ void k_hs_number(int n, const int* __restrict__ mate, const int* __restrict__ id,
-                            int* __restrict__ agg) {
+// rep[i]: the lower member of i's pair; a node the handshakes left alone
+// joins the pair of its most strongly coupled matched neighbour (first such
+// maximum in slot order), or stays alone.  flag[i] = 1 where i represents.
+__global__ void k_hs_rep(int n, Ell g, const float* __restrict__ w, const int* __restrict__ mate,
+                         int* __restrict__ rep, int* __restrict__ flag) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int m = mate[i];
-    agg[i] = id[(m >= 0 && m < i) ? m : i];
+    int r = m >= 0 ? min(i, m) : i;
+    if (m < 0) {
+      const int s = i >> 5, base = g.sp[s] + (i & 31), ws = g.sw[s];
+      float bw = 0.0f;
+      for (int k = 0; k < ws; ++k) {
+        const int e = base + k * 32;
+        const int j = g.col[e];
+        if (j < 0 || j == i || mate[j] < 0) continue;
+        if (w[e] > bw) {
+          bw = w[e];
+          r = min(j, mate[j]);
+        }
+      }
+    }
+    rep[i] = r;
+    flag[i] = r == i ? 1 : 0;
   }
+}
+
+// agg[i] = number of i's representative
+__global__ void k_hs_number(int n, const int* __restrict__ rep, const int* __restrict__ id,
+                            int* __restrict__ agg) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    agg[i] = id[rep[i]];
 }
 __global__ void k_compose(int n, int* __restrict__ comp, const int* __restrict__ agg) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)

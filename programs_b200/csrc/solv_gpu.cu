@@ -680,7 +680,7 @@ int gpu_aggregate(solv_gpu_ctx* c, mgb::Ell g, const float* w, int n, int passes
                   int* nc_out) {
   cudaStream_t s = c->stream;
   const int B = 256;
-  DevBuf mate, prop, flag, id, aggp, bs, size, used;
+  DevBuf mate, prop, flag, id, aggp, bs, size, used, rep;
   CoarseDev P;       // the current pass graph (after the first pass)
   DevBuf pw, pw2;    // its strengths
   CUDA_TRY(c, agg.ensure((size_t)n * sizeof(int)));
@@ -699,11 +699,12 @@ int gpu_aggregate(solv_gpu_ctx* c, mgb::Ell g, const float* w, int n, int passes
       mgb::k_hs_propose<<<G, B, 0, s>>>(np, gp, wp, mate.as<int>(), prop.as<int>());
       mgb::k_hs_accept<<<G, B, 0, s>>>(np, prop.as<int>(), mate.as<int>());
     }
-    mgb::k_hs_lead<<<G, B, 0, s>>>(np, mate.as<int>(), flag.as<int>());
+    CUDA_TRY(c, rep.ensure((size_t)np * sizeof(int)));
+    mgb::k_hs_rep<<<G, B, 0, s>>>(np, gp, wp, mate.as<int>(), rep.as<int>(), flag.as<int>());
     int nn = 0;
     int rc = dev_scan(c, flag.as<int>(), id.as<int>(), np, bs, &nn);
     if (rc) return rc;
-    mgb::k_hs_number<<<G, B, 0, s>>>(np, mate.as<int>(), id.as<int>(), aggp.as<int>());
+    mgb::k_hs_number<<<G, B, 0, s>>>(np, rep.as<int>(), id.as<int>(), aggp.as<int>());
     if (p == 0)
       CUDA_TRY(c, cudaMemcpyAsync(agg.p, aggp.p, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, s));
     else

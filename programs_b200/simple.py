@@ -33,7 +33,7 @@ from .solver import GpuSolver, OPT_PRECISION
 def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15, seed=0,
         p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None, p_imat=1,
         m_precision=0, device=0, log_every=0, make_solver=None, reference_terms=False,
-        reference_weights=False):
+        reference_weights=False, p_scale=False):
     """Returns (u (N,3), p (N,), history, timings).  learned: weights array
     (FCG with the learned preconditioner for the pressure correction) or
     None (plain FP64 PCG with imat p_imat).  make_solver(device) builds the
@@ -48,7 +48,12 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
     pressures at the auxiliary points in the face fluxes (:611-620).
     run_device does the same on the GPU.  reference_weights takes the
     reference's face distance and interpolation weight
-    (Mesh.set_face_weights)."""
+    (Mesh.set_face_weights).  p_scale multiplies each pressure-correction
+    right-hand side by the power of two nearest n_cell / sum|b| before the
+    solve and divides the solution by it after: exact in floating point, so
+    the solvers' arithmetic is unchanged except that the reference's
+    absolute guard 1e-20 on the CG step (solv_cg.f90:67-68) acts on numbers
+    of order one instead of the shrinking mass imbalance."""
     rho = 1.0
     mu = rho * u_lid * 1.0 / re
     m = Mesh.hex(size, jitter=jitter, seed=seed, permute=True)
@@ -110,12 +115,14 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
         else:
             sp.matrix_values(P.p, P.n, P.pl)
         pp = np.zeros((N, 1))
-        res0 = np.asfortranarray(b.reshape(-1, 1))
+        sc = rhs_scale(N, imb) if p_scale else 1.0
+        res0 = np.asfortranarray(b.reshape(-1, 1) * sc)
         rn_p = np.zeros(1)
         if learned is not None:
             stp = sp.solv_fcg(p_reduc, p_iter, pp, res0, rn_p, not_r0=True)
         else:
             stp = sp.solv_cg(p_imat, p_reduc, p_iter, pp, res0, rn_p, not_r0=True)
+        pp /= sc
         t_solve_p += time.time() - ts
         ta = time.time()
         gradpp = grad_p(pp[:, 0])
@@ -136,7 +143,7 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
 def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15,
                seed=0, p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None,
                p_imat=1, m_precision=0, device=0, log_every=0, reference_weights=False,
-               reference_terms=False, renumber="rcm"):
+               reference_terms=False, renumber="rcm", p_scale=False):
     """The same outer loop with everything on the GPU: assembly, gradients
     (the corrected sweeps too), the explicit momentum terms, fluxes and
     corrections by the fv_gpu kernels (bit-for-bit the host functions),
@@ -224,12 +231,17 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
             ts = time.time()
             sp.matrix_values_dev(Pp.data_ptr(), Pn.data_ptr(), Ppl.data_ptr())
             pp = torch.zeros(N, dtype=torch.float64, device=dev)
+            sc = rhs_scale(N, imb) if p_scale else 1.0
+            if sc != 1.0:
+                b *= sc
             if learned is not None:
                 rn_p, stp = sp.solv_fcg_dev(p_reduc, p_iter, pp.data_ptr(), b.data_ptr(),
                                             not_r0=True)
             else:
                 rn_p, stp = sp.solv_cg_dev(p_imat, p_reduc, p_iter, 1, pp.data_ptr(),
                                            b.data_ptr(), not_r0=True)
+            if sc != 1.0:
+                pp /= sc
             t_solve_p += sync_time(ts)
             ta = time.time()
             gradpp = grad_p(pp)
@@ -249,6 +261,13 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
     timing = {"total_s": total, "assembly_s": t_asm, "momentum_solve_s": t_solve_m,
               "pressure_solve_s": t_solve_p, "n_cell": N}
     return u_h, p_h, hist, timing
+
+
+def rhs_scale(n_cell, total):
+    """The power of two nearest n_cell / total (1 for a zero total)."""
+    if not total > 0:
+        return 1.0
+    return float(2.0 ** int(round(np.log2(n_cell / total))))
 
 
 def rel_l2(a, b):
@@ -276,6 +295,8 @@ def main(argv=None):
                          "auxiliary-point face pressures")
     ap.add_argument("--renumber", default="rcm", choices=["rcm", "color"],
                     help="cell order of the device loop's mesh")
+    ap.add_argument("--p-scale", action="store_true",
+                    help="normalise each pressure right-hand side by an exact power of two")
     ap.add_argument("--learned-m-precision", type=int, default=1,
                     help="momentum solves of the learned run: 1 FP32 inner iterations with "
                          "FP64 refinement, 0 FP64")
@@ -284,14 +305,15 @@ def main(argv=None):
     a = ap.parse_args(argv)
     loop = run_device if a.device_assembly else run
     kw = dict(p_reduc=a.p_reduc, p_iter=a.p_iter, p_imat=a.p_imat, m_reduc=a.m_reduc,
-              m_iter=a.m_iter, log_every=a.log_every, reference_weights=a.reference_weights)
+              m_iter=a.m_iter, log_every=a.log_every, reference_weights=a.reference_weights,
+              p_scale=a.p_scale)
     if a.reference_terms:
         kw["reference_terms"] = True
     if a.device_assembly:
         kw["renumber"] = a.renumber
     u0, p0, h0, t0 = loop(a.size, a.outer, a.re, **kw)
     out = {"size": a.size, "outer": a.outer, "re": a.re, "p_reduc": a.p_reduc,
-           "p_imat": a.p_imat, "reference_terms": a.reference_terms,
+           "p_imat": a.p_imat, "reference_terms": a.reference_terms, "p_scale": a.p_scale,
            "renumber": a.renumber if a.device_assembly else "rcm",
            "plain": t0, "final_mass_plain": h0[-1]["mass"], "first_mass": h0[0]["mass"],
            "p_iters_plain": int(np.sum([h["p_iters"] for h in h0]))}

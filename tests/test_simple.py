@@ -339,3 +339,18 @@ def test_face_flux_at_the_auxiliary_points():
         big = np.abs(dp_aux) > 1e-10
         assert big.sum() > inner.size // 2
         assert np.all(f1[inner][big] / dp_aux[big] < 0)  # -d dp_aux with d > 0
+
+
+def test_pressure_rhs_scaling_is_exact():
+    """p_scale multiplies the pressure right-hand side by a power of two and
+    divides the solution by it: exact in floating point, so with the
+    oracle's solvers at the reference's settings (where the absolute guard
+    is far from binding) the loop's fields come out the same."""
+    from programs_b200 import simple
+    assert simple.rhs_scale(1000, 1.0) == 1024.0 and simple.rhs_scale(8, 0.0) == 1.0
+    kw = dict(size=6, n_outer=6, re=100.0, p_reduc=0.1, p_iter=20, p_imat=1,
+              make_solver=_OracleSolver)
+    u0, p0, _, _ = simple.run(**kw)
+    u1, p1, _, _ = simple.run(p_scale=True, **kw)
+    assert np.allclose(u1, u0, rtol=1e-12, atol=1e-15) and np.allclose(p1, p0, rtol=1e-12,
+                                                                        atol=1e-15)
