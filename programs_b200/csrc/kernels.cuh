@@ -537,7 +537,18 @@ __global__ void k_fill_pending(long long n, T* __restrict__ x) {
 // that makes every dependency point to an earlier (or the same) slice.  A
 // warp whose lanes wait spins for kSweepSpin polls, then sleeps briefly
 // between polls.
-constexpr int kSweepSpin = 64;
+#ifndef SG_SWEEP_SPIN
+#define SG_SWEEP_SPIN 64
+#endif
+#ifndef SG_SWEEP_SLEEP
+#define SG_SWEEP_SLEEP 64
+#endif
+#ifndef SG_SWEEP_PEEK
+#define SG_SWEEP_PEEK 0
+#endif
+constexpr int kSweepSpin = SG_SWEEP_SPIN;
+constexpr int kSweepSleep = SG_SWEEP_SLEEP;
+constexpr bool kSweepPeek = SG_SWEEP_PEEK != 0;
 
 template <bool UP, typename Step>
 __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ slice_w,
@@ -558,7 +569,7 @@ __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ 
         if (lane == 0) atomicExch(&ctl->err, 1);
         break;
       }
-      if (poll >= kSweepSpin) __nanosleep(64);
+      if (poll >= kSweepSpin) __nanosleep(kSweepSleep);
       if (k < w) k = step(i, k, false);
     }
   }
@@ -570,8 +581,21 @@ __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ 
 // first one still pending.  `use(e, xv)` folds a ready value in.  Returns
 // the slot to resume from (w when the row is complete).
 template <int C, int V, typename T, typename Dep, typename Use>
-__device__ __forceinline__ int advance(const Rows<T>& R, int base, int w, int k, const T* vals,
-                                       Dep&& dep, Use&& use) {
+__device__ __forceinline__ int advance(const Rows<T>& R, int base, int w, int k, bool retry,
+                                       const T* vals, Dep&& dep, Use&& use) {
+  if (kSweepPeek && retry && k < w) {
+    // a retry: poll the one slot that was pending before loading a chunk
+    const int j = __ldg(&R.col[base + k * kWarp]);
+    if (j >= 0 && dep(j)) {
+      T xv[V];
+      bool rdy = true;
+#pragma unroll
+      for (int v = 0; v < V; ++v) rdy &= take(&vals[(size_t)j * V + v], xv[v]);
+      if (!rdy) return k;
+      use(base + k * kWarp, xv);
+    }
+    ++k;
+  }
   while (k < w) {
     int j[C];
     T xv[C][V];
@@ -617,7 +641,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_precond_sf(
       d = R.diag[i];
     }
     if (imat == 1 || imat == 2) {
-      k = advance<4, 1>(R, base, w, k, c, [&](int j) { return j < i; },
+      k = advance<4, 1>(R, base, w, k, !first, c, [&](int j) { return j < i; },
                         [&](int e, const double (&cj)[1]) {
                           const int f = __ldg(&slot_src[e]) >> 1;
                           if (imat == 1) {
@@ -666,7 +690,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_fwd_sf(
 #pragma unroll
       for (int v = 0; v < V; ++v) acc[v] = bvec[(size_t)i * V + v];
     }
-    k = advance<SweepChunk<V>::value, V>(R, base, w, k, t, [&](int j) { return j < i; },
+    k = advance<SweepChunk<V>::value, V>(R, base, w, k, !first, t, [&](int j) { return j < i; },
                                          [&](int e, const T (&xv)[V]) {
                                            const T a = R.sval[e];
 #pragma unroll
@@ -704,7 +728,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_bwd_sf(
 #pragma unroll
       for (int v = 0; v < V; ++v) acc[v] = mul(t[(size_t)i * V + v], cr);
     }
-    k = advance<SweepChunk<V>::value, V>(R, base, w, k, x, [&](int j) { return j > i; },
+    k = advance<SweepChunk<V>::value, V>(R, base, w, k, !first, x, [&](int j) { return j > i; },
                                          [&](int e, const T (&xv)[V]) {
                                            const T a = R.sval[e];
 #pragma unroll

@@ -711,7 +711,11 @@ int gpu_aggregate(solv_gpu_ctx* c, mgb::Ell g, const float* w, int n, int passes
       mgb::k_compose<<<grid_for(c, n), B, 0, s>>>(n, agg.as<int>(), aggp.as<int>());
     if (p + 1 < passes && nn < np) {  // the next pass graph and its strengths
       CoarseDev Q;
-      if ((rc = gpu_galerkin(c, gp, np, aggp.as<int>(), nn, Q))) return rc;
+      if ((rc = gpu_galerkin(c, gp, np, aggp.as<int>(), nn, Q))) {
+        if (rc != SOLV_GPU_TOO_LARGE) return rc;
+        np = nn;  // a pass graph too dense for 255 slots a row: pair no further
+        break;
+      }
       CUDA_TRY(c, pw2.ensure((size_t)std::max(Q.n_slots, 1) * sizeof(float)));
       mgb::k_sum_abs<<<grid_for(c, Q.n_slots), B, 0, s>>>(Q.n_slots, Q.gptr.as<int>(),
                                                            Q.gsrc.as<int>(), wp, pw2.as<float>());
@@ -1138,6 +1142,9 @@ int coop_launch(solv_gpu_ctx* c, void (*kern)(KArgs...), Args... args) {
   } else {
     CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sg::kSweepThreads, 0));
     if (per_sm < 1) return set_err(c, SOLV_GPU_DEVICE_ERROR, "sweep kernel cannot be resident");
+#ifdef SG_SWEEP_BLOCKS
+    per_sm = std::min(per_sm, SG_SWEEP_BLOCKS);
+#endif
     c->coop_blocks[(const void*)kern] = per_sm;
   }
   const long long warps = ((long long)c->N + 31) / 32;

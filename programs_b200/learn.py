@@ -33,7 +33,7 @@ import time
 import numpy as np
 
 from .mesh import Mesh, cavity_field, momentum_field, poisson_rhs, pressure_correction
-from .solver import GpuSolver
+from .solver import BAD_INPUT, GpuSolver, SolverError
 
 H, NF, NL = 32, 4, 3
 P_WIN = 0
@@ -250,6 +250,7 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
     hist = []
     t0 = time.time()
     step = 0
+    skipped = 0
     with torch.cuda.stream(stream):
         # held-out systems of the same kind (another seed), each kept whole
         val_sys = []
@@ -278,7 +279,15 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
                 if data == "loop" and step % 2 == 1:  # the other kind of right-hand side
                     b_dev = torch.from_numpy(poisson_rhs(b_dev.shape[0], seed * 7919 + step)).to(dev)
                 rs = _residual_samples(s, b_dev, samples, rng, torch)
-                val = s.gnn_grad_dev(b_dev.data_ptr(), rs.data_ptr(), rs.shape[0])
+                try:
+                    val = s.gnn_grad_dev(b_dev.data_ptr(), rs.data_ptr(), rs.shape[0])
+                except SolverError as e:
+                    # the multigrid loss on a system whose hierarchy could not
+                    # be built (coarsening stalled): no gradient from it
+                    if loss != 2 or e.code != BAD_INPUT:
+                        raise
+                    skipped += 1
+                    continue
                 s.gnn_adam(lr, 1.0)
                 step += 1
                 hist.append(val)
@@ -290,7 +299,7 @@ def train(size=64, n_mesh=40, per_mesh=50, samples=4, epochs=1, lr=2e-3, seed=0,
     p = s.gnn_get_params()
     s.close()
     return p, hist, {"val_loss_before": val_before, "val_loss_after": val_after,
-                     "val_systems": len(val_sys)}
+                     "val_systems": len(val_sys), "skipped_systems": skipped}
 
 
 def main(argv=None):

@@ -106,3 +106,46 @@ def test_gpu_and_host_builds_precondition_alike(gpu):
         gpu.set_option(OPT_MG_SMOOTHER, 1)
         gpu.set_option(OPT_PRECISION, 0)
     assert abs(its[0] - its[1]) <= 0.25 * its[1] + 2, its
+
+
+def _hub_system(per_hub=250, seed=7):
+    """Two strongly coupled hub cells, each with per_hub neighbours; every
+    neighbour has a private, strongly coupled partner and the partners form a
+    weak chain.  The first matching pass pairs the hubs and each neighbour
+    with its partner, so the hubs' aggregate touches 2 x per_hub others: a
+    pass graph (and a coarse level) whose row is wider than the 255 slots of
+    the slice format."""
+    from programs_b200.mesh import FaceMatrix
+    rng = np.random.default_rng(seed)
+    L = 2 * per_hub
+    leaf = 2 + np.arange(L)
+    part = 2 + L + np.arange(L)
+    a = [np.array([0]), np.where(np.arange(L) < per_hub, 0, 1), leaf, part[:-1]]
+    b = [np.array([1]), leaf, part, part[1:]]
+    w = [np.array([50.0]), rng.uniform(0.5, 1.0, L), rng.uniform(20.0, 30.0, L),
+         rng.uniform(0.1, 0.2, L - 1)]
+    ip, inb, wf = (np.concatenate(x) for x in (a, b, w))
+    N = 2 + 2 * L
+    diag = np.bincount(ip, wf, N) + np.bincount(inb, wf, N) + 1.0
+    return FaceMatrix(N, (ip + 1).astype(np.int32), (inb + 1).astype(np.int32), -wf, -wf.copy(),
+                      diag)
+
+
+@pytest.mark.parametrize("build", [0, 1])
+def test_too_dense_a_coarse_row_means_one_level(gpu, build):
+    """Where coarsening meets a row wider than the slice format holds, the
+    hierarchy is given up (GPU and host builds alike) and the flexible CG
+    runs with the one-level preconditioner: a solution, not an error."""
+    A = _hub_system()
+    b = poisson_rhs(A.n_cell, 9)
+    ref = Oracle.from_matrix(A).solv_cg(0, 1e-12, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
+    gpu.gnn_set_params(learn.init_params(0))
+    gpu.set_option(OPT_MG_BUILD, build)
+    try:
+        gpu.matrix_set(A)
+        phi = np.zeros((A.n_cell, 1))
+        st = gpu.solv_fcg(1e-12, 20000, phi, np.asfortranarray(b.reshape(-1, 1).copy()), np.zeros(1))
+    finally:
+        gpu.set_option(OPT_MG_BUILD, 0)
+    assert st["status"] == OK and st["mg_levels"] == 0
+    assert np.linalg.norm(phi - ref[0]) / np.linalg.norm(ref[0]) <= 1e-8
