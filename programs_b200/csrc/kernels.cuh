@@ -576,35 +576,43 @@ __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ 
 }
 
 // One advance of a recurrence row: from slot k, the slots of the dependency
-// side (`dep(j)`) are taken in chunks of C -- all their values loaded at
-// once (one round trip to L2 per chunk), then added in slot order up to the
-// first one still pending.  `use(e, xv)` folds a ready value in.  Returns
-// the slot to resume from (w when the row is complete).
-template <int C, int V, typename T, typename Dep, typename Use>
+// side (`dep(j)`) are taken in chunks of C -- their neighbour values and
+// their coefficients (`coef(e)`, read-only data) loaded at once, so that a
+// coefficient never waits behind a value that has just arrived -- then
+// added in slot order up to the first one still pending.  `use(a, xv)`
+// folds a ready value in.  Returns the slot to resume from (w when the row
+// is complete).
+template <int C, int V, typename T, typename Dep, typename Coef, typename Use>
 __device__ __forceinline__ int advance(const Rows<T>& R, int base, int w, int k, bool retry,
-                                       const T* vals, Dep&& dep, Use&& use) {
+                                       const T* vals, Dep&& dep, Coef&& coef, Use&& use) {
+  using A = decltype(coef(0));
   if (kSweepPeek && retry && k < w) {
     // a retry: poll the one slot that was pending before loading a chunk
-    const int j = __ldg(&R.col[base + k * kWarp]);
+    const int e = base + k * kWarp;
+    const int j = __ldg(&R.col[e]);
     if (j >= 0 && dep(j)) {
+      const A a = coef(e);
       T xv[V];
       bool rdy = true;
 #pragma unroll
       for (int v = 0; v < V; ++v) rdy &= take(&vals[(size_t)j * V + v], xv[v]);
       if (!rdy) return k;
-      use(base + k * kWarp, xv);
+      use(a, xv);
     }
     ++k;
   }
   while (k < w) {
     int j[C];
+    A a[C];
     T xv[C][V];
     bool rdy[C];
 #pragma unroll
     for (int u = 0; u < C; ++u) {
-      j[u] = k + u < w ? __ldg(&R.col[base + (k + u) * kWarp]) : -1;
+      const int e = base + (k + u) * kWarp;
+      j[u] = k + u < w ? __ldg(&R.col[e]) : -1;
       rdy[u] = true;
       if (j[u] >= 0 && dep(j[u])) {
+        a[u] = coef(e);
 #pragma unroll
         for (int v = 0; v < V; ++v) rdy[u] &= take(&vals[(size_t)j[u] * V + v], xv[u][v]);
       }
@@ -614,7 +622,7 @@ __device__ __forceinline__ int advance(const Rows<T>& R, int base, int w, int k,
       if (k >= w) return w;
       if (j[u] >= 0 && dep(j[u])) {
         if (!rdy[u]) return k;
-        use(base + k * kWarp, xv[u]);
+        use(a[u], xv[u]);
       }
       ++k;
     }
@@ -641,16 +649,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_precond_sf(
       d = R.diag[i];
     }
     if (imat == 1 || imat == 2) {
-      k = advance<4, 1>(R, base, w, k, !first, c, [&](int j) { return j < i; },
-                        [&](int e, const double (&cj)[1]) {
-                          const int f = __ldg(&slot_src[e]) >> 1;
-                          if (imat == 1) {
-                            const double nf = fn[f];
-                            d = sub(d, mul(mul(nf, nf), cj[0]));
-                          } else {
-                            d = sub(d, mul(mul(fp[f], cj[0]), fn[f]));
-                          }
-                        });
+      k = advance<4, 1>(
+          R, base, w, k, !first, c, [&](int j) { return j < i; },
+          [&](int e) {
+            const int f = __ldg(&slot_src[e]) >> 1;
+            return make_double2(__ldg(imat == 1 ? &fn[f] : &fp[f]), __ldg(&fn[f]));
+          },
+          [&](const double2& a, const double (&cj)[1]) {
+            if (imat == 1)
+              d = sub(d, mul(mul(a.y, a.y), cj[0]));
+            else
+              d = sub(d, mul(mul(a.x, cj[0]), a.y));
+          });
       if (k < w) return k;
     }
     c_r[i] = d;
@@ -669,7 +679,10 @@ __global__ void k_precond_jacobi(int n, const double* __restrict__ diag, double*
   }
 }
 
-template <int V> struct SweepChunk { static constexpr int value = V == 1 ? 4 : 2; };
+// slots per chunk: fewer for wide FP64 rows, which would spill
+template <typename T, int V> struct SweepChunk {
+  static constexpr int value = V == 1 ? 4 : (V >= 4 && sizeof(T) == 8 ? 1 : 2);
+};
 
 // solv_direct.f90:12-24 forward sweep, x_i = (b_i - sum_{j<i} n x_j) c_i, into
 // t (which starts out pending); the backward sweep's output x is reset to
@@ -680,25 +693,25 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_fwd_sf(
     SweepCtl* ctl, const int* __restrict__ n_active) {
   if (n_active && *n_active == 0) return;
   const int lane = threadIdx.x & 31;
-  T acc[V];
+  T acc[V], ci = T(0);
   int base = 0;
   sweep_slices<false>(n, R.slice_w, ctl, [&](int i, int k, bool first) -> int {
     const int w = __ldg(&R.slice_w[i >> 5]);
     if (first) {
       if (i >= n) return w;
       base = __ldg(&R.slice_ptr[i >> 5]) + lane;
+      ci = __ldg(&c[i]);
 #pragma unroll
       for (int v = 0; v < V; ++v) acc[v] = bvec[(size_t)i * V + v];
     }
-    k = advance<SweepChunk<V>::value, V>(R, base, w, k, !first, t, [&](int j) { return j < i; },
-                                         [&](int e, const T (&xv)[V]) {
-                                           const T a = R.sval[e];
+    k = advance<SweepChunk<T, V>::value, V>(
+        R, base, w, k, !first, t, [&](int j) { return j < i; },
+        [&](int e) { return __ldg(&R.sval[e]); },
+        [&](const T a, const T (&xv)[V]) {
 #pragma unroll
-                                           for (int v = 0; v < V; ++v)
-                                             acc[v] = sub(acc[v], mul(a, xv[v]));
-                                         });
+          for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, xv[v]));
+        });
     if (k < w) return k;
-    const T ci = c[i];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       st_relaxed(&t[(size_t)i * V + v], mul(acc[v], ci));
@@ -717,26 +730,26 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_bwd_sf(
     SweepCtl* ctl, const int* __restrict__ n_active) {
   if (n_active && *n_active == 0) return;
   const int lane = threadIdx.x & 31;
-  T acc[V];
+  T acc[V], ci = T(0);
   int base = 0;
   sweep_slices<true>(n, R.slice_w, ctl, [&](int i, int k, bool first) -> int {
     const int w = __ldg(&R.slice_w[i >> 5]);
     if (first) {
       if (i >= n) return w;
       base = __ldg(&R.slice_ptr[i >> 5]) + lane;
+      ci = __ldg(&c[i]);
       const T cr = c_r[i];
 #pragma unroll
       for (int v = 0; v < V; ++v) acc[v] = mul(t[(size_t)i * V + v], cr);
     }
-    k = advance<SweepChunk<V>::value, V>(R, base, w, k, !first, x, [&](int j) { return j > i; },
-                                         [&](int e, const T (&xv)[V]) {
-                                           const T a = R.sval[e];
+    k = advance<SweepChunk<T, V>::value, V>(
+        R, base, w, k, !first, x, [&](int j) { return j > i; },
+        [&](int e) { return __ldg(&R.sval[e]); },
+        [&](const T a, const T (&xv)[V]) {
 #pragma unroll
-                                           for (int v = 0; v < V; ++v)
-                                             acc[v] = sub(acc[v], mul(a, xv[v]));
-                                         });
+          for (int v = 0; v < V; ++v) acc[v] = sub(acc[v], mul(a, xv[v]));
+        });
     if (k < w) return k;
-    const T ci = c[i];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
       st_relaxed(&x[(size_t)i * V + v], mul(acc[v], ci));

@@ -160,14 +160,15 @@ __global__ void k_hs_accept(int n, const int* __restrict__ prop, int* __restrict
 }
 
 // rep[i]: the lower member of i's pair; a node the handshakes left alone
-// joins the pair of its most strongly coupled matched neighbour (first such
-// maximum in slot order), or stays alone.  flag[i] = 1 where i represents.
+// stays alone, or with `join` joins the pair of its most strongly coupled
+// matched neighbour (first such maximum in slot order).  flag[i] = 1 where
+// i represents.
 __global__ void k_hs_rep(int n, Ell g, const float* __restrict__ w, const int* __restrict__ mate,
-                         int* __restrict__ rep, int* __restrict__ flag) {
+                         int join, int* __restrict__ rep, int* __restrict__ flag) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int m = mate[i];
     int r = m >= 0 ? min(i, m) : i;
-    if (m < 0) {
+    if (m < 0 && join) {
       const int s = i >> 5, base = g.sp[s] + (i & 31), ws = g.sw[s];
       float bw = 0.0f;
       for (int k = 0; k < ws; ++k) {

@@ -700,10 +700,14 @@ int gpu_aggregate(solv_gpu_ctx* c, mgb::Ell g, const float* w, int n, int passes
       mgb::k_hs_accept<<<G, B, 0, s>>>(np, prop.as<int>(), mate.as<int>());
     }
     CUDA_TRY(c, rep.ensure((size_t)np * sizeof(int)));
-    mgb::k_hs_rep<<<G, B, 0, s>>>(np, gp, wp, mate.as<int>(), rep.as<int>(), flag.as<int>());
-    int nn = 0;
-    int rc = dev_scan(c, flag.as<int>(), id.as<int>(), np, bs, &nn);
-    if (rc) return rc;
+    // nodes the handshakes left alone stay alone for this pass, unless the
+    // pass would then keep more than 3/4 of its nodes: then they join a pair
+    int nn = 0, rc = 0;
+    for (int join = 0; join < 2; ++join) {
+      mgb::k_hs_rep<<<G, B, 0, s>>>(np, gp, wp, mate.as<int>(), join, rep.as<int>(), flag.as<int>());
+      if ((rc = dev_scan(c, flag.as<int>(), id.as<int>(), np, bs, &nn))) return rc;
+      if (nn <= 0.75 * np) break;
+    }
     mgb::k_hs_number<<<G, B, 0, s>>>(np, rep.as<int>(), id.as<int>(), aggp.as<int>());
     if (p == 0)
       CUDA_TRY(c, cudaMemcpyAsync(agg.p, aggp.p, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice, s));

