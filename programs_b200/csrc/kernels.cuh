@@ -1325,7 +1325,8 @@ __global__ void SG_BOUNDS(1) k_fcg_update(SegMap sm, T* __restrict__ phi, T* __r
 
 // ============ persistent fused Jacobi PCG: one thread-block cluster per system ============
 // The whole Krylov loop of solv_cg.f90:37-84 with imat = 0 in one launch:
-// each cluster of kPcgCluster CTAs owns one system (segment) and iterates it
+// each cluster of CTAs (kPcgCluster, or kPcgClusterMax where the GPU holds
+// a cluster that large at once) owns one system (segment) and iterates it
 // to its stopping test, fusing the Jacobi step into the direction update,
 // the product with p.q, and the solution / residual update with |r|_1 and
 // r.z.  Per iteration three cluster barriers (after p; after the p.q
@@ -1336,7 +1337,8 @@ __global__ void SG_BOUNDS(1) k_fcg_update(SegMap sm, T* __restrict__ phi, T* __r
 // deterministic.  Per-cell arithmetic is the graph path's (k_cg_p,
 // k_cg_spmv, k_cg_update with JAC), so a solve differs from it only in the
 // reduction trees.  The loop is bounded by the lane's n_iter.
-constexpr int kPcgCluster = 8;
+constexpr int kPcgCluster = 8;      // portable cluster size
+constexpr int kPcgClusterMax = 16;  // non-portable, one system's whole GPC
 constexpr int kPcgThreads = 1024;
 
 __device__ __forceinline__ double cluster_block_sum(double v, double* red) {
@@ -1356,6 +1358,63 @@ __device__ __forceinline__ double cluster_block_sum(double v, double* red) {
   return red[32];
 }
 
+// Two fixed-order block sums in one pass (red holds 2 x 33 doubles).
+__device__ __forceinline__ void cluster_block_sum2(double& a, double& b, double* red) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  a = warp_sum(a);
+  b = warp_sum(b);
+  __syncthreads();
+  if (l == 0) {
+    red[w] = a;
+    red[33 + w] = b;
+  }
+  __syncthreads();
+  if (w == 0) {
+    const bool in = l < (int)(blockDim.x >> 5);
+    double ta = warp_sum(in ? red[l] : 0.0);
+    double tb = warp_sum(in ? red[33 + l] : 0.0);
+    if (l == 0) {
+      red[32] = ta;
+      red[65] = tb;
+    }
+  }
+  __syncthreads();
+  a = red[32];
+  b = red[65];
+}
+
+// y_i = (A p)_i for two rows at once (i1 < 0: none), each summed in slot
+// order as row_apply does; slot k of both rows is loaded before either is
+// added, so two independent gathers are in flight (two slots a row spilled
+// under the 64 registers a 1024-thread block allows).
+__device__ __forceinline__ void row_pair_apply(const Rows<double>& R, int i0, int i1,
+                                               const double* p, double& y0, double& y1) {
+  RowIt<double> r0(R, i0);
+  RowIt<double> r1(R, i1 >= 0 ? i1 : i0);
+  const int w0 = r0.w, w1 = i1 >= 0 ? r1.w : 0;
+  y0 = mul(R.diag[i0], __ldcg(&p[i0]));
+  y1 = i1 >= 0 ? mul(R.diag[i1], __ldcg(&p[i1])) : 0.0;
+  const int wm = max(w0, w1);
+  for (int k = 0; k < wm; ++k) {
+    int j0 = -1, j1 = -1;
+    double a0 = 0.0, a1 = 0.0;
+    if (k < w0) {
+      const int e = r0.base + k * kWarp;
+      j0 = __ldg(&R.col[e]);
+      a0 = __ldg(&R.val[e]);
+    }
+    if (k < w1) {
+      const int e = r1.base + k * kWarp;
+      j1 = __ldg(&R.col[e]);
+      a1 = __ldg(&R.val[e]);
+    }
+    const double x0 = j0 >= 0 ? __ldcg(&p[j0]) : 0.0;
+    const double x1 = j1 >= 0 ? __ldcg(&p[j1]) : 0.0;
+    if (j0 >= 0) y0 = add(y0, mul(a0, x0));
+    if (j1 >= 0) y1 = add(y1, mul(a1, x1));
+  }
+}
+
 __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
     Rows<double> R, const int* __restrict__ seg_c0, const int* __restrict__ seg_c1,
     const double* __restrict__ c, double* __restrict__ phi, double* __restrict__ r,
@@ -1363,15 +1422,21 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
     int* __restrict__ n_active) {
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
-  __shared__ double red[33];
+  __shared__ double red[66];
   __shared__ double part[2][2];  // this CTA's partials: [product][update]
   const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
   const int sys = blockIdx.x / cs;
   const int c0 = seg_c0[sys], c1 = seg_c1[sys];
   const int stride = cs * blockDim.x;
   const int first = c0 + rank * blockDim.x + threadIdx.x;
-  Lane L = lanes[sys];
-  if (!L.active) return;  // uniform over the cluster
+  // the lane's scalars, in registers (the Lane itself is written back once)
+  const Lane L0 = lanes[sys];
+  if (!L0.active) return;  // uniform over the cluster
+  const double res0_n = L0.res0_n, reduc = L0.reduc;
+  const int n_iter = L0.n_iter;
+  double s_cur = L0.s, s_prev = L0.s_prev, beta = 0.0, alpha = L0.alpha, pq = L0.pq;
+  double l1v = L0.l1, ratio = L0.ratio;
+  int iter = L0.iter;
   auto cluster_total = [&](int slot, int k) {
     double t = 0.0;
     for (int q2 = 0; q2 < cs; ++q2) t += *cl.map_shared_rank(&part[slot][k], q2);
@@ -1388,10 +1453,10 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
     if (threadIdx.x == 0) part[1][0] = a;
     cl.sync();
     const double s_new = cluster_total(1, 0);
-    const double beta = 1.0 / L.s;
-    L.s_prev = L.s;
-    L.s = s_new;
-    L.beta = beta * L.s;
+    const double b0 = 1.0 / s_cur;
+    s_prev = s_cur;
+    s_cur = s_new;
+    beta = b0 * s_cur;
   }
   int status = kLaneRunning;
   while (true) {
@@ -1399,61 +1464,66 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
     // p = z + beta p, z = c r (k_cg_p with JAC)
     for (int i = first; i < c1; i += stride) {
       const double zi = mul(r[i], c[i]);
-      p[i] = add(zi, mul(L.beta, p[i]));
+      p[i] = add(zi, mul(beta, p[i]));
     }
     cl.sync();  // p complete in the cluster
-    // q = A p, p.q (k_cg_spmv); neighbours' p read past L1
+    // q = A p, p.q (k_cg_spmv); neighbours' p read past L1; two rows at a time
     double a = 0.0;
-    for (int i = first; i < c1; i += stride) {
-      RowIt<double> it(R, i);
-      const double pi = __ldcg(&p[i]);
-      double y = mul(R.diag[i], pi);
-      for (int k = 0; k < it.w; ++k) {
-        const int e = it.base + k * kWarp;
-        const int j = __ldg(&R.col[e]);
-        if (j >= 0) y = add(y, mul(R.val[e], __ldcg(&p[j])));
+    for (int i = first; i < c1; i += 2 * stride) {
+      const int i1 = i + stride < c1 ? i + stride : -1;
+      double y0, y1;
+      row_pair_apply(R, i, i1, p, y0, y1);
+      q[i] = y0;
+      a += prod(__ldcg(&p[i]), y0);
+      if (i1 >= 0) {
+        q[i1] = y1;
+        a += prod(__ldcg(&p[i1]), y1);
       }
-      q[i] = y;
-      a += prod(pi, y);
     }
     a = cluster_block_sum(a, red);
     if (threadIdx.x == 0) part[0][0] = a;
     cl.sync();
-    const double pq = cluster_total(0, 0);
-    L.pq = pq;
-    L.alpha = L.s / (pq + kSmall);  // solv_cg.f90:67-68
+    pq = cluster_total(0, 0);
+    alpha = s_cur / (pq + kSmall);  // solv_cg.f90:67-68
     // phi += alpha p; r -= alpha q; |r|_1; r.(c r) (k_cg_update with JAC)
     double l1 = 0.0, rz = 0.0;
     for (int i = first; i < c1; i += stride) {
-      phi[i] = add(phi[i], mul(L.alpha, p[i]));
-      const double rn = sub(r[i], mul(L.alpha, q[i]));
+      phi[i] = add(phi[i], mul(alpha, p[i]));
+      const double rn = sub(r[i], mul(alpha, q[i]));
       r[i] = rn;
       l1 += fabs(rn);
       rz += prod(rn, mul(rn, c[i]));
     }
-    l1 = cluster_block_sum(l1, red);
-    rz = cluster_block_sum(rz, red);
+    cluster_block_sum2(l1, rz, red);
     if (threadIdx.x == 0) {
       part[1][0] = l1;
       part[1][1] = rz;
     }
     cl.sync();
     const double t1 = cluster_total(1, 0), t2 = cluster_total(1, 1);
-    L.iter += 1;
-    L.l1 = t1;
-    const double ratio = t1 / (L.res0_n + kSmall);  // solv_cg.f90:81
-    L.ratio = ratio;
+    iter += 1;
+    l1v = t1;
+    ratio = t1 / (res0_n + kSmall);  // solv_cg.f90:81
     if (!(ratio == ratio) || isinf(ratio)) status = kLaneNaN;
-    else if (ratio < L.reduc) status = kLaneConverged;  // :82
-    else if (L.iter >= L.n_iter) status = kLaneMaxIter;
+    else if (ratio < reduc) status = kLaneConverged;  // :82
+    else if (iter >= n_iter) status = kLaneMaxIter;
     if (status != kLaneRunning) break;
-    const double beta = 1.0 / L.s;
-    L.s_prev = L.s;
-    L.s = t2;
-    L.beta = beta * L.s;
+    const double b1 = 1.0 / s_cur;
+    s_prev = s_cur;
+    s_cur = t2;
+    beta = b1 * s_cur;
   }
   cl.sync();  // no CTA leaves while others may still read its partials
   if (rank == 0 && threadIdx.x == 0) {
+    Lane L = L0;
+    L.s = s_cur;
+    L.s_prev = s_prev;
+    L.beta = beta;
+    L.alpha = alpha;
+    L.pq = pq;
+    L.iter = iter;
+    L.l1 = l1v;
+    L.ratio = ratio;
     L.active = 0;
     L.status = status;
     lanes[sys] = L;

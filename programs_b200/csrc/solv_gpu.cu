@@ -173,6 +173,7 @@ struct solv_gpu_ctx {
   // times the value at the start of the window
   int row_chunk = sg::kRowChunk;       // FP32 products: matrix slots a thread loads per step
   int persistent = 0;                  // FP64 Jacobi PCG as one cluster-persistent launch
+  int pcg_max16 = -1;                  // clusters of 16 resident at once (-1: not asked yet)
   int fcg_stall_iters = 1000;
   double fcg_stall_drop = 0.9;
 };
@@ -1533,14 +1534,37 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   CUDA_TRY(c, cudaGetLastError());
   int gl = 0;
   if (fused) {  // the whole loop in one launch: one cluster per system
+    // 16 blocks per cluster where all the systems' clusters fit at once,
+    // else the portable 8 (more clusters resident side by side)
+    if (c->pcg_max16 < 0) {
+      c->pcg_max16 = 0;
+      if (cudaFuncSetAttribute(sg::k_pcg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed,
+                               1) == cudaSuccess) {
+        cudaLaunchConfig_t q = {};
+        q.gridDim = dim3(sg::kPcgClusterMax);
+        q.blockDim = dim3(sg::kPcgThreads);
+        cudaLaunchAttribute qa[1];
+        qa[0].id = cudaLaunchAttributeClusterDimension;
+        qa[0].val.clusterDim.x = sg::kPcgClusterMax;
+        qa[0].val.clusterDim.y = 1;
+        qa[0].val.clusterDim.z = 1;
+        q.attrs = qa;
+        q.numAttrs = 1;
+        int n16 = 0;
+        if (cudaOccupancyMaxActiveClusters(&n16, sg::k_pcg_cluster, &q) == cudaSuccess)
+          c->pcg_max16 = n16;
+      }
+      cudaGetLastError();  // a refused query leaves the portable size
+    }
+    const int cs = c->n_seg <= c->pcg_max16 ? sg::kPcgClusterMax : sg::kPcgCluster;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(c->n_seg * sg::kPcgCluster));
+    cfg.gridDim = dim3((unsigned)(c->n_seg * cs));
     cfg.blockDim = dim3(sg::kPcgThreads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = sg::kPcgCluster;
+    attr[0].val.clusterDim.x = cs;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
