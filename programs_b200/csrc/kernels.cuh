@@ -43,10 +43,12 @@ struct Lane {
   double res0_n, ratio, reduc, l1;
   double gs;                           // FCG: residual scale fed to the network
   double s_prev;                       // CG: r.z of the previous iteration
+  double l1_stop;                      // FP32 inner iterations: stop for a reliable
+                                       // update once |r|_1 falls below this (0: never)
   int iter, n_iter, active, status;
 };
 enum : int { kLaneRunning = 0, kLaneConverged = 1, kLaneMaxIter = 2, kLaneNaN = 3,
-             kLaneStall = 4 };
+             kLaneStall = 4, kLaneRefine = 5 };
 
 // Flexible-CG beta = -(z.q)/(p.q) for the next direction p = z + beta p,
 // restarted (beta = 0) each time the lane has taken a multiple of n
@@ -791,7 +793,7 @@ __global__ void k_lane_init(Lane* lanes, int nl, int n_iter, double reduc, int* 
   L.rho = 0.0; L.beta0 = 1.0; L.gam = 1.0; L.omeg = 0.0;   // solv_bicg.f90:31-33
   L.res0_n = lanes[l].res0_n;
   L.ratio = 0.0; L.reduc = reduc; L.l1 = 0.0;
-  L.iter = 0; L.n_iter = n_iter; L.active = 1; L.status = kLaneRunning;
+  L.iter = 0; L.n_iter = n_iter; L.active = 1; L.status = kLaneRunning; L.l1_stop = 0.0;
   if (n_iter <= 0) { L.active = 0; L.status = kLaneMaxIter; }  // n_active set by the host
   lanes[l] = L;
 }
@@ -973,6 +975,7 @@ __global__ void SG_BOUNDS(V) k_cg_update(SegMap sm, const T* __restrict__ c, T* 
       if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);
       else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);  // :82
       else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
+      else if (tot[v] < L.l1_stop) lane_stop(L, kLaneRefine, sm.n_active);
       if (JAC && FLEX && L.active) {
         L.beta = flex_beta(L, tot[V + v], c1 - c0);
       } else if (JAC && L.active) {
@@ -1174,6 +1177,7 @@ __global__ void SG_BOUNDS(V) k_bi_update(SegMap sm, T* __restrict__ phi, T* __re
       if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);
       else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);
       else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
+      else if (tot[v] < L.l1_stop) lane_stop(L, kLaneRefine, sm.n_active);
       if (L.active) {
         L.rho = tot[V + v];
         if constexpr (sizeof(T) == 4) L.omeg = div0(L.rho * L.gam, L.alpha * L.beta0);
@@ -1320,6 +1324,7 @@ __global__ void SG_BOUNDS(1) k_fcg_update(SegMap sm, T* __restrict__ phi, T* __r
     if (!(ratio == ratio) || isinf(ratio)) lane_stop(L, kLaneNaN, sm.n_active);
     else if (ratio < L.reduc) lane_stop(L, kLaneConverged, sm.n_active);
     else if (L.iter >= L.n_iter) lane_stop(L, kLaneMaxIter, sm.n_active);
+    else if (tot[0] < L.l1_stop) lane_stop(L, kLaneRefine, sm.n_active);
   }
 }
 
@@ -1331,10 +1336,10 @@ __global__ void SG_BOUNDS(1) k_fcg_update(SegMap sm, T* __restrict__ phi, T* __r
 // the product with p.q, and the solution / residual update with |r|_1 and
 // r.z.  Per iteration three cluster barriers (after p; after the p.q
 // partials; after the update's partials); each CTA reduces its cells in a
-// fixed tree, puts its partials in shared memory, and every CTA sums the
-// cluster's partials in rank order over distributed shared memory -- so all
-// CTAs hold the same scalars and take the same branch, and the sums are
-// deterministic.  Per-cell arithmetic is the graph path's (k_cg_p,
+// fixed tree, puts its partials in shared memory, and in every CTA one warp
+// reads the cluster's partials over distributed shared memory (a lane per
+// rank) and sums them in a fixed tree -- so all CTAs hold the same scalars
+// and take the same branch, and the sums are deterministic.  Per-cell arithmetic is the graph path's (k_cg_p,
 // k_cg_spmv, k_cg_update with JAC), so a solve differs from it only in the
 // reduction trees.  The loop is bounded by the lane's n_iter.
 constexpr int kPcgCluster = 8;      // portable cluster size
@@ -1424,6 +1429,7 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
   cg::cluster_group cl = cg::this_cluster();
   __shared__ double red[66];
   __shared__ double part[2][2];  // this CTA's partials: [product][update]
+  __shared__ double tot_s[2];
   const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
   const int sys = blockIdx.x / cs;
   const int c0 = seg_c0[sys], c1 = seg_c1[sys];
@@ -1437,10 +1443,28 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
   double s_cur = L0.s, s_prev = L0.s_prev, beta = 0.0, alpha = L0.alpha, pq = L0.pq;
   double l1v = L0.l1, ratio = L0.ratio;
   int iter = L0.iter;
-  auto cluster_total = [&](int slot, int k) {
-    double t = 0.0;
-    for (int q2 = 0; q2 < cs; ++q2) t += *cl.map_shared_rank(&part[slot][k], q2);
-    return t;
+  // the cluster's totals of one partial slot: lane q of warp 0 reads rank
+  // q's pair over distributed shared memory, the warp sums them in a fixed
+  // tree (the same in every CTA), and the block takes the pair from there
+  auto cluster_totals = [&](int slot, double& t0, double& t1) {
+    if (threadIdx.x < 32) {
+      const int l = threadIdx.x;
+      double a = 0.0, b = 0.0;
+      if (l < cs) {
+        const double* pp = cl.map_shared_rank(&part[slot][0], l);
+        a = pp[0];
+        b = pp[1];
+      }
+      a = warp_sum(a);
+      b = warp_sum(b);
+      if (l == 0) {
+        tot_s[0] = a;
+        tot_s[1] = b;
+      }
+    }
+    __syncthreads();
+    t0 = tot_s[0];
+    t1 = tot_s[1];
   };
   // s = r.(c r), beta = (1/s_old) s (k_cg_rz with JAC)
   {
@@ -1450,9 +1474,13 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
       a += prod(ri, mul(ri, c[i]));
     }
     a = cluster_block_sum(a, red);
-    if (threadIdx.x == 0) part[1][0] = a;
+    if (threadIdx.x == 0) {
+      part[1][0] = a;
+      part[1][1] = 0.0;
+    }
     cl.sync();
-    const double s_new = cluster_total(1, 0);
+    double s_new, unused;
+    cluster_totals(1, s_new, unused);
     const double b0 = 1.0 / s_cur;
     s_prev = s_cur;
     s_cur = s_new;
@@ -1481,9 +1509,13 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
       }
     }
     a = cluster_block_sum(a, red);
-    if (threadIdx.x == 0) part[0][0] = a;
+    if (threadIdx.x == 0) {
+      part[0][0] = a;
+      part[0][1] = 0.0;
+    }
     cl.sync();
-    pq = cluster_total(0, 0);
+    double unused2;
+    cluster_totals(0, pq, unused2);
     alpha = s_cur / (pq + kSmall);  // solv_cg.f90:67-68
     // phi += alpha p; r -= alpha q; |r|_1; r.(c r) (k_cg_update with JAC)
     double l1 = 0.0, rz = 0.0;
@@ -1500,7 +1532,8 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
       part[1][1] = rz;
     }
     cl.sync();
-    const double t1 = cluster_total(1, 0), t2 = cluster_total(1, 1);
+    double t1, t2;
+    cluster_totals(1, t1, t2);
     iter += 1;
     l1v = t1;
     ratio = t1 / (res0_n + kSmall);  // solv_cg.f90:81

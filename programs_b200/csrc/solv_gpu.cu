@@ -103,6 +103,7 @@ struct solv_gpu_ctx {
   int max_refine = 30;
   int inner_max_iter = 2000;
   double reliable_delta = 0.1;
+  double fcg_reliable_delta = 1e-3;  // the learned flexible CG's reliable-update drop
   int gnn_loss = 1;  // training loss: 0 energy, 1 scale-free (best-step energy)
 
   // matrix (caller sizes)
@@ -1800,7 +1801,14 @@ int solve_mixed(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
 // dropped by `reliable_delta` since the last update (or claims
 // convergence), the FP32 correction is added to the FP64 solution, the
 // FP64 residual b - A x replaces the FP32 one, and the search direction
-// carries on.  Only the FP64 residual decides convergence.
+// carries on.  Only the FP64 residual decides convergence.  A flexible-CG
+// lane of the learned preconditioner stops itself at that drop
+// (Lane::l1_stop, kLaneRefine), whatever the graph length: iterations past
+// it would only push the FP32 recursive residual below what FP32 can
+// represent of the true one.  Jacobi-CG lanes are checked between graph
+// launches only: on a pinned Poisson system their slowest mode (the one the
+// pin barely holds) converges late relative to the residual, and stopping
+// each lane at the first 0.1 drop left it 1e-7 off at a 1e-10 residual.
 template <int V>
 int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
                          double* phi_dev, double* res0_dev, double* res0_n, int not_r0,
@@ -1876,6 +1884,9 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     }
     L.status = sg::kLaneRunning;
     l1_last[l] = l1[l];
+    // the learned FCG lane stops itself for the update (Jacobi CG lanes are
+    // checked between graph launches: their near-null modes want the longer runs)
+    L.l1_stop = solver == 2 ? c->fcg_reliable_delta * l1[l] : 0.0;
     na += L.active;
     hl[l] = L;
   }
@@ -1908,7 +1919,6 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     c->launches++;
   }
   CUDA_TRY(c, cudaGetLastError());
-  const double delta = c->reliable_delta;
   int updates = 0, gl_total = 0, launched = 0;
   // The learned preconditioner hands over to Jacobi-PCG, from the current
   // iterate, when it loses positive curvature or produces NaN (the lane
@@ -1917,6 +1927,9 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
   // value at the start of that window -- or when the FP64 residual stops
   // improving across reliable updates.
   int cur = solver;
+  // the residual drop between reliable updates: the learned FCG's own, or
+  // (after a hand-over, and for CG) the CG one
+  auto delta_of = [&]() { return cur == 2 ? c->fcg_reliable_delta : c->reliable_delta; };
   c->fallbacks = 0;
   std::vector<int> win_iter(nl, 0);
   std::vector<double> win_l1(l1_last);
@@ -1940,7 +1953,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     std::vector<char> trig(nl, 0);
     for (int l = 0; l < nl; ++l) {
       if (final_[l]) continue;
-      if (!hl[l].active || hl[l].l1 < delta * l1_last[l]) need = trig[l] = 1;
+      if (!hl[l].active || hl[l].l1 < delta_of() * l1_last[l]) need = trig[l] = 1;
       if (cur != 2) continue;
       if (hl[l].status == sg::kLaneStall) {
         hand_over();  // no positive curvature from the network
@@ -2003,6 +2016,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
       }
       if (final_[l]) L.active = 0;
       if (trig[l]) l1_last[l] = l1[l];  // lanes along for the ride keep their window
+      L.l1_stop = cur == 2 ? delta_of() * l1_last[l] : 0.0;
       win_iter[l] = L.iter;  // the stall window restarts from the FP64 residual
       win_l1[l] = l1[l];
       na += L.active;
@@ -2256,6 +2270,11 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
     case SOLV_OPT_RELIABLE_DELTA:
       if (!(value > 0 && value < 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "reliable delta in (0,1)");
       c->reliable_delta = value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_FCG_RELIABLE_DELTA:
+      if (!(value > 0 && value < 1))
+        return set_err(c, SOLV_GPU_BAD_INPUT, "reliable delta in (0,1)");
+      c->fcg_reliable_delta = value;
       return SOLV_GPU_OK;
     case SOLV_OPT_MG_LEVELS:  // 0 keeps a built hierarchy aside; another maximum rebuilds it
       if (value < 0 || value > mg::kMaxLevels)

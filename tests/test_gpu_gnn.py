@@ -25,7 +25,8 @@ from oracle import gnn_ref
 from oracle.oracle import Oracle
 from programs_b200 import learn
 from programs_b200.mesh import Mesh, cavity_field, momentum_field, pressure_correction, uniform
-from programs_b200.solver import (OK, OPT_FCG_STALL_DROP, OPT_FCG_STALL_ITERS, OPT_MG_LEVELS,
+from programs_b200.solver import (OK, OPT_FCG_RELIABLE_DELTA, OPT_FCG_STALL_DROP,
+                                  OPT_FCG_STALL_ITERS, OPT_GRAPH_ITERS, OPT_MG_LEVELS,
                                   OPT_MG_SCALE_MIN, OPT_MG_SMOOTHER, OPT_PRECISION)
 
 pytestmark = pytest.mark.gpu
@@ -257,6 +258,33 @@ def test_committed_weights_solve_to_the_oracle_solution(gpu):
     S = A.to_scipy()
     assert np.abs(b - S @ phi[:, 0]).sum() / rn[0] < 1e-10
     assert st["iters"][0] < int(ref[3][0])  # fewer iterations than Jacobi-PCG
+
+
+@pytest.mark.skipif(not os.path.exists(learn.DEFAULT_WEIGHTS), reason="no trained weights")
+@pytest.mark.parametrize("delta", [1e-1, 1e-3])
+def test_reliable_updates_do_not_depend_on_the_graph_length(gpu, delta):
+    """A learned-FCG lane stops itself for each reliable update (its FP32
+    residual down by SOLV_OPT_FCG_RELIABLE_DELTA), so how many iterations
+    one graph launch holds changes nothing: the same iterations, updates
+    and solution, bit for bit."""
+    A = _system(28, seed=23, lid=1.1, jitter=0.2)
+    gpu.matrix_set(A)
+    gpu.gnn_set_params(learn.load_params())
+    b = _rhs(A, 13)
+    out = {}
+    gpu.set_option(OPT_FCG_RELIABLE_DELTA, delta)
+    try:
+        for k in (4, 32):
+            gpu.set_option(OPT_GRAPH_ITERS, k)
+            phi, st, rn = _solve_fcg(gpu, A, b)
+            assert st["status"] == OK and st["fallbacks"] == 0
+            assert np.abs(b - A.to_scipy() @ phi[:, 0]).sum() / rn[0] < 1e-10
+            out[k] = (phi, st["iters"][0], st["refinements"])
+    finally:
+        gpu.set_option(OPT_GRAPH_ITERS, 16)
+        gpu.set_option(OPT_FCG_RELIABLE_DELTA, 1e-3)
+    assert out[4][1:] == out[32][1:]
+    assert np.array_equal(out[4][0], out[32][0])
 
 
 def _ref_iters(A, b):
