@@ -1564,4 +1564,229 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster(
   }
 }
 
+// The same loop for a system small enough for one cluster to hold
+// (at most cs x 1024 x RPT cells): each CTA owns a contiguous block of
+// B = 1024 x RPT cells, keeps their r, c, phi, p and q in registers (RPT
+// cells a thread) and their p in shared memory, and the product reads a
+// neighbour's p over distributed shared memory from the CTA that owns it
+// -- no vector goes through L2 inside the loop, only the matrix slots
+// (read-only, L1-resident after the first pass).  Per-cell arithmetic and
+// the slot order of the sums are the global-memory kernel's.
+template <int RPT>
+__global__ void __launch_bounds__(kPcgThreads) k_pcg_cluster_res(
+    Rows<double> R, const int* __restrict__ seg_c0, const int* __restrict__ seg_c1,
+    const double* __restrict__ c, double* __restrict__ phi, double* __restrict__ r,
+    double* __restrict__ p, double* __restrict__ q, Lane* __restrict__ lanes,
+    int* __restrict__ n_active) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  constexpr int B = kPcgThreads * RPT;
+  constexpr int LOGB = RPT == 1 ? 10 : 11;
+  static_assert(RPT == 1 || RPT == 2, "one or two cells a thread");
+  __shared__ double p_s[B];
+  __shared__ double red[66];
+  __shared__ double part[2][2];
+  __shared__ double tot_s[2];
+  const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
+  const int sys = blockIdx.x / cs;
+  const int c0 = seg_c0[sys], c1 = seg_c1[sys];
+  const Lane L0 = lanes[sys];
+  if (!L0.active) return;  // uniform over the cluster
+  int row[RPT];
+  double rr[RPT], cc[RPT], ph[RPT], pp[RPT], qq[RPT];
+#pragma unroll
+  for (int u = 0; u < RPT; ++u) {
+    row[u] = c0 + rank * B + u * kPcgThreads + (int)threadIdx.x;
+    const bool h = row[u] < c1;
+    rr[u] = h ? r[row[u]] : 0.0;
+    cc[u] = h ? c[row[u]] : 0.0;
+    ph[u] = h ? phi[row[u]] : 0.0;
+    pp[u] = h ? p[row[u]] : 0.0;
+    qq[u] = 0.0;
+    if (!h) row[u] = -1;
+  }
+  const double res0_n = L0.res0_n, reduc = L0.reduc;
+  const int n_iter = L0.n_iter;
+  double s_cur = L0.s, s_prev = L0.s_prev, beta = 0.0, alpha = L0.alpha, pq = L0.pq;
+  double l1v = L0.l1, ratio = L0.ratio;
+  int iter = L0.iter;
+  auto cluster_totals = [&](int slot, double& t0, double& t1) {
+    if (threadIdx.x < 32) {
+      const int l = threadIdx.x;
+      double a = 0.0, b = 0.0;
+      if (l < cs) {
+        const double* pr = cl.map_shared_rank(&part[slot][0], l);
+        a = pr[0];
+        b = pr[1];
+      }
+      a = warp_sum(a);
+      b = warp_sum(b);
+      if (l == 0) {
+        tot_s[0] = a;
+        tot_s[1] = b;
+      }
+    }
+    __syncthreads();
+    t0 = tot_s[0];
+    t1 = tot_s[1];
+  };
+  // s = r.(c r), beta = (1/s_old) s
+  {
+    double a = 0.0;
+#pragma unroll
+    for (int u = 0; u < RPT; ++u)
+      if (row[u] >= 0) a += prod(rr[u], mul(rr[u], cc[u]));
+    a = cluster_block_sum(a, red);
+    if (threadIdx.x == 0) {
+      part[1][0] = a;
+      part[1][1] = 0.0;
+    }
+    cl.sync();
+    double s_new, unused;
+    cluster_totals(1, s_new, unused);
+    const double b0 = 1.0 / s_cur;
+    s_prev = s_cur;
+    s_cur = s_new;
+    beta = b0 * s_cur;
+  }
+  int status = kLaneRunning;
+  while (true) {
+    // p = z + beta p, z = c r; this CTA's p into shared memory
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) {
+      if (row[u] >= 0) pp[u] = add(mul(rr[u], cc[u]), mul(beta, pp[u]));
+      p_s[u * kPcgThreads + threadIdx.x] = pp[u];
+    }
+    cl.sync();  // every CTA's p visible in the cluster
+    // q = A p, p.q: neighbours' p from their owners' shared memory
+    double a = 0.0;
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) {
+      if (row[u] < 0) continue;
+      RowIt<double> it(R, row[u]);
+      double y = mul(__ldg(&R.diag[row[u]]), pp[u]);
+      for (int k0 = 0; k0 < it.w; k0 += 4) {
+        int j[4];
+        double av[4], xv[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          j[v] = -1;
+          av[v] = 0.0;
+          if (k0 + v < it.w) {
+            const int e = it.base + (k0 + v) * kWarp;
+            j[v] = __ldg(&R.col[e]);
+            av[v] = __ldg(&R.val[e]);
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          xv[v] = 0.0;
+          if (j[v] >= 0) {
+            const int o = j[v] - c0;
+            xv[v] = *cl.map_shared_rank(&p_s[o & (B - 1)], o >> LOGB);
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          if (j[v] >= 0) y = add(y, mul(av[v], xv[v]));
+      }
+      qq[u] = y;
+      a += prod(pp[u], y);
+    }
+    a = cluster_block_sum(a, red);
+    if (threadIdx.x == 0) {
+      part[0][0] = a;
+      part[0][1] = 0.0;
+    }
+    cl.sync();
+    double unused2;
+    cluster_totals(0, pq, unused2);
+    alpha = s_cur / (pq + kSmall);  // solv_cg.f90:67-68
+    double l1 = 0.0, rz = 0.0;
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) {
+      if (row[u] < 0) continue;
+      ph[u] = add(ph[u], mul(alpha, pp[u]));
+      const double rn = sub(rr[u], mul(alpha, qq[u]));
+      rr[u] = rn;
+      l1 += fabs(rn);
+      rz += prod(rn, mul(rn, cc[u]));
+    }
+    cluster_block_sum2(l1, rz, red);
+    if (threadIdx.x == 0) {
+      part[1][0] = l1;
+      part[1][1] = rz;
+    }
+    cl.sync();
+    double t1, t2;
+    cluster_totals(1, t1, t2);
+    iter += 1;
+    l1v = t1;
+    ratio = t1 / (res0_n + kSmall);  // solv_cg.f90:81
+    if (!(ratio == ratio) || isinf(ratio)) status = kLaneNaN;
+    else if (ratio < reduc) status = kLaneConverged;  // :82
+    else if (iter >= n_iter) status = kLaneMaxIter;
+    if (status != kLaneRunning) break;
+    const double b1 = 1.0 / s_cur;
+    s_prev = s_cur;
+    s_cur = t2;
+    beta = b1 * s_cur;
+  }
+#pragma unroll
+  for (int u = 0; u < RPT; ++u) {
+    if (row[u] < 0) continue;
+    phi[row[u]] = ph[u];
+    r[row[u]] = rr[u];
+    p[row[u]] = pp[u];
+    q[row[u]] = qq[u];
+  }
+  cl.sync();  // no CTA leaves while others may still read its shared memory
+  if (rank == 0 && threadIdx.x == 0) {
+    Lane L = L0;
+    L.s = s_cur;
+    L.s_prev = s_prev;
+    L.beta = beta;
+    L.alpha = alpha;
+    L.pq = pq;
+    L.iter = iter;
+    L.l1 = l1v;
+    L.ratio = ratio;
+    L.active = 0;
+    L.status = status;
+    lanes[sys] = L;
+    atomicSub(n_active, 1);
+  }
+}
+
+// How local a structure is for k_pcg_cluster_res: over all slots, how many
+// have their neighbour in the same block of 2^logb cells of the system as
+// the row (cnt[0] slots, cnt[1] local ones).  seg_c0/seg_c1 are sorted.
+__global__ void k_block_locality(int n, Rows<double> R, const int* __restrict__ seg_c0,
+                                 const int* __restrict__ seg_c1, int n_seg, int logb,
+                                 unsigned long long* __restrict__ cnt) {
+  unsigned long long tot = 0, loc = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int lo = 0, hi = n_seg - 1;  // the system of row i
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (seg_c0[mid] <= i) lo = mid;
+      else hi = mid - 1;
+    }
+    const int c0 = seg_c0[lo];
+    RowIt<double> it(R, i);
+    for (int k = 0; k < it.w; ++k) {
+      const int j = R.col[it.base + k * kWarp];
+      if (j < 0) continue;
+      ++tot;
+      loc += ((j - c0) >> logb) == ((i - c0) >> logb);
+    }
+  }
+  tot = (unsigned long long)warp_sum((double)tot);
+  loc = (unsigned long long)warp_sum((double)loc);
+  if ((threadIdx.x & 31) == 0 && tot) {
+    atomicAdd(&cnt[0], tot);
+    atomicAdd(&cnt[1], loc);
+  }
+}
+
 }  // namespace sg

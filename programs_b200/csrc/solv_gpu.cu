@@ -174,7 +174,8 @@ struct solv_gpu_ctx {
   // times the value at the start of the window
   int row_chunk = sg::kRowChunk;       // FP32 products: matrix slots a thread loads per step
   int persistent = 0;                  // FP64 Jacobi PCG as one cluster-persistent launch
-  int pcg_max16 = -1;                  // clusters of 16 resident at once (-1: not asked yet)
+  std::map<const void*, int> pcg_max16;  // clusters of 16 resident at once, per kernel
+  std::map<int, double> pcg_local;       // share of slots within their own block of 2^k cells
   int fcg_stall_iters = 1000;
   double fcg_stall_drop = 0.9;
 };
@@ -438,6 +439,7 @@ int matrix_structure(solv_gpu_ctx* c, int N, int F, const int* ip, const int* in
   c->g_feat_valid = false;
   c->mg_valid = false;
   c->mg.clear();
+  c->pcg_local.clear();
   cudaStream_t st = c->stream;
   CUDA_TRY(c, c->old_of_new.ensure(N * sizeof(int)));
   CUDA_TRY(c, c->slice_ptr.ensure((ns + 1) * sizeof(int)));
@@ -1535,29 +1537,72 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
   CUDA_TRY(c, cudaGetLastError());
   int gl = 0;
   if (fused) {  // the whole loop in one launch: one cluster per system
-    // 16 blocks per cluster where all the systems' clusters fit at once,
-    // else the portable 8 (more clusters resident side by side)
-    if (c->pcg_max16 < 0) {
-      c->pcg_max16 = 0;
-      if (cudaFuncSetAttribute(sg::k_pcg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed,
-                               1) == cudaSuccess) {
-        cudaLaunchConfig_t q = {};
-        q.gridDim = dim3(sg::kPcgClusterMax);
-        q.blockDim = dim3(sg::kPcgThreads);
+    // systems of at most 16 x 2048 cells run with their vectors in the
+    // cluster's registers and shared memory (k_pcg_cluster_res), larger
+    // ones from global memory (k_pcg_cluster); 16 blocks per cluster where
+    // all the systems' clusters fit at once, else the portable 8
+    int maxn = 0;
+    for (size_t k = 0; k < c->seg_c0_caller.size(); ++k)
+      maxn = std::max(maxn, c->seg_c1_caller[k] - c->seg_c0_caller[k]);
+    using PcgKernel = void (*)(Rows<double>, const int*, const int*, const double*, double*,
+                               double*, double*, double*, Lane*, int*);
+    auto clusters16 = [&](PcgKernel kern) {
+      auto it = c->pcg_max16.find((const void*)kern);
+      if (it != c->pcg_max16.end()) return it->second;
+      int n16 = 0;
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) ==
+          cudaSuccess) {
+        cudaLaunchConfig_t qc = {};
+        qc.gridDim = dim3(sg::kPcgClusterMax);
+        qc.blockDim = dim3(sg::kPcgThreads);
         cudaLaunchAttribute qa[1];
         qa[0].id = cudaLaunchAttributeClusterDimension;
         qa[0].val.clusterDim.x = sg::kPcgClusterMax;
         qa[0].val.clusterDim.y = 1;
         qa[0].val.clusterDim.z = 1;
-        q.attrs = qa;
-        q.numAttrs = 1;
-        int n16 = 0;
-        if (cudaOccupancyMaxActiveClusters(&n16, sg::k_pcg_cluster, &q) == cudaSuccess)
-          c->pcg_max16 = n16;
+        qc.attrs = qa;
+        qc.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&n16, kern, &qc) != cudaSuccess) n16 = 0;
       }
       cudaGetLastError();  // a refused query leaves the portable size
+      c->pcg_max16[(const void*)kern] = n16;
+      return n16;
+    };
+    // the resident form reads a neighbour's p from the block that owns it:
+    // fast where most neighbours are in the reader's own block (RCM-like
+    // orders), slower than L2 where a warp's neighbours scatter over the
+    // cluster (a permuted order), so it runs only on mostly local structures
+    auto local_share = [&](int logb) -> double {
+      auto it = c->pcg_local.find(logb);
+      if (it != c->pcg_local.end()) return it->second;
+      unsigned long long h[2] = {0, 0};
+      DevBuf cnt;
+      if (cnt.ensure(2 * sizeof(unsigned long long)) != cudaSuccess) return 0.0;
+      cudaMemsetAsync(cnt.p, 0, 2 * sizeof(unsigned long long), s);
+      sg::k_block_locality<<<grid_for(c, N), c->block, 0, s>>>(
+          N, rows<double>(c), sm.seg_c0, sm.seg_c1, c->n_seg, logb,
+          cnt.as<unsigned long long>());
+      cudaMemcpyAsync(h, cnt.p, sizeof(h), cudaMemcpyDeviceToHost, s);
+      if (cudaStreamSynchronize(s) != cudaSuccess) return 0.0;
+      const double f = h[0] ? (double)h[1] / (double)h[0] : 1.0;
+      c->pcg_local[logb] = f;
+      return f;
+    };
+    PcgKernel kern = sg::k_pcg_cluster;
+    int cs = sg::kPcgCluster;
+    const PcgKernel res[2] = {sg::k_pcg_cluster_res<1>, sg::k_pcg_cluster_res<2>};
+    for (int rpt = 1; rpt <= 2 && kern == sg::k_pcg_cluster; ++rpt) {
+      const int cap = sg::kPcgThreads * rpt;
+      if (maxn > sg::kPcgClusterMax * cap || local_share(rpt == 1 ? 10 : 11) < 0.5) continue;
+      if (c->n_seg <= clusters16(res[rpt - 1]) && maxn <= sg::kPcgClusterMax * cap) {
+        kern = res[rpt - 1];
+        cs = sg::kPcgClusterMax;
+      } else if (maxn <= sg::kPcgCluster * cap) {
+        kern = res[rpt - 1];
+        cs = sg::kPcgCluster;
+      }
     }
-    const int cs = c->n_seg <= c->pcg_max16 ? sg::kPcgClusterMax : sg::kPcgCluster;
+    if (kern == sg::k_pcg_cluster && c->n_seg <= clusters16(kern)) cs = sg::kPcgClusterMax;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(c->n_seg * cs));
     cfg.blockDim = dim3(sg::kPcgThreads);
@@ -1570,7 +1615,7 @@ int solve_fp64(solv_gpu_ctx* c, int solver, int imat, double reduc, int n_iter,
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CUDA_TRY(c, cudaLaunchKernelEx(&cfg, sg::k_pcg_cluster, rows<double>(c), sm.seg_c0, sm.seg_c1,
+    CUDA_TRY(c, cudaLaunchKernelEx(&cfg, kern, rows<double>(c), sm.seg_c0, sm.seg_c1,
                                    (const double*)w.c, w.phi, w.r, w.p, w.q, c->lanes.as<Lane>(),
                                    c->n_active.as<int>()));
     c->launches++;
