@@ -142,17 +142,36 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
+// Four 8x8 BF16 matrices from shared memory into the mma fragment layout
+// (lane l gives the address of row l & 15 of matrix l >> 4's column block);
+// TRANS transposes each 8x8 matrix on the way (B stored k-major).
+template <bool TRANS>
+__device__ __forceinline__ void ldmatrix_x4(const __nv_bfloat16* p, uint32_t& r0, uint32_t& r1,
+                                            uint32_t& r2, uint32_t& r3) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  if constexpr (TRANS)
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(a));
+  else
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(a));
+}
+
 // One message-passing layer on the tensor cores.  Block = 4 warps, each
 // warp 16 cells: gather [h | agg] rows into shared memory (lane =
 // channel), then C[16x32] = A[16x64] B[64x32] with 4 k-steps x 4 n-tiles of
-// m16n8k16, then bias, relu, residual, store BF16.
+// m16n8k16, then bias, relu, residual; the BF16 result goes back into the
+// warp's shared tile and out as whole 64-byte rows.
 constexpr int TC_CELLS = 16;
 constexpr int TC_WARPS = 4;
+constexpr int TC_CHUNK = 4;  // neighbour rows loaded at once per lane
 __global__ void __launch_bounds__(TC_WARPS * 32)
 k_gnn_layer_tc(int n, sg::Rows<float> R, Feat F, const __nv_bfloat16* __restrict__ hin,
                __nv_bfloat16* __restrict__ hout, const __nv_bfloat16* __restrict__ wcat,
                const float* __restrict__ bias) {
-  __shared__ __nv_bfloat16 sB[2 * H][H + 8];
+  __shared__ __align__(16) __nv_bfloat16 sB[2 * H][H + 8];
   __shared__ __align__(16) __nv_bfloat16 sA[TC_WARPS][TC_CELLS][2 * H + 8];
   __shared__ float sbias[H];
   for (int t = threadIdx.x; t < 2 * H * H; t += blockDim.x) sB[t / H][t % H] = wcat[t];
@@ -164,8 +183,9 @@ k_gnn_layer_tc(int n, sg::Rows<float> R, Feat F, const __nv_bfloat16* __restrict
   for (int tile = blockIdx.x * TC_WARPS + w; tile < tiles; tile += gridDim.x * TC_WARPS) {
     const int c0 = tile * TC_CELLS;
     // gather: four lanes per cell row (8 channels each, one 16-byte load per
-    // row), 8 cells of the tile at a time; per channel the neighbours add up
-    // in row order, as in the training kernels
+    // row), 8 cells of the tile at a time, TC_CHUNK neighbour rows in flight
+    // per lane; per channel the neighbours add up in row order, as in the
+    // training kernels
     const int sub = lane >> 2, cb = (lane & 3) * 8;
     for (int cc0 = 0; cc0 < TC_CELLS; cc0 += 8) {
       const int cc = cc0 + sub;
@@ -177,18 +197,33 @@ k_gnn_layer_tc(int n, sg::Rows<float> R, Feat F, const __nv_bfloat16* __restrict
       if (i < n) {
         hv = *reinterpret_cast<const uint4*>(hin + (size_t)i * H + cb);
         sg::RowIt<float> it(R, i);
-        for (int k = 0; k < it.w; ++k) {
-          const int e = it.base + k * sg::kWarp;
-          const int j = R.col[e];
-          if (j >= 0) {
-            const float wgt = F.gw[e];
-            const uint4 v = *reinterpret_cast<const uint4*>(hin + (size_t)j * H + cb);
-            const __nv_bfloat162* p2 = reinterpret_cast<const __nv_bfloat162*>(&v);
+        for (int k0 = 0; k0 < it.w; k0 += TC_CHUNK) {
+          int j[TC_CHUNK];
+          float wg[TC_CHUNK];
+          uint4 v[TC_CHUNK];
+#pragma unroll
+          for (int u = 0; u < TC_CHUNK; ++u) {
+            j[u] = -1;
+            wg[u] = 0.0f;
+            if (k0 + u < it.w) {
+              const int e = it.base + (k0 + u) * sg::kWarp;
+              j[u] = __ldg(&R.col[e]);
+              wg[u] = __ldg(&F.gw[e]);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < TC_CHUNK; ++u)
+            v[u] = j[u] >= 0 ? __ldg(reinterpret_cast<const uint4*>(hin + (size_t)j[u] * H + cb))
+                             : make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+          for (int u = 0; u < TC_CHUNK; ++u) {
+            if (j[u] < 0) continue;
+            const __nv_bfloat162* p2 = reinterpret_cast<const __nv_bfloat162*>(&v[u]);
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
               const float2 f = __bfloat1622float2(p2[t]);
-              af[2 * t] += wgt * f.x;
-              af[2 * t + 1] += wgt * f.y;
+              af[2 * t] += wg[u] * f.x;
+              af[2 * t + 1] += wg[u] * f.y;
             }
           }
         }
@@ -206,33 +241,42 @@ k_gnn_layer_tc(int n, sg::Rows<float> R, Feat F, const __nv_bfloat16* __restrict
     for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
       for (int q = 0; q < 4; ++q) acc[nt][q] = 0.0f;
+    // fragments by ldmatrix: A rows (lane & 15), k block (lane >> 4) of the
+    // tile; B k rows (lane & 15) of two n tiles (lane >> 4), transposed
+    const int lr = lane & 15, lc = (lane >> 4) * 8;
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks) {
       const int k0 = ks * 16;
-      const uint32_t a0 = pack_bf16(sA[w][g][k0 + 2 * tg], sA[w][g][k0 + 2 * tg + 1]);
-      const uint32_t a1 = pack_bf16(sA[w][g + 8][k0 + 2 * tg], sA[w][g + 8][k0 + 2 * tg + 1]);
-      const uint32_t a2 = pack_bf16(sA[w][g][k0 + 2 * tg + 8], sA[w][g][k0 + 2 * tg + 9]);
-      const uint32_t a3 = pack_bf16(sA[w][g + 8][k0 + 2 * tg + 8], sA[w][g + 8][k0 + 2 * tg + 9]);
+      uint32_t a0, a1, a2, a3;
+      ldmatrix_x4<false>(&sA[w][lr][k0 + lc], a0, a1, a2, a3);
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const int n0 = nt * 8;
-        const uint32_t b0 = pack_bf16(sB[k0 + 2 * tg][n0 + g], sB[k0 + 2 * tg + 1][n0 + g]);
-        const uint32_t b1 = pack_bf16(sB[k0 + 2 * tg + 8][n0 + g], sB[k0 + 2 * tg + 9][n0 + g]);
+      for (int nt = 0; nt < 4; nt += 2) {
+        uint32_t b0, b1, b2, b3;  // (b0, b1) of tile nt, (b2, b3) of tile nt + 1
+        ldmatrix_x4<true>(&sB[k0 + lr][nt * 8 + lc], b0, b1, b2, b3);
         mma_bf16(acc[nt], a0, a1, a2, a3, b0, b1);
+        mma_bf16(acc[nt + 1], a0, a1, a2, a3, b2, b3);
       }
     }
+    __syncwarp();  // every lane has read the tile: the result may overwrite h
 #pragma unroll
     for (int nt = 0; nt < 4; ++nt) {
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const int row = g + (q >> 1) * 8, col = nt * 8 + 2 * tg + (q & 1);
-        const int i = c0 + row;
-        if (i < n) {
-          const float pre = acc[nt][q] + sbias[col];
-          const float hold = __bfloat162float(sA[w][row][col]);
-          hout[(size_t)i * H + col] = __float2bfloat16(hold + fmaxf(pre, 0.0f));
-        }
+        const float pre = acc[nt][q] + sbias[col];
+        const float hold = __bfloat162float(sA[w][row][col]);
+        sA[w][row][col] = __float2bfloat16(hold + fmaxf(pre, 0.0f));
       }
+    }
+    __syncwarp();
+    // 16 rows x 64 bytes: two 16-byte stores a lane
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const int idx = t * 32 + lane, row = idx >> 2, part = (idx & 3) * 8;
+      const int i = c0 + row;
+      if (i < n)
+        *reinterpret_cast<uint4*>(hout + (size_t)i * H + part) =
+            *reinterpret_cast<const uint4*>(&sA[w][row][part]);
     }
     __syncwarp();
   }

@@ -176,6 +176,7 @@ struct solv_gpu_ctx {
   int persistent = 0;                  // FP64 Jacobi PCG as one cluster-persistent launch
   std::map<const void*, int> pcg_max16;  // clusters of 16 resident at once, per kernel
   std::map<int, double> pcg_local;       // share of slots within their own block of 2^k cells
+  int gnn_layer_blocks = 0;              // resident blocks per SM of k_gnn_layer_tc
   int fcg_stall_iters = 1000;
   double fcg_stall_drop = 0.9;
 };
@@ -565,13 +566,21 @@ void gnn_build(solv_gpu_ctx* c, const T* r0) {
   const int N = c->N;
   gnn::Feat F = gnn_feat(c);
   const float* P = c->g_param.as<float>();
-  const int gw = gnn_grid_warps(c, (long long)N * 32);
   __nv_bfloat16* h0 = c->g_h0.as<__nv_bfloat16>();
   __nv_bfloat16* h1 = c->g_h1.as<__nv_bfloat16>();
-  gnn::k_gnn_enc<T><<<gw, 256, 0, c->stream>>>(N, F, r0, P, c->lanes.as<Lane>(), h0,
-                                                c->g_u.as<float>());
+  gnn::k_gnn_enc<T><<<gnn_grid_warps(c, (long long)N * 32), 256, 0, c->stream>>>(
+      N, F, r0, P, c->lanes.as<Lane>(), h0, c->g_u.as<float>());
   const int tiles = (N + gnn::TC_CELLS - 1) / gnn::TC_CELLS;
-  const int tcb = std::max(1, std::min((tiles + gnn::TC_WARPS - 1) / gnn::TC_WARPS, c->n_sm * 8));
+  if (c->gnn_layer_blocks <= 0) {  // resident blocks per SM of the layer kernel
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gnn::k_gnn_layer_tc,
+                                                      gnn::TC_WARPS * 32, 0) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 8;
+    c->gnn_layer_blocks = per_sm;
+  }
+  const int tcb = std::max(1, std::min((tiles + gnn::TC_WARPS - 1) / gnn::TC_WARPS,
+                                       c->n_sm * c->gnn_layer_blocks));
   __nv_bfloat16 *hin = h0, *hout = h1;
   for (int l = 0; l < gnn::NL; ++l) {
     gnn::k_gnn_layer_tc<<<tcb, gnn::TC_WARPS * 32, 0, c->stream>>>(
