@@ -71,7 +71,20 @@ extern "C" {
 #define SOLV_OPT_INNER_REDUC 2  /* inner relative drop per refinement
                                    sweep (FP32 mode), default 1e-6         */
 #define SOLV_OPT_GRAPH_ITERS 3  /* Krylov iterations per CUDA-graph launch
-                                   (0 = no graphs, plain launches)         */
+                                   (0 = no graphs, plain launches); with
+                                   SOLV_OPT_GRAPH_LOOP 1 the host checks
+                                   (reliable updates, stall windows) come
+                                   every this many iterations             */
+#define SOLV_OPT_GRAPH_LOOP 21  /* 1: the iterations run in a conditional
+                                   WHILE graph that stops on the device
+                                   once every lane has stopped (no
+                                   iterations past it, no host round trip
+                                   in between; each pass of the loop costs
+                                   about 3 us, which small systems feel);
+                                   0 (default): a graph of exactly
+                                   SOLV_OPT_GRAPH_ITERS iterations per
+                                   launch.  Where the driver has no
+                                   conditional graph nodes, 0 is used      */
 #define SOLV_OPT_BLOCK 4        /* threads per block for the cell kernels
                                    (64..256, multiple of 32)               */
 #define SOLV_OPT_GRID_PER_SM 5  /* resident blocks per SM for reductions

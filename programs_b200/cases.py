@@ -20,7 +20,8 @@ import numpy as np
 
 from .mesh import Mesh, poisson_rhs, uniform
 from .solver import (GpuSolver, OPT_GRAPH_ITERS, OPT_MG_ALPHA, OPT_MG_LEVELS, OPT_MG_OMEGA,
-                     OPT_MG_SMOOTHER, OPT_PERSISTENT, OPT_PRECISION, OPT_RELIABLE_DELTA)
+                     OPT_MG_SMOOTHER, OPT_PERSISTENT, OPT_PRECISION, OPT_RELIABLE_DELTA,
+                     OPT_GRAPH_LOOP)
 
 
 def make_system(size, system="pressure", seed=0, renumber="rcm"):
@@ -89,6 +90,8 @@ def main(argv=None):
     ap.add_argument("--alpha", type=float, default=2.0)
     ap.add_argument("--reliable-delta", type=float, default=0.1,
                     help="mixed precision: FP32 residual drop between reliable updates")
+    ap.add_argument("--graph-loop", type=int, default=0,
+                    help="1: iterations in a conditional WHILE graph; 0: graph_iters per launch")
     ap.add_argument("--persistent", type=int, default=0,
                     help="cg, imat 0, FP64: 1 runs the cluster-persistent fused PCG")
     a = ap.parse_args(argv)
@@ -103,6 +106,7 @@ def main(argv=None):
     s.set_option(OPT_MG_ALPHA, a.alpha)
     s.set_option(OPT_PERSISTENT, a.persistent)
     s.set_option(OPT_RELIABLE_DELTA, a.reliable_delta)
+    s.set_option(OPT_GRAPH_LOOP, a.graph_loop)
     out = {"case": a.what}
     if a.what == "batch":
         mats, rhs = batch_meshes(a.n_sys, a.min, a.max)

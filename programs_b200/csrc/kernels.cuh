@@ -1789,4 +1789,15 @@ __global__ void k_block_locality(int n, Rows<double> R, const int* __restrict__ 
   }
 }
 
+// Loop control of a WHILE graph of Krylov iterations: one pass per
+// iteration, on until every lane has stopped or the budget is spent.
+__global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int* __restrict__ n_active,
+                           int* __restrict__ budget) {
+  if (threadIdx.x == 0) {
+    const int b = *budget - 1;
+    *budget = b;
+    cudaGraphSetConditional(h, (b > 0 && *n_active > 0) ? 1u : 0u);
+  }
+}
+
 }  // namespace sg

@@ -137,7 +137,10 @@ struct solv_gpu_ctx {
   std::map<const void*, int> coop_blocks;  // resident blocks per SM, per sweep kernel
 
   // captured iteration graphs, keyed by (solver, imat, V, fp32)
-  std::map<std::tuple<int, int, int, int>, cudaGraphExec_t> graphs;
+  std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs;  // last: 1 = WHILE graph
+  bool cond_graphs = true;             // conditional WHILE graphs usable here
+  int graph_loop = 0;                  // SOLV_OPT_GRAPH_LOOP: 1 WHILE graphs, 0 K per launch
+  DevBuf loop_budget;                  // iterations left in the running WHILE graph
   int launches = 0;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -197,7 +200,8 @@ int set_err(solv_gpu_ctx* c, int code, const std::string& msg) {
   } while (0)
 
 void drop_graphs(solv_gpu_ctx* c) {
-  for (auto& kv : c->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto& kv : c->graphs)
+    if (kv.second) cudaGraphExecDestroy(kv.second);
   c->graphs.clear();
 }
 
@@ -1416,7 +1420,48 @@ void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
   c->launches += 5;
 }
 
-// Run Krylov iterations until every lane stops (device counter), launching
+// A WHILE graph of one Krylov iteration (body) and the loop control: a
+// launch runs iterations until every lane has stopped or the budget in
+// c->loop_budget is spent, with no host round trip in between.  Returns the
+// CUDA error of building it (conditional nodes unsupported, or a node the
+// body graph cannot hold); rc carries body()'s own status.
+template <typename Body>
+cudaError_t build_while_graph(solv_gpu_ctx* c, Body&& body, int& rc, cudaGraphExec_t& exec) {
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaGraphCreate(&g, 0);
+  if (e != cudaSuccess) return e;
+  cudaGraphConditionalHandle h;
+  e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+  if (e == cudaSuccess) {
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, nullptr, 0, &p);
+    if (e == cudaSuccess) {
+      cudaGraph_t bg = p.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(c->stream, bg, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        rc = body();
+        if (!rc)
+          sg::k_loop_ctl<<<1, 32, 0, c->stream>>>(h, c->n_active.as<int>(),
+                                                  c->loop_budget.as<int>());
+        cudaGraph_t out = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(c->stream, &out);
+        if (e == cudaSuccess) e = e2;
+      }
+      if (e == cudaSuccess && !rc) e = cudaGraphInstantiate(&exec, g, 0);
+    }
+  }
+  cudaGraphDestroy(g);
+  return e;
+}
+
+// Run Krylov iterations until every lane stops (device counter): one launch
+// of a WHILE graph where conditional nodes are available, else
 // `graph_iters` iterations per CUDA-graph launch.
 template <typename T, int V>
 int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& graph_launches) {
@@ -1428,8 +1473,35 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     return SOLV_GPU_OK;
   };
   cudaGraphExec_t exec = nullptr;
-  if (K > 0) {
-    auto key = std::make_tuple(solver, imat > 0 ? imat : 0, V, (int)std::is_same<T, float>::value);
+  bool loop = false;  // exec is a WHILE graph: one launch runs until the lanes stop
+  if (K > 0 && c->graph_loop && c->cond_graphs) {
+    auto key = std::make_tuple(solver, imat > 0 ? imat : 0, V, (int)std::is_same<T, float>::value, 1);
+    auto it = c->graphs.find(key);
+    if (it != c->graphs.end()) {
+      exec = it->second;  // null: this body cannot be a WHILE graph
+      loop = exec != nullptr;
+    } else {
+      CUDA_TRY(c, c->loop_budget.ensure(sizeof(int)));
+      int l0 = c->launches;
+      int rc = SOLV_GPU_OK;
+      cudaError_t e = build_while_graph(c, body, rc, exec);
+      c->launches = l0;
+      if (rc) return rc;
+      if (e == cudaSuccess) {
+        c->graphs[key] = exec;
+        loop = true;
+      } else {  // not as a WHILE graph: K iterations per launch instead
+        cudaGetLastError();
+        if (e == cudaErrorNotSupported || e == cudaErrorCallRequiresNewerDriver)
+          c->cond_graphs = false;  // no conditional nodes at all
+        else
+          c->graphs[key] = nullptr;  // this body only
+        exec = nullptr;
+      }
+    }
+  }
+  if (K > 0 && !loop) {
+    auto key = std::make_tuple(solver, imat > 0 ? imat : 0, V, (int)std::is_same<T, float>::value, 0);
     auto it = c->graphs.find(key);
     if (it != c->graphs.end()) {
       exec = it->second;
@@ -1465,7 +1537,16 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     c->launches = l0;
   }
   while (done < n_iter) {
-    if (exec) {
+    if (loop) {  // up to n_iter - done iterations in one launch
+      const int b = n_iter - done;
+      c->h_n_active[1] = b;
+      CUDA_TRY(c, cudaMemcpyAsync(c->loop_budget.p, &c->h_n_active[1], sizeof(int),
+                                  cudaMemcpyHostToDevice, c->stream));
+      CUDA_TRY(c, cudaGraphLaunch(exec, c->stream));
+      CUDA_TRY(c, cudaMemcpyAsync(&c->h_n_active[1], c->loop_budget.p, sizeof(int),
+                                  cudaMemcpyDeviceToHost, c->stream));
+      graph_launches++;
+    } else if (exec) {
       CUDA_TRY(c, cudaGraphLaunch(exec, c->stream));
       graph_launches++;
       c->launches += K * per_launch_kernels;
@@ -1477,6 +1558,11 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     CUDA_TRY(c, cudaGetLastError());
     CUDA_TRY(c, cudaMemcpyAsync(c->h_n_active, c->n_active.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    if (loop) {
+      const int ran = std::max(1, n_iter - done - c->h_n_active[1]);
+      c->launches += ran * (per_launch_kernels + 1);
+      done += ran;
+    }
     if (*c->h_n_active <= 0) break;
   }
   return SOLV_GPU_OK;
@@ -2246,7 +2332,7 @@ int solv_gpu_create(solv_gpu_ctx** out, int device) {
   c->dev = device;
   if (cudaSetDevice(device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMallocHost(&c->h_n_active, sizeof(int)) != cudaSuccess ||
+      cudaMallocHost(&c->h_n_active, 2 * sizeof(int)) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
     delete c;
     return SOLV_GPU_DEVICE_ERROR;
@@ -2324,6 +2410,10 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
     case SOLV_OPT_RELIABLE_DELTA:
       if (!(value > 0 && value < 1)) return set_err(c, SOLV_GPU_BAD_INPUT, "reliable delta in (0,1)");
       c->reliable_delta = value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_GRAPH_LOOP:
+      if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "graph loop is 0 or 1");
+      c->graph_loop = (int)value;
       return SOLV_GPU_OK;
     case SOLV_OPT_FCG_RELIABLE_DELTA:
       if (!(value > 0 && value < 1))

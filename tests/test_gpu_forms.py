@@ -184,3 +184,44 @@ def test_batch_rejects_coupled_systems(gpu):
     assert rc == 4
     with pytest.raises(SolverError):
         gpu._check(rc)
+
+
+@pytest.mark.parametrize("solver,imat,precision", [("cg", 0, 0), ("cg", 1, 0), ("bicg", 2, 0),
+                                                   ("cg", 0, 1), ("bicg", 2, 1)])
+def test_while_graph_equals_fixed_graphs(gpu, solver, imat, precision):
+    """SOLV_OPT_GRAPH_LOOP 1 runs the iterations in a conditional WHILE graph
+    that ends on the device once every lane has stopped; 0 launches graphs of
+    SOLV_OPT_GRAPH_ITERS iterations.  The iterations are the same kernels in
+    the same order, so the two give the same iterations and the same
+    solution, bit for bit; the FP64 solve is one WHILE launch, or one
+    launch per 8 iterations."""
+    from programs_b200.solver import OPT_GRAPH_ITERS, OPT_GRAPH_LOOP
+    m = Mesh.hex(14, seed=8)
+    m.renumber(Mesh.RCM)
+    if solver == "cg":
+        A = m.pressure(pin=1)
+        b = poisson_rhs(A.n_cell, 3)
+    else:
+        A, _ = m.momentum()
+        b = uniform(5, A.n_cell)
+    gpu.matrix_set(A)
+    out = {}
+    gpu.set_option(OPT_PRECISION, precision)
+    gpu.set_option(OPT_GRAPH_ITERS, 8)
+    try:
+        for loop in (1, 0):
+            gpu.set_option(OPT_GRAPH_LOOP, loop)
+            phi = np.zeros((A.n_cell, 1))
+            st = getattr(gpu, "solv_" + solver)(imat, 1e-10, 5000, phi,
+                                                np.asfortranarray(b.reshape(-1, 1).copy()),
+                                                np.zeros(1))
+            assert st["status"] == OK
+            out[loop] = (phi, st["iters"][0], st["graph_launches"])
+    finally:
+        gpu.set_option(OPT_GRAPH_LOOP, 0)
+        gpu.set_option(OPT_GRAPH_ITERS, 16)
+        gpu.set_option(OPT_PRECISION, 0)
+    assert out[1][1] == out[0][1]
+    assert np.array_equal(out[1][0], out[0][0])
+    if precision == 0:
+        assert out[1][2] == 1 and out[0][2] == -(-int(out[0][1]) // 8)
