@@ -539,18 +539,8 @@ __global__ void k_fill_pending(long long n, T* __restrict__ x) {
 // that makes every dependency point to an earlier (or the same) slice.  A
 // warp whose lanes wait spins for kSweepSpin polls, then sleeps briefly
 // between polls.
-#ifndef SG_SWEEP_SPIN
-#define SG_SWEEP_SPIN 64
-#endif
-#ifndef SG_SWEEP_SLEEP
-#define SG_SWEEP_SLEEP 64
-#endif
-#ifndef SG_SWEEP_PEEK
-#define SG_SWEEP_PEEK 0
-#endif
-constexpr int kSweepSpin = SG_SWEEP_SPIN;
-constexpr int kSweepSleep = SG_SWEEP_SLEEP;
-constexpr bool kSweepPeek = SG_SWEEP_PEEK != 0;
+constexpr int kSweepSpin = 64;
+constexpr int kSweepSleep = 64;  // ns
 
 template <bool UP, typename Step>
 __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ slice_w,
@@ -585,24 +575,9 @@ __device__ __forceinline__ void sweep_slices(int n, const uint8_t* __restrict__ 
 // folds a ready value in.  Returns the slot to resume from (w when the row
 // is complete).
 template <int C, int V, typename T, typename Dep, typename Coef, typename Use>
-__device__ __forceinline__ int advance(const Rows<T>& R, int base, int w, int k, bool retry,
-                                       const T* vals, Dep&& dep, Coef&& coef, Use&& use) {
+__device__ __forceinline__ int advance(const Rows<T>& R, int base, int w, int k, const T* vals,
+                                       Dep&& dep, Coef&& coef, Use&& use) {
   using A = decltype(coef(0));
-  if (kSweepPeek && retry && k < w) {
-    // a retry: poll the one slot that was pending before loading a chunk
-    const int e = base + k * kWarp;
-    const int j = __ldg(&R.col[e]);
-    if (j >= 0 && dep(j)) {
-      const A a = coef(e);
-      T xv[V];
-      bool rdy = true;
-#pragma unroll
-      for (int v = 0; v < V; ++v) rdy &= take(&vals[(size_t)j * V + v], xv[v]);
-      if (!rdy) return k;
-      use(a, xv);
-    }
-    ++k;
-  }
   while (k < w) {
     int j[C];
     A a[C];
@@ -652,7 +627,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_precond_sf(
     }
     if (imat == 1 || imat == 2) {
       k = advance<4, 1>(
-          R, base, w, k, !first, c, [&](int j) { return j < i; },
+          R, base, w, k, c, [&](int j) { return j < i; },
           [&](int e) {
             const int f = __ldg(&slot_src[e]) >> 1;
             return make_double2(__ldg(imat == 1 ? &fn[f] : &fp[f]), __ldg(&fn[f]));
@@ -707,7 +682,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_fwd_sf(
       for (int v = 0; v < V; ++v) acc[v] = bvec[(size_t)i * V + v];
     }
     k = advance<SweepChunk<T, V>::value, V>(
-        R, base, w, k, !first, t, [&](int j) { return j < i; },
+        R, base, w, k, t, [&](int j) { return j < i; },
         [&](int e) { return __ldg(&R.sval[e]); },
         [&](const T a, const T (&xv)[V]) {
 #pragma unroll
@@ -745,7 +720,7 @@ __global__ void __launch_bounds__(kSweepThreads, 4) k_bwd_sf(
       for (int v = 0; v < V; ++v) acc[v] = mul(t[(size_t)i * V + v], cr);
     }
     k = advance<SweepChunk<T, V>::value, V>(
-        R, base, w, k, !first, x, [&](int j) { return j > i; },
+        R, base, w, k, x, [&](int j) { return j > i; },
         [&](int e) { return __ldg(&R.sval[e]); },
         [&](const T a, const T (&xv)[V]) {
 #pragma unroll

@@ -298,14 +298,6 @@ int grid_resident(solv_gpu_ctx* c, long long n) {
   return (int)std::max(1LL, std::min(g, cap));
 }
 
-// Grid of the FP64 product y = A x: one thread per row.
-#ifndef SG_SPMV64_FULL
-#define SG_SPMV64_FULL 0
-#endif
-int grid_spmv64(solv_gpu_ctx* c, long long n) {
-  if (!SG_SPMV64_FULL) return grid_resident(c, n);
-  return (int)std::max(1LL, std::min((n + c->block - 1) / c->block, (long long)INT32_MAX));
-}
 
 // Run f with the FP32 products' gather width (slots loaded per step) as a
 // compile-time constant: f(std::integral_constant<int, CH>()).
@@ -1172,9 +1164,6 @@ int coop_launch(solv_gpu_ctx* c, void (*kern)(KArgs...), Args... args) {
   } else {
     CUDA_TRY(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, sg::kSweepThreads, 0));
     if (per_sm < 1) return set_err(c, SOLV_GPU_DEVICE_ERROR, "sweep kernel cannot be resident");
-#ifdef SG_SWEEP_BLOCKS
-    per_sm = std::min(per_sm, SG_SWEEP_BLOCKS);
-#endif
     c->coop_blocks[(const void*)kern] = per_sm;
   }
   const long long warps = ((long long)c->N + 31) / 32;
@@ -2633,7 +2622,7 @@ int solv_gpu_spmv_dev(solv_gpu_ctx* c, const double* x_dev, double* y_dev, int r
   if (repeat < 1) repeat = 1;
   CUDA_TRY(c, cudaEventRecord(c->ev0, s));
   for (int k = 0; k < repeat; ++k)
-    sg::k_spmv<double, 1><<<grid_spmv64(c, N), c->block, 0, s>>>(N, rows<double>(c), c->w_x.as<double>(),
+    sg::k_spmv<double, 1><<<grid_resident(c, N), c->block, 0, s>>>(N, rows<double>(c), c->w_x.as<double>(),
                                                                 c->w_b.as<double>());
   CUDA_TRY(c, cudaEventRecord(c->ev1, s));
   sg::k_phi_out<double><<<grid_for(c, N), c->block, 0, s>>>(N, 1, o2n, c->w_b.as<double>(), y_dev);
@@ -2666,10 +2655,10 @@ int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_l
     WS<double> w;
     if ((rc = ensure_ws<double>(c, 1, w))) return rc;
     CUDA_TRY(c, cudaMemsetAsync(w.p, 0, N * sizeof(double), s));
-    sg::k_spmv<double, 1><<<grid_spmv64(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
+    sg::k_spmv<double, 1><<<grid_resident(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
     CUDA_TRY(c, cudaEventRecord(c->ev0, s));
     for (int k = 0; k < repeat; ++k)
-      sg::k_spmv<double, 1><<<grid_spmv64(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
+      sg::k_spmv<double, 1><<<grid_resident(c, N), c->block, 0, s>>>(N, rows<double>(c), w.p, w.q);
     CUDA_TRY(c, cudaEventRecord(c->ev1, s));
   } else {
     WS<float> f;
