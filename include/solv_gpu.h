@@ -52,6 +52,9 @@ extern "C" {
 #define SOLV_GPU_NAN 3          /* NaN / Inf seen in a reduction           */
 #define SOLV_GPU_BAD_INPUT 4    /* index out of range, sizes, null, ...    */
 #define SOLV_GPU_DEVICE_ERROR 5 /* CUDA error (message: solv_gpu_last_error) */
+#define SOLV_GPU_TIMEOUT 6      /* a bounded device wait ran out (a DIC/DILU
+                                   recurrence's neighbour never arrived);
+                                   the context stays usable                 */
 #define SOLV_GPU_NO_MATRIX 7    /* no solv_gpu_matrix_set yet              */
 #define SOLV_GPU_ZERO_RHS 8     /* maxval(res0_n) < small: the solve ends
                                    at once as solv_cg.f90:21 does; reported

@@ -1194,7 +1194,7 @@ int sweep_check(solv_gpu_ctx* c) {
   if (!h.err) return SOLV_GPU_OK;
   CUDA_TRY(c, cudaMemsetAsync(c->sweep_ctl.p, 0, sizeof(sg::SweepCtl), c->stream));
   c->t_ready = c->tf_ready = false;
-  return set_err(c, SOLV_GPU_DEVICE_ERROR, "triangular sweep: a wait for a neighbour ran out");
+  return set_err(c, SOLV_GPU_TIMEOUT, "triangular sweep: a wait for a neighbour ran out");
 }
 
 // solv_precond: c, c_r in internal order (FP64).  DIC / DILU is one
@@ -2305,6 +2305,7 @@ const char* solv_gpu_status_string(int s) {
     case SOLV_GPU_NO_MATRIX: return "no matrix set";
     case SOLV_GPU_ZERO_RHS: return "zero initial residual (early return)";
     case SOLV_GPU_TOO_LARGE: return "problem larger than the fixed scratch";
+    case SOLV_GPU_TIMEOUT: return "a bounded device wait ran out";
     default: return "unknown status";
   }
 }

@@ -26,6 +26,7 @@ import numpy as np
 from ._lib import load
 
 OK, MAXITER, NAN, BAD_INPUT, DEVICE_ERROR, NO_MATRIX, ZERO_RHS = 0, 1, 3, 4, 5, 7, 8
+TIMEOUT = 6
 MAX_VC = 4
 OPT_PRECISION, OPT_INNER_REDUC, OPT_GRAPH_ITERS, OPT_BLOCK, OPT_GRID_PER_SM, OPT_MAX_REFINE = (
     1, 2, 3, 4, 5, 6)
