@@ -237,6 +237,12 @@ int solv_gpu_spmv_dev(solv_gpu_ctx *ctx, const double *x_dev, double *y_dev,
 int solv_gpu_kernel_time(solv_gpu_ctx *ctx, int which, int repeat,
                          float *ms_per_launch);
 
+/* Diagnostic (no counterpart in the reference): one DIC/DILU-style bounded
+ * wait on a value that nothing writes, through the sweeps' own wait driver.
+ * Returns SOLV_GPU_TIMEOUT after about a second when the bound works; the
+ * context stays usable. */
+int solv_gpu_selftest_sweep_wait(solv_gpu_ctx *ctx);
+
 /* -- learned preconditioner ---------------------------------------------- */
 /* No counterpart in the reference.  Flexible CG, FCG(1), in FP32 with
  * FP64 reliable updates.  A 3-layer, width-32 message-passing network over

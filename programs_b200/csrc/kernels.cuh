@@ -1775,4 +1775,16 @@ __global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int* __restrict__
   }
 }
 
+// Self-test of the recurrences' bounded wait: one slice whose only cell
+// waits on a value nothing ever writes, through the same driver
+// (sweep_slices) as the sweeps, so the wait runs out after kSweepPolls
+// polls and sets ctl->err.  slice_w holds {1}; never is pending.
+__global__ void k_sweep_selftest(const uint8_t* __restrict__ slice_w, const double* never,
+                                 SweepCtl* ctl) {
+  sweep_slices<false>(1, slice_w, ctl, [&](int i, int k, bool first) -> int {
+    double v;
+    return i == 0 && take(never, v) ? 1 : (i == 0 ? 0 : 1);
+  });
+}
+
 }  // namespace sg

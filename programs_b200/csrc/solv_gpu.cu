@@ -2642,6 +2642,24 @@ int solv_gpu_spmv_dev(solv_gpu_ctx* c, const double* x_dev, double* y_dev, int r
 // which 0 = FP64 matrix product, 1 = FP32 matrix product, 2 = the learned
 // preconditioner's application (FP32; needs parameters, builds M^-1 from a
 // constant residual first).
+int solv_gpu_selftest_sweep_wait(solv_gpu_ctx* c) {
+  if (!c) return SOLV_GPU_BAD_INPUT;
+  CUDA_TRY(c, cudaSetDevice(c->dev));
+  DevBuf w, v;
+  CUDA_TRY(c, w.ensure(16));
+  CUDA_TRY(c, v.ensure(sizeof(double)));
+  if (!c->sweep_ctl.p) {
+    CUDA_TRY(c, c->sweep_ctl.ensure(sizeof(sg::SweepCtl)));
+    CUDA_TRY(c, cudaMemsetAsync(c->sweep_ctl.p, 0, sizeof(sg::SweepCtl), c->stream));
+  }
+  const uint8_t one = 1;
+  CUDA_TRY(c, cudaMemcpyAsync(w.p, &one, 1, cudaMemcpyHostToDevice, c->stream));
+  sg::k_fill_pending<double><<<1, 32, 0, c->stream>>>(1, v.as<double>());
+  sg::k_sweep_selftest<<<1, 32, 0, c->stream>>>(w.as<uint8_t>(), v.as<double>(), sweep_ctl(c));
+  CUDA_TRY(c, cudaGetLastError());
+  return sweep_check(c);  // synchronises; SOLV_GPU_TIMEOUT when the wait ran out
+}
+
 int solv_gpu_kernel_time(solv_gpu_ctx* c, int which, int repeat, float* ms_per_launch) {
   if (!c) return SOLV_GPU_BAD_INPUT;
   if (!c->has_matrix) return set_err(c, SOLV_GPU_NO_MATRIX, "no matrix set");

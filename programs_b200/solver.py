@@ -75,7 +75,8 @@ EXPORTS = [
     "solv_gpu_fcg", "solv_gpu_fcg_dev", "solv_gpu_gnn_n_params", "solv_gpu_gnn_set_params",
     "solv_gpu_gnn_get_params", "solv_gpu_gnn_forward_dev", "solv_gpu_gnn_grad_dev",
     "solv_gpu_gnn_get_grad", "solv_gpu_gnn_zero_grad", "solv_gpu_gnn_adam",
-    "solv_gpu_kernel_time", "solv_gpu_mg_aggregates", "solv_gpu_mg_aggregate",
+    "solv_gpu_kernel_time", "solv_gpu_selftest_sweep_wait", "solv_gpu_mg_aggregates",
+    "solv_gpu_mg_aggregate",
     "solv_gpu_create_", "solv_gpu_destroy_", "solv_gpu_matrix_set_", "solv_gpu_matrix_values_",
     "solv_gpu_res_", "solv_gpu_precond_", "solv_gpu_direct_", "solv_gpu_cg_", "solv_gpu_bicg_",
 ]
@@ -128,6 +129,7 @@ def lib():
     L.solv_gpu_gnn_grad_dev.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                         ctypes.c_int]
     L.solv_gpu_gnn_adam.argtypes = [vp, ctypes.c_float, ctypes.c_float]
+    L.solv_gpu_selftest_sweep_wait.argtypes = [vp]
     L.solv_gpu_kernel_time.argtypes = [vp, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_float)]
     L.solv_gpu_mg_aggregates.argtypes = [vp, ctypes.c_int, _i32p, ctypes.c_int, _i32p]
@@ -433,6 +435,11 @@ class GpuSolver:
         d.update(res0_n=rn.reshape(-1, n_vc), iters_all=iters.reshape(-1, n_vc),
                  ratio_all=ratio.reshape(-1, n_vc))
         return d
+
+    def selftest_sweep_wait(self) -> int:
+        """Status of one bounded sweep wait on a value nothing writes
+        (solv_gpu_selftest_sweep_wait): TIMEOUT when the bound works."""
+        return int(self._lib.solv_gpu_selftest_sweep_wait(self._h))
 
     def kernel_time(self, which: int, repeat: int = 20) -> float:
         """ms per launch (solv_gpu_kernel_time): 0 FP64 SpMV, 1 FP32 SpMV, 2 the
