@@ -141,7 +141,7 @@ extern "C" {
 #define SOLV_OPT_FCG_RELIABLE_DELTA 20 /* the learned flexible CG (FP32
                                    inner iterations): the drop of the FP32
                                    residual at which a lane stops for a
-                                   reliable update (default 1e-3; CG lanes
+                                   reliable update (default 0.1; CG lanes
                                    use SOLV_OPT_RELIABLE_DELTA)            */
 #define SOLV_OPT_MG_BUILD 17    /* where the aggregation hierarchy is built:
                                    0 on the GPU (default: handshake

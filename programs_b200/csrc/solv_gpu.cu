@@ -103,7 +103,7 @@ struct solv_gpu_ctx {
   int max_refine = 30;
   int inner_max_iter = 2000;
   double reliable_delta = 0.1;
-  double fcg_reliable_delta = 1e-3;  // the learned flexible CG's reliable-update drop
+  double fcg_reliable_delta = 0.1;  // the learned flexible CG's reliable-update drop
   int gnn_loss = 1;  // training loss: 0 energy, 1 scale-free (best-step energy)
 
   // matrix (caller sizes)

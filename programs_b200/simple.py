@@ -27,7 +27,7 @@ import numpy as np
 
 from .mesh import (Mesh, face_flux, gradient, gradient_sweeps, mass_imbalance,
                    momentum_deferred, momentum_field, pressure_correction, simple_correct)
-from .solver import GpuSolver, OPT_PRECISION
+from .solver import GpuSolver, OPT_FCG_RELIABLE_DELTA, OPT_PRECISION
 
 
 def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15, seed=0,
@@ -143,7 +143,7 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
 def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15,
                seed=0, p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None,
                p_imat=1, m_precision=0, device=0, log_every=0, reference_weights=False,
-               reference_terms=False, renumber="rcm", p_scale=False):
+               reference_terms=False, renumber="rcm", p_scale=False, fcg_delta=None):
     """The same outer loop with everything on the GPU: assembly, gradients
     (the corrected sweeps too), the explicit momentum terms, fluxes and
     corrections by the fv_gpu kernels (bit-for-bit the host functions),
@@ -179,6 +179,8 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
     for s_ in (sm, sp):
         s_.set_stream(stream.cuda_stream)
     sm.set_option(OPT_PRECISION, m_precision)
+    if fcg_delta is not None:
+        sp.set_option(OPT_FCG_RELIABLE_DELTA, fcg_delta)
     if learned is not None:
         sp.gnn_set_params(learned)
     # the structure once (values come from the device each iteration)
@@ -302,6 +304,9 @@ def main(argv=None):
                          "FP64 refinement, 0 FP64")
     ap.add_argument("--reference-weights", action="store_true",
                     help="the reference's face distance and interpolation weight")
+    ap.add_argument("--fcg-delta", type=float, default=None,
+                    help="device loop, learned run: the flexible CG's reliable-update drop "
+                         "(SOLV_OPT_FCG_RELIABLE_DELTA; default the library's)")
     a = ap.parse_args(argv)
     loop = run_device if a.device_assembly else run
     kw = dict(p_reduc=a.p_reduc, p_iter=a.p_iter, p_imat=a.p_imat, m_reduc=a.m_reduc,
@@ -311,6 +316,8 @@ def main(argv=None):
         kw["reference_terms"] = True
     if a.device_assembly:
         kw["renumber"] = a.renumber
+        if a.fcg_delta is not None:
+            kw["fcg_delta"] = a.fcg_delta
     u0, p0, h0, t0 = loop(a.size, a.outer, a.re, **kw)
     out = {"size": a.size, "outer": a.outer, "re": a.re, "p_reduc": a.p_reduc,
            "p_imat": a.p_imat, "reference_terms": a.reference_terms, "p_scale": a.p_scale,

@@ -282,7 +282,7 @@ def test_reliable_updates_do_not_depend_on_the_graph_length(gpu, delta):
             out[k] = (phi, st["iters"][0], st["refinements"])
     finally:
         gpu.set_option(OPT_GRAPH_ITERS, 16)
-        gpu.set_option(OPT_FCG_RELIABLE_DELTA, 1e-3)
+        gpu.set_option(OPT_FCG_RELIABLE_DELTA, 0.1)
     assert out[4][1:] == out[32][1:]
     assert np.array_equal(out[4][0], out[32][0])
 
