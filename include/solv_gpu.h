@@ -138,6 +138,11 @@ extern "C" {
                                    Krylov, flexible CG, V-cycle): matrix
                                    slots each thread loads before it sums
                                    them, 2, 4 (default) or 8              */
+#define SOLV_OPT_FCG_FALLBACK 22 /* the PCG a stalled learned solve hands
+                                   over to: 0 (default) Jacobi, 1 DIC, 2
+                                   DILU (the reference's pressure solver is
+                                   DIC-PCG, cfd_setup.f90:662); the
+                                   factorisation is made at the hand-over  */
 #define SOLV_OPT_FCG_RELIABLE_DELTA 20 /* the learned flexible CG (FP32
                                    inner iterations): the drop of the FP32
                                    residual at which a lane stops for a

@@ -104,6 +104,7 @@ struct solv_gpu_ctx {
   int inner_max_iter = 2000;
   double reliable_delta = 0.1;
   double fcg_reliable_delta = 0.1;  // the learned flexible CG's reliable-update drop
+  int fcg_fallback_imat = 0;         // the PCG a stalled learned solve hands over to
   int gnn_loss = 1;  // training loss: 0 energy, 1 scale-free (best-step energy)
 
   // matrix (caller sizes)
@@ -2056,9 +2057,25 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
   // value at the start of that window -- or when the FP64 residual stops
   // improving across reliable updates.
   int cur = solver;
+  int imat_cur = imat;  // the hand-over may bring in the DIC/DILU factorisation
   // the residual drop between reliable updates: the learned FCG's own, or
   // (after a hand-over, and for CG) the CG one
   auto delta_of = [&]() { return cur == 2 ? c->fcg_reliable_delta : c->reliable_delta; };
+  // after a hand-over: restart the direction (it may hold NaN) and, when
+  // asked for, factorise for the reference's DIC/DILU-PCG
+  auto restart_fallback = [&]() -> int {
+    CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
+    CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
+    if (imat_cur <= 0 && c->fcg_fallback_imat > 0) {
+      int r = launch_precond(c, c->fcg_fallback_imat, w.c, w.cr);
+      if (r) return r;
+      sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.c, f.c);
+      sg::k_convert<double, float><<<grid_for(c, N), c->block, 0, s>>>(N, w.cr, f.cr);
+      c->launches += 2;
+      imat_cur = c->fcg_fallback_imat;
+    }
+    return SOLV_GPU_OK;
+  };
   c->fallbacks = 0;
   std::vector<int> win_iter(nl, 0);
   std::vector<double> win_l1(l1_last);
@@ -2072,7 +2089,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
   const int K = std::max(1, c->graph_iters);
   while (na > 0) {
     int gl = 0;
-    if ((rc = iterate<float, V>(c, cur, imat, K, f, gl))) return rc;  // K iterations at most
+    if ((rc = iterate<float, V>(c, cur, imat_cur, K, f, gl))) return rc;  // K iterations at most
     gl_total += gl;
     launched += K;
     CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->lanes.p, nl * sizeof(Lane), cudaMemcpyDeviceToHost, s));
@@ -2094,10 +2111,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
         need = trig[l] = 1;
       }
     }
-    if (fell_back) {  // restart the search direction (it may hold NaN)
-      CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
-      CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
-    }
+    if (fell_back && (rc = restart_fallback())) return rc;
     if (!need && launched <= n_iter + K) continue;
     // reliable update of every lane still in play
     for (int l = 0; l < nl; ++l) mask[l] = !final_[l];
@@ -2150,10 +2164,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
       win_l1[l] = l1[l];
       na += L.active;
     }
-    if (fell_back) {
-      CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
-      CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
-    }
+    if (fell_back && (rc = restart_fallback())) return rc;
     CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
     CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
     if (na == 0) break;
@@ -2164,13 +2175,15 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     // sweep-preconditioned CG take beta
     // from the current z already; alpha always comes from p.r of the next
     // step.
-    if (cur == 0 && imat <= 0) {
+    if (cur == 0 && imat_cur <= 0) {
       sg::k_cg_rz<float, V, true, true><<<G, B, 0, s>>>(sm, f.c, f.r, f.z, c->part.as<double>(),
                                                         c->lanes.as<Lane>(), f.q);
       c->launches++;
     }
     CUDA_TRY(c, cudaGetLastError());
   }
+  // the caller's check of the sweeps' waits covers its own imat only
+  if (imat_cur > 0 && imat <= 0 && (rc = sweep_check(c))) return rc;
   if (not_r0) {
     sg::k_add<<<grid_for(c, NV), c->block, 0, s>>>(NV, w.phi, w.v);
     c->launches++;
@@ -2404,6 +2417,11 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
     case SOLV_OPT_GRAPH_LOOP:
       if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "graph loop is 0 or 1");
       c->graph_loop = (int)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_FCG_FALLBACK:
+      if (value != 0 && value != 1 && value != 2)
+        return set_err(c, SOLV_GPU_BAD_INPUT, "fallback preconditioner is 0, 1 or 2");
+      c->fcg_fallback_imat = (int)value;
       return SOLV_GPU_OK;
     case SOLV_OPT_FCG_RELIABLE_DELTA:
       if (!(value > 0 && value < 1))

@@ -27,7 +27,7 @@ import numpy as np
 
 from .mesh import (Mesh, face_flux, gradient, gradient_sweeps, mass_imbalance,
                    momentum_deferred, momentum_field, pressure_correction, simple_correct)
-from .solver import GpuSolver, OPT_FCG_RELIABLE_DELTA, OPT_PRECISION
+from .solver import GpuSolver, OPT_FCG_FALLBACK, OPT_FCG_RELIABLE_DELTA, OPT_PRECISION
 
 
 def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15, seed=0,
@@ -183,6 +183,8 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
         sp.set_option(OPT_FCG_RELIABLE_DELTA, fcg_delta)
     if learned is not None:
         sp.gnn_set_params(learned)
+        # a stalled learned solve hands over to the plain run's own PCG
+        sp.set_option(OPT_FCG_FALLBACK, max(0, min(int(p_imat), 2)))
     # the structure once (values come from the device each iteration)
     F_ = ip.shape[0]
     shell = FaceMatrix(N, ip, inb, np.zeros(F_), np.zeros(F_), np.ones(N))

@@ -34,6 +34,7 @@ OPT_INNER_MAX_ITER, OPT_RELIABLE_DELTA, OPT_GNN_LOSS = 7, 8, 9
 OPT_MG_LEVELS, OPT_MG_SMOOTHER, OPT_MG_OMEGA, OPT_MG_ALPHA = 10, 11, 12, 13
 OPT_FCG_STALL_ITERS, OPT_FCG_STALL_DROP, OPT_MG_SCALE_MIN, OPT_MG_BUILD = 14, 15, 16, 17
 OPT_VECTOR_WIDTH, OPT_PERSISTENT, OPT_FCG_RELIABLE_DELTA, OPT_GRAPH_LOOP = 18, 19, 20, 21
+OPT_FCG_FALLBACK = 22
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f64p = ctypes.POINTER(ctypes.c_double)

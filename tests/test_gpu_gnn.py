@@ -25,7 +25,7 @@ from oracle import gnn_ref
 from oracle.oracle import Oracle
 from programs_b200 import learn
 from programs_b200.mesh import Mesh, cavity_field, momentum_field, pressure_correction, uniform
-from programs_b200.solver import (OK, OPT_FCG_RELIABLE_DELTA, OPT_FCG_STALL_DROP,
+from programs_b200.solver import (OK, OPT_FCG_FALLBACK, OPT_FCG_RELIABLE_DELTA, OPT_FCG_STALL_DROP,
                                   OPT_FCG_STALL_ITERS, OPT_GRAPH_ITERS, OPT_MG_LEVELS,
                                   OPT_MG_SCALE_MIN, OPT_MG_SMOOTHER, OPT_PRECISION)
 
@@ -393,6 +393,35 @@ def test_starved_smoother_stalls_and_hands_over_to_pcg(gpu):
     phi, st, rn = _solve_fcg(gpu, A, b)
     assert st["status"] == OK and st["fallbacks"] == 0, st
     assert _rel(phi, x_ref) <= AGREE_1E10
+
+
+@pytest.mark.parametrize("fallback", [1, 2])
+def test_stalled_learned_solve_hands_over_to_dic_pcg(gpu, fallback):
+    """SOLV_OPT_FCG_FALLBACK 1 / 2: the starved network's stall hands over to
+    the reference's own DIC (DILU) PCG, factorised at the hand-over, which
+    converges to the oracle's solution in fewer iterations than the
+    Jacobi hand-over."""
+    A = _system(16, seed=9)
+    gpu.matrix_set(A)
+    p = learn.init_params(0)
+    p[learn.P_BA] = -30.0
+    gpu.gnn_set_params(p)
+    b = _rhs(A, 13)
+    x_ref, _ = _ref_iters(A, b)
+    its = {}
+    gpu.set_option(OPT_MG_SCALE_MIN, 0.0)
+    try:
+        for fb in (0, fallback):
+            gpu.set_option(OPT_FCG_FALLBACK, fb)
+            phi, st, rn = _solve_fcg(gpu, A, b)
+            assert st["status"] == OK and st["fallbacks"] == 1, st
+            assert np.abs(b - A.to_scipy() @ phi[:, 0]).sum() / rn[0] < 1e-10
+            assert _rel(phi, x_ref) <= AGREE_1E10
+            its[fb] = st["iters"][0]
+    finally:
+        gpu.set_option(OPT_MG_SCALE_MIN, 0.5)
+        gpu.set_option(OPT_FCG_FALLBACK, 0)
+    assert its[fallback] < its[0], its
 
 
 def test_stall_window_hands_over_once(gpu):
