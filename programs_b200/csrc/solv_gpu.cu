@@ -2896,6 +2896,17 @@ int solv_gpu_autotune(solv_gpu_ctx* c, int solver, int imat, int n_vc, solv_gpu_
     return SOLV_GPU_OK;
   };
   const bool fp32 = c->precision == 1 || solver == 2;
+  // the measured iterations are all real work: no lane stops early for a
+  // reliable update (it would leave the rest of a graph as early exits)
+  struct DeltaKeep {  // restored on every way out
+    solv_gpu_ctx* c;
+    double d, fd;
+    ~DeltaKeep() {
+      c->reliable_delta = d;
+      c->fcg_reliable_delta = fd;
+    }
+  } delta_keep{c, c->reliable_delta, c->fcg_reliable_delta};
+  c->reliable_delta = c->fcg_reliable_delta = 1e-300;
   const int blocks[] = {128, 256};
   const int gps[] = {4, 8, 16};
   const int graphs[] = {8, 32};
