@@ -84,10 +84,14 @@ extern "C" {
                                    iterations past it, no host round trip
                                    in between; each pass of the loop costs
                                    about 3 us, which small systems feel);
-                                   0 (default): a graph of exactly
+                                   0: a graph of exactly
                                    SOLV_OPT_GRAPH_ITERS iterations per
-                                   launch.  Where the driver has no
-                                   conditional graph nodes, 0 is used      */
+                                   launch; 2 (default): WHILE graphs for
+                                   the learned flexible CG, whose lanes
+                                   stop inside a graph for each reliable
+                                   update, fixed ones for CG and BiCGSTAB.
+                                   Where the driver has no conditional
+                                   graph nodes, 0 is used                  */
 #define SOLV_OPT_BLOCK 4        /* threads per block for the cell kernels
                                    (64..256, multiple of 32)               */
 #define SOLV_OPT_GRID_PER_SM 5  /* resident blocks per SM for reductions

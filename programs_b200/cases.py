@@ -92,8 +92,9 @@ def main(argv=None):
                     help="mixed precision: FP32 residual drop between reliable updates")
     ap.add_argument("--fcg-delta", type=float, default=None,
                     help="fcg: FP32 residual drop at which a lane stops for a reliable update")
-    ap.add_argument("--graph-loop", type=int, default=0,
-                    help="1: iterations in a conditional WHILE graph; 0: graph_iters per launch")
+    ap.add_argument("--graph-loop", type=int, default=2,
+                    help="1: iterations in a conditional WHILE graph; 0: graph_iters per launch; "
+                         "2: WHILE for fcg only")
     ap.add_argument("--persistent", type=int, default=0,
                     help="cg, imat 0, FP64: 1 runs the cluster-persistent fused PCG")
     a = ap.parse_args(argv)

@@ -140,7 +140,8 @@ struct solv_gpu_ctx {
   // captured iteration graphs, keyed by (solver, imat, V, fp32)
   std::map<std::tuple<int, int, int, int, int>, cudaGraphExec_t> graphs;  // last: 1 = WHILE graph
   bool cond_graphs = true;             // conditional WHILE graphs usable here
-  int graph_loop = 0;                  // SOLV_OPT_GRAPH_LOOP: 1 WHILE graphs, 0 K per launch
+  int graph_loop = 2;                  // SOLV_OPT_GRAPH_LOOP: 1 WHILE graphs, 0 K per launch,
+                                       // 2 WHILE for the learned FCG only
   DevBuf loop_budget;                  // iterations left in the running WHILE graph
   int launches = 0;
 
@@ -1464,7 +1465,10 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
   };
   cudaGraphExec_t exec = nullptr;
   bool loop = false;  // exec is a WHILE graph: one launch runs until the lanes stop
-  if (K > 0 && c->graph_loop && c->cond_graphs) {
+  // WHILE graphs where lanes stop inside a graph for reliable updates (the
+  // learned FCG), fixed ones elsewhere (a WHILE pass costs ~3 us)
+  const bool want_loop = c->graph_loop == 1 || (c->graph_loop == 2 && solver == 2);
+  if (K > 0 && want_loop && c->cond_graphs) {
     auto key = std::make_tuple(solver, imat > 0 ? imat : 0, V, (int)std::is_same<T, float>::value, 1);
     auto it = c->graphs.find(key);
     if (it != c->graphs.end()) {
@@ -2415,7 +2419,8 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
       c->reliable_delta = value;
       return SOLV_GPU_OK;
     case SOLV_OPT_GRAPH_LOOP:
-      if (value != 0 && value != 1) return set_err(c, SOLV_GPU_BAD_INPUT, "graph loop is 0 or 1");
+      if (value != 0 && value != 1 && value != 2)
+        return set_err(c, SOLV_GPU_BAD_INPUT, "graph loop is 0, 1 or 2");
       c->graph_loop = (int)value;
       return SOLV_GPU_OK;
     case SOLV_OPT_FCG_FALLBACK:

@@ -218,7 +218,7 @@ def test_while_graph_equals_fixed_graphs(gpu, solver, imat, precision):
             assert st["status"] == OK
             out[loop] = (phi, st["iters"][0], st["graph_launches"])
     finally:
-        gpu.set_option(OPT_GRAPH_LOOP, 0)
+        gpu.set_option(OPT_GRAPH_LOOP, 2)
         gpu.set_option(OPT_GRAPH_ITERS, 16)
         gpu.set_option(OPT_PRECISION, 0)
     assert out[1][1] == out[0][1]
