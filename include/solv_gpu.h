@@ -90,7 +90,7 @@ extern "C" {
                                    the learned flexible CG, whose lanes
                                    stop inside a graph for each reliable
                                    update, fixed ones for CG and BiCGSTAB.
-                                   Where the driver has no conditional
+                                   Where the CUDA driver has no conditional
                                    graph nodes, 0 is used                  */
 #define SOLV_OPT_BLOCK 4        /* threads per block for the cell kernels
                                    (64..256, multiple of 32)               */
