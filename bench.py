@@ -232,6 +232,17 @@ def _oracle_iteration_s(o, b, n):
     return (time.perf_counter() - t) / n
 
 
+def oracle_cost(o, b, n_long, n_short=1):
+    """(seconds per PCG iteration, fixed seconds per call) of the oracle on
+    this system, from one call of n_short and one of n_long iterations: the
+    difference removes what every call pays once (the initial residual, the
+    preconditioner, the work arrays' first touch)."""
+    t1 = _oracle_iteration_s(o, b, n_short) * n_short
+    t2 = _oracle_iteration_s(o, b, n_long) * n_long
+    per = max(t2 - t1, 0.0) / max(n_long - n_short, 1)
+    return per, max(t1 - n_short * per, 0.0)
+
+
 def oracle_iterations(A, b, size):
     """The oracle's iteration count for this system: recorded for the large
     sizes, solved in full here otherwise."""
@@ -245,32 +256,36 @@ def oracle_iterations(A, b, size):
 
 
 def extrapolation_check(sizes=(32, 64), sample=20):
-    """Full oracle solves against the per-iteration extrapolation the CPU
-    baseline uses, at sizes the oracle finishes in seconds."""
+    """Full oracle solves against the extrapolation the CPU baseline uses
+    (fixed cost + seconds per iteration x iterations), at sizes the oracle
+    finishes in seconds."""
     from oracle.oracle import Oracle
     out = {}
     for n in sizes:
         A, b = build_system(n)
         o = Oracle.from_matrix(A)
-        per = _oracle_iteration_s(o, b, min(sample, 50))
+        per, fixed = oracle_cost(o, b, min(sample, 50))
         t = time.perf_counter()
         r = o.solv_cg(0, 1e-10, 100000, np.zeros((A.n_cell, 1)), b.reshape(-1, 1))
         full = time.perf_counter() - t
         it = int(r[3][0])
+        est = fixed + per * it
         out[f"{n}^3"] = {"iterations": it, "full_solve_s": full,
-                         "extrapolated_s": per * it, "extrapolated_over_full": per * it / full}
+                         "extrapolated_s": est, "extrapolated_over_full": est / full}
     return out
 
 
 def cpu_oracle_sample(A, b, budget_s, repeats=1):
-    """Seconds per oracle PCG iteration (single core: the reference is
-    serial) over `repeats` samples of about budget_s seconds each; returns
-    (seconds per iteration of each sample, iterations per sample)."""
+    """The oracle's cost on this system (single core: the reference is
+    serial): `repeats` samples of about budget_s seconds, each a short and a
+    long call; returns ([seconds per iteration], [fixed seconds per call],
+    iterations of the long call)."""
     from oracle.oracle import Oracle
     o = Oracle.from_matrix(A)
-    per = _oracle_iteration_s(o, b, 2)
-    s = max(2, min(400, int(budget_s / max(per, 1e-6))))
-    return [_oracle_iteration_s(o, b, s) for _ in range(repeats)], s
+    per0, _ = oracle_cost(o, b, 3)
+    s = max(4, min(400, int(budget_s / max(per0, 1e-6))))
+    out = [oracle_cost(o, b, s) for _ in range(repeats)]
+    return [p for p, _ in out], [f for _, f in out], s
 
 
 def _config(args, A):
@@ -288,19 +303,22 @@ def run_reference(args, rank):
     iters, iters_src = oracle_iterations(A, b, args.size)
     from oracle.oracle import Oracle
     o = Oracle.from_matrix(A)
-    per0 = _oracle_iteration_s(o, b, 2)
-    sample = max(2, min(400, int(STEP_SAMPLE_S / max(per0, 1e-6))))
+    per0, _ = oracle_cost(o, b, 3)
+    sample = max(4, min(400, int(STEP_SAMPLE_S / max(per0, 1e-6))))
     for _ in range(args.warmup):
         _oracle_iteration_s(o, b, 1)
-    per, step_s = [], []
+    per, fixed, step_s = [], [], []
     for _ in range(args.steps):
         t = time.perf_counter()
-        per.append(_oracle_iteration_s(o, b, sample))
+        p_, f_ = oracle_cost(o, b, sample)
+        per.append(p_)
+        fixed.append(f_)
         step_s.append(time.perf_counter() - t)
-    v = statistics.mean(per) * iters
+    v = statistics.mean(fixed) + statistics.mean(per) * iters
     check = extrapolation_check()
-    desc = (f"EXTRAPOLATED: each step times {sample} oracle PCG iterations of the {args.size}^3 "
-            f"system (single core; the reference is serial); value = mean seconds per iteration "
+    desc = (f"EXTRAPOLATED: each step times one 1-iteration and one {sample}-iteration oracle "
+            f"PCG call on the {args.size}^3 system (single core; the reference is serial); "
+            f"value = the fixed cost of a call + mean seconds per iteration (their difference) "
             f"x the oracle's own {iters}-iteration full solve ({iters_src}); ms_per_step is the "
             f"time each step actually took")
     print(json.dumps({
@@ -597,12 +615,13 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         iters_o, src = oracle_iterations(A, b, args.size)
-        per, sample = cpu_oracle_sample(A, b, 5.0, repeats=3)
-        cpu = {"value": statistics.median(per) * iters_o, "unit": "s/solve", "cores": 1,
-               "kind": "port",
-               "sample": f"EXTRAPOLATED: median of 3 runs of {sample} oracle PCG iterations of this "
-                         f"system (single core), x the oracle's own {iters_o}-iteration full "
-                         f"solve ({src})",
+        per, fixed, sample = cpu_oracle_sample(A, b, 5.0, repeats=3)
+        cpu = {"value": statistics.median(fixed) + statistics.median(per) * iters_o,
+               "unit": "s/solve", "cores": 1, "kind": "port",
+               "sample": f"EXTRAPOLATED: 3 samples of a 1- and a {sample}-iteration oracle PCG "
+                         f"call on this system (single core); the fixed cost of a call + the "
+                         f"median seconds per iteration (their difference) x the oracle's own "
+                         f"{iters_o}-iteration full solve ({src})",
                **host_cpu()}
 
     if rank == 0:

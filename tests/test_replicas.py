@@ -104,14 +104,17 @@ def test_clock_sampler_reads_nvidia_smi_lines(line, reasons):
 
 
 def test_cpu_oracle_sample_is_bounded(built):
-    """bench.cpu_oracle_sample: the oracle's plain PCG timed per iteration
-    over bounded samples (the CPU baseline extrapolates from these)."""
+    """bench.cpu_oracle_sample: the oracle's plain PCG timed over bounded
+    samples, each a short and a long call, whose difference gives the cost
+    per iteration and the rest the fixed cost of a call (the CPU baseline
+    extrapolates from these)."""
     import bench
     from programs_b200.mesh import Mesh, poisson_rhs
     A = Mesh.hex(10, jitter=0.15, seed=0, permute=True).pressure(pin=1)
     b = poisson_rhs(A.n_cell, 1)
-    per, s = bench.cpu_oracle_sample(A, b, 0.3, repeats=3)
-    assert len(per) == 3 and all(p > 0 for p in per) and 2 <= s <= 400
+    per, fixed, s = bench.cpu_oracle_sample(A, b, 0.3, repeats=3)
+    assert len(per) == len(fixed) == 3 and 4 <= s <= 400
+    assert all(p > 0 for p in per) and all(f >= 0 for f in fixed)
 
 
 def test_oracle_iteration_counts_are_the_oracles_own(built):
