@@ -143,14 +143,16 @@ def run(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter
 def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3, jitter=0.15,
                seed=0, p_reduc=1e-10, p_iter=20000, m_reduc=0.1, m_iter=5, learned=None,
                p_imat=1, m_precision=0, device=0, log_every=0, reference_weights=False,
-               reference_terms=False, renumber="rcm", p_scale=False, fcg_delta=None):
+               reference_terms=False, renumber="rcm", p_scale=False, fcg_delta=None,
+               p_options=None):
     """The same outer loop with everything on the GPU: assembly, gradients
     (the corrected sweeps too), the explicit momentum terms, fluxes and
     corrections by the fv_gpu kernels (bit-for-bit the host functions),
     solves through the device-pointer entry points; only the mass-imbalance
     norm comes back per iteration.  Same arguments and returns as run();
     renumber "color" takes the multicolour cell order (two-level DIC / DILU
-    recurrences); timings are wall clock with the stream synchronised."""
+    recurrences); timings are wall clock with the stream synchronised.
+    p_options: further {option key: value} for the pressure solver."""
     import torch
 
     from .fv import GpuFv
@@ -185,6 +187,8 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
         sp.gnn_set_params(learned)
         # a stalled learned solve hands over to the plain run's own PCG
         sp.set_option(OPT_FCG_FALLBACK, max(0, min(int(p_imat), 2)))
+    for key, value in (p_options or {}).items():  # further pressure-solver options
+        sp.set_option(key, value)
     # the structure once (values come from the device each iteration)
     F_ = ip.shape[0]
     shell = FaceMatrix(N, ip, inb, np.zeros(F_), np.zeros(F_), np.ones(N))
