@@ -257,7 +257,8 @@ def run_device(size=32, n_outer=200, re=1000.0, u_lid=1.0, urf_u=0.7, urf_p=0.3,
             t_asm += sync_time(ta)
             rec = {"it": k, "mass": float(imb), "mom_res0": list(map(float, rn_m)),
                    "p_iters": stp["iters"][0], "m_iters": stm["iters"],
-                   "fallbacks": stp.get("fallbacks", 0)}
+                   "fallbacks": stp.get("fallbacks", 0),
+                   "p_refinements": stp.get("refinements", 0)}
             hist.append(rec)
             if log_every and (k % log_every == 0 or k == n_outer - 1):
                 print(json.dumps(rec), flush=True)
