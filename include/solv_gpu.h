@@ -142,6 +142,12 @@ extern "C" {
                                    Krylov, flexible CG, V-cycle): matrix
                                    slots each thread loads before it sums
                                    them, 2, 4 (default) or 8              */
+#define SOLV_OPT_FCG_SLOW_ITERS 23 /* the learned solve: when the network-
+                                   smoothed V-cycle needs more than this
+                                   many flexible-CG iterations for one
+                                   reliable-update drop, damped Jacobi
+                                   smooths the same hierarchy for the rest
+                                   of the solve (default 25; 0 never)     */
 #define SOLV_OPT_FCG_FALLBACK 22 /* the PCG a stalled learned solve hands
                                    over to: 0 (default) Jacobi, 1 DIC, 2
                                    DILU (the reference's pressure solver is
@@ -175,6 +181,9 @@ typedef struct {
                                     plain PCG (solv_gpu_fcg)               */
   int mg_levels;                 /* coarse levels of the aggregation
                                     hierarchy used (solv_gpu_fcg)          */
+  int smoother_switches;         /* the learned solve's network smoother
+                                    gave way to damped Jacobi in the same
+                                    V-cycle (SOLV_OPT_FCG_SLOW_ITERS)      */
 } solv_gpu_stats;
 
 /* -- context ------------------------------------------------------------ */

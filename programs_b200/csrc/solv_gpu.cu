@@ -105,6 +105,9 @@ struct solv_gpu_ctx {
   double reliable_delta = 0.1;
   double fcg_reliable_delta = 0.1;  // the learned flexible CG's reliable-update drop
   int fcg_fallback_imat = 0;         // the PCG a stalled learned solve hands over to
+  int fcg_slow_iters = 25;           // network smoother -> Jacobi after this many
+                                     // iterations for one reliable-update drop (0: never)
+  int smoother_switches = 0;         // of the last learned solve
   int gnn_loss = 1;  // training loss: 0 energy, 1 scale-free (best-step energy)
 
   // matrix (caller sizes)
@@ -1411,6 +1414,14 @@ void fcg_iteration(solv_gpu_ctx* c, WS<T>& w) {
   c->launches += 5;
 }
 
+// The preconditioner part of a graph's key: the recurrence (imat) for CG
+// and BiCGSTAB, the V-cycle's smoother for the learned FCG (a solve may
+// switch it, and both graphs stay cached).
+int graph_imat_key(const solv_gpu_ctx* c, int solver, int imat) {
+  if (solver == 2) return 10 + c->mg_smoother;
+  return imat > 0 ? imat : 0;
+}
+
 // A WHILE graph of one Krylov iteration (body) and the loop control: a
 // launch runs iterations until every lane has stopped or the budget in
 // c->loop_budget is spent, with no host round trip in between.  Returns the
@@ -1469,7 +1480,8 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
   // learned FCG), fixed ones elsewhere (a WHILE pass costs ~3 us)
   const bool want_loop = c->graph_loop == 1 || (c->graph_loop == 2 && solver == 2);
   if (K > 0 && want_loop && c->cond_graphs) {
-    auto key = std::make_tuple(solver, imat > 0 ? imat : 0, V, (int)std::is_same<T, float>::value, 1);
+    auto key = std::make_tuple(solver, graph_imat_key(c, solver, imat), V,
+                               (int)std::is_same<T, float>::value, 1);
     auto it = c->graphs.find(key);
     if (it != c->graphs.end()) {
       exec = it->second;  // null: this body cannot be a WHILE graph
@@ -1495,7 +1507,8 @@ int iterate(solv_gpu_ctx* c, int solver, int imat, int n_iter, WS<T>& w, int& gr
     }
   }
   if (K > 0 && !loop) {
-    auto key = std::make_tuple(solver, imat > 0 ? imat : 0, V, (int)std::is_same<T, float>::value, 0);
+    auto key = std::make_tuple(solver, graph_imat_key(c, solver, imat), V,
+                               (int)std::is_same<T, float>::value, 0);
     auto it = c->graphs.find(key);
     if (it != c->graphs.end()) {
       exec = it->second;
@@ -2081,6 +2094,19 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     return SOLV_GPU_OK;
   };
   c->fallbacks = 0;
+  c->smoother_switches = 0;
+  // a network smoother that needs more than fcg_slow_iters iterations for
+  // one reliable-update drop (the Jacobi-smoothed V-cycle needs about 5 on
+  // the systems measured) gives way to damped Jacobi for the rest of the
+  // solve, the hierarchy kept
+  const int smoother_keep = c->mg_smoother;
+  struct SmootherKeep {  // restored on every way out
+    solv_gpu_ctx* c;
+    int m;
+    ~SmootherKeep() { c->mg_smoother = m; }
+  } smoother_keep_guard{c, smoother_keep};
+  std::vector<int> upd_iter(nl, 0);
+  bool switch_smoother = false;
   std::vector<int> win_iter(nl, 0);
   std::vector<double> win_l1(l1_last);
   bool fell_back = false;
@@ -2161,6 +2187,10 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
           status_v[l] = sg::kLaneMaxIter;
         }
       }
+      if (trig[l] && cur == 2 && !final_[l] && c->mg_smoother >= 1 && mg_on(c) &&
+          c->fcg_slow_iters > 0 && L.iter - upd_iter[l] > c->fcg_slow_iters)
+        switch_smoother = true;
+      if (trig[l]) upd_iter[l] = L.iter;
       if (final_[l]) L.active = 0;
       if (trig[l]) l1_last[l] = l1[l];  // lanes along for the ride keep their window
       L.l1_stop = cur == 2 ? delta_of() * l1_last[l] : 0.0;
@@ -2169,6 +2199,13 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
       na += L.active;
     }
     if (fell_back && (rc = restart_fallback())) return rc;
+    if (switch_smoother && cur == 2 && c->mg_smoother >= 1) {
+      c->mg_smoother = 0;  // the next iterate() takes the Jacobi-smoothed graph
+      c->smoother_switches++;
+      CUDA_TRY(c, cudaMemsetAsync(f.p, 0, NV * sizeof(float), s));
+      CUDA_TRY(c, cudaMemsetAsync(f.q, 0, NV * sizeof(float), s));
+    }
+    switch_smoother = false;
     CUDA_TRY(c, cudaMemcpyAsync(c->lanes.p, hl.data(), nl * sizeof(Lane), cudaMemcpyHostToDevice, s));
     CUDA_TRY(c, cudaMemcpyAsync(c->n_active.p, &na, sizeof(int), cudaMemcpyHostToDevice, s));
     if (na == 0) break;
@@ -2210,6 +2247,7 @@ int solve_mixed_reliable(solv_gpu_ctx* c, int solver, int imat, double reduc, in
     st->status = status;
     st->refinements = updates;
     st->fallbacks = c->fallbacks;
+    st->smoother_switches = c->smoother_switches;
     st->mg_levels = solver == 2 && mg_on(c) ? (int)c->mg.size() : 0;
     st->graph_launches += gl_total;
   }
@@ -2422,6 +2460,10 @@ int solv_gpu_set_option(solv_gpu_ctx* c, int key, double value) {
       if (value != 0 && value != 1 && value != 2)
         return set_err(c, SOLV_GPU_BAD_INPUT, "graph loop is 0, 1 or 2");
       c->graph_loop = (int)value;
+      return SOLV_GPU_OK;
+    case SOLV_OPT_FCG_SLOW_ITERS:
+      if (value < 0 || value > 1e7) return set_err(c, SOLV_GPU_BAD_INPUT, "slow-iteration limit in 0..1e7");
+      c->fcg_slow_iters = (int)value;
       return SOLV_GPU_OK;
     case SOLV_OPT_FCG_FALLBACK:
       if (value != 0 && value != 1 && value != 2)

@@ -34,7 +34,7 @@ OPT_INNER_MAX_ITER, OPT_RELIABLE_DELTA, OPT_GNN_LOSS = 7, 8, 9
 OPT_MG_LEVELS, OPT_MG_SMOOTHER, OPT_MG_OMEGA, OPT_MG_ALPHA = 10, 11, 12, 13
 OPT_FCG_STALL_ITERS, OPT_FCG_STALL_DROP, OPT_MG_SCALE_MIN, OPT_MG_BUILD = 14, 15, 16, 17
 OPT_VECTOR_WIDTH, OPT_PERSISTENT, OPT_FCG_RELIABLE_DELTA, OPT_GRAPH_LOOP = 18, 19, 20, 21
-OPT_FCG_FALLBACK = 22
+OPT_FCG_FALLBACK, OPT_FCG_SLOW_ITERS = 22, 23
 
 _i32p = ctypes.POINTER(ctypes.c_int)
 _f64p = ctypes.POINTER(ctypes.c_double)
@@ -46,7 +46,7 @@ class Stats(ctypes.Structure):
                 ("n_levels", ctypes.c_int), ("refinements", ctypes.c_int),
                 ("graph_launches", ctypes.c_int), ("kernel_launches", ctypes.c_int),
                 ("solve_ms", ctypes.c_double), ("fallbacks", ctypes.c_int),
-                ("mg_levels", ctypes.c_int)]
+                ("mg_levels", ctypes.c_int), ("smoother_switches", ctypes.c_int)]
 
     def as_dict(self):
         V = self.n_vc
@@ -54,7 +54,8 @@ class Stats(ctypes.Structure):
                 "status": self.status, "n_levels": self.n_levels,
                 "refinements": self.refinements, "graph_launches": self.graph_launches,
                 "kernel_launches": self.kernel_launches, "solve_ms": self.solve_ms,
-                "fallbacks": self.fallbacks, "mg_levels": self.mg_levels}
+                "fallbacks": self.fallbacks, "mg_levels": self.mg_levels,
+                "smoother_switches": self.smoother_switches}
 
 
 class Tune(ctypes.Structure):

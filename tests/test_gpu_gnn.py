@@ -25,7 +25,8 @@ from oracle import gnn_ref
 from oracle.oracle import Oracle
 from programs_b200 import learn
 from programs_b200.mesh import Mesh, cavity_field, momentum_field, pressure_correction, uniform
-from programs_b200.solver import (OK, OPT_FCG_FALLBACK, OPT_FCG_RELIABLE_DELTA, OPT_FCG_STALL_DROP,
+from programs_b200.solver import (OK, OPT_FCG_FALLBACK, OPT_FCG_RELIABLE_DELTA, OPT_FCG_SLOW_ITERS,
+                                  OPT_FCG_STALL_DROP,
                                   OPT_FCG_STALL_ITERS, OPT_GRAPH_ITERS, OPT_MG_LEVELS,
                                   OPT_MG_SCALE_MIN, OPT_MG_SMOOTHER, OPT_PRECISION)
 
@@ -383,10 +384,12 @@ def test_starved_smoother_stalls_and_hands_over_to_pcg(gpu):
     b = _rhs(A, 13)
     x_ref, _ = _ref_iters(A, b)
     gpu.set_option(OPT_MG_SCALE_MIN, 0.0)
+    gpu.set_option(OPT_FCG_SLOW_ITERS, 0)  # the hand-over path, not the smoother switch
     try:
         phi, st, rn = _solve_fcg(gpu, A, b)
     finally:
         gpu.set_option(OPT_MG_SCALE_MIN, 0.5)
+        gpu.set_option(OPT_FCG_SLOW_ITERS, 25)
     assert st["status"] == OK and st["fallbacks"] == 1, st
     assert np.abs(b - A.to_scipy() @ phi[:, 0]).sum() / rn[0] < 1e-10
     assert _rel(phi, x_ref) <= AGREE_1E10
@@ -410,6 +413,7 @@ def test_stalled_learned_solve_hands_over_to_dic_pcg(gpu, fallback):
     x_ref, _ = _ref_iters(A, b)
     its = {}
     gpu.set_option(OPT_MG_SCALE_MIN, 0.0)
+    gpu.set_option(OPT_FCG_SLOW_ITERS, 0)  # the hand-over path, not the smoother switch
     try:
         for fb in (0, fallback):
             gpu.set_option(OPT_FCG_FALLBACK, fb)
@@ -421,7 +425,44 @@ def test_stalled_learned_solve_hands_over_to_dic_pcg(gpu, fallback):
     finally:
         gpu.set_option(OPT_MG_SCALE_MIN, 0.5)
         gpu.set_option(OPT_FCG_FALLBACK, 0)
+        gpu.set_option(OPT_FCG_SLOW_ITERS, 25)
     assert its[fallback] < its[0], its
+
+
+def test_slow_network_smoother_gives_way_to_jacobi(gpu):
+    """SOLV_OPT_FCG_SLOW_ITERS: the starved network (per-cell scales near
+    zero, the scale floor off) smooths nothing, so the V-cycle needs many
+    iterations for each reliable-update drop; after the first such drop the
+    solve carries on with damped-Jacobi smoothing over the same hierarchy
+    (stats smoother_switches 1, no hand-over to PCG) and reaches the
+    oracle's solution in fewer iterations than with the switch off."""
+    A = _system(16, seed=9)
+    gpu.matrix_set(A)
+    p = learn.init_params(0)
+    p[learn.P_BA] = -30.0
+    gpu.gnn_set_params(p)
+    b = _rhs(A, 13)
+    x_ref, _ = _ref_iters(A, b)
+    out = {}
+    gpu.set_option(OPT_MG_SCALE_MIN, 0.0)
+    try:
+        for slow in (25, 0):
+            gpu.set_option(OPT_FCG_SLOW_ITERS, slow)
+            phi, st, rn = _solve_fcg(gpu, A, b)
+            assert st["status"] == OK
+            assert np.abs(b - A.to_scipy() @ phi[:, 0]).sum() / rn[0] < 1e-10
+            assert _rel(phi, x_ref) <= AGREE_1E10
+            out[slow] = st
+    finally:
+        gpu.set_option(OPT_MG_SCALE_MIN, 0.5)
+        gpu.set_option(OPT_FCG_SLOW_ITERS, 25)
+    assert out[25]["smoother_switches"] == 1 and out[25]["fallbacks"] == 0, out[25]
+    assert out[0]["smoother_switches"] == 0
+    assert out[25]["iters"][0] < out[0]["iters"][0], (out[25]["iters"], out[0]["iters"])
+    # the network smoother is back for the next solve
+    gpu.gnn_set_params(learn.init_params(0))
+    phi, st, rn = _solve_fcg(gpu, A, b)
+    assert st["status"] == OK and st["smoother_switches"] == 0
 
 
 def test_stall_window_hands_over_once(gpu):
@@ -435,11 +476,13 @@ def test_stall_window_hands_over_once(gpu):
     x_ref, _ = _ref_iters(A, b)
     gpu.set_option(OPT_FCG_STALL_ITERS, 1)
     gpu.set_option(OPT_FCG_STALL_DROP, 1e-6)
+    gpu.set_option(OPT_FCG_SLOW_ITERS, 0)
     try:
         phi, st, rn = _solve_fcg(gpu, A, b)
     finally:
         gpu.set_option(OPT_FCG_STALL_ITERS, 1000)
         gpu.set_option(OPT_FCG_STALL_DROP, 0.9)
+        gpu.set_option(OPT_FCG_SLOW_ITERS, 25)
     assert st["status"] == OK and st["fallbacks"] == 1, st
     assert _rel(phi, x_ref) <= AGREE_1E10
 
