@@ -21,7 +21,7 @@ import numpy as np
 from .mesh import Mesh, poisson_rhs, uniform
 from .solver import (GpuSolver, OPT_GRAPH_ITERS, OPT_MG_ALPHA, OPT_MG_LEVELS, OPT_MG_OMEGA,
                      OPT_MG_SMOOTHER, OPT_PERSISTENT, OPT_PRECISION, OPT_RELIABLE_DELTA,
-                     OPT_GRAPH_LOOP, OPT_FCG_RELIABLE_DELTA)
+                     OPT_GRAPH_LOOP, OPT_FCG_RELIABLE_DELTA, OPT_FCG_SLOW_ITERS)
 
 
 def make_system(size, system="pressure", seed=0, renumber="rcm"):
@@ -92,6 +92,9 @@ def main(argv=None):
                     help="mixed precision: FP32 residual drop between reliable updates")
     ap.add_argument("--fcg-delta", type=float, default=None,
                     help="fcg: FP32 residual drop at which a lane stops for a reliable update")
+    ap.add_argument("--fcg-slow", type=int, default=None,
+                    help="fcg: iterations per reliable-update drop before the network smoother "
+                         "gives way to Jacobi (0 never)")
     ap.add_argument("--graph-loop", type=int, default=2,
                     help="1: iterations in a conditional WHILE graph; 0: graph_iters per launch; "
                          "2: WHILE for fcg only")
@@ -112,6 +115,8 @@ def main(argv=None):
     s.set_option(OPT_GRAPH_LOOP, a.graph_loop)
     if a.fcg_delta is not None:
         s.set_option(OPT_FCG_RELIABLE_DELTA, a.fcg_delta)
+    if a.fcg_slow is not None:
+        s.set_option(OPT_FCG_SLOW_ITERS, a.fcg_slow)
     out = {"case": a.what}
     if a.what == "batch":
         mats, rhs = batch_meshes(a.n_sys, a.min, a.max)
