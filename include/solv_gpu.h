@@ -147,7 +147,7 @@ extern "C" {
                                    many flexible-CG iterations for one
                                    reliable-update drop, damped Jacobi
                                    smooths the same hierarchy for the rest
-                                   of the solve (default 25; 0 never)     */
+                                   of the solve (default 15; 0 never)     */
 #define SOLV_OPT_FCG_FALLBACK 22 /* the PCG a stalled learned solve hands
                                    over to: 0 (default) Jacobi, 1 DIC, 2
                                    DILU (the reference's pressure solver is

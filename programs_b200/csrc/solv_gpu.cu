@@ -105,7 +105,7 @@ struct solv_gpu_ctx {
   double reliable_delta = 0.1;
   double fcg_reliable_delta = 0.1;  // the learned flexible CG's reliable-update drop
   int fcg_fallback_imat = 0;         // the PCG a stalled learned solve hands over to
-  int fcg_slow_iters = 25;           // network smoother -> Jacobi after this many
+  int fcg_slow_iters = 15;           // network smoother -> Jacobi after this many
                                      // iterations for one reliable-update drop (0: never)
   int smoother_switches = 0;         // of the last learned solve
   int gnn_loss = 1;  // training loss: 0 energy, 1 scale-free (best-step energy)

@@ -389,7 +389,7 @@ def test_starved_smoother_stalls_and_hands_over_to_pcg(gpu):
         phi, st, rn = _solve_fcg(gpu, A, b)
     finally:
         gpu.set_option(OPT_MG_SCALE_MIN, 0.5)
-        gpu.set_option(OPT_FCG_SLOW_ITERS, 25)
+        gpu.set_option(OPT_FCG_SLOW_ITERS, 15)
     assert st["status"] == OK and st["fallbacks"] == 1, st
     assert np.abs(b - A.to_scipy() @ phi[:, 0]).sum() / rn[0] < 1e-10
     assert _rel(phi, x_ref) <= AGREE_1E10
@@ -425,7 +425,7 @@ def test_stalled_learned_solve_hands_over_to_dic_pcg(gpu, fallback):
     finally:
         gpu.set_option(OPT_MG_SCALE_MIN, 0.5)
         gpu.set_option(OPT_FCG_FALLBACK, 0)
-        gpu.set_option(OPT_FCG_SLOW_ITERS, 25)
+        gpu.set_option(OPT_FCG_SLOW_ITERS, 15)
     assert its[fallback] < its[0], its
 
 
@@ -446,7 +446,7 @@ def test_slow_network_smoother_gives_way_to_jacobi(gpu):
     out = {}
     gpu.set_option(OPT_MG_SCALE_MIN, 0.0)
     try:
-        for slow in (25, 0):
+        for slow in (15, 0):
             gpu.set_option(OPT_FCG_SLOW_ITERS, slow)
             phi, st, rn = _solve_fcg(gpu, A, b)
             assert st["status"] == OK
@@ -455,10 +455,10 @@ def test_slow_network_smoother_gives_way_to_jacobi(gpu):
             out[slow] = st
     finally:
         gpu.set_option(OPT_MG_SCALE_MIN, 0.5)
-        gpu.set_option(OPT_FCG_SLOW_ITERS, 25)
-    assert out[25]["smoother_switches"] == 1 and out[25]["fallbacks"] == 0, out[25]
+        gpu.set_option(OPT_FCG_SLOW_ITERS, 15)
+    assert out[15]["smoother_switches"] == 1 and out[15]["fallbacks"] == 0, out[15]
     assert out[0]["smoother_switches"] == 0
-    assert out[25]["iters"][0] < out[0]["iters"][0], (out[25]["iters"], out[0]["iters"])
+    assert out[15]["iters"][0] < out[0]["iters"][0], (out[15]["iters"], out[0]["iters"])
     # the network smoother is back for the next solve
     gpu.gnn_set_params(learn.init_params(0))
     phi, st, rn = _solve_fcg(gpu, A, b)
@@ -482,7 +482,7 @@ def test_stall_window_hands_over_once(gpu):
     finally:
         gpu.set_option(OPT_FCG_STALL_ITERS, 1000)
         gpu.set_option(OPT_FCG_STALL_DROP, 0.9)
-        gpu.set_option(OPT_FCG_SLOW_ITERS, 25)
+        gpu.set_option(OPT_FCG_SLOW_ITERS, 15)
     assert st["status"] == OK and st["fallbacks"] == 1, st
     assert _rel(phi, x_ref) <= AGREE_1E10
 
